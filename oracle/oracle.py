@@ -1,0 +1,180 @@
+"""ORACLE — test infrastructure only.
+
+ctypes bindings of the FP64 CPU restatement in fits.cpp (liblarmor_oracle.so). Only the tests,
+the smoke check and bench.py's CPU-baseline leg import this module; the product path
+(larmor_b200) never does.
+
+Each function mirrors the reference call it restates:
+    fit_log_signal     larmor._core.fit_log_signal   cpp/src/python/dwi.cpp:42
+    lsi_design         larmor._core.LsiDesign        cpp/src/sd/lsi.cpp:75
+    fit_lsi            larmor._core.fit_lsi          cpp/src/python/sd.cpp:370
+    nnls               larmor._core.lsqnonneg        cpp/src/sd/nnls.cpp:332
+    ridge_nnls         FodSolver.l2nnls + fit_single_tissue  cpp/src/sd/solver.cpp:422
+    fit_multi_tissue   larmor._core.fit_multi_tissue cpp/src/python/sd.cpp:310
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liblarmor_oracle.so"
+
+_i64 = ctypes.c_int64
+_dbl = ctypes.c_double
+_ptr = ctypes.c_void_p
+
+_lib: ctypes.CDLL | None = None
+
+
+def build() -> Path:
+    """Builds liblarmor_oracle.so with the Makefile beside this file."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        _lib = ctypes.CDLL(str(LIB_PATH))
+        _lib.oracle_last_error.restype = ctypes.c_char_p
+        _lib.oracle_median.restype = _dbl
+        _lib.oracle_median.argtypes = [_ptr, _i64]
+    return _lib
+
+
+def _p(a: np.ndarray | None) -> ctypes.c_void_p:
+    return ctypes.c_void_p(None if a is None else a.ctypes.data)
+
+
+def _check(code: int) -> None:
+    if code != 0:
+        raise ValueError(lib().oracle_last_error().decode())
+
+
+def _c64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def default_threads() -> int:
+    return os.cpu_count() or 1
+
+
+def fit_log_signal(x, g, log_s, weighted, max_iter=20, tol=1e-6, n_threads=1, iterations=False):
+    """Parameters (v, p), broke (v,) [, IRLS iterations (v,)] of every row of log_s (v, n)."""
+    x, log_s = _c64(x), _c64(log_s)
+    n, p = x.shape
+    g = np.zeros((0, p)) if g is None else _c64(g)
+    v = log_s.shape[0]
+    params = np.empty((v, p))
+    broke = np.zeros(v, np.uint8)
+    iters = np.zeros(v, np.int32)
+    _check(lib().oracle_fit_log_signal(
+        _p(x), _i64(n), _i64(p), _p(g), _i64(g.shape[0]), _p(log_s), _i64(v), int(bool(weighted)),
+        _i64(max_iter), _dbl(tol), int(n_threads), _p(params), _p(broke), _p(iters)))
+    if iterations:
+        return params, broke.astype(bool), iters
+    return params, broke.astype(bool)
+
+
+def log_design(x):
+    """Column scales (p,) and the pseudo-inverse (p, n) of the scaled design."""
+    x = _c64(x)
+    n, p = x.shape
+    scales, pinv = np.empty(p), np.empty((p, n))
+    _check(lib().oracle_log_design(_p(x), _i64(n), _i64(p), _p(scales), _p(pinv)))
+    return scales, pinv
+
+
+def lsi_design(a, g, ridge):
+    """The prepared LSI problem: dict of q_t, back, e, gram, abs_sums."""
+    a, g = _c64(a), _c64(g)
+    m, n = a.shape
+    k = g.shape[0]
+    out = dict(q_t=np.empty((n, m)), back=np.empty((n, n)), e=np.empty((k, n)),
+               gram=np.empty((k, k)), abs_sums=np.empty(k))
+    _check(lib().oracle_lsi_design(_p(a), _i64(m), _i64(n), _p(g), _i64(k), _dbl(ridge),
+                                   *(_p(out[key]) for key in ("q_t", "back", "e", "gram", "abs_sums"))))
+    return out
+
+
+def fit_lsi(a, g, ridge, signals, only_qr=False, n_threads=1, details=False):
+    """Solutions (v, n) and converged (v,) [, status, outer steps, active (v, k)]."""
+    a, g, signals = _c64(a), _c64(g), _c64(signals)
+    m, n = a.shape
+    k = g.shape[0]
+    v = signals.shape[0]
+    x = np.empty((v, n))
+    conv = np.zeros(v, np.uint8)
+    status = np.zeros(v, np.int32)
+    outer = np.zeros(v, np.int32)
+    active = np.zeros((v, k), np.uint8) if details else None
+    _check(lib().oracle_fit_lsi(_p(a), _i64(m), _i64(n), _p(g), _i64(k), _dbl(ridge), _p(signals),
+                                _i64(v), int(bool(only_qr)), int(n_threads), _p(x), _p(conv),
+                                _p(status), _p(outer), _p(active)))
+    if details:
+        return x, conv.astype(bool), status, outer, active.astype(bool)
+    return x, conv.astype(bool)
+
+
+def nnls(c, d, tol=None, max_inner=None):
+    """x (cols,) and converged of min ||c x - d||, x >= 0."""
+    c, d = _c64(c), _c64(d)
+    rows, cols = c.shape
+    x = np.empty(cols)
+    conv = np.zeros(1, np.uint8)
+    _check(lib().oracle_nnls(_p(c), _i64(rows), _i64(cols), _p(d), _dbl(-1.0 if tol is None else tol),
+                             _i64(-1 if max_inner is None else max_inner), _p(x), _p(conv)))
+    return x, bool(conv[0])
+
+
+def ridge_nnls(k, ridge, tol_x, signals, n_threads=1):
+    """FODs (v, c) of min ||k f - s||^2 + ridge^2 ||f||^2, f >= 0, per row of signals."""
+    k, signals = _c64(k), _c64(signals)
+    m, c = k.shape
+    v = signals.shape[0]
+    out = np.empty((v, c))
+    _check(lib().oracle_ridge_nnls(_p(k), _i64(m), _i64(c), _dbl(ridge), _dbl(tol_x), _p(signals),
+                                   _i64(v), int(n_threads), _p(out)))
+    return out
+
+
+def fit_multi_tissue(signals, weights, lr, hr, lr_ridge=0.0, hr_ridge=0.1, tol_x=1e-6,
+                     max_rounds=50, fraction_tol=1e-7, final_tol=1e-2, n_threads=1, rounds=False):
+    """HR FODs (v, ca_hr) and fractions (v, n_blocks + ci) of the multi-tissue fit.
+
+    lr and hr are dicts with k_aniso (m, ca), k_iso (m, ci), w_k_iso, w_k_aniso and, for hr,
+    blocks [(start, stop), ...].
+    """
+    signals, weights = _c64(signals), _c64(weights)
+    v, m = signals.shape
+    la, ha = (_c64(lr["k_aniso"]), _c64(hr["k_aniso"]))
+    ci = lr["k_iso"].shape[1]
+    blocks = np.ascontiguousarray(np.array(hr["blocks"], dtype=np.int64).reshape(-1))
+    nb = len(hr["blocks"])
+    fods = np.empty((v, ha.shape[1]))
+    fr = np.empty((v, nb + ci))
+    rd = np.zeros(v, np.int32)
+    keep = [_c64(lr[key]) for key in ("k_iso", "w_k_iso", "w_k_aniso")] + \
+           [_c64(hr[key]) for key in ("k_iso", "w_k_iso", "w_k_aniso")]
+    _check(lib().oracle_fit_multi_tissue(
+        _p(signals), _i64(v), _i64(m), _p(weights),
+        _p(la), _i64(la.shape[1]), _p(keep[0]), _p(keep[1]), _p(keep[2]), _dbl(lr_ridge), _dbl(tol_x),
+        _p(ha), _i64(ha.shape[1]), _p(keep[3]), _p(keep[4]), _p(keep[5]), _dbl(hr_ridge), _dbl(tol_x),
+        _i64(ci), _p(blocks), _i64(nb), _i64(max_rounds), _dbl(fraction_tol), _dbl(final_tol),
+        int(n_threads), _p(fods), _p(fr), _p(rd)))
+    if rounds:
+        return fods, fr, rd
+    return fods, fr
+
+
+def median(values) -> float:
+    values = _c64(values)
+    return float(lib().oracle_median(_p(values), _i64(len(values))))

@@ -1,0 +1,234 @@
+"""Generates the golden fixtures of tests/golden from the reference (larmor-dmri 2.2.0).
+
+Run in a container that has the reference checkout (default /root/reference, or the path given
+as the first argument):
+
+    python tests/golden/make_golden.py [/path/to/reference]
+
+The reference's compiled core cannot be built without Eigen and nanobind, and its Python layer
+needs Python >= 3.14. Its numpy/scipy code does run on 3.12 from a temporary copy of its source
+tree with three mechanical changes, made here in the copy only:
+
+1. `from __future__ import annotations` at the top of every module (3.14 defers annotations);
+2. `except A, B:` rewritten to `except (A, B):` (3.14 syntax);
+3. stand-ins for `larmor._core` (whose fits this project replaces) and `skimage.morphology`.
+
+What the fixtures hold, all from the reference's own code and data:
+- dki_block.npz: the CFIN 8x8x8x133 test block's masked signals (tests/data/dki), its gradient
+  table, the DTI and DKI design and constraint matrices the models build, the MRtrix dwi2tensor
+  golden fits (mrtrix_dt_ref.npz, mrtrix_dkt_ref.npz) and the outputs of the reference's numpy
+  oracle tests/dwi/reference_fitting.py (ols_fit, wls_fit, constrain) on those signals, plus the
+  reference's metric functions (compute_dti_metrics, compute_kurtosis_metrics) on the numpy fits.
+- mfod.npz: the MRIToolkit mFOD fixture (tests/data/mfod: 512 voxels, the MATLAB FODs and
+  fractions) with the high- and low-resolution kernels Larmor builds for it (sd/kernel.py), its
+  shell weights and the SH projection matrices of sd/model.py:_to_sh.
+- msmt.npz: the forward and constraint matrices and ridge of MSMT-CSD (sd/msmt.py) for the
+  responses of tests/data/msmt on a seeded three-shell table, as tests/sd/test_msmt.py builds them.
+- dirs300.npy: the reference's 300 FOD directions (src/larmor/data/dir300.txt), a table the
+  SD models must share exactly.
+"""
+
+from __future__ import annotations
+
+import re
+import shutil
+import sys
+import tempfile
+import types
+from pathlib import Path
+
+import numpy as np
+
+OUT = Path(__file__).resolve().parent
+
+
+def _patched_copy(reference: Path) -> Path:
+    tmp = Path(tempfile.mkdtemp(prefix="larmor_ref_"))
+    src = tmp / "src"
+    shutil.copytree(reference / "src", src, ignore=shutil.ignore_patterns("viewer"))
+    for path in src.rglob("*.py"):
+        text = path.read_text()
+        text = re.sub(r"except (\w+(?:\.\w+)*), (\w+(?:\.\w+)*):", r"except (\1, \2):", text)
+        if "from __future__ import annotations" not in text:
+            lines = text.split("\n")
+            # After the module docstring, if any.
+            insert = 0
+            if lines and lines[0].startswith('"""'):
+                if lines[0].count('"""') >= 2 and len(lines[0]) > 3:
+                    insert = 1
+                else:
+                    for i in range(1, len(lines)):
+                        if '"""' in lines[i]:
+                            insert = i + 1
+                            break
+            lines.insert(insert, "from __future__ import annotations")
+            text = "\n".join(lines)
+        path.write_text(text)
+    return tmp
+
+
+def _install_stubs() -> None:
+    core = types.ModuleType("larmor._core")
+    core.MAX_LMAX = 20
+
+    def _missing(*_args, **_kwargs):
+        raise RuntimeError("the reference's compiled core is not built here")
+
+    for name in ("fit_log_signal", "LsiDesign", "fit_lsi", "FodSolver", "DeconvKernel",
+                 "fit_multi_tissue", "fit_single_tissue"):
+        setattr(core, name, _missing)
+    sys.modules["larmor._core"] = core
+    skimage = types.ModuleType("skimage")
+    morphology = types.ModuleType("skimage.morphology")
+    morphology.reconstruction = _missing
+    skimage.morphology = morphology
+    sys.modules["skimage"] = skimage
+    sys.modules["skimage.morphology"] = morphology
+
+
+def main(reference: Path) -> None:
+    tmp = _patched_copy(reference)
+    sys.path.insert(0, str(tmp / "src"))
+    _install_stubs()
+    import larmor  # noqa: F401
+
+    sys.modules["larmor"]._core = sys.modules["larmor._core"]
+    sys.path.insert(0, str(reference / "tests" / "dwi"))
+    from reference_fitting import constrain, ols_fit, wls_fit
+    from scipy.io import loadmat
+
+    from larmor.dwi.dki import _constraint_matrix, _design_matrix, compute_kurtosis_metrics
+    from larmor.dwi.dti import compute_dti_metrics
+    from larmor.io import load_dwi
+    from larmor.sd import AnisotropicRF, IsotropicRF, NoddiRF
+    from larmor.sd.kernel import Kernel
+    from larmor.sd.model import compute_shell_weights, low_resolution_dirs
+    from larmor.sd.msmt import constraint_matrix, forward_matrix, NORM_REG
+    from larmor.sd.rf import ZonalSHRF
+    from larmor.sd.sh import build_basis_matrix
+    from larmor.sd.sphere import DIRS_300, get_theta_phi
+
+    # ---- DKI/DTI block ------------------------------------------------------------------
+    dki_dir = reference / "tests" / "data" / "dki"
+    volume, gtab = load_dwi(dki_dir / "dwi.nii.gz", bvals=dki_dir / "bvals",
+                            bvecs=dki_dir / "bvecs", frame="fsl")
+    dt_ref = np.load(dki_dir / "mrtrix_dt_ref.npz")
+    dkt_ref = np.load(dki_dir / "mrtrix_dkt_ref.npz")
+    mask = dkt_ref["mask"]
+    s = volume.as_float()[mask].astype(np.float64)
+    positive = (s > 0).all(axis=1)
+    sp = s[positive]
+    dti_design = np.column_stack([np.ones(len(gtab.bvals)), -gtab.b_matrix])
+    dki_design = _design_matrix(gtab)
+    dki_g = _constraint_matrix(gtab)
+    out = dict(
+        signals_f32=volume.as_float()[mask].astype(np.float32),
+        mask=mask,
+        dt_mask=dt_ref["mask"],
+        bvals=gtab.bvals,
+        bvecs=gtab.bvecs,
+        b_matrix=gtab.b_matrix,
+        b0_mask=gtab.b0_mask,
+        dti_design=dti_design,
+        dki_design=dki_design,
+        dki_constraints=dki_g,
+        positive=positive,
+        mrtrix_dt_ols=dt_ref["dt_ols"], mrtrix_dt_wls=dt_ref["dt_wls"],
+        mrtrix_dt_wls_settled=dt_ref["wls_settled"],
+        mrtrix_dkt_dt_ols=dkt_ref["dt_ols"], mrtrix_dkt_dt_wls=dkt_ref["dt_wls"],
+        mrtrix_dkt_kt_ols=dkt_ref["kt_ols"], mrtrix_dkt_kt_wls=dkt_ref["kt_wls"],
+        mrtrix_dkt_wls_settled=dkt_ref["wls_settled"],
+    )
+    # The reference's numpy oracle on the positive voxels (tests/dwi/test_dki.py:581-602).
+    for name, fit in (("ols", ols_fit), ("wls", wls_fit)):
+        out[f"np_dti_{name}"] = fit(dti_design, sp)
+        p = fit(dki_design, sp)
+        out[f"np_dki_{name}"] = p
+        pc, broke = constrain(dki_design, np.log(sp), p, gtab, name == "wls")
+        out[f"np_dki_{name}_constrained"] = pc
+        out[f"np_dki_{name}_broke"] = broke
+    # The reference's metric functions on its numpy DTI and DKI fits.
+    unit = np.ones((len(sp), 1, 1), dtype=bool)
+    for name in ("ols", "wls"):
+        d = out[f"np_dti_{name}"][1:7]
+        dt, fa, md, ad, rd, pe, ev, npd = compute_dti_metrics(d, unit)
+        out[f"metrics_dti_{name}"] = np.column_stack(
+            [fa[:, 0, 0], md[:, 0, 0], ad[:, 0, 0], rd[:, 0, 0], ev[:, 0, 0], pe[:, 0, 0]]).astype(np.float64)
+        out[f"metrics_dti_{name}_npd"] = npd[:, 0, 0]
+        p = out[f"np_dki_{name}_constrained"]
+        d = p[1:7]
+        md_ = (d[0] + d[3] + d[5]) / 3
+        w = np.divide(p[7:], md_**2, out=np.zeros_like(p[7:]), where=md_ > 0)
+        mk, ak, rk, ka = compute_kurtosis_metrics(d, w)
+        out[f"metrics_dki_{name}"] = np.column_stack([mk, ak, rk, ka])
+    np.savez_compressed(OUT / "dki_block.npz", **out)
+
+    # ---- mFOD (MRIToolkit fixture) -------------------------------------------------------
+    mfod_dir = reference / "tests" / "data" / "mfod"
+    kref = loadmat(mfod_dir / "mfod_kernel.mat", simplify_cells=True)["kernel"]
+    ref = loadmat(mfod_dir / "mfod_ref.mat", simplify_cells=True)["ref"]
+    bvals = kref["bvals"].astype(np.float64)
+    bvecs = kref["bvecs"].astype(np.float64)
+    rfs = [AnisotropicRF([1.7e-3, 0.2e-3, 0.2e-3], 0.0), NoddiRF(), IsotropicRF(3e-3)]
+    weights = compute_shell_weights(bvals, 1.0)
+    hr = Kernel(rfs, bvals, bvecs, dirs=DIRS_300, weights=weights)
+    lr = Kernel(rfs, bvals, bvecs, dirs=low_resolution_dirs(rfs, len(bvals)), weights=weights)
+    theta, phi = get_theta_phi(DIRS_300)
+    basis8 = build_basis_matrix(theta, phi, 8)
+    np.savez_compressed(
+        OUT / "mfod.npz",
+        bvals=bvals, bvecs=bvecs, weights=weights,
+        signal=ref["signal"].astype(np.float64), ijk=ref["ijk"],
+        matlab_fod=ref["fod"].astype(np.float64), matlab_fractions=ref["fractions"].astype(np.float64),
+        hr_k_aniso=hr.k_aniso, hr_k_iso=hr.k_iso, hr_w_k_aniso=hr.w_k_aniso, hr_w_k_iso=hr.w_k_iso,
+        hr_blocks=np.array([(b.start, b.stop) for b in hr.aniso_blocks]),
+        lr_k_aniso=lr.k_aniso, lr_k_iso=lr.k_iso, lr_w_k_aniso=lr.w_k_aniso, lr_w_k_iso=lr.w_k_iso,
+        sh_basis_tournier_l8=basis8,
+    )
+
+    # ---- MSMT-CSD matrices (tests/sd/test_msmt.py's set-up: _gradients, _tensor_response,
+    # _isotropic_response) -------------------------------------------------------------------
+    from larmor.sd.sphere import get_dirs
+    from larmor.types import GradientTable
+
+    shells = np.array([0.0, 1000.0, 2000.0, 3000.0])
+    dirs40 = get_dirs(40)
+    tb = [np.zeros((2, 3))]
+    for k in range(3):
+        ang = 0.4 * k
+        rot = np.array([[np.cos(ang), -np.sin(ang), 0.0], [np.sin(ang), np.cos(ang), 0.0], [0.0, 0.0, 1.0]])
+        tb.append(dirs40 @ rot.T)
+    tgtab = GradientTable(np.concatenate([[0.0, 0.0], np.repeat(shells[1:], 40)]), np.vstack(tb))
+
+    def tensor_response(s0, par, perp):
+        nodes, wts = np.polynomial.legendre.leggauss(64)
+        th = np.arccos(nodes)
+        rows = []
+        for b in shells:
+            profile = s0 * np.exp(-b * (perp + (par - perp) * nodes**2))
+            zonal = build_basis_matrix(th, np.zeros_like(th), 8)[:, [0, 3, 10, 21, 36]]
+            rows.append(2 * np.pi * (wts * profile) @ zonal)
+        return ZonalSHRF(bvals=shells, coefficients=np.array(rows))
+
+    def isotropic_response(s0, diff):
+        sig = s0 * np.exp(-shells * diff)
+        return ZonalSHRF(bvals=shells, coefficients=np.sqrt(4 * np.pi) * sig[:, None])
+
+    rfs_msmt = [tensor_response(1000.0, 1.7e-3, 0.2e-3), isotropic_response(1500.0, 0.8e-3),
+                isotropic_response(2000.0, 3e-3)]
+    lmaxes = [8, 0, 0]
+    fwd = forward_matrix(rfs_msmt, lmaxes, tgtab.bvals, tgtab.bvecs)
+    g = constraint_matrix(lmaxes, DIRS_300)
+    np.savez_compressed(
+        OUT / "msmt.npz", forward=fwd, constraints=g,
+        ridge=float(np.sqrt(NORM_REG * np.max(np.sum(fwd**2, axis=0)))),
+        bvals=tgtab.bvals, bvecs=tgtab.bvecs, shells=shells,
+        wm_coefficients=rfs_msmt[0].coefficients, gm_coefficients=rfs_msmt[1].coefficients,
+        csf_coefficients=rfs_msmt[2].coefficients)
+    np.save(OUT / "dirs300.npy", np.asarray(DIRS_300, dtype=np.float64))
+    shutil.rmtree(tmp)
+    print("wrote", sorted(p.name for p in OUT.glob("*.np*")))
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
