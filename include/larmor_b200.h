@@ -1,0 +1,83 @@
+/*
+ * larmor_b200 — C ABI of the B200-native voxelwise fitting hot path of Larmor (larmor-dmri).
+ *
+ * Every entry point returns an int status (LAR_OK = 0) and never throws; lar_last_error()
+ * gives the message of the last failure on the calling host thread. Per-voxel numerical
+ * failure never fails a call: it is encoded in the outputs (fallback parameters, flags), as in
+ * the reference. Array arguments are plain pointers with explicit sizes, row-major, one voxel
+ * per row. "device" arrays live in the current CUDA device's memory; "host" arrays in host
+ * memory. `stream` is a cudaStream_t (NULL for the legacy default stream); the calls are
+ * asynchronous on it unless stated otherwise.
+ *
+ * Design handles copy their matrices at creation (to host and device memory) and are
+ * immutable afterwards, as the reference's design objects are (cpp/src/python/sd.cpp:42-62).
+ *
+ * Reference interfaces replaced (paths within the larmor-dmri project):
+ *   lar_log_design_*, lar_fit_log_signal     larmor._core.fit_log_signal
+ *                                            (cpp/src/python/dwi.cpp:42, src/larmor/_core.pyi:223)
+ *   lar_fit_dti_maps                         DTIModel.fit's chunk loop + compute_dti_metrics
+ *                                            (src/larmor/dwi/dti.py:156-163, :170-235)
+ */
+#ifndef LARMOR_B200_H
+#define LARMOR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LAR_OK 0
+#define LAR_ERR_INVALID 1 /* bad shape, size or argument: ValueError in the Python layer */
+#define LAR_ERR_CUDA 2    /* a CUDA runtime call failed */
+#define LAR_ERR_MEMORY 3  /* out of host or device memory */
+
+/* Arithmetic of a fit: FP64 follows the reference's double precision; FP32 is the plain
+ * single-precision variant of the same kernels, kept as the comparison baseline. */
+#define LAR_FP64 0
+#define LAR_FP32 1
+
+/* Message of the last failed call on this host thread ("" if none). */
+const char* lar_last_error(void);
+
+/* Library version string. */
+const char* lar_version(void);
+
+/* ---- Log-signal fits (DTI, DKI) ------------------------------------------------------- */
+
+typedef struct lar_log_design_s* lar_log_design;
+
+/* Prepares the design x (n, p), n >= p, of full column rank, and constraints g (m, p), m >= 0
+ * (host arrays): unit-norm columns, the pseudo-inverse, the constraints with the same column
+ * scales. Replaces make_log_signal_design (cpp/src/dwi/log_fit.cpp:220). */
+int lar_log_design_create(const double* x, int64_t n, int64_t p, const double* g, int64_t m,
+                          lar_log_design* out);
+void lar_log_design_destroy(lar_log_design design);
+
+/* Fits each row of log_s (v, n) (device) by least squares on the design: ordinary, or
+ * weighted by the predicted signal iterated until no predicted log signal changes by more than
+ * tol or for max_iter weighted fits; a voxel whose weighted normal equations are singular or
+ * whose fit is not finite keeps the ordinary fit. With constraints, a voxel with g p < 0 in
+ * some row is fitted again subject to g p >= 0 (least distance by NNLS) and flagged in broke.
+ * Writes params (v, p) (device, double) and broke (v,) (device, uint8). iterations (v,)
+ * (device, int32, may be NULL) receives each voxel's number of weighted fits.
+ * Replaces larmor._core.fit_log_signal (cpp/src/python/dwi.cpp:42-82). */
+int lar_fit_log_signal(lar_log_design design, const double* log_s, int64_t v, int weighted,
+                       int64_t max_iter, double tol, int precision, double* params,
+                       uint8_t* broke, int32_t* iterations, void* stream);
+
+/* The fused DTI path of DTIModel.fit: float32 signals (v, n) (device) are floored (a sample
+ * that is not finite and positive becomes floor[voxel], device double (v,)), logged, fitted as
+ * lar_fit_log_signal does (design columns [1, -b_matrix]), and turned into the maps of
+ * compute_dti_metrics. maps (16, v) (device float32, one row per map) holds dt (6: xx, xy, xz,
+ * yy, yz, zz), fa, md, ad, rd, pe (3), eigen_vals (3, descending); npd (v,) (device uint8) is
+ * l3 <= 0. params (v, 7) (device double) may be NULL. */
+int lar_fit_dti_maps(lar_log_design design, const float* signals, const double* floor,
+                     int64_t v, int weighted, int64_t max_iter, double tol, int precision,
+                     float* maps, uint8_t* npd, double* params, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LARMOR_B200_H */

@@ -1,0 +1,58 @@
+"""Builds the CUDA library liblarmor_b200.so in-tree for sm_100a (B200).
+
+    python -m larmor_b200.build
+
+nvcc cross-compiles without a GPU. The library links the CUDA runtime statically, so it loads
+next to any PyTorch build; its C ABI is declared in include/larmor_b200.h.
+"""
+
+from __future__ import annotations
+
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PACKAGE = Path(__file__).resolve().parent
+ROOT = PACKAGE.parent
+CSRC = PACKAGE / "csrc"
+LIB = PACKAGE / "liblarmor_b200.so"
+SOURCES = ["capi.cu", "log_fit.cu"]
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo", "-O3", "-std=c++17",
+    "-Xcompiler", "-fPIC,-O3", "-shared",
+    "-I", str(ROOT / "include"),
+]
+
+
+def nvcc() -> str:
+    found = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(found).exists():
+        raise RuntimeError("nvcc not found: the CUDA toolkit is needed to build larmor_b200")
+    return found
+
+
+def stale() -> bool:
+    if not LIB.exists():
+        return True
+    mtime = LIB.stat().st_mtime
+    deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp"))
+    deps.append(ROOT / "include" / "larmor_b200.h")
+    return any(p.stat().st_mtime > mtime for p in deps)
+
+
+def build(verbose: bool = False, force: bool = False) -> Path:
+    """Compiles every CUDA source into liblarmor_b200.so; returns its path."""
+    if not force and not stale():
+        return LIB
+    cmd = [nvcc(), *NVCC_FLAGS, *(str(CSRC / s) for s in SOURCES), "-o", str(LIB)]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))

@@ -1,0 +1,5 @@
+"""DWI models on the GPU: DTI (and DKI), with the API of larmor.dwi."""
+
+from larmor_b200.dwi.dti import DTIFit, DTIModel
+
+__all__ = ["DTIFit", "DTIModel"]
