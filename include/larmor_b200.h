@@ -17,6 +17,8 @@
  *                                            (cpp/src/python/dwi.cpp:42, src/larmor/_core.pyi:223)
  *   lar_fit_dti_maps                         DTIModel.fit's chunk loop + compute_dti_metrics
  *                                            (src/larmor/dwi/dti.py:156-163, :170-235)
+ *   lar_fit_dki_maps, lar_dki_maps           DKIModel.fit's chunk loop + compute_kurtosis_metrics
+ *                                            (src/larmor/dwi/dki.py:243-282, :285-540)
  */
 #ifndef LARMOR_B200_H
 #define LARMOR_B200_H
@@ -75,6 +77,25 @@ int lar_fit_log_signal(lar_log_design design, const double* log_s, int64_t v, in
 int lar_fit_dti_maps(lar_log_design design, const float* signals, const double* floor,
                      int64_t v, int weighted, int64_t max_iter, double tol, int precision,
                      float* maps, uint8_t* npd, double* params, void* stream);
+
+/* The DKI maps of 22-parameter fits params (v, 22) (device double): maps (36, v) (device
+ * float32) holds rows 0-15 as lar_fit_dti_maps, rows 16-30 kt (W1111 ... W3312), row 31 s0,
+ * rows 32-35 mk, ak, rk, ka; npd (v,) is l3 <= 0. Replaces compute_kurtosis_metrics and the
+ * map assembly of DKIModel.fit (src/larmor/dwi/dki.py:261-282, :285-342). */
+int lar_dki_maps(const double* params, int64_t v, float* maps, uint8_t* npd, void* stream);
+
+/* The fused DKI path of DKIModel.fit: float32 signals (v, n) (device) are prepared as the
+ * reference does (src/larmor/dwi/dki.py:243-250): with s0 (v,) (device double, or NULL for a
+ * table without b0) the b0 samples of a voxel whose own b0 mean differs from s0 become s0 and
+ * the diffusion-weighted samples are capped at s0; samples that are not finite and positive
+ * become floor[voxel]. is_b0 (n,) (device uint8) marks the b0 measurements. The log signals
+ * are fitted (constrained when the design has constraints; the re-fit of violators runs in
+ * FP64), params (v, 22) (device double, required) receives the parameters, broke (v,) the
+ * constraint flags, and maps/npd the maps of lar_dki_maps. */
+int lar_fit_dki_maps(lar_log_design design, const float* signals, const double* s0, const double* floor,
+                     const uint8_t* is_b0, int64_t v, int weighted, int64_t max_iter, double tol,
+                     int precision, float* maps, uint8_t* npd, uint8_t* broke, double* params,
+                     void* stream);
 
 #ifdef __cplusplus
 }

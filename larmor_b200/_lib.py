@@ -24,6 +24,8 @@ SIGNATURES: dict[str, tuple] = {
     "lar_log_design_destroy": (None, [_p]),
     "lar_fit_log_signal": (_i32, [_p, _p, _i64, _i32, _i64, _f64, _i32, _p, _p, _p, _p]),
     "lar_fit_dti_maps": (_i32, [_p, _p, _p, _i64, _i32, _i64, _f64, _i32, _p, _p, _p, _p]),
+    "lar_dki_maps": (_i32, [_p, _i64, _p, _p, _p]),
+    "lar_fit_dki_maps": (_i32, [_p, _p, _p, _p, _p, _i64, _i32, _i64, _f64, _i32, _p, _p, _p, _p, _p]),
 }
 
 LAR_OK, LAR_ERR_INVALID, LAR_ERR_CUDA, LAR_ERR_MEMORY = 0, 1, 2, 3

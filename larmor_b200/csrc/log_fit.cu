@@ -22,9 +22,32 @@
 #include "common.cuh"
 #include "host_la.hpp"
 #include "log_fit.cuh"
+#include "log_fit_warp.cuh"
+#include "tensor_maps.cuh"
+
+// Device scratch of a design handle: the violator list and the constrained re-fit's warp
+// slots, grown on demand. Calls on one handle must not overlap on the GPU.
+struct LogScratch {
+    void* base = nullptr;
+    size_t bytes = 0;
+    ~LogScratch() {
+        if (base) cudaFree(base);
+    }
+    void* reserve(size_t need) {
+        if (need > bytes) {
+            if (base) lar::cuda_check(cudaFree(base), "cudaFree");
+            base = nullptr;
+            bytes = 0;
+            lar::cuda_check(cudaMalloc(&base, need), "cudaMalloc (log-fit scratch)");
+            bytes = need;
+        }
+        return base;
+    }
+};
 
 struct lar_log_design_s {
     lar::host::LogDesignHost host;
+    LogScratch scratch;
     lar::LogDesignDevice<double> d64;
     lar::LogDesignDevice<float> d32;
     lar::DeviceArray<double> x64, pinvt64, z64, g64, scales64;
@@ -44,53 +67,6 @@ __device__ __forceinline__ bool all_finite(const T (&v)[P]) {
     for (int i = 0; i < P; ++i) ok &= isfinite(v[i]);
     return ok;
 }
-
-// ---- signal sources ---------------------------------------------------------------------
-//
-// A CTA owns `count` consecutive voxels, whose rows are contiguous in memory: it copies them
-// into shared memory with coalesced loads, then each thread turns its own row into log
-// signals (T) in a thread-strided shared array ys[j * BLOCK + tid], computed once per voxel.
-
-// log_s (v, n) double, as larmor._core.fit_log_signal receives it.
-struct LogSource {
-    const double* log_s;
-    int64_t n;
-    static constexpr int raw_bytes = 8;
-    template <class T, int BLOCK>
-    __device__ __forceinline__ void stage(int64_t first, int count, unsigned char* raw, T* ys) const {
-        const double* src = log_s + first * n;
-        double* dst = reinterpret_cast<double*>(raw);
-        const int total = count * int(n);
-        for (int i = threadIdx.x; i < total; i += BLOCK) dst[i] = src[i];
-        __syncthreads();
-        if (threadIdx.x < count)
-            for (int j = 0; j < n; ++j) ys[j * BLOCK + threadIdx.x] = T(dst[threadIdx.x * n + j]);
-    }
-};
-
-// float32 signals (v, n) with a per-voxel floor for samples that are not finite and positive
-// (src/larmor/dwi/inputs.py:227-252), logged in T.
-struct FlooredSource {
-    const float* s;
-    const double* floor;
-    int64_t n;
-    static constexpr int raw_bytes = 4;
-    template <class T, int BLOCK>
-    __device__ __forceinline__ void stage(int64_t first, int count, unsigned char* raw, T* ys) const {
-        const float* src = s + first * n;
-        float* dst = reinterpret_cast<float*>(raw);
-        const int total = count * int(n);
-        for (int i = threadIdx.x; i < total; i += BLOCK) dst[i] = src[i];
-        __syncthreads();
-        if (threadIdx.x < count) {
-            const T log_floor = dev_log<T>(T(floor[first + threadIdx.x]));
-            for (int j = 0; j < n; ++j) {
-                const float v = dst[threadIdx.x * n + j];
-                ys[j * BLOCK + threadIdx.x] = (isfinite(v) && v > 0.0f) ? dev_log<T>(T(v)) : log_floor;
-            }
-        }
-    }
-};
 
 // ---- the small-p thread-per-voxel IRLS --------------------------------------------------
 
@@ -260,118 +236,6 @@ __global__ void __launch_bounds__(BLOCK) fit_log_small_kernel(LogDesignDevice<T>
     if (iterations) iterations[voxel] = it;
 }
 
-// ---- DTI maps ---------------------------------------------------------------------------
-
-// Eigen-decomposition of a symmetric 3x3 matrix by cyclic Jacobi rotations (Jacobi 1846;
-// Golub & Van Loan 8.5): eigenvalues in w, eigenvectors in the columns of q.
-template <class T>
-__device__ __forceinline__ T eps_of();
-template <>
-__device__ __forceinline__ double eps_of<double>() { return 2.220446049250313e-16; }
-template <>
-__device__ __forceinline__ float eps_of<float>() { return 1.1920929e-07f; }
-
-template <class T>
-__device__ __forceinline__ void jacobi3(T (&a)[3][3], T (&w)[3], T (&q)[3][3]) {
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) q[i][j] = i == j ? T(1) : T(0);
-    for (int sweep = 0; sweep < 12; ++sweep) {
-        bool rotated = false;
-#pragma unroll
-        for (int pq = 0; pq < 3; ++pq) {
-            const int p = pq == 2 ? 1 : 0;
-            const int r = pq == 0 ? 1 : 2;
-            const T apq = a[p][r];
-            const T app = a[p][p], arr = a[r][r];
-            // An off-diagonal entry below rounding of its diagonal pair is zero.
-            if (fabs(apq) <= T(1e-3) * eps_of<T>() * (fabs(app) + fabs(arr)) ||
-                apq == T(0)) {
-                a[p][r] = a[r][p] = T(0);
-                continue;
-            }
-            rotated = true;
-            const T theta = (arr - app) / (T(2) * apq);
-            const T t = (theta >= T(0) ? T(1) : T(-1)) / (fabs(theta) + sqrt(theta * theta + T(1)));
-            const T c = T(1) / sqrt(t * t + T(1));
-            const T s = t * c;
-            a[p][p] = app - t * apq;
-            a[r][r] = arr + t * apq;
-            a[p][r] = a[r][p] = T(0);
-            const int o = 3 - p - r;
-            const T aop = a[o][p], aor = a[o][r];
-            a[o][p] = a[p][o] = c * aop - s * aor;
-            a[o][r] = a[r][o] = s * aop + c * aor;
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const T qp = q[i][p], qr = q[i][r];
-                q[i][p] = c * qp - s * qr;
-                q[i][r] = s * qp + c * qr;
-            }
-        }
-        if (!rotated) break;
-    }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) w[i] = a[i][i];
-}
-
-template <class T>
-__device__ __forceinline__ T zero_nan(T x) { return isnan(x) ? T(0) : x; }
-
-// The maps of compute_dti_metrics (src/larmor/dwi/dti.py:170-235) of one voxel's tensor
-// elements d (xx, xy, xz, yy, yz, zz), written as 16 rows of maps (stride v).
-template <class T>
-__device__ __forceinline__ void dti_maps(const T (&d)[6], int64_t voxel, int64_t v,
-                                         float* __restrict__ maps, uint8_t* __restrict__ npd) {
-    T ev[3] = {T(0), T(0), T(0)};
-    T pe[3] = {T(NAN), T(NAN), T(NAN)};
-    bool finite = true;
-#pragma unroll
-    for (int i = 0; i < 6; ++i) finite &= isfinite(d[i]);
-    if (finite) {
-        T a[3][3] = {{d[0], d[1], d[2]}, {d[1], d[3], d[4]}, {d[2], d[4], d[5]}};
-        T w[3], q[3][3];
-        jacobi3<T>(a, w, q);
-        // Descending order by a sorting network on (value, column) pairs; selects keep
-        // everything in registers.
-        T c0[3] = {q[0][0], q[1][0], q[2][0]}, c1[3] = {q[0][1], q[1][1], q[2][1]},
-          c2[3] = {q[0][2], q[1][2], q[2][2]};
-        T w0 = w[0], w1 = w[1], w2 = w[2];
-        auto swap_if = [](T& wa, T (&ca)[3], T& wb, T (&cb)[3]) {
-            const bool s = wa < wb;
-            const T t = wa; wa = s ? wb : wa; wb = s ? t : wb;
-#pragma unroll
-            for (int i = 0; i < 3; ++i) { const T u = ca[i]; ca[i] = s ? cb[i] : ca[i]; cb[i] = s ? u : cb[i]; }
-        };
-        swap_if(w0, c0, w1, c1);
-        swap_if(w1, c1, w2, c2);
-        swap_if(w0, c0, w1, c1);
-        ev[0] = w0; ev[1] = w1; ev[2] = w2;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) pe[i] = c0[i];
-    }
-    const T l1 = zero_nan(ev[0]), l2 = zero_nan(ev[1]), l3 = zero_nan(ev[2]);
-    const T md = zero_nan((d[0] + d[3] + d[5]) / T(3));
-    const T num_sq = (l1 - l2) * (l1 - l2) + (l2 - l3) * (l2 - l3) + (l3 - l1) * (l3 - l1);
-    const T num = sqrt(fmax(num_sq, T(0)));
-    const T den = sqrt(l1 * l1 + l2 * l2 + l3 * l3);
-    T fa = den > T(1e-12) ? sqrt(T(0.5)) * (num / den) : T(0);
-    fa = zero_nan(fmin(fmax(fa, T(0)), T(1)));
-#pragma unroll
-    for (int i = 0; i < 6; ++i) maps[i * v + voxel] = float(d[i]);
-    maps[6 * v + voxel] = float(fa);
-    maps[7 * v + voxel] = float(md);
-    maps[8 * v + voxel] = float(l1);
-    maps[9 * v + voxel] = float((l2 + l3) / T(2));
-#pragma unroll
-    for (int i = 0; i < 3; ++i) maps[(10 + i) * v + voxel] = float(pe[i]);
-    maps[13 * v + voxel] = float(l1);
-    maps[14 * v + voxel] = float(l2);
-    maps[15 * v + voxel] = float(l3);
-    npd[voxel] = l3 <= T(0) ? 1 : 0;
-}
-
 template <class T, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) fit_dti_maps_kernel(LogDesignDevice<T> d, FlooredSource src,
                                                              int64_t v, int weighted, int max_rw, T tol,
@@ -419,14 +283,65 @@ void set_smem(Kernel kernel, size_t bytes) {
                "cudaFuncSetAttribute");
 }
 
+// Scratch layout for a constrained fit of v voxels: [count, queue] ints, voxel ids, scaled
+// parameters, then the warp slots of the re-fit.
+struct ScratchPlan {
+    size_t ids_off, params_off, slots_off, total;
+    int slots;
+};
+
+inline ScratchPlan plan_scratch(const lar::host::LogDesignHost& h, int64_t v) {
+    ScratchPlan s{};
+    const size_t align = 256;
+    auto up = [&](size_t x) { return (x + align - 1) / align * align; };
+    s.ids_off = align;
+    s.params_off = up(s.ids_off + size_t(v) * sizeof(int64_t));
+    s.slots_off = up(s.params_off + size_t(v) * h.p * sizeof(double));
+    const int64_t cap = int64_t(sm_count()) * 8;
+    s.slots = int(std::max<int64_t>(4, std::min<int64_t>((v + 3) / 4 * 4, cap)));
+    s.total = s.slots_off + size_t(s.slots) * constrained_slot_doubles(int(h.n), int(h.p), int(h.m)) * sizeof(double);
+    return s;
+}
+
+template <class T, class Src>
+void launch_general(lar_log_design_s* h, const Src& src, int64_t v, int weighted, int max_rw, double tol,
+                    double* params, uint8_t* broke, int32_t* iterations, cudaStream_t stream) {
+    const auto& d = device_view<T>(h);
+    require(h->host.p <= 32, "the log fit takes at most 32 parameters");
+    ViolatorList<T> vl;
+    ViolatorList<double> vl64;
+    ScratchPlan plan{};
+    char* base = nullptr;
+    if (h->host.m > 0) {
+        require(h->host.p <= 31, "the constrained log fit takes at most 31 parameters");
+        require(v < (int64_t(1) << 31), "at most 2^31 - 1 voxels per constrained call");
+        plan = plan_scratch(h->host, v);
+        base = static_cast<char*>(h->scratch.reserve(plan.total));
+        cuda_check(cudaMemsetAsync(base, 0, 2 * sizeof(int), stream), "cudaMemsetAsync");
+        vl.count = reinterpret_cast<int*>(base);
+        vl.capacity = int(v);
+        vl.voxel = reinterpret_cast<int64_t*>(base + plan.ids_off);
+        vl.params = reinterpret_cast<double*>(base + plan.params_off);
+        vl64.count = vl.count;
+        vl64.capacity = vl.capacity;
+        vl64.voxel = vl.voxel;
+        vl64.params = vl.params;
+    }
+    launch_log_warp<T>(d, src, v, weighted, max_rw, tol, params, broke, iterations, vl, stream);
+    if (h->host.m > 0) {
+        launch_constrained<Src>(h->d64, src, weighted, vl64, int(v), reinterpret_cast<int*>(base) + 1,
+                                reinterpret_cast<double*>(base + plan.slots_off), plan.slots, params, stream);
+    }
+}
+
 template <class T>
-void launch_fit(const lar_log_design_s* h, const double* log_s, int64_t v, int weighted,
+void launch_fit(lar_log_design_s* h, const double* log_s, int64_t v, int weighted,
                 int max_rw, double tol, double* params, uint8_t* broke, int32_t* iterations,
                 cudaStream_t stream) {
     const auto& d = device_view<T>(h);
     const int p = int(h->host.p);
+    LogSource src{log_s, h->host.n};
     if (p == 7 && h->host.m == 0) {
-        LogSource src{log_s, h->host.n};
         const size_t sm = SmallFit<T, 7>::bytes(d.n, kSmallBlock, LogSource::raw_bytes);
         auto kernel = fit_log_small_kernel<T, 7, kSmallBlock, LogSource>;
         set_smem(kernel, sm);
@@ -436,8 +351,7 @@ void launch_fit(const lar_log_design_s* h, const double* log_s, int64_t v, int w
         cuda_check(cudaGetLastError(), "fit_log_small_kernel launch");
         return;
     }
-    throw Error(LAR_ERR_INVALID, "this build fits designs with p = 7 and no constraints; got p = " +
-                                     std::to_string(p) + ", m = " + std::to_string(h->host.m));
+    launch_general<T>(h, src, v, weighted, max_rw, tol, params, broke, iterations, stream);
 }
 
 template <class T>
@@ -489,6 +403,8 @@ void upload_design(lar_log_design_s* h, DeviceArray<T>& x, DeviceArray<T>& pinvt
 }
 
 }  // namespace
+
+void launch_dki_maps(const double* params, int64_t v, float* maps, uint8_t* npd, cudaStream_t stream);
 
 }  // namespace lar
 
@@ -552,6 +468,39 @@ int lar_fit_dti_maps(lar_log_design design, const float* signals, const double* 
             launch_dti_maps<double>(design, signals, floor, v, weighted, rw, tol, maps, npd, params, s);
         else
             launch_dti_maps<float>(design, signals, floor, v, weighted, rw, tol, maps, npd, params, s);
+    });
+}
+
+int lar_dki_maps(const double* params, int64_t v, float* maps, uint8_t* npd, void* stream) {
+    return guarded([&] {
+        require(v >= 0, "v must be at least 0");
+        if (v == 0) return;
+        require(params && maps && npd, "params, maps and npd must not be NULL");
+        launch_dki_maps(params, v, maps, npd, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int lar_fit_dki_maps(lar_log_design design, const float* signals, const double* s0, const double* floor,
+                     const uint8_t* is_b0, int64_t v, int weighted, int64_t max_iter, double tol,
+                     int precision, float* maps, uint8_t* npd, uint8_t* broke, double* params,
+                     void* stream) {
+    return guarded([&] {
+        require(design != nullptr, "design must not be NULL");
+        require(design->host.p == 22, "the DKI maps need the 22-column DKI design");
+        require(v >= 0, "v must be at least 0");
+        require(max_iter >= 0, "max_iter must be at least 0");
+        require(precision == LAR_FP64 || precision == LAR_FP32, "precision must be LAR_FP64 or LAR_FP32");
+        if (v == 0) return;
+        require(signals && floor && is_b0 && maps && npd && broke && params,
+                "signals, floor, is_b0, maps, npd, broke and params must not be NULL");
+        const int rw = int(std::min<int64_t>(max_iter, 1 << 20));
+        auto st = static_cast<cudaStream_t>(stream);
+        CappedSource src{signals, s0, floor, is_b0, design->host.n};
+        if (precision == LAR_FP64)
+            launch_general<double>(design, src, v, weighted, rw, tol, params, broke, nullptr, st);
+        else
+            launch_general<float>(design, src, v, weighted, rw, tol, params, broke, nullptr, st);
+        launch_dki_maps(params, v, maps, npd, st);
     });
 }
 

@@ -1,0 +1,269 @@
+// The log-signal fit for designs of up to 32 parameters (DKI: p = 22), one warp per voxel.
+//
+// Follows cpp/src/dwi/log_fit.cpp: the ordinary fit pinv y (:251), the reweighted fit
+// (reweighted_fit :114-147) and the constraint check (breaks_a_constraint :150). The design
+// (unit-norm columns, pseudo-inverse) sits in shared memory, shared by the CTA's warps; each
+// warp keeps its voxel's log signals, weights and normal matrix in its own shared-memory
+// slice. Lanes split the measurements for predictions and weights, the normal-matrix entries
+// for the weighted Gram, and the rows for the L D L^T solve.
+//
+// Voxels whose unconstrained solution breaks a constraint are appended to a compacted list
+// (voxel index and scaled parameters) for the constrained re-fit (constrained_fit.cu).
+
+#include <cstdint>
+
+#include "common.cuh"
+#include "log_fit.cuh"
+#include "log_fit_warp.cuh"
+
+namespace lar {
+
+namespace {
+
+constexpr int kWarps = 4;
+
+template <class T>
+struct WarpLayout {
+    int n, p, px, pp;
+    // Shared memory: X (n, px), pinv^T (n, p), the (a, b) of each normal-matrix entry,
+    // then per warp: y (n), w (n), normal matrix (p, px), 4 vectors of 32.
+    __host__ __device__ size_t design_elems() const { return size_t(n) * px + size_t(n) * p; }
+    __host__ __device__ size_t warp_elems() const { return 2 * size_t(n) + size_t(p) * px + 4 * 32; }
+    __host__ __device__ size_t bytes(int warps) const {
+        return (design_elems() + warps * warp_elems()) * sizeof(T) + 2 * size_t(pp) + 16;
+    }
+};
+
+// Solves the symmetric system held in the lower triangle of a (p x px, shared) by L D L^T in
+// place, with b (shared, p) overwritten by the solution. Returns false on an exactly zero pivot
+// (singular weighted normal equations; cpp/src/dwi/log_fit.cpp:128-133). All lanes return the
+// same value.
+template <class T>
+__device__ bool warp_ldlt_solve(T* a, int p, int px, T* b, T* col, int lane) {
+    for (int k = 0; k < p; ++k) {
+        __syncwarp();
+        const T d = a[k * px + k];
+        if (d == T(0)) return false;
+        const int i = k + 1 + lane;
+        T l = T(0);
+        if (i < p) {
+            const T c = a[i * px + k];
+            col[i] = c;
+            l = c / d;
+        }
+        __syncwarp();
+        if (i < p) {
+            for (int j = k + 1; j <= i; ++j) a[i * px + j] = fma(-l, col[j], a[i * px + j]);
+            a[i * px + k] = l;
+        }
+    }
+    // L z = b, then z / d, then L^T x = z.
+    for (int k = 0; k < p; ++k) {
+        __syncwarp();
+        const T zk = b[k];
+        const int i = k + 1 + lane;
+        if (i < p) b[i] = fma(-a[i * px + k], zk, b[i]);
+    }
+    __syncwarp();
+    if (lane < p) b[lane] = b[lane] / a[lane * px + lane];
+    for (int k = p - 1; k >= 0; --k) {
+        __syncwarp();
+        const T zk = b[k];
+        if (lane < k) b[lane] = fma(-a[k * px + lane], zk, b[lane]);
+    }
+    __syncwarp();
+    return true;
+}
+
+template <class T, class Src>
+__global__ void __launch_bounds__(kWarps * 32) fit_log_warp_kernel(
+    LogDesignDevice<T> d, Src src, int64_t v, int weighted, int max_rw, T tol,
+    double* __restrict__ params, uint8_t* __restrict__ broke, int32_t* __restrict__ iterations,
+    ViolatorList<T> violators) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = d.n, p = d.p, px = p | 1, pp = p * (p + 1) / 2;
+    const WarpLayout<T> lay{n, p, px, pp};
+    T* xs = reinterpret_cast<T*>(smem_raw);
+    T* pinvt = xs + size_t(n) * px;
+    uint8_t* ea = reinterpret_cast<uint8_t*>(reinterpret_cast<T*>(smem_raw) + lay.design_elems() +
+                                             kWarps * lay.warp_elems());
+    uint8_t* eb = ea + pp;
+    for (int i = threadIdx.x; i < n * p; i += blockDim.x) {
+        const int r = i / p, c = i % p;
+        xs[r * px + c] = d.x[i];
+        pinvt[i] = d.pinvt[i];
+    }
+    for (int e = threadIdx.x; e < pp; e += blockDim.x) {
+        // Entry e of the packed upper triangle, row by row.
+        int a = 0, rem = e;
+        while (rem >= p - a) { rem -= p - a; ++a; }
+        ea[e] = uint8_t(a);
+        eb[e] = uint8_t(a + rem);
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    T* ys = reinterpret_cast<T*>(smem_raw) + lay.design_elems() + warp * lay.warp_elems();
+    T* ws = ys + n;
+    T* gm = ws + n;
+    T* pv = gm + size_t(p) * px;  // current parameters
+    T* rv = pv + 32;              // right-hand side / next parameters
+    T* ov = rv + 32;              // ordinary fit
+    T* cv = ov + 32;              // column scratch of the solve
+
+    for (int64_t voxel = int64_t(blockIdx.x) * kWarps + warp; voxel < v;
+         voxel += int64_t(gridDim.x) * kWarps) {
+        src.template warp_stage<T>(voxel, ys, lane);
+        __syncwarp();
+        // Ordinary fit.
+        if (lane < p) {
+            T acc = T(0);
+            for (int j = 0; j < n; ++j) acc = fma(pinvt[j * p + lane], ys[j], acc);
+            ov[lane] = acc;
+            pv[lane] = acc;
+        }
+        __syncwarp();
+        bool finite = true;
+        for (int a = 0; a < p; ++a) finite &= bool(isfinite(pv[a]));
+        int it = 0;
+        if (weighted && finite) {
+            T mx = -INFINITY;
+            for (int j = lane; j < n; j += 32) {
+                T pred = T(0);
+                for (int a = 0; a < p; ++a) pred = fma(xs[j * px + a], pv[a], pred);
+                mx = fmax(mx, pred);
+            }
+            mx = warp_max(mx);
+            for (; it < max_rw; ++it) {
+                for (int j = lane; j < n; j += 32) {
+                    T pred = T(0);
+                    for (int a = 0; a < p; ++a) pred = fma(xs[j * px + a], pv[a], pred);
+                    ws[j] = dev_exp<T>(T(2) * (pred - mx));
+                }
+                __syncwarp();
+                for (int e = lane; e < pp; e += 32) {
+                    const int a = ea[e], b = eb[e];
+                    T acc = T(0);
+                    for (int j = 0; j < n; ++j) acc = fma(ws[j] * xs[j * px + a], xs[j * px + b], acc);
+                    gm[b * px + a] = acc;  // lower triangle
+                }
+                if (lane < p) {
+                    T acc = T(0);
+                    for (int j = 0; j < n; ++j) acc = fma(ws[j] * xs[j * px + lane], ys[j], acc);
+                    rv[lane] = acc;
+                }
+                __syncwarp();
+                bool ok = warp_ldlt_solve<T>(gm, p, px, rv, cv, lane);
+                if (ok) {
+                    for (int a = 0; a < p; ++a) ok &= bool(isfinite(rv[a]));
+                }
+                if (!ok) {
+                    if (lane < p) pv[lane] = ov[lane];
+                    __syncwarp();
+                    ++it;
+                    break;
+                }
+                T change = T(0), mxn = -INFINITY;
+                for (int j = lane; j < n; j += 32) {
+                    T po = T(0), pn = T(0);
+                    for (int a = 0; a < p; ++a) {
+                        po = fma(xs[j * px + a], pv[a], po);
+                        pn = fma(xs[j * px + a], rv[a], pn);
+                    }
+                    change = fmax(change, fabs(pn - po));
+                    mxn = fmax(mxn, pn);
+                }
+                change = warp_max(change);
+                mxn = warp_max(mxn);
+                __syncwarp();
+                if (lane < p) pv[lane] = rv[lane];
+                __syncwarp();
+                mx = mxn;
+                if (!(change > tol)) {
+                    ++it;
+                    break;
+                }
+            }
+        }
+        // Constraint check on the scaled parameters (cpp/src/dwi/log_fit.cpp:150,256).
+        bool violated = false;
+        if (d.m > 0) {
+            bool fin = true;
+            for (int a = 0; a < p; ++a) fin &= bool(isfinite(pv[a]));
+            if (fin) {
+                bool neg = false;
+                for (int i = lane; i < d.m; i += 32) {
+                    T val = T(0);
+                    for (int a = 0; a < p; ++a) val = fma(d.g[size_t(i) * p + a], pv[a], val);
+                    neg |= val < T(0);
+                }
+                violated = __any_sync(0xffffffffu, neg);
+            }
+        }
+        if (lane < p) params[voxel * p + lane] = double(pv[lane]) / d.scales64[lane];
+        if (lane == 0) {
+            broke[voxel] = violated ? 1 : 0;
+            if (iterations) iterations[voxel] = it;
+        }
+        if (violated && violators.count != nullptr) {
+            int slot = 0;
+            if (lane == 0) slot = atomicAdd(violators.count, 1);
+            slot = __shfl_sync(0xffffffffu, slot, 0);
+            if (slot < violators.capacity) {
+                if (lane == 0) violators.voxel[slot] = voxel;
+                if (lane < p) violators.params[size_t(slot) * p + lane] = double(pv[lane]);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <class T, class Src>
+void launch_warp_impl(const LogDesignDevice<T>& d, const Src& src, int64_t v, int weighted, int max_rw,
+                      double tol, double* params, uint8_t* broke, int32_t* iterations,
+                      const ViolatorList<T>& violators, cudaStream_t stream) {
+    const WarpLayout<T> lay{d.n, d.p, d.p | 1, d.p * (d.p + 1) / 2};
+    const size_t smem = lay.bytes(kWarps);
+    require(smem <= 227 * 1024, "the design is too large for the shared-memory log fit");
+    auto kernel = fit_log_warp_kernel<T, Src>;
+    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+               "cudaFuncSetAttribute");
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kWarps * 32, smem),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    const int64_t need = (v + kWarps - 1) / kWarps;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sm_count()) * std::max(per_sm, 1) * 4));
+    kernel<<<unsigned(grid), kWarps * 32, smem, stream>>>(d, src, v, weighted, max_rw, T(tol), params, broke,
+                                                          iterations, violators);
+    cuda_check(cudaGetLastError(), "fit_log_warp_kernel launch");
+}
+
+}  // namespace
+
+template <class T>
+void launch_log_warp(const LogDesignDevice<T>& d, const LogSource& src, int64_t v, int weighted, int max_rw,
+                     double tol, double* params, uint8_t* broke, int32_t* iterations,
+                     const ViolatorList<T>& violators, cudaStream_t stream) {
+    launch_warp_impl<T, LogSource>(d, src, v, weighted, max_rw, tol, params, broke, iterations, violators, stream);
+}
+
+template <class T>
+void launch_log_warp(const LogDesignDevice<T>& d, const CappedSource& src, int64_t v, int weighted, int max_rw,
+                     double tol, double* params, uint8_t* broke, int32_t* iterations,
+                     const ViolatorList<T>& violators, cudaStream_t stream) {
+    launch_warp_impl<T, CappedSource>(d, src, v, weighted, max_rw, tol, params, broke, iterations, violators,
+                                      stream);
+}
+
+template void launch_log_warp<double>(const LogDesignDevice<double>&, const LogSource&, int64_t, int, int, double,
+                                      double*, uint8_t*, int32_t*, const ViolatorList<double>&, cudaStream_t);
+template void launch_log_warp<float>(const LogDesignDevice<float>&, const LogSource&, int64_t, int, int, double,
+                                     double*, uint8_t*, int32_t*, const ViolatorList<float>&, cudaStream_t);
+template void launch_log_warp<double>(const LogDesignDevice<double>&, const CappedSource&, int64_t, int, int,
+                                      double, double*, uint8_t*, int32_t*, const ViolatorList<double>&,
+                                      cudaStream_t);
+template void launch_log_warp<float>(const LogDesignDevice<float>&, const CappedSource&, int64_t, int, int,
+                                     double, double*, uint8_t*, int32_t*, const ViolatorList<float>&,
+                                     cudaStream_t);
+
+}  // namespace lar

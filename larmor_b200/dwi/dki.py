@@ -1,0 +1,208 @@
+"""Diffusion kurtosis imaging (DKI) on the GPU, with the API of src/larmor/dwi/dki.py.
+
+`DKIModel(fit_method=..., constrained=...).fit(volume, gtab, mask)` returns the reference's
+`DKIFit` maps. The host estimates S0 and the sample floor and gathers the masked float32
+signals; on the device one kernel caps and floors the samples and runs the 22-parameter
+(I)RLS fit (a warp per voxel), a second re-fits the voxels that break a constraint (least
+distance by NNLS, FP64), and a third computes the DTI and kurtosis maps.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from larmor_b200 import _core, _lib
+from larmor_b200._log import LarmorLogger
+from larmor_b200._threads import n_threads
+from larmor_b200.dwi.dti import LOG_SIGNAL_TOL, MAX_REWEIGHTINGS, PRECISIONS
+from larmor_b200.dwi.inputs import (
+    as_mask,
+    check_dwi,
+    estimate_s0,
+    largest_finite_signal,
+    masked_signals,
+    sample_floors,
+)
+from larmor_b200.dwi.mask import unmask
+from larmor_b200.types import GradientTable, Volume
+
+FIT_METHODS = ("ols", "wls")
+# The 15 unique elements of the kurtosis tensor (0 = x), in the order of DKIFit.kt, and the
+# number of distinct permutations of each (src/larmor/dwi/dki.py:30-48).
+KT_INDICES = (
+    (0, 0, 0, 0), (1, 1, 1, 1), (2, 2, 2, 2), (0, 0, 0, 1), (0, 0, 0, 2), (1, 1, 1, 0),
+    (1, 1, 1, 2), (2, 2, 2, 0), (2, 2, 2, 1), (0, 0, 1, 1), (0, 0, 2, 2), (1, 1, 2, 2),
+    (0, 0, 1, 2), (1, 1, 0, 2), (2, 2, 0, 1),
+)
+KT_MULTIPLICITY = (1, 1, 1, 4, 4, 4, 4, 4, 4, 6, 6, 6, 12, 12, 12)
+# Constant C of the bound K(n) <= C / (b_max D(n)), and the constraint directions.
+KURTOSIS_BOUND_C = 3.0
+N_CONSTRAINT_DIRS = 256
+
+
+@dataclass(frozen=True)
+class DKIFit:
+    """Result of a DKI fit as float32 maps on the grid (zero outside the fitted mask); the
+    fields are the reference's DKIFit (src/larmor/dwi/dki.py:64-113)."""
+
+    dt: np.ndarray
+    kt: np.ndarray
+    s0: np.ndarray
+    fa: np.ndarray
+    md: np.ndarray
+    ad: np.ndarray
+    rd: np.ndarray
+    pe: np.ndarray
+    eigen_vals: np.ndarray
+    npd: np.ndarray
+    mk: np.ndarray
+    ak: np.ndarray
+    rk: np.ndarray
+    ka: np.ndarray
+
+
+def _kt_rows(dirs: np.ndarray) -> np.ndarray:
+    return np.stack([m * dirs[:, i] * dirs[:, j] * dirs[:, k] * dirs[:, q]
+                     for (i, j, k, q), m in zip(KT_INDICES, KT_MULTIPLICITY)], axis=1)
+
+
+def dki_design(gtab: GradientTable) -> np.ndarray:
+    """The design (N, 22): log S0, the six D elements, the fifteen of MD^2 W
+    (src/larmor/dwi/dki.py:345-380)."""
+    if gtab.count_shells() < 2:
+        raise ValueError(
+            "DKI needs at least two non-zero b-value shells; the gradient table has "
+            f"{gtab.count_shells()}."
+        )
+    b2 = gtab.bvals**2 / 6
+    g = gtab.bvecs
+    kt_columns = [m * b2 * g[:, i] * g[:, j] * g[:, k] * g[:, q]
+                  for (i, j, k, q), m in zip(KT_INDICES, KT_MULTIPLICITY)]
+    design = np.column_stack([np.ones(len(b2)), -gtab.b_matrix, *kt_columns])
+    norms = np.linalg.norm(design, axis=0)
+    if np.linalg.matrix_rank(design / np.where(norms > 0, norms, 1.0)) < design.shape[1]:
+        raise ValueError(
+            "The b-values and b-vectors cannot determine the diffusion and kurtosis tensors: "
+            "DKI needs a b0 or a third shell, and enough non-collinear directions."
+        )
+    return design
+
+
+def fibonacci_half_sphere(n: int) -> np.ndarray:
+    """n unit vectors (n, 3) spread over the half sphere z > 0 (src/larmor/dwi/dki.py:414-420)."""
+    i = np.arange(n) + 0.5
+    z = 1 - i / n
+    phi = np.pi * (3 - np.sqrt(5)) * i
+    r = np.sqrt(1 - z**2)
+    return np.stack([r * np.cos(phi), r * np.sin(phi), z], axis=1)
+
+
+def dki_constraints(gtab: GradientTable) -> np.ndarray:
+    """G (768, 22) of D(n) >= 0, MD^2 W(n) >= 0 and the kurtosis upper bound on 256 directions
+    (src/larmor/dwi/dki.py:383-411)."""
+    dirs = fibonacci_half_sphere(N_CONSTRAINT_DIRS)
+    x, y, z = dirs.T
+    d_rows = np.stack([x * x, 2 * x * y, 2 * x * z, y * y, 2 * y * z, z * z], axis=1)
+    v_rows = _kt_rows(dirs)
+    zero_1 = np.zeros((len(dirs), 1))
+    bound = KURTOSIS_BOUND_C / float(gtab.bvals.max())
+    return np.vstack([
+        np.hstack([zero_1, d_rows, np.zeros_like(v_rows)]),
+        np.hstack([zero_1, np.zeros_like(d_rows), v_rows]),
+        np.hstack([zero_1, bound * d_rows, -v_rows]),
+    ])
+
+
+class DKIModel:
+    """Diffusion kurtosis imaging: a diffusion and a kurtosis tensor per voxel.
+
+    Args:
+        fit_method: "ols" or "wls" (default).
+        constrained: Whether D(n) >= 0, K(n) >= 0 and K(n) <= 3 / (b_max D(n)) are imposed on
+            256 directions (default True).
+        precision: "fp64" (default) or "fp32" for the unconstrained fit; the constrained re-fit
+            and the maps are FP64.
+    """
+
+    def __init__(self, *, fit_method: str = "wls", constrained: bool = True,
+                 precision: str = "fp64") -> None:
+        if fit_method not in FIT_METHODS:
+            raise ValueError(
+                f"Unknown DKI fit method {fit_method!r}: use one of {', '.join(FIT_METHODS)}."
+            )
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {', '.join(PRECISIONS)}, got {precision!r}")
+        self.fit_method = fit_method
+        self.constrained = constrained
+        self.precision = precision
+
+    def fit(self, volume: Volume, gtab: GradientTable, mask=None, *, n_jobs: int = -1) -> DKIFit:
+        """Fits both tensors in every voxel of the mask; see the reference's DKIModel.fit
+        (src/larmor/dwi/dki.py:153-282). A mask is required."""
+        n_threads(n_jobs)
+        check_dwi(volume, gtab)
+        design = dki_design(gtab)
+        if mask is None:
+            raise ValueError("DKIModel.fit needs a mask on the volume's grid.")
+        mask = as_mask(volume, mask)
+        fitted = mask.copy()
+        is_b0 = gtab.b0_mask
+        s0 = None
+        if is_b0.any():
+            s0 = estimate_s0(volume, gtab, mask)[mask]
+            usable = np.isfinite(s0) & (s0 > 0)
+            if not usable.all():
+                LarmorLogger.warning(
+                    "%d mask voxels have no usable S0 (no plausible b0 in them or near them); "
+                    "they are not fitted and come out as 0.", int((~usable).sum()))
+            fitted[mask] = usable
+            s0 = s0[usable]
+        voxels = np.nonzero(fitted)
+        signals = masked_signals(volume, voxels)
+        largest = largest_finite_signal(signals) if s0 is None else None
+        floor = sample_floors(s0, largest, len(signals))
+        g = dki_constraints(gtab) if self.constrained else np.zeros((0, design.shape[1]))
+        maps, npd, broke = fit_dki_signals(design, g, signals, s0, floor, is_b0,
+                                           self.fit_method == "wls", PRECISIONS[self.precision])
+        if self.constrained:
+            LarmorLogger.info("%d of %d voxels break a constraint.", int(broke.sum()), len(broke))
+        return DKIFit(
+            dt=unmask(maps[0:6].T, fitted), kt=unmask(maps[16:31].T, fitted),
+            s0=unmask(maps[31], fitted), fa=unmask(maps[6], fitted), md=unmask(maps[7], fitted),
+            ad=unmask(maps[8], fitted), rd=unmask(maps[9], fitted), pe=unmask(maps[10:13].T, fitted),
+            eigen_vals=unmask(maps[13:16].T, fitted),
+            npd=unmask(npd, fitted, fill_value=False, dtype=bool),
+            mk=unmask(maps[32], fitted), ak=unmask(maps[33], fitted), rk=unmask(maps[34], fitted),
+            ka=unmask(maps[35], fitted),
+        )
+
+
+def fit_dki_signals(design, g, signals, s0, floor, is_b0, weighted, precision=_lib.LAR_FP64):
+    """Fits float32 signals (v, N) on the device; returns maps (36, v), npd (v,), broke (v,)."""
+    torch = _core._torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    handle = _core.LogDesign.cached(design, g)
+    v = len(signals)
+    maps = torch.empty((36, v), dtype=torch.float32, device=dev)
+    npd = torch.empty((v,), dtype=torch.uint8, device=dev)
+    broke = torch.empty((v,), dtype=torch.uint8, device=dev)
+    params = torch.empty((v, 22), dtype=torch.float64, device=dev)
+    if v:
+        s = torch.from_numpy(np.ascontiguousarray(signals, dtype=np.float32)).to(dev)
+        f = torch.from_numpy(np.ascontiguousarray(floor, dtype=np.float64)).to(dev)
+        b0 = torch.from_numpy(np.ascontiguousarray(is_b0, dtype=np.uint8)).to(dev)
+        s0d = None if s0 is None else torch.from_numpy(np.ascontiguousarray(s0, dtype=np.float64)).to(dev)
+        _lib.check(_lib.lib().lar_fit_dki_maps(
+            handle.handle, _lib.ptr(s), _lib.ptr(s0d), _lib.ptr(f), _lib.ptr(b0), v, int(weighted),
+            MAX_REWEIGHTINGS, LOG_SIGNAL_TOL, int(precision), _lib.ptr(maps), _lib.ptr(npd),
+            _lib.ptr(broke), _lib.ptr(params), _core._stream(torch)))
+    return maps.cpu().numpy(), npd.cpu().numpy().astype(bool), broke.cpu().numpy().astype(bool)
+
+
+def dki_maps_device(params, maps, npd) -> None:
+    """The 36 DKI maps of device params (v, 22)."""
+    torch = _core._torch()
+    _lib.check(_lib.lib().lar_dki_maps(_lib.ptr(params), params.shape[0], _lib.ptr(maps),
+                                       _lib.ptr(npd), _core._stream(torch)))
