@@ -97,6 +97,25 @@ int lar_fit_dki_maps(lar_log_design design, const float* signals, const double* 
                      int precision, float* maps, uint8_t* npd, uint8_t* broke, double* params,
                      void* stream);
 
+/* ---- A fit that allocates no device memory ------------------------------------------- */
+
+/* No counterpart in the reference: an entry point for callers that cannot allocate device
+ * memory (an application that owns all device memory through its own allocator or budget, a
+ * plugin host that hands out only its own buffers, code where an allocation is not allowed).
+ * It fits each row of log_s (v, n) (device) like lar_fit_log_signal at FP64, with the design
+ * x (n, p) and constraints g (m, p) given as host arrays and prepared on the host, and writes
+ * params (v, p) and broke (v,) (device). Everything else it needs on the device -- the
+ * prepared design, the violator list and the constrained re-fit's workspace -- lives in one
+ * static device array of 32 MiB that every GPU loading this library holds until exit; the
+ * call returns LAR_ERR_INVALID, with the largest voxel count that fits, when the design and v
+ * need more. It calls no cudaMalloc or cudaFree. Its first call on a device looks up the
+ * array's address there (cudaGetSymbolAddress): make that first call before any stream
+ * capture. Calls share the array: calls whose work overlaps on the GPU race and must be
+ * serialised by the caller. The call waits for its stream once, after copying the design. */
+int lar_fit_log_signal_noalloc(const double* x, int64_t n, int64_t p, const double* g, int64_t m,
+                               const double* log_s, int64_t v, int weighted, int64_t max_iter,
+                               double tol, double* params, uint8_t* broke, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,6 +26,7 @@ SIGNATURES: dict[str, tuple] = {
     "lar_fit_dti_maps": (_i32, [_p, _p, _p, _i64, _i32, _i64, _f64, _i32, _p, _p, _p, _p]),
     "lar_dki_maps": (_i32, [_p, _i64, _p, _p, _p]),
     "lar_fit_dki_maps": (_i32, [_p, _p, _p, _p, _p, _i64, _i32, _i64, _f64, _i32, _p, _p, _p, _p, _p]),
+    "lar_fit_log_signal_noalloc": (_i32, [_p, _i64, _i64, _p, _i64, _p, _i64, _i32, _i64, _f64, _p, _p, _p]),
 }
 
 LAR_OK, LAR_ERR_INVALID, LAR_ERR_CUDA, LAR_ERR_MEMORY = 0, 1, 2, 3
