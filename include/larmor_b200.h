@@ -19,6 +19,8 @@
  *                                            (src/larmor/dwi/dti.py:156-163, :170-235)
  *   lar_fit_dki_maps, lar_dki_maps           DKIModel.fit's chunk loop + compute_kurtosis_metrics
  *                                            (src/larmor/dwi/dki.py:243-282, :285-540)
+ *   lar_lsi_design_*, lar_fit_lsi            larmor._core.LsiDesign, larmor._core.fit_lsi
+ *                                            (cpp/src/python/sd.cpp:361-392, cpp/src/sd/lsi.cpp)
  */
 #ifndef LARMOR_B200_H
 #define LARMOR_B200_H
@@ -96,6 +98,34 @@ int lar_fit_dki_maps(lar_log_design design, const float* signals, const double* 
                      const uint8_t* is_b0, int64_t v, int weighted, int64_t max_iter, double tol,
                      int precision, float* maps, uint8_t* npd, uint8_t* broke, double* params,
                      void* stream);
+
+/* ---- Least squares with inequality constraints (MSMT-CSD) ----------------------------- */
+
+typedef struct lar_lsi_design_s* lar_lsi_design;
+
+/* Prepares min ||a x - s||^2 + ridge^2 ||x||^2 subject to g x >= 0 for a (m, n) and g (k, n)
+ * (host arrays), n <= 63: the column-pivoted QR of [a; ridge I], q_t, P R^-1, the unit-row
+ * E = G P R^-1, its Gram and absolute row sums, in FP64, copied to the device. Fails with
+ * LAR_ERR_INVALID when [a; ridge I] does not have full column rank or ridge < 0.
+ * Replaces larmor._core.LsiDesign (cpp/src/python/sd.cpp:361, cpp/src/sd/lsi.cpp:75). */
+int lar_lsi_design_create(const double* a, int64_t m, int64_t n, const double* g, int64_t k, double ridge,
+                          lar_lsi_design* out);
+void lar_lsi_design_destroy(lar_lsi_design design);
+
+/* Copies the prepared matrices to host arrays (any may be NULL): q_t (n, m), back (n, n),
+ * e (k, n), gram (k, k), abs_sums (k,). */
+int lar_lsi_design_matrices(lar_lsi_design design, double* q_t, double* back, double* e, double* gram,
+                            double* abs_sums);
+
+/* Solves the problem for every row of signals (v, m) (device double): x (v, n) (device double)
+ * and converged (v,) (device uint8), 0 where the NNLS stopped at its limit of inner steps.
+ * Optional (NULL to skip): status (v,) 0 Cholesky path, 1 QR fallback, 2 no bound active;
+ * outer (v,) int32 outer steps; active (v, k) uint8 the constraints with a non-zero
+ * multiplier. only_qr forces the fallback (cpp/src/sd/lsi.cpp:346). Calls on one design handle
+ * must not overlap on the GPU (they share its scratch).
+ * Replaces larmor._core.fit_lsi (cpp/src/python/sd.cpp:370-392). */
+int lar_fit_lsi(lar_lsi_design design, const double* signals, int64_t v, int only_qr, double* x,
+                uint8_t* converged, uint8_t* status, int32_t* outer, uint8_t* active, void* stream);
 
 /* ---- A fit that allocates no device memory ------------------------------------------- */
 

@@ -182,3 +182,85 @@ def fit_dti_maps_device(design: LogDesign, signals, floor, weighted: bool, maps,
         design.handle, _lib.ptr(signals), _lib.ptr(floor), signals.shape[0], int(weighted),
         int(max_iter), float(tol), int(precision), _lib.ptr(maps), _lib.ptr(npd), _lib.ptr(params),
         _stream(torch)))
+
+
+class LsiDesign:
+    """A least-squares problem with inequality constraints, prepared once for many voxels.
+
+    Prepares min ||a x - s||^2 + ridge^2 ||x||^2 subject to g x >= 0, a (m, n), g (k, n), as
+    cpp/src/sd/lsi.cpp:75-125 does (in FP64 on the host), and keeps it on the device.
+
+    Raises:
+        TypeError: If a or g is not a float64 numpy array.
+        ValueError: If the shapes do not match, ridge is negative, or [a; ridge I] does not
+            have full column rank.
+    """
+
+    def __init__(self, a, g, ridge) -> None:
+        a = _array(a, "a", 2)
+        g = _array(g, "g", 2)
+        if g.shape[1] != a.shape[1]:
+            raise ValueError(f"the constraints have {g.shape[1]} columns but the design has {a.shape[1]}")
+        if not ridge >= 0.0:
+            raise ValueError("the ridge must be at least 0")
+        self.m, self.n = a.shape
+        self.k = g.shape[0]
+        self._handle = ctypes.c_void_p()
+        _lib.check(_lib.lib().lar_lsi_design_create(_lib.ptr(a), self.m, self.n, _lib.ptr(g), self.k,
+                                                    float(ridge), ctypes.byref(self._handle)))
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._handle
+
+    def matrices(self) -> dict:
+        """The prepared matrices q_t (n, m), back (n, n), e (k, n), gram (k, k), abs_sums (k,)."""
+        out = dict(q_t=np.empty((self.n, self.m)), back=np.empty((self.n, self.n)),
+                   e=np.empty((self.k, self.n)), gram=np.empty((self.k, self.k)), abs_sums=np.empty(self.k))
+        _lib.check(_lib.lib().lar_lsi_design_matrices(
+            self._handle, *(_lib.ptr(out[key]) for key in ("q_t", "back", "e", "gram", "abs_sums"))))
+        return out
+
+    def __del__(self) -> None:
+        handle = getattr(self, "_handle", None)
+        if handle is not None and handle.value:
+            try:
+                _lib.lib().lar_lsi_design_destroy(handle)
+            except Exception:
+                pass
+
+
+def fit_lsi(signals, design: LsiDesign, n_threads):
+    """Solves the constrained least-squares problem of every row of signals (v, m).
+
+    Returns the solutions (v, n) and whether each voxel's NNLS converged (v,).
+
+    Raises:
+        TypeError: If signals is not a float64 numpy array.
+        ValueError: If signals is not C-contiguous, does not have the design's number of
+            measurements, or n_threads is 0.
+    """
+    signals = _array(signals, "signals", 2)
+    if signals.shape[1] != design.m:
+        raise ValueError(f"signals {signals.shape} do not have the design's {design.m} measurements")
+    _require_threads(n_threads)
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    v = signals.shape[0]
+    x = torch.empty((v, design.n), dtype=torch.float64, device=dev)
+    conv = torch.empty((v,), dtype=torch.uint8, device=dev)
+    if v:
+        s = torch.from_numpy(signals).to(dev)
+        fit_lsi_device(design, s, x, conv)
+    return x.cpu().numpy(), conv.cpu().numpy().astype(bool)
+
+
+def fit_lsi_device(design: LsiDesign, signals, x, converged, status=None, outer=None, active=None,
+                   only_qr: bool = False) -> None:
+    """The device-resident fit_lsi: torch CUDA tensors in and out; status (0 Cholesky path,
+    1 QR fallback, 2 no constraint active), outer steps and active-constraint flags (v, k) are
+    optional diagnostics."""
+    torch = _torch()
+    _lib.check(_lib.lib().lar_fit_lsi(
+        design.handle, _lib.ptr(signals), signals.shape[0], int(only_qr), _lib.ptr(x), _lib.ptr(converged),
+        _lib.ptr(status), _lib.ptr(outer), _lib.ptr(active), _stream(torch)))

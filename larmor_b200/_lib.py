@@ -26,6 +26,10 @@ SIGNATURES: dict[str, tuple] = {
     "lar_fit_dti_maps": (_i32, [_p, _p, _p, _i64, _i32, _i64, _f64, _i32, _p, _p, _p, _p]),
     "lar_dki_maps": (_i32, [_p, _i64, _p, _p, _p]),
     "lar_fit_dki_maps": (_i32, [_p, _p, _p, _p, _p, _i64, _i32, _i64, _f64, _i32, _p, _p, _p, _p, _p]),
+    "lar_lsi_design_create": (_i32, [_p, _i64, _i64, _p, _i64, _f64, _p]),
+    "lar_lsi_design_destroy": (None, [_p]),
+    "lar_lsi_design_matrices": (_i32, [_p, _p, _p, _p, _p, _p]),
+    "lar_fit_lsi": (_i32, [_p, _p, _i64, _i32, _p, _p, _p, _p, _p, _p]),
     "lar_fit_log_signal_noalloc": (_i32, [_p, _i64, _i64, _p, _i64, _p, _i64, _i32, _i64, _f64, _p, _p, _p]),
 }
 

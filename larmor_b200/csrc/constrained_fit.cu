@@ -25,13 +25,14 @@
 #include "common.cuh"
 #include "log_fit.cuh"
 #include "log_fit_warp.cuh"
+#include "warp_nnls.cuh"
 
 namespace lar {
 
 namespace {
 
 constexpr int kCWarps = 4;
-constexpr double kEps = 2.220446049250313e-16;
+constexpr double kEps = kEps64;
 constexpr double kFeasibilityMargin = 1e-12;
 constexpr int kInnerStepsPerConstraint = 50;
 constexpr double kConstraintTolerance = 1e-9;
@@ -39,179 +40,15 @@ constexpr double kConstraintTolerance = 1e-9;
 __device__ __forceinline__ double wsum(double v) { return warp_sum(v); }
 __device__ __forceinline__ double wmax(double v) { return warp_max(v); }
 
-// Index of the largest value among the lanes' candidates, the smallest index on a tie;
-// lanes without a candidate pass index -1.
-__device__ __forceinline__ int warp_argmax_first(double v, int idx) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
-        const bool take = oi >= 0 && (idx < 0 || ov > v || (ov == v && oi < idx));
-        v = take ? ov : v;
-        idx = take ? oi : idx;
-    }
-    return idx;
-}
-
-// Index of the smallest value, the smallest index on a tie; -1 candidates are ignored.
-__device__ __forceinline__ int warp_argmin_first(double v, int idx, double* best) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
-        const bool take = oi >= 0 && (idx < 0 || ov < v || (ov == v && oi < idx));
-        v = take ? ov : v;
-        idx = take ? oi : idx;
-    }
-    *best = v;
-    return idx;
-}
-
 // Per-warp shared state.
 struct WarpShared {
-    double vec[4][64];  // p-sized vectors: free solution, scratch
-    double tau[64];
-    double rvec[64];    // NNLS residual rows / rotated data of the small QR
-    double nrm_u[kMaxActive], nrm_d[kMaxActive];
-    int act[kMaxActive];   // active columns, increasing
-    int perm[kMaxActive];
+    double vec[4][64];  // p-sized vectors: unconstrained and free solutions, scratch
+    double tau[64];     // reflectors of the weighted design
+    double qtau[kMaxActive], qnu[kMaxActive], qnd[kMaxActive], rv[64], res[64];
+    int qperm[kMaxActive];
+    int act[kMaxActive];
     int n_act;
 };
-
-// Least squares on the active columns of c ((rows) x m, row-major) for the data e_{rows-1}:
-// column-pivoted Householder QR with threshold max(rows, k) eps (cpp/src/sd/nnls.cpp:119-139);
-// columns past the numerical rank get 0. Writes the coefficients of all m columns into z
-// (zero off the active set).
-__device__ void active_least_squares(const double* c, int rows, int m, double* sub, WarpShared& sh,
-                                     double* z, int lane) {
-    const int k = sh.n_act;
-    for (int j = lane; j < m; j += 32) z[j] = 0.0;
-    __syncwarp();
-    if (k == 0) return;
-    // sub (rows x kMaxActive) <- the active columns; column norms.
-    for (int q = lane; q < k; q += 32) {
-        const int col = sh.act[q];
-        double s = 0.0;
-        for (int r = 0; r < rows; ++r) {
-            const double x = c[size_t(r) * m + col];
-            sub[r * kMaxActive + q] = x;
-            s += x * x;
-        }
-        sh.nrm_u[q] = sh.nrm_d[q] = sqrt(s);
-        sh.perm[q] = q;
-    }
-    __syncwarp();
-    double biggest = 0.0;
-    for (int q = 0; q < k; ++q) biggest = fmax(biggest, sh.nrm_u[q]);
-    const double th = biggest * kEps;
-    const double small_sq = th * th / double(rows);
-    const int size = min(rows, k);
-    int nonzero = size;
-    double maxpivot = 0.0;
-    for (int kk = 0; kk < size; ++kk) {
-        // Pivot: the largest remaining norm, the first on a tie.
-        double v = -1.0;
-        int idx = -1;
-        for (int q = kk + lane; q < k; q += 32) {
-            const double sq = sh.nrm_u[q] * sh.nrm_u[q];
-            if (idx < 0 || sq > v) { v = sq; idx = q; }
-        }
-        const int best = warp_argmax_first(v, idx);
-        const double best_sq = sh.nrm_u[best] * sh.nrm_u[best];
-        if (nonzero == size && best_sq < small_sq * double(rows - kk)) nonzero = kk;
-        __syncwarp();
-        if (best != kk) {
-            for (int r = lane; r < rows; r += 32) {
-                const double t = sub[r * kMaxActive + kk];
-                sub[r * kMaxActive + kk] = sub[r * kMaxActive + best];
-                sub[r * kMaxActive + best] = t;
-            }
-            if (lane == 0) {
-                double t = sh.nrm_u[kk]; sh.nrm_u[kk] = sh.nrm_u[best]; sh.nrm_u[best] = t;
-                t = sh.nrm_d[kk]; sh.nrm_d[kk] = sh.nrm_d[best]; sh.nrm_d[best] = t;
-                const int pt = sh.perm[kk]; sh.perm[kk] = sh.perm[best]; sh.perm[best] = pt;
-            }
-        }
-        __syncwarp();
-        // Householder reflector of column kk, rows kk.. (LAPACK dlarfg convention).
-        const double c0 = sub[kk * kMaxActive + kk];
-        double tail = 0.0;
-        for (int r = kk + 1 + lane; r < rows; r += 32) tail += sub[r * kMaxActive + kk] * sub[r * kMaxActive + kk];
-        tail = wsum(tail);
-        double tau, beta;
-        if (tail <= DBL_MIN) {
-            tau = 0.0;
-            beta = c0;
-            for (int r = kk + 1 + lane; r < rows; r += 32) sub[r * kMaxActive + kk] = 0.0;
-        } else {
-            beta = sqrt(c0 * c0 + tail);
-            if (c0 >= 0.0) beta = -beta;
-            const double den = c0 - beta;
-            for (int r = kk + 1 + lane; r < rows; r += 32) sub[r * kMaxActive + kk] /= den;
-            tau = (beta - c0) / beta;
-        }
-        __syncwarp();
-        if (lane == 0) {
-            sub[kk * kMaxActive + kk] = beta;
-            sh.tau[kk] = tau;
-        }
-        maxpivot = fmax(maxpivot, fabs(beta));
-        __syncwarp();
-        // Apply to the remaining columns and downdate their norms; lanes over columns.
-        for (int q = kk + 1 + lane; q < k; q += 32) {
-            if (tau != 0.0) {
-                double dot = sub[kk * kMaxActive + q];
-                for (int r = kk + 1; r < rows; ++r) dot += sub[r * kMaxActive + kk] * sub[r * kMaxActive + q];
-                sub[kk * kMaxActive + q] -= tau * dot;
-                for (int r = kk + 1; r < rows; ++r) sub[r * kMaxActive + q] -= tau * sub[r * kMaxActive + kk] * dot;
-            }
-            double& u = sh.nrm_u[q];
-            if (u != 0.0) {
-                double t = fabs(sub[kk * kMaxActive + q]) / u;
-                t = fmax(0.0, (1.0 + t) * (1.0 - t));
-                const double ratio = u / sh.nrm_d[q];
-                if (t * ratio * ratio <= sqrt(kEps)) {
-                    double s = 0.0;
-                    for (int r = kk + 1; r < rows; ++r) s += sub[r * kMaxActive + q] * sub[r * kMaxActive + q];
-                    sh.nrm_d[q] = sqrt(s);
-                    u = sh.nrm_d[q];
-                } else {
-                    u *= sqrt(t);
-                }
-            }
-        }
-        __syncwarp();
-    }
-    const double thr = double(max(rows, k)) * kEps;
-    int rank = 0;
-    for (int i = 0; i < nonzero; ++i)
-        if (fabs(sub[i * kMaxActive + i]) > maxpivot * thr) ++rank;
-    // rotated = Q^T e_last with the first `rank` reflectors.
-    for (int r = lane; r < rows; r += 32) sh.rvec[r] = (r == rows - 1) ? 1.0 : 0.0;
-    __syncwarp();
-    for (int kk = 0; kk < rank; ++kk) {
-        const double tau = sh.tau[kk];
-        if (tau == 0.0) continue;
-        double dot = 0.0;
-        for (int r = kk + 1 + lane; r < rows; r += 32) dot += sub[r * kMaxActive + kk] * sh.rvec[r];
-        dot = wsum(dot) + sh.rvec[kk];
-        __syncwarp();
-        if (lane == 0) sh.rvec[kk] -= tau * dot;
-        for (int r = kk + 1 + lane; r < rows; r += 32) sh.rvec[r] -= tau * sub[r * kMaxActive + kk] * dot;
-        __syncwarp();
-    }
-    // R11 b = rotated[:rank], then scatter through the pivots.
-    if (lane == 0) {
-        for (int i = rank - 1; i >= 0; --i) {
-            double s = sh.rvec[i];
-            for (int j = i + 1; j < rank; ++j) s -= sub[i * kMaxActive + j] * sh.rvec[j];
-            sh.rvec[i] = s / sub[i * kMaxActive + i];
-        }
-    }
-    __syncwarp();
-    for (int i = lane; i < rank; i += 32) z[sh.act[sh.perm[i]]] = sh.rvec[i];
-    __syncwarp();
-}
 
 template <class Src>
 __global__ void __launch_bounds__(kCWarps * 32) constrained_fit_kernel(
@@ -224,11 +61,12 @@ __global__ void __launch_bounds__(kCWarps * 32) constrained_fit_kernel(
     double* slot = workspace + (size_t(blockIdx.x) * kCWarps + warp) * slot_doubles;
     double* qr = slot;                          // (n, p) row-major
     double* cm = qr + size_t(n) * p;            // (rows, m) row-major
-    double* sub = cm + size_t(rows) * m;        // (rows, kMaxActive)
+    double* sub = cm + size_t(rows) * m;        // (kMaxActive, rows) QR of the active columns
     double* u = sub + size_t(rows) * kMaxActive;  // (m,)
     double* z = u + m;                          // (m,)
-    double* ys = z + m;                         // (n,) log signals, then root weights after
-    double* rw = ys + n;                        // (n,) root weights; also the rotated data
+    double* ys = z + m;                         // (n,) log signals, then weighted
+    double* rw = ys + n;                        // (n,) root weights
+    uint8_t* flag = reinterpret_cast<uint8_t*>(rw + n);  // (m,) active flags
     const int total = min(*list.count, list.capacity);
     for (;;) {
         int idx = 0;
@@ -339,101 +177,18 @@ __global__ void __launch_bounds__(kCWarps * 32) constrained_fit_kernel(
         }
         colsum_max = wmax(colsum_max);
         const double tol = 10.0 * kEps * colsum_max * double(max(rows, m));
-        if (lane == 0) sh.n_act = 0;
-        __syncwarp();
         // Lawson-Hanson (cpp/src/sd/nnls.cpp:187-221) on C u ~ e_p.
-        const int max_inner = kInnerStepsPerConstraint * m;
-        int inner = 0;
-        bool converged = true, overflow = false;
+        double* unit = sh.rv;  // e_p, then the residual rows below
+        for (int r = lane; r < rows; r += 32) unit[r] = (r == p) ? 1.0 : 0.0;
+        __syncwarp();
+        double* unit_copy = sh.vec[2];
+        for (int r = lane; r < rows; r += 32) unit_copy[r] = unit[r];
+        __syncwarp();
+        NnlsScratch ns{u, z, flag, sh.act, &sh.n_act, sh.res,
+                       QrScratch{sub, sh.qtau, sh.qnu, sh.qnd, sh.qperm, sh.rv}, kMaxActive};
+        const int outcome = warp_nnls_explicit(cm, rows, m, unit_copy, tol, kInnerStepsPerConstraint * m, ns, lane);
+        if (outcome != 1) continue;
         double* res = sh.vec[2];
-        for (;;) {
-            // r = e_p - C u over the active columns (u is zero elsewhere); lane = row.
-            if (lane < rows) {
-                double s = (lane == p) ? 1.0 : 0.0;
-                for (int q = 0; q < sh.n_act; ++q) {
-                    const int col = sh.act[q];
-                    s -= cm[size_t(lane) * m + col] * u[col];
-                }
-                res[lane] = s;
-            }
-            __syncwarp();
-            // The steepest inactive gradient C^T r, the first on a tie.
-            double bestv = 0.0;
-            int besti = -1;
-            for (int c = lane; c < m; c += 32) {
-                bool active = false;
-                for (int q = 0; q < sh.n_act; ++q) active |= (sh.act[q] == c);
-                if (active) continue;
-                double gval = 0.0;
-                for (int i = 0; i < rows; ++i) gval += cm[size_t(i) * m + c] * res[i];
-                if (besti < 0 || gval > bestv) { bestv = gval; besti = c; }
-            }
-            const int e = warp_argmax_first(bestv, besti);
-            double ge = __shfl_sync(0xffffffffu, bestv, 0);
-            {
-                // The value of the winner: recompute on every lane (uniform).
-                double gval = 0.0;
-                if (e >= 0)
-                    for (int i = 0; i < rows; ++i) gval += cm[size_t(i) * m + e] * res[i];
-                ge = gval;
-            }
-            if (e < 0 || ge <= tol) break;
-            if (sh.n_act >= kMaxActive) { overflow = true; break; }
-            // Insert e keeping the list increasing.
-            if (lane == 0) {
-                int q = sh.n_act;
-                while (q > 0 && sh.act[q - 1] > e) { sh.act[q] = sh.act[q - 1]; --q; }
-                sh.act[q] = e;
-                ++sh.n_act;
-            }
-            __syncwarp();
-            active_least_squares(cm, rows, m, sub, sh, z, lane);
-            for (;;) {
-                bool any = false;
-                for (int q = lane; q < sh.n_act; q += 32) any |= z[sh.act[q]] <= 0.0;
-                if (!__any_sync(0xffffffffu, any)) break;
-                if (++inner > max_inner) { converged = false; break; }
-                // Blocking step: the smallest u/(u - z) over active columns with z <= 0.
-                double sv = INFINITY;
-                int si = -1;
-                for (int q = lane; q < sh.n_act; q += 32) {
-                    const int col = sh.act[q];
-                    if (z[col] > 0.0) continue;
-                    const double dist = u[col] - z[col];
-                    const double st = dist > 0.0 ? u[col] / dist : 0.0;
-                    if (si < 0 || st < sv || (st == sv && col < si)) { sv = st; si = col; }
-                }
-                double step;
-                const int bcol = warp_argmin_first(sv, si, &step);
-                step = __shfl_sync(0xffffffffu, step, 0);
-                for (int q = lane; q < sh.n_act; q += 32) {
-                    const int col = sh.act[q];
-                    u[col] += step * (z[col] - u[col]);
-                }
-                __syncwarp();
-                if (lane == 0) {
-                    u[bcol] = 0.0;
-                    // Drop the blocking column and any whose coefficient rounding left below tol.
-                    int w = 0;
-                    for (int q = 0; q < sh.n_act; ++q) {
-                        const int col = sh.act[q];
-                        if (col == bcol || !(fabs(u[col]) >= tol)) {
-                            if (col != bcol) { /* stays at its value, inactive */ }
-                            continue;
-                        }
-                        sh.act[w++] = col;
-                    }
-                    sh.n_act = w;
-                }
-                __syncwarp();
-                active_least_squares(cm, rows, m, sub, sh, z, lane);
-            }
-            if (!converged) break;
-            // u = z (zero off the active set).
-            for (int c = lane; c < m; c += 32) u[c] = z[c];
-            __syncwarp();
-        }
-        if (!converged || overflow) continue;
         // Residual C u - e_p over all columns with non-zero u.
         if (lane < rows) {
             double s = (lane == p) ? -1.0 : 0.0;

@@ -1,0 +1,7 @@
+"""Spherical deconvolution on the GPU: MSMT-CSD (and mFOD), with the API of larmor.sd."""
+
+from larmor_b200.sd.model import SDFit
+from larmor_b200.sd.msmt_csd import MSMTCSDModel
+from larmor_b200.sd.rf import AnisotropicRF, IsotropicRF, ZonalSHRF
+
+__all__ = ["AnisotropicRF", "IsotropicRF", "MSMTCSDModel", "SDFit", "ZonalSHRF"]

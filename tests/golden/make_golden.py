@@ -25,7 +25,8 @@ What the fixtures hold, all from the reference's own code and data:
 - msmt.npz: the forward and constraint matrices and ridge of MSMT-CSD (sd/msmt.py) for the
   responses of tests/data/msmt on a seeded three-shell table, as tests/sd/test_msmt.py builds them.
 - dirs300.npy: the reference's 300 FOD directions (src/larmor/data/dir300.txt), a table the
-  SD models must share exactly.
+  SD models must share exactly; also written to larmor_b200/data/dirs300.npy, where the
+  package reads it.
 """
 
 from __future__ import annotations
@@ -226,6 +227,8 @@ def main(reference: Path) -> None:
         wm_coefficients=rfs_msmt[0].coefficients, gm_coefficients=rfs_msmt[1].coefficients,
         csf_coefficients=rfs_msmt[2].coefficients)
     np.save(OUT / "dirs300.npy", np.asarray(DIRS_300, dtype=np.float64))
+    # The same table ships with the package: the SD models' FOD directions.
+    np.save(OUT.parents[1] / "larmor_b200" / "data" / "dirs300.npy", np.asarray(DIRS_300, dtype=np.float64))
     shutil.rmtree(tmp)
     print("wrote", sorted(p.name for p in OUT.glob("*.np*")))
 
