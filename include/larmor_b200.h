@@ -21,6 +21,11 @@
  *                                            (src/larmor/dwi/dki.py:243-282, :285-540)
  *   lar_lsi_design_*, lar_fit_lsi            larmor._core.LsiDesign, larmor._core.fit_lsi
  *                                            (cpp/src/python/sd.cpp:361-392, cpp/src/sd/lsi.cpp)
+ *   lar_l2nnls_create, lar_fod_solver_*      larmor._core.FodSolver.l2nnls (cpp/src/python/sd.cpp:89)
+ *   lar_deconv_kernel_*                      larmor._core.DeconvKernel (cpp/src/python/sd.cpp:260)
+ *   lar_fit_multi_tissue                     larmor._core.fit_multi_tissue (cpp/src/python/sd.cpp:310,
+ *                                            cpp/src/sd/multi_tissue.cpp:76-148)
+ *   lar_fit_single_tissue                    larmor._core.fit_single_tissue (cpp/src/sd/solver.cpp:422)
  */
 #ifndef LARMOR_B200_H
 #define LARMOR_B200_H
@@ -126,6 +131,47 @@ int lar_lsi_design_matrices(lar_lsi_design design, double* q_t, double* back, do
  * Replaces larmor._core.fit_lsi (cpp/src/python/sd.cpp:370-392). */
 int lar_fit_lsi(lar_lsi_design design, const double* signals, int64_t v, int only_qr, double* x,
                 uint8_t* converged, uint8_t* status, int32_t* outer, uint8_t* active, void* stream);
+
+/* ---- Multi-tissue spherical deconvolution (SDModel, method mFOD) ---------------------- */
+
+typedef struct lar_fod_solver_s* lar_fod_solver;
+typedef struct lar_deconv_kernel_s* lar_deconv_kernel;
+
+/* Prepares the ridge-penalised NNLS min ||k f - s||^2 + reg^2 ||f||^2 over f >= 0 for the
+ * weighted anisotropic kernel k (m, c) (host): its Gram k^T k + reg^2 I and whether the fits
+ * use the normal equations (reg = 0, or a condition bound (||k||_F^2 + reg^2) / reg^2 <= 1e8;
+ * otherwise QR). A coefficient enters only when its gradient exceeds tol_x. Fails with
+ * LAR_ERR_INVALID for reg < 0 or tol_x <= 0. Replaces FodSolver.l2nnls
+ * (cpp/src/python/sd.cpp:89-102, cpp/src/sd/nnls.cpp:348-360). */
+int lar_l2nnls_create(const double* k, int64_t m, int64_t c, double reg, double tol_x, lar_fod_solver* out);
+void lar_fod_solver_destroy(lar_fod_solver solver);
+
+/* One resolution of a multi-tissue kernel (host arrays): k_aniso (m, ca), k_iso and w_k_iso
+ * (m, ci), and the (start, stop) columns of each anisotropic response, blocks (nb, 2). Fails
+ * with LAR_ERR_INVALID for an empty block or one outside 0..ca. Replaces DeconvKernel
+ * (cpp/src/python/sd.cpp:260-292). */
+int lar_deconv_kernel_create(const double* k_aniso, int64_t m, int64_t ca, const double* k_iso,
+                             const double* w_k_iso, int64_t ci, const int64_t* blocks, int64_t nb,
+                             lar_deconv_kernel* out);
+void lar_deconv_kernel_destroy(lar_deconv_kernel kernel);
+
+/* Fits the FODs and tissue fractions of every row of signals (v, m) (device double, normalised
+ * by S0): up to max_outer rounds of a low-resolution FOD fit and a fraction fit, until no
+ * fraction changes by fraction_tol, then the high-resolution FOD and the final fractions (NNLS
+ * tolerance final_tol_x), normalised to sum to 1. weights (m,) (host) are the shell weights of
+ * the FOD fits. Writes fods (v, ca_hr) and fractions (v, nb_hr + ci) (device double); rounds
+ * (v,) int32 and status (v,) uint8 (1 where an active set outgrew the QR workspace) may be
+ * NULL. Waits for its stream. Calls sharing hr_solver must not overlap on the GPU.
+ * Replaces larmor._core.fit_multi_tissue (cpp/src/python/sd.cpp:310-358). */
+int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights, lar_deconv_kernel lr,
+                         lar_fod_solver lr_solver, lar_deconv_kernel hr, lar_fod_solver hr_solver,
+                         int64_t max_outer, double fraction_tol, double final_tol_x, double* fods,
+                         double* fractions, int32_t* rounds, uint8_t* status, void* stream);
+
+/* The FOD (v, c) of every row of signals (v, m) (device double) with one L2NNLS solver.
+ * Replaces larmor._core.fit_single_tissue (cpp/src/python/sd.cpp, cpp/src/sd/solver.cpp:422). */
+int lar_fit_single_tissue(const double* signals, int64_t v, lar_fod_solver solver, double* fods,
+                          uint8_t* status, void* stream);
 
 /* ---- A fit that allocates no device memory ------------------------------------------- */
 

@@ -264,3 +264,149 @@ def fit_lsi_device(design: LsiDesign, signals, x, converged, status=None, outer=
     _lib.check(_lib.lib().lar_fit_lsi(
         design.handle, _lib.ptr(signals), signals.shape[0], int(only_qr), _lib.ptr(x), _lib.ptr(converged),
         _lib.ptr(status), _lib.ptr(outer), _lib.ptr(active), _stream(torch)))
+
+
+class _Handle:
+    """Owns a C-ABI handle and destroys it with the given function."""
+
+    _destroy = ""
+
+    def __init__(self) -> None:
+        self._handle = ctypes.c_void_p()
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._handle
+
+    def __del__(self) -> None:
+        handle = getattr(self, "_handle", None)
+        if handle is not None and handle.value:
+            try:
+                getattr(_lib.lib(), self._destroy)(handle)
+            except Exception:
+                pass
+
+
+class FodSolver(_Handle):
+    """An FOD solver with the matrices it needs from one kernel, copied to the device
+    (cpp/src/python/sd.cpp:399-438). Only the L2NNLS method (mFOD's) is part of this package."""
+
+    _destroy = "lar_fod_solver_destroy"
+
+    @staticmethod
+    def l2nnls(k, reg, tol_x) -> "FodSolver":
+        """Non-negative least squares with a ridge penalty: each voxel's FOD f minimises
+        ||k f - s||^2 + reg^2 ||f||^2 with f >= 0; a coefficient enters only when its gradient
+        exceeds tol_x.
+
+        Raises:
+            TypeError: If k is not a float64 numpy array.
+            ValueError: If reg is negative or tol_x is not positive.
+        """
+        k = _array(k, "k", 2)
+        if not reg >= 0.0:
+            raise ValueError("reg must be at least 0")
+        if not tol_x > 0.0:
+            raise ValueError("tol_x must be positive")
+        solver = FodSolver()
+        solver.n_meas, solver.n_dirs = k.shape
+        _lib.check(_lib.lib().lar_l2nnls_create(_lib.ptr(k), k.shape[0], k.shape[1], float(reg), float(tol_x),
+                                                ctypes.byref(solver._handle)))
+        return solver
+
+    @staticmethod
+    def drl(*_args, **_kwargs):
+        raise NotImplementedError("the damped Richardson-Lucy solver (GRL) is not part of larmor_b200")
+
+    @staticmethod
+    def lasso(*_args, **_kwargs):
+        raise NotImplementedError("the elastic-net solver is not part of larmor_b200")
+
+    @property
+    def n_unconverged(self) -> int:
+        return 0
+
+
+class DeconvKernel(_Handle):
+    """One resolution of a multi-tissue kernel, copied to the device
+    (cpp/src/python/sd.cpp:260-292)."""
+
+    _destroy = "lar_deconv_kernel_destroy"
+
+    def __init__(self, k_aniso, k_iso, w_k_iso, aniso_blocks) -> None:
+        super().__init__()
+        k_aniso = _array(k_aniso, "k_aniso", 2)
+        m, ca = k_aniso.shape
+        if k_iso is None:
+            k_iso = np.zeros((m, 0))
+            w_k_iso = np.zeros((m, 0))
+        k_iso = _array(k_iso, "k_iso", 2)
+        w_k_iso = _array(w_k_iso, "w_k_iso", 2)
+        if k_iso.shape[0] != m or w_k_iso.shape != k_iso.shape:
+            raise ValueError(f"k_aniso {k_aniso.shape}, k_iso {k_iso.shape} and w_k_iso {w_k_iso.shape} "
+                             "do not match")
+        blocks = np.ascontiguousarray(np.array(list(aniso_blocks), dtype=np.int64).reshape(-1, 2))
+        self.m, self.ca, self.ci, self.nb = m, ca, k_iso.shape[1], len(blocks)
+        _lib.check(_lib.lib().lar_deconv_kernel_create(
+            _lib.ptr(k_aniso), m, ca, _lib.ptr(k_iso if k_iso.size else None),
+            _lib.ptr(w_k_iso if w_k_iso.size else None), k_iso.shape[1], _lib.ptr(blocks), len(blocks),
+            ctypes.byref(self._handle)))
+
+
+def fit_multi_tissue(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol, final_tol_x,
+                     n_threads):
+    """Fits the FODs and tissue fractions of every row of signals (n, m); the shell weights
+    (m,) apply to the FOD fits only. Returns the high-resolution FODs (n, ca_hr) and the
+    fractions (n, n_aniso_rfs + ci), summing to 1 (cpp/src/python/sd.cpp:310-358).
+
+    Raises:
+        TypeError: If signals or weights is not float64.
+        ValueError: If signals is not C-contiguous, the shapes do not match, a solver does not
+            match its kernel, or n_threads is 0.
+    """
+    signals = _array(signals, "signals", 2)
+    weights = _array(weights, "weights", 1)
+    if signals.shape[1] != hr.m or weights.shape[0] != hr.m or lr.m != hr.m:
+        raise ValueError(f"signals {signals.shape}, weights {weights.shape[0]} and the kernels' {hr.m} "
+                         "measurements do not match")
+    _require_threads(n_threads)
+    if max_outer < 0:
+        raise ValueError("max_outer must be at least 0")
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    v = signals.shape[0]
+    fods = torch.empty((v, hr.ca), dtype=torch.float64, device=dev)
+    fractions = torch.empty((v, hr.nb + hr.ci), dtype=torch.float64, device=dev)
+    if v:
+        s = torch.from_numpy(signals).to(dev)
+        fit_multi_tissue_device(s, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol, final_tol_x,
+                                fods, fractions)
+    return fods.cpu().numpy(), fractions.cpu().numpy()
+
+
+def fit_multi_tissue_device(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol,
+                            final_tol_x, fods, fractions, rounds=None, status=None) -> None:
+    """The device-resident fit_multi_tissue (torch CUDA tensors; weights a host array)."""
+    torch = _torch()
+    weights = np.ascontiguousarray(weights, dtype=np.float64)
+    _lib.check(_lib.lib().lar_fit_multi_tissue(
+        _lib.ptr(signals), signals.shape[0], _lib.ptr(weights), lr.handle, lr_solver.handle, hr.handle,
+        hr_solver.handle, int(max_outer), float(fraction_tol), float(final_tol_x), _lib.ptr(fods),
+        _lib.ptr(fractions), _lib.ptr(rounds), _lib.ptr(status), _stream(torch)))
+
+
+def fit_single_tissue(signals, solver: FodSolver, n_threads):
+    """The FOD (n, c) of every row of signals (n, m) with one solver."""
+    signals = _array(signals, "signals", 2)
+    if signals.shape[1] != solver.n_meas:
+        raise ValueError(f"signals {signals.shape} do not have the solver's {solver.n_meas} measurements")
+    _require_threads(n_threads)
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    v = signals.shape[0]
+    fods = torch.empty((v, solver.n_dirs), dtype=torch.float64, device=dev)
+    if v:
+        s = torch.from_numpy(signals).to(dev)
+        _lib.check(_lib.lib().lar_fit_single_tissue(_lib.ptr(s), v, solver.handle, _lib.ptr(fods), None,
+                                                    _stream(torch)))
+    return fods.cpu().numpy()

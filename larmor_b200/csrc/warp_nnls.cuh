@@ -59,17 +59,25 @@ struct QrScratch {
     double* rv;    // (rows,) rotated data, then the solution
 };
 
-// Least squares of d (rows) on the columns act[0..k) of c (rows x ldc, row-major): writes the
-// coefficients of those columns into z (indexed by column; other entries untouched).
-__device__ inline void warp_qr_least_squares(const double* __restrict__ c, int rows, int ldc,
-                                             const int* act, int k, const double* d, QrScratch s,
-                                             double* z, int lane) {
+// Column loader of a row-major matrix: entry (r, col).
+struct RowMajorColumns {
+    const double* c;
+    int ldc;
+    __device__ __forceinline__ double operator()(int r, int col, int /*q*/) const { return c[size_t(r) * ldc + col]; }
+};
+
+// Least squares of d (rows) on the columns act[0..k) of a matrix whose entry (r, act[q]) the
+// loader gives: writes the coefficients of those columns into z (indexed by column; other
+// entries untouched).
+template <class Columns>
+__device__ inline void warp_qr_least_squares_cols(const Columns& cols, int rows, const int* act, int k,
+                                                  const double* d, QrScratch s, double* z, int lane) {
     if (k == 0) return;
     for (int q = 0; q < k; ++q) {
         const int col = act[q];
         double sq = 0.0;
         for (int r = lane; r < rows; r += 32) {
-            const double x = c[size_t(r) * ldc + col];
+            const double x = cols(r, col, q);
             s.sub[size_t(q) * rows + r] = x;
             sq += x * x;
         }
@@ -193,6 +201,13 @@ __device__ inline void warp_qr_least_squares(const double* __restrict__ c, int r
     for (int i = lane; i < rank; i += 32) z[act[s.perm[i]]] = s.rv[i];
     for (int i = rank + lane; i < k; i += 32) z[act[s.perm[i]]] = 0.0;
     __syncwarp();
+}
+
+// Least squares of d on the columns act[0..k) of c (rows x ldc, row-major).
+__device__ inline void warp_qr_least_squares(const double* __restrict__ c, int rows, int ldc,
+                                             const int* act, int k, const double* d, QrScratch s,
+                                             double* z, int lane) {
+    warp_qr_least_squares_cols(RowMajorColumns{c, ldc}, rows, act, k, d, s, z, lane);
 }
 
 // Workspace of warp_nnls_explicit for an m-column problem with at most `acap` active columns.

@@ -1,7 +1,9 @@
 """Spherical deconvolution on the GPU: MSMT-CSD (and mFOD), with the API of larmor.sd."""
 
-from larmor_b200.sd.model import SDFit
+from larmor_b200.sd.method import SDMethod
+from larmor_b200.sd.model import SDFit, SDModel
+from larmor_b200.sd.solvers import L2NNLS
 from larmor_b200.sd.msmt_csd import MSMTCSDModel
 from larmor_b200.sd.rf import AnisotropicRF, IsotropicRF, ZonalSHRF
 
-__all__ = ["AnisotropicRF", "IsotropicRF", "MSMTCSDModel", "SDFit", "ZonalSHRF"]
+__all__ = ["AnisotropicRF", "IsotropicRF", "L2NNLS", "MSMTCSDModel", "SDFit", "SDMethod", "SDModel", "ZonalSHRF"]

@@ -18,3 +18,146 @@ class SDFit:
     basis: str
     lmax: int
     peak_relative_threshold: float = 0.1
+
+
+# ---- SDModel ---------------------------------------------------------------------------
+
+from larmor_b200._log import LarmorLogger  # noqa: E402
+from larmor_b200._threads import n_threads  # noqa: E402
+from larmor_b200.dwi.inputs import as_mask, check_dwi, estimate_s0, masked_signals  # noqa: E402
+from larmor_b200.dwi.mask import unmask  # noqa: E402
+from larmor_b200.sd.kernel import Kernel, order_rfs  # noqa: E402
+from larmor_b200.sd.rf import IsotropicRF  # noqa: E402
+from larmor_b200.sd.sh import BASES, fit_sh  # noqa: E402
+from larmor_b200.sd.sphere import DIRS_300, get_dirs  # noqa: E402
+
+SHELL_TOLERANCE = 100.0
+# The relative peak threshold of SDModel's FODs (their truncation leaves side lobes).
+SD_MODEL_PEAK_RELATIVE_THRESHOLD = 0.2
+
+
+def shell_mask(bvals: np.ndarray, shell: float, *, tol: float = SHELL_TOLERANCE) -> np.ndarray:
+    return np.abs(bvals - shell) < tol
+
+
+def compute_max_lmax(bvals: np.ndarray, proposed_lmax: int) -> int:
+    """The largest even lmax <= proposed whose coefficients the highest shell's directions
+    can determine (src/larmor/sd/model.py:443-468)."""
+    n_dirs = np.sum(shell_mask(bvals, np.max(bvals)))
+    lmax = proposed_lmax
+    while lmax > 0:
+        if n_dirs >= (lmax + 1) * (lmax + 2) // 2:
+            return lmax
+        lmax -= 2
+    raise ValueError(f"Not enough gradient directions ({n_dirs}) to fit even lmax=2.")
+
+
+def compute_shell_weights(bvals: np.ndarray, inner_weight: float = 0.2) -> np.ndarray:
+    weights = np.full(bvals.shape, inner_weight, dtype=np.float64)
+    weights[shell_mask(bvals, np.max(bvals))] = 1.0
+    return weights
+
+
+def low_resolution_dirs(rfs, n_meas: int) -> list[np.ndarray]:
+    """Each anisotropic response's coarse directions: the spiral of min(n_meas, its count)
+    points without its last, which repeats the first (src/larmor/sd/model.py:394-409)."""
+    return [get_dirs(min(n_meas, rf.low_resolution_dirs))[:-1] for rf in rfs if not isinstance(rf, IsotropicRF)]
+
+
+def to_sh(fods: np.ndarray, lmax: int, basis: str, *, exact_integral: bool = False) -> np.ndarray:
+    """Amplitudes on DIRS_300 to SH coefficients, times 300 / (4 pi); with exact_integral c00 is
+    the amplitudes' sum / sqrt(4 pi) (src/larmor/sd/model.py:412-440)."""
+    density = len(DIRS_300) / (4.0 * np.pi)
+    coeffs = fit_sh(fods, DIRS_300, lmax, basis=basis) * density
+    if exact_integral:
+        coeffs[:, 0] = fods.sum(axis=1) / np.sqrt(4.0 * np.pi)
+    return coeffs
+
+
+class SDModel:
+    """Spherical deconvolution with the mFOD method (L2NNLS FODs, one per anisotropic response,
+    all shells weighted equally), on the GPU; the reference's SDModel (src/larmor/sd/model.py:84).
+    GRL (damped Richardson-Lucy) is outside this package."""
+
+    def __init__(self, rfs, *, method="mFOD", solver=None, inner_shell_weight=None, lmax: int = 8,
+                 basis: str = "tournier", progress: bool = False) -> None:
+        from larmor_b200.sd.method import SDMethod
+
+        if basis not in BASES:
+            raise ValueError(f"Invalid basis {basis}, expected one of {', '.join(BASES)}")
+        if lmax < 2 or lmax % 2 != 0:
+            raise ValueError(f"lmax must be even and at least 2, got {lmax}")
+        if inner_shell_weight is not None and not 0 < inner_shell_weight <= 1:
+            raise ValueError(f"inner_shell_weight must be in (0, 1], got {inner_shell_weight}")
+        self.rfs = order_rfs(rfs)
+        self.method = SDMethod(method)
+        self.method._check_rfs(self.rfs)
+        self.solver = solver
+        self.inner_shell_weight = self.method.inner_shell_weight if inner_shell_weight is None else inner_shell_weight
+        self.lmax = lmax
+        self.basis = basis
+        self.num_iso = sum(1 for rf in self.rfs if isinstance(rf, IsotropicRF))
+        self.is_multi_tissue = self.num_iso > 0 or len(self.rfs) - self.num_iso > 1
+        self.progress = progress
+
+    def fit(self, volume, gtab, mask=None, *, n_jobs: int = -1) -> SDFit:
+        """The FODs (SH coefficients in the model's basis) and fractions of every voxel of the
+        mask (every voxel when None); see src/larmor/sd/model.py:171-260."""
+        from larmor_b200.sd.solvers import L2NNLS
+
+        solver = self.solver if self.solver is not None else self.method.default_solver()
+        if not isinstance(solver, L2NNLS):
+            raise NotImplementedError("larmor_b200 runs the L2NNLS solver only")
+        threads = n_threads(n_jobs)
+        check_dwi(volume, gtab)
+        lmax = compute_max_lmax(gtab.bvals, self.lmax)
+        if lmax < self.lmax:
+            LarmorLogger.warning(f"lmax {self.lmax} needs more directions than the highest shell has, "
+                                 f"lowering to {lmax}")
+        mask = np.ones(volume.data.shape[:-1], dtype=bool) if mask is None else as_mask(volume, mask)
+        s0 = estimate_s0(volume, gtab, mask)[mask]
+        voxels = np.nonzero(mask)
+        signals = masked_signals(volume, voxels).astype(np.float64)
+        normalised = signals / s0[:, np.newaxis]
+        finite = np.isfinite(normalised).all(axis=1)
+        if not finite.all():
+            LarmorLogger.warning(f"{int((~finite).sum())} voxels have a NaN or infinite signal or no S0; "
+                                 "their FODs and fractions are NaN.")
+        # Diffusion weighting only lowers the signal: a value above S0 is noise.
+        normalised = np.minimum(normalised[finite], 1.0)
+        amplitudes, fitted_fractions, hr = self._fit_normalised(normalised, gtab, solver, threads)
+        n_coeffs = (lmax + 1) * (lmax + 2) // 2
+        fods = []
+        for block in hr.aniso_blocks:
+            sh = np.full((len(finite), n_coeffs), np.nan)
+            sh[finite] = to_sh(amplitudes[:, block], lmax, self.basis, exact_integral=True)
+            fods.append(unmask(sh, mask))
+        fractions = None
+        if fitted_fractions is not None:
+            fr = np.full((len(finite), fitted_fractions.shape[1]), np.nan)
+            fr[finite] = fitted_fractions
+            fractions = unmask(fr, mask)
+        return SDFit(fods=fods, tissue_fractions=fractions, basis=self.basis, lmax=lmax,
+                     peak_relative_threshold=SD_MODEL_PEAK_RELATIVE_THRESHOLD)
+
+    def _prepare(self, solver, bvals, bvecs):
+        """The kernels and solvers of the fit (src/larmor/sd/model.py:272-321)."""
+        from larmor_b200.sd.solvers import Stage
+
+        if not self.is_multi_tissue:
+            kernel = Kernel(self.rfs, bvals, bvecs, dirs=DIRS_300)
+            return kernel, None, solver._prepare(kernel, bvals, Stage.SINGLE), None
+        weights = compute_shell_weights(bvals, self.inner_shell_weight)
+        hr = Kernel(self.rfs, bvals, bvecs, dirs=DIRS_300, weights=weights)
+        lr = Kernel(self.rfs, bvals, bvecs, dirs=low_resolution_dirs(self.rfs, len(bvals)), weights=weights)
+        return hr, lr, solver._prepare(hr, bvals, Stage.HIGH_RES), solver._prepare(lr, bvals, Stage.LOW_RES)
+
+    def _fit_normalised(self, signals, gtab, solver, threads):
+        from larmor_b200.sd.solvers import fit_multi_tissue, fit_single_tissue
+
+        hr, lr, hr_solver, lr_solver = self._prepare(solver, gtab.bvals, gtab.bvecs)
+        if lr is None:
+            return fit_single_tissue(signals, hr_solver, threads), None, hr
+        fods, fractions = fit_multi_tissue(signals, lr, hr, lr_solver, hr_solver, threads,
+                                           fraction_tol=self.method._fraction_tolerance)
+        return fods, fractions, hr

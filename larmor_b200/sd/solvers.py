@@ -1,0 +1,68 @@
+"""The L2NNLS FOD solver and the multi-tissue fit (src/larmor/sd/solvers.py), on the GPU."""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+from enum import Enum, auto
+from math import isfinite
+
+import numpy as np
+
+from larmor_b200 import _core
+from larmor_b200.sd.kernel import Kernel
+
+# Maximum number of rounds of the multi-tissue loop.
+MAX_ROUNDS = 50
+# Default change in every fraction below which a voxel leaves the loop.
+FRACTION_TOL = 1e-3
+# In the final fraction fit, a tissue worth less than about this share of the signal gets 0.
+FINAL_FRACTION_TOL_X = 1e-2
+
+
+class Stage(Enum):
+    SINGLE = auto()
+    LOW_RES = auto()
+    HIGH_RES = auto()
+
+
+@dataclass(frozen=True, kw_only=True)
+class L2NNLS:
+    """NNLS with a ridge penalty reg (0 = plain NNLS), the mFOD method's solver; the loop's
+    low-resolution solves use reg 0 (src/larmor/sd/solvers.py:151-210)."""
+
+    reg: float = 0.1
+    tol_x: float = 1e-6
+
+    def __post_init__(self) -> None:
+        if not isfinite(self.reg) or self.reg < 0:
+            raise ValueError(f"reg must be a finite number >= 0, got {self.reg}")
+        if not self.tol_x > 0:
+            raise ValueError(f"tol_x must be positive, got {self.tol_x}")
+
+    def _prepare(self, kernel: Kernel, bvals: np.ndarray, stage: Stage) -> _core.FodSolver:
+        reg = 0.0 if stage is Stage.LOW_RES else self.reg
+        return _core.FodSolver.l2nnls(np.ascontiguousarray(kernel.w_k_aniso), reg, self.tol_x)
+
+
+def _deconv_kernel(kernel: Kernel) -> _core.DeconvKernel:
+    return _core.DeconvKernel(
+        np.ascontiguousarray(kernel.k_aniso),
+        None if kernel.k_iso is None else np.ascontiguousarray(kernel.k_iso),
+        None if kernel.w_k_iso is None else np.ascontiguousarray(kernel.w_k_iso),
+        [(b.start, b.stop) for b in kernel.aniso_blocks],
+    )
+
+
+def fit_single_tissue(signals, solver, n_threads):
+    return _core.fit_single_tissue(np.ascontiguousarray(signals, dtype=np.float64), solver, n_threads=n_threads)
+
+
+def fit_multi_tissue(signals, lr_kernel: Kernel, hr_kernel: Kernel, lr_solver, hr_solver, n_threads: int = 1,
+                     fraction_tol: float = FRACTION_TOL):
+    """The high-resolution FOD amplitudes (n, ca_hr) and the fractions (n, n_rfs)
+    (src/larmor/sd/solvers.py:329-373)."""
+    return _core.fit_multi_tissue(
+        np.ascontiguousarray(signals, dtype=np.float64),
+        np.ascontiguousarray(lr_kernel.weights, dtype=np.float64),
+        _deconv_kernel(lr_kernel), lr_solver, _deconv_kernel(hr_kernel), hr_solver,
+        max_outer=MAX_ROUNDS, fraction_tol=fraction_tol, final_tol_x=FINAL_FRACTION_TOL_X, n_threads=n_threads)

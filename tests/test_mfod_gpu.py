@@ -1,0 +1,98 @@
+"""The mFOD multi-tissue fit on the GPU against the oracle and MRIToolkit's MATLAB output
+(tests/sd/test_matlab_match.py:143-165), and the single-tissue L2NNLS fit."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from test_oracle import mfod_inputs
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu_fit(z, signals, rounds=False):
+    import torch
+
+    from larmor_b200 import _core
+
+    lr = _core.DeconvKernel(np.ascontiguousarray(z["lr_k_aniso"]), np.ascontiguousarray(z["lr_k_iso"]),
+                            np.ascontiguousarray(z["lr_w_k_iso"]), [(0, z["lr_k_aniso"].shape[1])])
+    hr = _core.DeconvKernel(np.ascontiguousarray(z["hr_k_aniso"]), np.ascontiguousarray(z["hr_k_iso"]),
+                            np.ascontiguousarray(z["hr_w_k_iso"]), [tuple(b) for b in z["hr_blocks"]])
+    lr_solver = _core.FodSolver.l2nnls(np.ascontiguousarray(z["lr_w_k_aniso"]), 0.0, 1e-6)
+    hr_solver = _core.FodSolver.l2nnls(np.ascontiguousarray(z["hr_w_k_aniso"]), 0.1, 1e-6)
+    dev = torch.device("cuda")
+    v = len(signals)
+    s = torch.from_numpy(np.ascontiguousarray(signals)).to(dev)
+    fods = torch.empty((v, hr.ca), dtype=torch.float64, device=dev)
+    fr = torch.empty((v, hr.nb + hr.ci), dtype=torch.float64, device=dev)
+    rd = torch.empty((v,), dtype=torch.int32, device=dev)
+    st = torch.empty((v,), dtype=torch.uint8, device=dev)
+    _core.fit_multi_tissue_device(s, z["weights"], lr, lr_solver, hr, hr_solver, 50, 1e-7, 1e-2, fods, fr, rd, st)
+    return fods.cpu().numpy(), fr.cpu().numpy(), rd.cpu().numpy(), st.cpu().numpy()
+
+
+def test_multi_tissue_matches_the_oracle(cuda, oracle, mfod_fixture):
+    signals, lr, hr = mfod_inputs(mfod_fixture)
+    fods, fractions, rounds, status = _gpu_fit(mfod_fixture, signals)
+    rfods, rfr, rrounds = oracle.fit_multi_tissue(signals, mfod_fixture["weights"], lr, hr, n_threads=4, rounds=True)
+    assert (status == 0).all()
+    np.testing.assert_array_equal(rounds, rrounds)
+    # Identical active sets of the final FOD, and values to rounding.
+    np.testing.assert_array_equal(fods != 0, rfods != 0)
+    scale = np.abs(rfods).max(axis=1, keepdims=True)
+    assert (np.abs(fods - rfods) <= 1e-9 * scale).all()
+    np.testing.assert_allclose(fractions, rfr, rtol=0, atol=1e-10)
+
+
+def test_multi_tissue_matches_mritoolkit(cuda, mfod_fixture):
+    signals, _, _ = mfod_inputs(mfod_fixture)
+    fods, fractions, _, _ = _gpu_fit(mfod_fixture, signals)
+    ref_fod = mfod_fixture["matlab_fod"]
+    fod_err = np.abs(fods - ref_fod).max(axis=1) / ref_fod.max(axis=1)
+    assert fod_err.max() <= 1e-4
+    np.testing.assert_allclose(fractions, mfod_fixture["matlab_fractions"], rtol=0, atol=1e-5)
+
+
+@pytest.mark.parametrize("ridge", [0.0, 0.1])
+def test_single_tissue_l2nnls_matches_the_oracle(cuda, oracle, mfod_fixture, ridge):
+    from larmor_b200 import _core
+
+    signals, _, _ = mfod_inputs(mfod_fixture)
+    k = np.ascontiguousarray(mfod_fixture["hr_w_k_aniso"][:, :300])
+    solver = _core.FodSolver.l2nnls(k, ridge, 1e-6)
+    fods = _core.fit_single_tissue(np.ascontiguousarray(signals), solver, 1)
+    ref = oracle.ridge_nnls(k, ridge, 1e-6, signals, n_threads=4)
+    np.testing.assert_array_equal(fods != 0, ref != 0)
+    assert (np.abs(fods - ref) <= 1e-9 * np.abs(ref).max(axis=1, keepdims=True)).all()
+
+
+def test_sd_model_three_tissue_matches_the_oracle(cuda, oracle):
+    from larmor_b200.sd import AnisotropicRF, IsotropicRF, SDModel
+    from larmor_b200.sd.model import to_sh
+    from larmor_b200.synthetic import mfod_signals, mfod_table
+    from larmor_b200.types import Volume
+
+    rng = np.random.default_rng(3)
+    gtab = mfod_table(rng)
+    sig = mfod_signals(rng, gtab, 64)
+    data = sig.reshape(4, 4, 4, -1).astype(np.float32)
+    rfs = [AnisotropicRF([1.7e-3, 0.2e-3, 0.2e-3], 0.0), IsotropicRF(0.8e-3), IsotropicRF(3e-3)]
+    model = SDModel(rfs, method="mFOD")
+    fit = model.fit(Volume(data, np.eye(4)), gtab)
+    # The oracle on the same normalised signals and kernels.
+    s = data.reshape(-1, data.shape[-1]).astype(np.float64)
+    s0 = s[:, gtab.b0_mask].mean(axis=1)
+    norm = np.minimum(s / s0[:, None], 1.0)
+    from larmor_b200.sd.solvers import L2NNLS
+
+    hr, lr, _, _ = model._prepare(L2NNLS(), gtab.bvals, gtab.bvecs)
+    lrd = dict(k_aniso=lr.k_aniso, k_iso=lr.k_iso, w_k_iso=lr.w_k_iso, w_k_aniso=lr.w_k_aniso)
+    hrd = dict(k_aniso=hr.k_aniso, k_iso=hr.k_iso, w_k_iso=hr.w_k_iso, w_k_aniso=hr.w_k_aniso,
+               blocks=[(b.start, b.stop) for b in hr.aniso_blocks])
+    rfods, rfr = oracle.fit_multi_tissue(norm, lr.weights, lrd, hrd)
+    ref_sh = to_sh(rfods, fit.lmax, "tournier", exact_integral=True)
+    # The maps are float32, as the reference's.
+    np.testing.assert_allclose(fit.fods[0].reshape(-1, ref_sh.shape[1]), ref_sh, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(fit.tissue_fractions.reshape(-1, 3), rfr, rtol=0, atol=1e-6)
