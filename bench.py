@@ -121,6 +121,7 @@ class DtiWorkload:
 
     name = "dti_wlls_64x64x40"
     kernel = "fit_dti_maps_kernel"
+    has_fp32 = True
     # Algorithmic bytes per voxel: 31 float32 samples in, 16 float32 maps + 1 byte out
     # (the 8-byte floor per voxel is host-prepared input too).
     bytes_per_voxel = 4 * 31 + 8 + 16 * 4 + 1
@@ -182,7 +183,231 @@ class DtiWorkload:
         return done, time.perf_counter() - t0, f"whole volume ({self.v} voxels) repeated for ~{budget_s:.0f} s"
 
 
-WORKLOADS = {"dti": DtiWorkload}
+class DkiWorkload:
+    """Config 2: constrained DKI WLLS on the 96x96x60 volume (199,768 voxels, 6 b0 + 2 x 64)."""
+
+    name = "dki_wlls_96x96x60"
+    kernel = "fit_log_warp_kernel"
+    has_fp32 = True
+    # 134 float32 samples + S0 and floor (double) in; 36 float32 maps + npd + broke out.
+    bytes_per_voxel = 4 * 134 + 16 + 36 * 4 + 2
+
+    def __init__(self, seed: int) -> None:
+        from larmor_b200.dwi.dki import dki_constraints, dki_design
+        from larmor_b200.dwi.inputs import estimate_s0, masked_signals, sample_floors
+        from larmor_b200.synthetic import dki_volume
+
+        w = dki_volume(seed=2 + 10 * (seed - 1))
+        self.design = dki_design(w.gtab)
+        self.g = dki_constraints(w.gtab)
+        s0 = estimate_s0(w.volume, w.gtab, w.mask)[w.mask]
+        self.s0 = s0
+        self.signals = masked_signals(w.volume, np.nonzero(w.mask))
+        self.floor = sample_floors(s0, None, len(self.signals))
+        self.is_b0 = w.gtab.b0_mask.astype(np.uint8)
+        self.v = len(self.signals)
+        self.config = {"workload": self.name, "grid": [96, 96, 60], "voxels": self.v, "measurements": 134,
+                       "fit": "wls, constrained (768 constraints)", "l2": "flushed (256 MiB write) before each step"}
+
+    def device_setup(self, torch, dev):
+        from larmor_b200 import _core
+
+        self.torch = torch
+        self.handle = _core.LogDesign.cached(self.design, self.g)
+        up = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+        self.d_signals, self.d_s0, self.d_floor, self.d_b0 = up(self.signals), up(self.s0), up(self.floor), up(self.is_b0)
+        self.d_maps = torch.empty((36, self.v), dtype=torch.float32, device=dev)
+        self.d_npd = torch.empty((self.v,), dtype=torch.uint8, device=dev)
+        self.d_broke = torch.empty((self.v,), dtype=torch.uint8, device=dev)
+        self.d_params = torch.empty((self.v, 22), dtype=torch.float64, device=dev)
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+        self.h_signals, self.h_s0, self.h_floor = pin(self.signals), pin(self.s0), pin(self.floor)
+        self.h_maps = torch.empty((36, self.v), dtype=torch.float32).pin_memory()
+        self.h_npd = torch.empty((self.v,), dtype=torch.uint8).pin_memory()
+        self.h2d_bytes = self.signals.nbytes + self.s0.nbytes + self.floor.nbytes
+        self.d2h_bytes = 36 * 4 * self.v + self.v
+
+    def step_device(self, precision=0):
+        from larmor_b200 import _core, _lib
+
+        _lib.check(_lib.lib().lar_fit_dki_maps(
+            self.handle.handle, _lib.ptr(self.d_signals), _lib.ptr(self.d_s0), _lib.ptr(self.d_floor),
+            _lib.ptr(self.d_b0), self.v, 1, 20, 1e-6, precision, _lib.ptr(self.d_maps), _lib.ptr(self.d_npd),
+            _lib.ptr(self.d_broke), _lib.ptr(self.d_params), _core._stream(self.torch)))
+
+    def step_e2e(self):
+        self.d_signals.copy_(self.h_signals, non_blocking=True)
+        self.d_s0.copy_(self.h_s0, non_blocking=True)
+        self.d_floor.copy_(self.h_floor, non_blocking=True)
+        self.step_device()
+        self.h_maps.copy_(self.d_maps, non_blocking=True)
+        self.h_npd.copy_(self.d_npd, non_blocking=True)
+
+    def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
+        from oracle import oracle as o
+
+        n = min(self.v, 16384)
+        s = self.signals[:n].astype(np.float64)
+        is_b0 = self.is_b0.astype(bool)
+        s0 = self.s0[:n]
+        own = s[:, is_b0].mean(axis=1)
+        rep = ~np.isclose(s0, own, rtol=1e-9, atol=0.0)
+        s[np.ix_(rep, is_b0)] = s0[rep, None]
+        s[:, ~is_b0] = np.minimum(s[:, ~is_b0], s0[:, None])
+        bad = ~(np.isfinite(s) & (s > 0))
+        s[bad] = np.broadcast_to(self.floor[:n, None], s.shape)[bad]
+        log_s = np.log(s)
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget_s:
+            o.fit_log_signal(self.design, self.g, log_s, True, n_threads=threads)
+            done += n
+        return done, time.perf_counter() - t0, f"first {n} voxels of the volume, repeated for ~{budget_s:.0f} s (fit only)"
+
+
+class _SdWorkloadBase:
+    """The config-3 volume (110x110x70, 500,040 voxels, 10 b0 + 3 x 90) for the SD fits."""
+
+    def _volume(self, seed: int):
+        from larmor_b200.dwi.inputs import estimate_s0, masked_signals
+        from larmor_b200.synthetic import mfod_volume
+
+        w = mfod_volume(seed=3 + 10 * (seed - 1))
+        self.gtab = w.gtab
+        self.signals = masked_signals(w.volume, np.nonzero(w.mask)).astype(np.float64)
+        self.s0 = estimate_s0(w.volume, w.gtab, w.mask)[w.mask]
+        self.v = len(self.signals)
+
+
+class MfodWorkload(_SdWorkloadBase):
+    """Config 3: three-tissue mFOD (SDModel, method mFOD): WM L2NNLS FOD on 300 directions
+    (44 in the loop) + GM + CSF, up to 50 rounds, on S0-normalised signals."""
+
+    name = "mfod_3tissue_110x110x70"
+    kernel = "multi_tissue_kernel"
+    has_fp32 = False
+    # 280 double samples in, 300 double amplitudes + 3 fractions out.
+    bytes_per_voxel = 8 * 280 + 8 * 303
+
+    def __init__(self, seed: int) -> None:
+        from larmor_b200.synthetic import mfod_model_responses
+
+        from larmor_b200.sd.kernel import Kernel
+        from larmor_b200.sd.model import compute_shell_weights, low_resolution_dirs
+        from larmor_b200.sd.sphere import DIRS_300
+
+        self._volume(seed)
+        self.norm = np.ascontiguousarray(np.minimum(self.signals / self.s0[:, None], 1.0))
+        rfs = mfod_model_responses()
+        weights = compute_shell_weights(self.gtab.bvals, 1.0)
+        b, g = self.gtab.bvals, self.gtab.bvecs
+        self.hr = Kernel(rfs, b, g, dirs=DIRS_300, weights=weights)
+        self.lr = Kernel(rfs, b, g, dirs=low_resolution_dirs(rfs, len(b)), weights=weights)
+        self.config = {"workload": self.name, "grid": [110, 110, 70], "voxels": self.v, "measurements": 280,
+                       "tissues": "WM (lmax 8 output, 300 directions) + GM + CSF", "max_rounds": 50,
+                       "fraction_tol": 1e-7, "l2": "inputs (1.1 GB) larger than L2"}
+
+    def device_setup(self, torch, dev):
+        from larmor_b200.sd.solvers import L2NNLS, Stage, _deconv_kernel
+
+        self.torch = torch
+        self.k_lr, self.k_hr = _deconv_kernel(self.lr), _deconv_kernel(self.hr)
+        self.hr_solver = L2NNLS()._prepare(self.hr, self.gtab.bvals, Stage.HIGH_RES)
+        self.lr_solver = L2NNLS()._prepare(self.lr, self.gtab.bvals, Stage.LOW_RES)
+        self.d_signals = torch.from_numpy(self.norm).to(dev)
+        self.d_fods = torch.empty((self.v, self.k_hr.ca), dtype=torch.float64, device=dev)
+        self.d_fr = torch.empty((self.v, 3), dtype=torch.float64, device=dev)
+        self.h_signals = torch.from_numpy(self.norm).pin_memory()
+        self.h_fods = torch.empty((self.v, self.k_hr.ca), dtype=torch.float64).pin_memory()
+        self.h_fr = torch.empty((self.v, 3), dtype=torch.float64).pin_memory()
+        self.h2d_bytes = self.norm.nbytes
+        self.d2h_bytes = self.h_fods.numel() * 8 + self.h_fr.numel() * 8
+
+    def step_device(self, precision=0):
+        from larmor_b200 import _core
+
+        _core.fit_multi_tissue_device(self.d_signals, self.lr.weights, self.k_lr, self.lr_solver, self.k_hr,
+                                      self.hr_solver, 50, 1e-7, 1e-2, self.d_fods, self.d_fr)
+
+    def step_e2e(self):
+        self.d_signals.copy_(self.h_signals, non_blocking=True)
+        self.step_device()
+        self.h_fods.copy_(self.d_fods, non_blocking=True)
+        self.h_fr.copy_(self.d_fr, non_blocking=True)
+
+    def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
+        from oracle import oracle as o
+
+        n = min(self.v, 2048)
+        lr = dict(k_aniso=self.lr.k_aniso, k_iso=self.lr.k_iso, w_k_iso=self.lr.w_k_iso, w_k_aniso=self.lr.w_k_aniso)
+        hr = dict(k_aniso=self.hr.k_aniso, k_iso=self.hr.k_iso, w_k_iso=self.hr.w_k_iso, w_k_aniso=self.hr.w_k_aniso,
+                  blocks=[(b.start, b.stop) for b in self.hr.aniso_blocks])
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget_s:
+            o.fit_multi_tissue(self.norm[:n], self.lr.weights, lr, hr, n_threads=threads)
+            done += n
+        return done, time.perf_counter() - t0, f"first {n} voxels of the volume, repeated for ~{budget_s:.0f} s"
+
+
+class MsmtWorkload(_SdWorkloadBase):
+    """Config 3 through MSMT-CSD: LSI with 47 unknowns (WM lmax 8 + GM + CSF) and 302
+    constraints (300 directions + 2) per voxel."""
+
+    name = "msmt_csd_lsi_110x110x70"
+    kernel = "lsi_kernel"
+    has_fp32 = False
+    bytes_per_voxel = 8 * 280 + 8 * 47 + 1
+
+    def __init__(self, seed: int) -> None:
+        self._volume(seed)
+        self.config = {"workload": self.name, "grid": [110, 110, 70], "voxels": self.v, "measurements": 280,
+                       "unknowns": 47, "constraints": 302, "l2": "inputs (1.1 GB) larger than L2"}
+
+    def device_setup(self, torch, dev):
+        from larmor_b200.sd.msmt import prepare_msmt
+        from larmor_b200.sd.sphere import DIRS_300
+        from larmor_b200.synthetic import mfod_responses
+
+        self.torch = torch
+        self.design = prepare_msmt(mfod_responses(), [8, 0, 0], self.gtab.bvals, self.gtab.bvecs, DIRS_300)
+        self.d_signals = torch.from_numpy(self.signals).to(dev)
+        self.d_x = torch.empty((self.v, 47), dtype=torch.float64, device=dev)
+        self.d_conv = torch.empty((self.v,), dtype=torch.uint8, device=dev)
+        self.h_signals = torch.from_numpy(self.signals).pin_memory()
+        self.h_x = torch.empty((self.v, 47), dtype=torch.float64).pin_memory()
+        self.h_conv = torch.empty((self.v,), dtype=torch.uint8).pin_memory()
+        self.h2d_bytes = self.signals.nbytes
+        self.d2h_bytes = self.v * (47 * 8 + 1)
+
+    def step_device(self, precision=0):
+        from larmor_b200 import _core
+
+        _core.fit_lsi_device(self.design, self.d_signals, self.d_x, self.d_conv)
+
+    def step_e2e(self):
+        self.d_signals.copy_(self.h_signals, non_blocking=True)
+        self.step_device()
+        self.h_x.copy_(self.d_x, non_blocking=True)
+        self.h_conv.copy_(self.d_conv, non_blocking=True)
+
+    def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
+        from larmor_b200.sd.msmt import constraint_matrix, forward_matrix, NORM_REG
+        from larmor_b200.sd.sphere import DIRS_300
+        from larmor_b200.synthetic import mfod_responses
+        from oracle import oracle as o
+
+        f = forward_matrix(mfod_responses(), [8, 0, 0], self.gtab.bvals, self.gtab.bvecs)
+        g = constraint_matrix([8, 0, 0], DIRS_300)
+        ridge = float(np.sqrt(NORM_REG * np.max(np.sum(f**2, axis=0))))
+        n = min(self.v, 8192)
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget_s:
+            o.fit_lsi(f, g, ridge, self.signals[:n], n_threads=threads)
+            done += n
+        return done, time.perf_counter() - t0, f"first {n} voxels of the volume, repeated for ~{budget_s:.0f} s"
+
+
+WORKLOADS = {"dti": DtiWorkload, "dki": DkiWorkload, "mfod": MfodWorkload, "msmt": MsmtWorkload}
+
 
 
 # ---- runs --------------------------------------------------------------------------------
@@ -214,7 +439,7 @@ def main() -> int:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="dti", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="mfod", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="larmor_b200", choices=["larmor_b200", "reference"])
     ap.add_argument("--reference-budget", type=float, default=3.0,
                     help="seconds of CPU work per reference step")
@@ -292,10 +517,12 @@ def main() -> int:
     dev_ms = max_over_ranks(dev_ms)
 
     # The plain FP32 kernel, for comparison.
-    for _ in range(args.warmup):
-        wl.step_device(precision=1)
-    barrier()
-    fp32_ms = max_over_ranks(timed(lambda: wl.step_device(precision=1), args.steps))
+    fp32_ms = None
+    if wl.has_fp32:
+        for _ in range(args.warmup):
+            wl.step_device(precision=1)
+        barrier()
+        fp32_ms = max_over_ranks(timed(lambda: wl.step_device(precision=1), args.steps))
 
     # End to end through host buffers.
     for _ in range(args.warmup):
@@ -329,8 +556,9 @@ def main() -> int:
         "cpu_baseline": cpu,
         "e2e": {"value": voxels_all * args.steps / (e2e_ms / 1e3), "unit": "voxel fits/s",
                 "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes},
-        "plain_fp32": {"value": voxels_all * args.steps / (fp32_ms / 1e3), "unit": "voxel fits/s",
-                       "ms_per_step": fp32_ms / args.steps},
+        "plain_fp32": None if fp32_ms is None else {
+            "value": voxels_all * args.steps / (fp32_ms / 1e3), "unit": "voxel fits/s",
+            "ms_per_step": fp32_ms / args.steps},
         "gpu_launches": args.steps,
         "clocks": clocks.summary(),
     }

@@ -11,11 +11,13 @@
 //   the QR-based NNLS on the explicit [E^T; f^T] (warp_nnls.cuh); then
 //   x = back (scale E^T u / (1 - f.u) + rotated).
 //
-// Work distribution: a persistent grid of warps takes voxels from a device counter, since the
-// number of active-set steps differs from voxel to voxel. The Gram matrix (shared by every
-// voxel) is read row by row from L2; lanes split the k constraint columns for gradients and
-// steps, the n parameters for the projections, and the factor's rows for the triangular
-// solves. Each warp owns a slot of global scratch for its Cholesky factor and the fallback.
+// Work distribution: a persistent grid of warps, as many as fit on the SMs at once, takes voxels
+// from a device counter, since the number of active-set steps differs from voxel to voxel. Each
+// warp keeps its bounds, multipliers, candidate and packed Cholesky factor in shared memory
+// (warp_chol.cuh: the triangular solves run in registers with shuffles); the Gram matrix
+// (shared by every voxel) is read row by row from L2. Lanes split the k constraint columns for
+// gradients and steps, the n parameters for the projections. The rare QR fallback works in a
+// per-warp slot of global scratch.
 
 #include <algorithm>
 #include <cstdint>
@@ -25,6 +27,7 @@
 
 #include "common.cuh"
 #include "host_la.hpp"
+#include "warp_chol.cuh"
 #include "warp_nnls.cuh"
 
 namespace lar {
@@ -32,8 +35,9 @@ namespace lar {
 namespace {
 
 constexpr int kLsiWarps = 4;
-constexpr int kFactorCap = 64;   // columns the Cholesky factor can hold (> n + 1)
+constexpr int kFactorCap = 64;   // active columns the Cholesky factor can hold (>= n + 1)
 constexpr double kMinRelativePivot = 1e-12;
+constexpr int kColsPerLane = 16;  // constraint columns a lane holds gradients for (k <= 512)
 
 struct LsiDevice {
     int m, n, k;
@@ -45,87 +49,73 @@ struct LsiDevice {
     const double* abs_sums;  // (k,)
 };
 
+// Global scratch of one warp: the QR-based fallback's explicit matrix and workspaces.
 inline size_t lsi_slot_doubles(int n, int k) {
-    return size_t(kFactorCap) * kFactorCap  // L
-           + 5 * size_t(k)                  // f, u, z, fallback u, z
+    return 2 * size_t(k)                    // fallback u, z
            + size_t(n + 1) * k              // fallback matrix
            + size_t(kFactorCap) * (n + 1)   // fallback QR columns
-           + (2 * size_t(k) + 7) / 8        // flag bytes (two arrays)
-           + 256;
+           + (size_t(k) + 7) / 8            // fallback flags
+           + 64;
 }
 
-struct LsiShared {
-    double rot[64];
-    double a[kFactorCap];    // triangular-solve vector
-    double t[64];            // E^T u
-    double qtau[kFactorCap], qnu[kFactorCap], qnd[kFactorCap], rv[kFactorCap + 1], res[kFactorCap + 1];
-    double d[kFactorCap + 1];
-    int qperm[kFactorCap];
-    int act[kFactorCap];     // fallback active list
-    int n_act;
-    int cols[kFactorCap];    // factor columns in joining order
-    int sorted[kFactorCap];  // the same, increasing
+// Shared memory of one warp: bounds f, multipliers u, candidate z (k each), the packed factor and
+// its reciprocal diagonal (cap), small vectors, then the int and byte arrays.
+struct LsiWarpLayout {
+    int k, cap;
+    __host__ __device__ size_t doubles() const { return 3 * size_t(k) + packed_size(cap) + cap + 4 * 64; }
+    __host__ __device__ size_t ints() const { return 2 * size_t(cap) + 2 * 64 + 8; }
+    __host__ __device__ size_t bytes() const {
+        return (doubles() * sizeof(double) + ints() * sizeof(int) + size_t(k) + 15) / 16 * 16;
+    }
 };
 
-// H(r, c) = (E E^T)(r, c) + f_r f_c.
-__device__ __forceinline__ double ldp_h(const LsiDevice& D, const double* f, int r, int c) {
-    return D.gram[size_t(r) * D.k + c] + f[r] * f[c];
+struct LsiWarp {
+    double *f, *u, *z, *L, *inv, *rot, *t, *d, *res;
+    int *cols, *sorted, *act, *perm;
+    int* n_act;
+    uint8_t* flag;
+};
+
+__device__ LsiWarp carve_lsi(unsigned char* base, const LsiWarpLayout& lay) {
+    LsiWarp w;
+    double* p = reinterpret_cast<double*>(base);
+    w.f = p; p += lay.k;
+    w.u = p; p += lay.k;
+    w.z = p; p += lay.k;
+    w.L = p; p += packed_size(lay.cap);
+    w.inv = p; p += lay.cap;
+    w.rot = p; p += 64;
+    w.t = p; p += 64;
+    w.d = p; p += 64;
+    w.res = p; p += 64;
+    int* q = reinterpret_cast<int*>(p);
+    w.cols = q; q += lay.cap;
+    w.sorted = q; q += lay.cap;
+    w.act = q; q += 64;
+    w.perm = q; q += 64;
+    w.n_act = q; q += 8;
+    w.flag = reinterpret_cast<uint8_t*>(q);
+    return w;
 }
 
-// Removes position `pos` from the lower factor L (ld = kFactorCap) of `na` columns, keeping
-// L L^T of the others: a row shift and Givens rotations (cpp/src/sd/nnls.cpp:305-324).
-__device__ void remove_factor_column(double* L, int na, int pos, int lane) {
-    for (int j = lane; j < na; j += 32)
-        for (int row = pos; row < na - 1; ++row) L[row * kFactorCap + j] = L[(row + 1) * kFactorCap + j];
-    __syncwarp();
-    for (int col = pos; col < na - 1; ++col) {
-        const double diag = L[col * kFactorCap + col], above = L[col * kFactorCap + col + 1];
-        const double len = hypot(diag, above);
-        const double c = diag / len, s = above / len;
-        for (int row = col + lane; row < na - 1; row += 32) {
-            const double l = L[row * kFactorCap + col], r = L[row * kFactorCap + col + 1];
-            L[row * kFactorCap + col] = c * l + s * r;
-            L[row * kFactorCap + col + 1] = c * r - s * l;
-        }
-        __syncwarp();
-    }
-}
+// The small per-warp QR state of the fallback.
+struct LsiQrShared {
+    double tau[kFactorCap], nu[kFactorCap], nd[kFactorCap], rv[kFactorCap + 1];
+};
 
-// z <- the solution of H_AA z_A = f_A (zero elsewhere) from the factor.
-__device__ void factor_solve(const double* L, int na, const int* cols, const double* f, double* z, int k,
-                             double* a, int lane) {
-    for (int j = lane; j < k; j += 32) z[j] = 0.0;
-    for (int p = lane; p < na; p += 32) a[p] = f[cols[p]];
-    __syncwarp();
-    for (int j = 0; j < na; ++j) {
-        const double aj = a[j] / L[j * kFactorCap + j];
-        __syncwarp();
-        if (lane == 0) a[j] = aj;
-        for (int r = j + 1 + lane; r < na; r += 32) a[r] -= L[r * kFactorCap + j] * aj;
-        __syncwarp();
-    }
-    for (int j = na - 1; j >= 0; --j) {
-        const double aj = a[j] / L[j * kFactorCap + j];
-        __syncwarp();
-        if (lane == 0) a[j] = aj;
-        for (int r = lane; r < j; r += 32) a[r] -= L[j * kFactorCap + r] * aj;
-        __syncwarp();
-    }
-    for (int p = lane; p < na; p += 32) z[cols[p]] = a[p];
-    __syncwarp();
-}
-
-// The LDP multipliers (cpp/src/sd/lsi.cpp:253-297). Returns false when a Cholesky pivot fails
-// or the inner steps run out (the caller falls back to the QR-based NNLS).
-__device__ bool ldp_multipliers(const LsiDevice& D, const double* f, double* u, double* z, uint8_t* flag,
-                                double* L, LsiShared& sh, int* outer_steps, int lane) {
+// The LDP multipliers (cpp/src/sd/lsi.cpp:253-297) in w.u. Returns false when a Cholesky pivot
+// fails or the inner steps run out (the caller falls back to the QR-based NNLS).
+__device__ __noinline__ bool ldp_multipliers(const LsiDevice& D, const LsiWarp& w, int cap, int* outer_steps,
+                                             int lane) {
+    constexpr int VPL = kFactorCap / 32;
     const int k = D.k;
+    const WarpFactor fac{w.L, w.inv, w.cols, cap};
     double norm1 = 0.0;
     for (int j = lane; j < k; j += 32) {
-        norm1 = fmax(norm1, D.abs_sums[j] + fabs(f[j]));
-        u[j] = 0.0;
-        z[j] = 0.0;
-        flag[j] = 0;
+        norm1 = fmax(norm1, D.abs_sums[j] + fabs(w.f[j]));
+        w.u[j] = 0.0;
+        w.z[j] = 0.0;
+        w.flag[j] = 0;
     }
     norm1 = warp_max(norm1);
     const double tol = 10.0 * kEps64 * norm1 * double(max(D.n + 1, k));
@@ -134,104 +124,110 @@ __device__ bool ldp_multipliers(const LsiDevice& D, const double* f, double* u, 
     __syncwarp();
     for (;;) {
         double fu = 0.0;
-        for (int j = lane; j < k; j += 32) fu += f[j] * u[j];
+        for (int j = lane; j < k; j += 32) fu += w.f[j] * w.u[j];
         fu = warp_sum(fu);
-        // Steepest inactive gradient f (1 - f.u) - sum_c u_c (E E^T)_c, columns c in increasing order.
+        // Steepest inactive gradient f (1 - f.u) - sum_c u_c (E E^T)_c over the active columns in
+        // increasing order (u is zero elsewhere), the first on a tie.
+        double g[kColsPerLane];
+#pragma unroll
+        for (int t = 0; t < kColsPerLane; ++t) {
+            const int j = lane + 32 * t;
+            g[t] = j < k ? w.f[j] * (1.0 - fu) : 0.0;
+        }
+        for (int q = 0; q < na; ++q) {
+            const int c = w.sorted[q];
+            const double uc = w.u[c];
+            if (uc == 0.0) continue;
+            const double* row = D.gram + size_t(c) * k;
+#pragma unroll
+            for (int t = 0; t < kColsPerLane; ++t) {
+                const int j = lane + 32 * t;
+                if (j < k) g[t] -= uc * row[j];
+            }
+        }
         double bv = 0.0;
         int bi = -1;
-        for (int j = lane; j < k; j += 32) {
-            if (flag[j]) continue;
-            double g = f[j] * (1.0 - fu);
-            for (int q = 0; q < na; ++q) {
-                const int c = sh.sorted[q];
-                const double uc = u[c];
-                if (uc != 0.0) g -= uc * D.gram[size_t(c) * k + j];
-            }
-            if (bi < 0 || g > bv) { bv = g; bi = j; }
+#pragma unroll
+        for (int t = 0; t < kColsPerLane; ++t) {
+            const int j = lane + 32 * t;
+            if (j < k && !w.flag[j] && (bi < 0 || g[t] > bv)) { bv = g[t]; bi = j; }
         }
         const int e = warp_argmax_first(bv, bi);
         const double ge = e >= 0 ? __shfl_sync(0xffffffffu, bv, e & 31) : 0.0;
         if (e < 0 || ge <= tol) break;
         ++outer;
-        if (na >= kFactorCap) { *outer_steps = outer; return false; }
-        // Append e to the factor: L w = H_{A,e}, pivot = H_ee - w.w.
-        double* w = sh.a;
-        for (int r = lane; r < na; r += 32) w[r] = ldp_h(D, f, sh.cols[r], e);
-        __syncwarp();
-        for (int j = 0; j < na; ++j) {
-            const double wj = w[j] / L[j * kFactorCap + j];
-            __syncwarp();
-            if (lane == 0) w[j] = wj;
-            for (int r = j + 1 + lane; r < na; r += 32) w[r] -= L[r * kFactorCap + j] * wj;
-            __syncwarp();
+        // H(cols[r], e) = (E E^T)(cols[r], e) + f_cols[r] f_e, then append.
+        const double fe = w.f[e];
+        double h[VPL];
+#pragma unroll
+        for (int t = 0; t < VPL; ++t) {
+            const int r = lane + 32 * t;
+            h[t] = 0.0;
+            if (r < na) {
+                const int c = w.cols[r];
+                h[t] = D.gram[size_t(c) * k + e] + w.f[c] * fe;
+            }
         }
-        double sq = 0.0;
-        for (int r = lane; r < na; r += 32) sq += w[r] * w[r];
-        sq = warp_sum(sq);
-        const double hee = ldp_h(D, f, e, e);
-        const double pivot = hee - sq;
-        if (!(pivot > kMinRelativePivot * hee)) { *outer_steps = outer; return false; }
-        for (int r = lane; r < na; r += 32) L[na * kFactorCap + r] = w[r];
-        __syncwarp();
+        const double hee = D.gram[size_t(e) * k + e] + fe * fe;
+        if (!factor_append<VPL>(fac, na, h, hee, e, kMinRelativePivot, lane)) {
+            *outer_steps = outer;
+            return false;
+        }
         if (lane == 0) {
-            L[na * kFactorCap + na] = sqrt(pivot);
-            sh.cols[na] = e;
-            int q = na;
-            while (q > 0 && sh.sorted[q - 1] > e) { sh.sorted[q] = sh.sorted[q - 1]; --q; }
-            sh.sorted[q] = e;
-            flag[e] = 1;
+            w.flag[e] = 1;
+            int q = na - 1;
+            while (q > 0 && w.sorted[q - 1] > e) { w.sorted[q] = w.sorted[q - 1]; --q; }
+            w.sorted[q] = e;
         }
-        ++na;
         __syncwarp();
-        factor_solve(L, na, sh.cols, f, z, k, sh.a, lane);
+        factor_solve<VPL>(fac, na, w.f, w.z, k, lane);
         for (;;) {
             // Blocking step over active columns with z <= 0, the first on a tie.
             double sv = 0.0;
             int si = -1;
             for (int q = lane; q < na; q += 32) {
-                const int col = sh.cols[q];
-                if (z[col] > 0.0) continue;
-                const double dist = u[col] - z[col];
-                const double st = dist > 0.0 ? u[col] / dist : 0.0;
-                if (si < 0 || st < sv || (st == sv && col < si)) { sv = st; si = col; }
+                const int col = w.sorted[q];
+                if (w.z[col] > 0.0) continue;
+                const double dist = w.u[col] - w.z[col];
+                const double st = dist > 0.0 ? w.u[col] / dist : 0.0;
+                if (si < 0 || st < sv) { sv = st; si = col; }
             }
             double step;
             const int b = warp_argmin_first(sv, si, &step);
             if (b < 0) break;
-            if (++inner > max_inner) { *outer_steps = outer; return false; }
+            if (++inner > max_inner) {
+                *outer_steps = outer;
+                return false;
+            }
             for (int q = lane; q < na; q += 32) {
-                const int col = sh.cols[q];
-                u[col] += step * (z[col] - u[col]);
+                const int col = w.sorted[q];
+                w.u[col] += step * (w.z[col] - w.u[col]);
             }
             __syncwarp();
+            // The blocking coefficient leaves, and so does any that rounding left near zero.
             if (lane == 0) {
-                u[b] = 0.0;
+                w.u[b] = 0.0;
+                int kept = 0;
                 for (int q = 0; q < na; ++q) {
-                    const int col = sh.cols[q];
-                    if (col == b || fabs(u[col]) < tol) {
-                        flag[col] = 0;
-                        u[col] = 0.0;
+                    const int col = w.sorted[q];
+                    if (col == b || fabs(w.u[col]) < tol) {
+                        w.flag[col] = 0;
+                        w.u[col] = 0.0;
+                    } else {
+                        w.sorted[kept++] = col;
                     }
                 }
             }
             __syncwarp();
             // keep(): drop the factor columns that left, from the last position to the first.
             for (int pos = na - 1; pos >= 0; --pos) {
-                const int col = sh.cols[pos];
-                if (flag[col]) continue;
-                remove_factor_column(L, na, pos, lane);
-                if (lane == 0) {
-                    for (int q = pos; q < na - 1; ++q) sh.cols[q] = sh.cols[q + 1];
-                    int w2 = 0;
-                    for (int q = 0; q < na; ++q)
-                        if (sh.sorted[q] != col) sh.sorted[w2++] = sh.sorted[q];
-                }
+                if (w.flag[w.cols[pos]]) continue;
+                factor_remove(fac, na, pos, lane);
                 --na;
-                __syncwarp();
             }
-            factor_solve(L, na, sh.cols, f, z, k, sh.a, lane);
+            factor_solve<VPL>(fac, na, w.f, w.z, k, lane);
         }
-        for (int j = lane; j < k; j += 32) u[j] = z[j];
+        for (int j = lane; j < k; j += 32) w.u[j] = w.z[j];
         __syncwarp();
     }
     *outer_steps = outer;
@@ -239,27 +235,25 @@ __device__ bool ldp_multipliers(const LsiDevice& D, const double* f, double* u, 
 }
 
 __global__ void __launch_bounds__(kLsiWarps * 32) lsi_kernel(LsiDevice D, const double* __restrict__ signals,
-                                                             int64_t v, int only_qr, int* queue,
+                                                             int64_t v, int only_qr, int* queue, int cap,
                                                              double* __restrict__ workspace, size_t slot_doubles,
                                                              double* __restrict__ x, uint8_t* __restrict__ converged,
                                                              uint8_t* __restrict__ status,
                                                              int32_t* __restrict__ outer_out,
                                                              uint8_t* __restrict__ active_out) {
-    __shared__ LsiShared shared[kLsiWarps];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ LsiQrShared qr_shared[kLsiWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    LsiShared& sh = shared[warp];
+    const LsiWarpLayout lay{D.k, cap};
+    const LsiWarp w = carve_lsi(smem_raw + warp * lay.bytes(), lay);
+    LsiQrShared& qsh = qr_shared[warp];
     const int m = D.m, n = D.n, k = D.k, rows = n + 1;
     double* slot = workspace + (size_t(blockIdx.x) * kLsiWarps + warp) * slot_doubles;
-    double* L = slot;
-    double* f = L + kFactorCap * kFactorCap;
-    double* u = f + k;
-    double* z = u + k;
-    double* u2 = z + k;
+    double* u2 = slot;
     double* z2 = u2 + k;
     double* cmat = z2 + k;                        // (rows, k)
     double* sub = cmat + size_t(rows) * k;        // (kFactorCap, rows)
-    uint8_t* flag = reinterpret_cast<uint8_t*>(sub + size_t(kFactorCap) * rows);
-    uint8_t* flag2 = flag + k;
+    uint8_t* flag2 = reinterpret_cast<uint8_t*>(sub + size_t(kFactorCap) * rows);
     for (;;) {
         int64_t voxel = 0;
         if (lane == 0) voxel = atomicAdd(queue, 1);
@@ -270,15 +264,15 @@ __global__ void __launch_bounds__(kLsiWarps * 32) lsi_kernel(LsiDevice D, const 
         for (int i = lane; i < n; i += 32) {
             double acc = 0.0;
             for (int j = 0; j < m; ++j) acc += D.qt[size_t(j) * n + i] * s[j];
-            sh.rot[i] = acc;
+            w.rot[i] = acc;
         }
         __syncwarp();
         // f = -E rotated, scaled by max |f|.
         double scale = 0.0;
         for (int j = lane; j < k; j += 32) {
             double acc = 0.0;
-            for (int i = 0; i < n; ++i) acc += D.et[size_t(i) * k + j] * sh.rot[i];
-            f[j] = -acc;
+            for (int i = 0; i < n; ++i) acc += D.et[size_t(i) * k + j] * w.rot[i];
+            w.f[j] = -acc;
             scale = fmax(scale, fabs(acc));
         }
         scale = warp_max(scale);
@@ -289,37 +283,37 @@ __global__ void __launch_bounds__(kLsiWarps * 32) lsi_kernel(LsiDevice D, const 
             // f = 0: the unconstrained solution back * rotated.
             for (int i = lane; i < n; i += 32) {
                 double acc = 0.0;
-                for (int j = 0; j < n; ++j) acc += D.back[size_t(i) * n + j] * sh.rot[j];
+                for (int j = 0; j < n; ++j) acc += D.back[size_t(i) * n + j] * w.rot[j];
                 x[voxel * n + i] = acc;
             }
             if (active_out)
                 for (int j = lane; j < k; j += 32) active_out[voxel * k + j] = 0;
             st = 2;
         } else {
-            for (int j = lane; j < k; j += 32) f[j] /= scale;
+            for (int j = lane; j < k; j += 32) w.f[j] /= scale;
             __syncwarp();
-            const double* mult = u;
-            bool fast = !only_qr && ldp_multipliers(D, f, u, z, flag, L, sh, &outer, lane);
+            const double* mult = w.u;
+            const bool fast = !only_qr && ldp_multipliers(D, w, cap, &outer, lane);
             if (!fast) {
                 // QR-based NNLS on the explicit [E^T; f^T] (cpp/src/sd/lsi.cpp:321-332).
                 double colmax = 0.0;
                 for (int j = lane; j < k; j += 32) {
-                    double cs = fabs(f[j]);
+                    double cs = fabs(w.f[j]);
                     for (int i = 0; i < n; ++i) {
                         const double eij = D.e[size_t(j) * n + i];
                         cmat[size_t(i) * k + j] = eij;
                         cs += fabs(eij);
                     }
-                    cmat[size_t(n) * k + j] = f[j];
+                    cmat[size_t(n) * k + j] = w.f[j];
                     colmax = fmax(colmax, cs);
                 }
                 colmax = warp_max(colmax);
-                for (int r = lane; r < rows; r += 32) sh.d[r] = (r == n) ? 1.0 : 0.0;
+                for (int r = lane; r < rows; r += 32) w.d[r] = (r == n) ? 1.0 : 0.0;
                 __syncwarp();
                 const double tol = 10.0 * kEps64 * colmax * double(max(rows, k));
-                NnlsScratch ns{u2, z2, flag2, sh.act, &sh.n_act, sh.res,
-                               QrScratch{sub, sh.qtau, sh.qnu, sh.qnd, sh.qperm, sh.rv}, kFactorCap};
-                const int outcome = warp_nnls_explicit(cmat, rows, k, sh.d, tol, 3 * k, ns, lane);
+                NnlsScratch ns{u2, z2, flag2, w.act, w.n_act, w.res,
+                               QrScratch{sub, qsh.tau, qsh.nu, qsh.nd, w.perm, qsh.rv}, kFactorCap};
+                const int outcome = warp_nnls_explicit(cmat, rows, k, w.d, tol, 3 * k, ns, lane);
                 conv = outcome == 1 ? 1 : 0;
                 if (outcome < 0)
                     for (int j = lane; j < k; j += 32) u2[j] = 0.0;
@@ -329,7 +323,7 @@ __global__ void __launch_bounds__(kLsiWarps * 32) lsi_kernel(LsiDevice D, const 
             }
             // x = back (scale E^T u / (1 - f.u) + rotated).
             double fu = 0.0;
-            for (int j = lane; j < k; j += 32) fu += f[j] * mult[j];
+            for (int j = lane; j < k; j += 32) fu += w.f[j] * mult[j];
             fu = warp_sum(fu);
             for (int i = lane; i < n; i += 32) {
                 double acc = 0.0;
@@ -337,12 +331,12 @@ __global__ void __launch_bounds__(kLsiWarps * 32) lsi_kernel(LsiDevice D, const 
                     const double mj = mult[j];
                     if (mj != 0.0) acc += D.e[size_t(j) * n + i] * mj;
                 }
-                sh.t[i] = scale * acc / (1.0 - fu) + sh.rot[i];
+                w.t[i] = scale * acc / (1.0 - fu) + w.rot[i];
             }
             __syncwarp();
             for (int i = lane; i < n; i += 32) {
                 double acc = 0.0;
-                for (int j = 0; j < n; ++j) acc += D.back[size_t(i) * n + j] * sh.t[j];
+                for (int j = 0; j < n; ++j) acc += D.back[size_t(i) * n + j] * w.t[j];
                 x[voxel * n + i] = acc;
             }
             if (active_out)
@@ -382,6 +376,7 @@ int lar_lsi_design_create(const double* a, int64_t m, int64_t n, const double* g
         require(a != nullptr && m > 0 && n > 0, "a must be a non-empty (m, n) array");
         require(g != nullptr && k > 0, "g must be a non-empty (k, n) array");
         require(n + 1 <= 64, "the LSI fit takes at most 63 parameters");
+        require(k <= 512, "the LSI fit takes at most 512 constraints");
         require(m <= (int64_t(1) << 20) && k <= (int64_t(1) << 16), "the LSI design is too large");
         auto h = std::make_unique<lar_lsi_design_s>();
         h->host = host::prepare_lsi_design(a, m, n, g, k, ridge);
@@ -424,9 +419,18 @@ int lar_fit_lsi(lar_lsi_design design, const double* signals, int64_t v, int onl
         if (v == 0) return;
         require(signals && x && converged, "signals, x and converged must not be NULL");
         const auto& h = design->host;
-        const int slots = int(std::max<int64_t>(kLsiWarps, std::min<int64_t>(
-                                                              (v + kLsiWarps - 1) / kLsiWarps * kLsiWarps,
-                                                              int64_t(sm_count()) * 8)));
+        const int cap = int(std::min<int64_t>(kFactorCap, (h.n + 1 + 7) / 8 * 8));
+        const LsiWarpLayout lay{int(h.k), cap};
+        const size_t smem = lay.bytes() * kLsiWarps;
+        require(smem <= 200 * 1024, "the LSI problem has too many constraints for the shared-memory solver");
+        cuda_check(cudaFuncSetAttribute(lsi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+                   "cudaFuncSetAttribute");
+        int per_sm = 0;
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lsi_kernel, kLsiWarps * 32, smem),
+                   "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((v + kLsiWarps - 1) / kLsiWarps,
+                                                                      int64_t(sm_count()) * std::max(per_sm, 1)));
+        const int slots = int(blocks) * kLsiWarps;
         const size_t slot = lsi_slot_doubles(int(h.n), int(h.k));
         const size_t need = 256 + size_t(slots) * slot * sizeof(double);
         if (need > design->scratch_bytes) {
@@ -441,9 +445,9 @@ int lar_fit_lsi(lar_lsi_design design, const double* signals, int64_t v, int onl
         cuda_check(cudaMemsetAsync(base, 0, sizeof(int), st), "cudaMemsetAsync");
         LsiDevice D{int(h.m), int(h.n), int(h.k), design->qt.ptr, design->back.ptr, design->et.ptr,
                     design->e.ptr, design->gram.ptr, design->abs_sums.ptr};
-        lsi_kernel<<<slots / kLsiWarps, kLsiWarps * 32, 0, st>>>(
-            D, signals, v, only_qr, reinterpret_cast<int*>(base), reinterpret_cast<double*>(base + 256), slot, x,
-            converged, status, outer, active);
+        lsi_kernel<<<unsigned(blocks), kLsiWarps * 32, smem, st>>>(
+            D, signals, v, only_qr, reinterpret_cast<int*>(base), cap, reinterpret_cast<double*>(base + 256), slot,
+            x, converged, status, outer, active);
         cuda_check(cudaGetLastError(), "lsi_kernel launch");
     });
 }

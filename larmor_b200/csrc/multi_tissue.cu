@@ -1,4 +1,4 @@
-// Multi-tissue spherical deconvolution (SDModel's mFOD method) on the GPU, one warp per voxel.
+// Multi-tissue spherical deconvolution (SDModel's mFOD method) on the GPU.
 //
 // Follows cpp/src/sd/multi_tissue.cpp:76-148 per voxel (a voxel's rounds do not depend on the
 // other voxels of its block, cpp/tests/sd/test_multi_tissue.cpp:56): up to max_rounds rounds of
@@ -12,12 +12,17 @@
 // until no fraction changes by fraction_tol; then the high-resolution FOD (ridge NNLS) and the
 // per-block fractions with the final tolerance, normalised to sum to 1 (+1e-16).
 //
-// Work distribution: a persistent grid of warps pulls voxels from a device counter (the rounds
-// and active-set steps differ between voxels). Lanes split the kernel's columns for the
-// correlations K^T s and the NNLS gradients, the measurements for the fraction columns, and the
-// factor's rows for the triangular solves. Each warp owns a slot of global scratch: the
-// signals, the FOD vectors, the Cholesky factor (up to kCholCap active columns) and the QR
-// workspaces.
+// Work distribution: the voxels go through the rounds together, each round as three kernels
+// over the list of voxels still iterating:
+//   correlate_kernel  K^T max(s_w - W_iso f_iso, 0) for 32 voxels x 16 RC columns per CTA, the
+//                     signals built while the tile is staged in shared memory (a tiled FP64
+//                     product, each entry summed over the measurements in increasing order);
+//   ridge_nnls_kernel the active-set NNLS on the Gram matrix and those correlations, one warp per
+//                     voxel (no work of the measurements' length unless the QR fallback runs);
+//   lr_fractions_kernel  the fractions, the convergence test and the next round's voxel list.
+// The high-resolution FOD then runs the first two for all voxels, and hr_fractions_kernel the
+// final fractions. Each kernel's code is small (the warps of an SM share their instruction
+// cache), and the per-voxel state between kernels lives in HBM.
 
 #include <algorithm>
 #include <cmath>
@@ -28,6 +33,7 @@
 
 #include "common.cuh"
 #include "host_la.hpp"
+#include "warp_chol.cuh"
 #include "warp_nnls.cuh"
 
 namespace lar {
@@ -39,6 +45,7 @@ constexpr int kCholCap = 256;   // active columns the Cholesky factor holds
 constexpr int kQrCap = 64;      // active columns of the ridge QR fallback
 constexpr int kMaxGroups = 16;  // fraction columns (anisotropic groups + isotropic tissues)
 constexpr double kMinPivot = 1e-12;
+constexpr int kMaxColumns = 640;  // kernel columns (directions) a solver may have
 constexpr double kMedianTie = 1e-9;
 constexpr double kFractionSumOffset = 1e-16;
 
@@ -58,129 +65,136 @@ struct TissueDev {
     const int* blocks;   // (nb, 2)
 };
 
-struct Slot {
-    double *s, *ws, *as, *corr, *x, *z, *th, *L, *cols, *fu, *fz, *fsub, *qsub, *qd, *qrv, *frv;
-    uint8_t *flag, *inf, *fflag;
+// The signal a ridge NNLS fits, entry i of voxel v: s(v, i) itself (single tissue), or
+// max(s(v, i) w_i - sum_t W_iso(i, t) f_iso(v, t), 0) (cpp/src/sd/multi_tissue.cpp:68-72).
+struct SignalDev {
+    const double* s;     // (v, m)
+    const double* w;     // (m,) or null: the plain signal
+    const double* wiso;  // (m, ci)
+    const double* fiso;  // (v, ci)
+    int m, ci;
+    __device__ __forceinline__ double operator()(int64_t voxel, int i) const {
+        const double si = s[voxel * m + i];
+        if (w == nullptr) return si;
+        const double ws = __dmul_rn(si, w[i]);
+        double r = 0.0;
+        for (int t = 0; t < ci; ++t) r = fma(wiso[size_t(i) * ci + t], fiso[voxel * ci + t], r);
+        return fmax(ws - r, 0.0);
+    }
 };
 
-inline size_t slot_doubles(int m, int cmax, int ng) {
-    return 3 * size_t(m) + 4 * size_t(cmax) + size_t(kCholCap) * kCholCap + size_t(m) * ng + 2 * size_t(ng) +
-           size_t(ng) * m + size_t(m + kQrCap) * kQrCap + 2 * size_t(m + kQrCap) + size_t(m) +
-           (2 * size_t(cmax) + ng + 7) / 8 + 64;
+// The voxel at position p of a round's list (the identity when there is no list).
+__device__ __forceinline__ int64_t listed(const int* list, int64_t p) { return list ? int64_t(list[p]) : p; }
+
+// ---- correlations ----------------------------------------------------------------------
+
+constexpr int kCorrVoxels = 32;  // voxels per CTA tile
+constexpr int kCorrDepth = 16;   // measurements per shared-memory stage
+
+// corr(v, j) = sum_i K(i, j) signal(v, i), i increasing, for the listed voxels: 128 threads as
+// 8 voxel lanes x 16 column lanes, each with 4 voxels x RC columns of the tile.
+template <int RC>
+__global__ void __launch_bounds__(128) correlate_kernel(SignalDev S, const int* __restrict__ list, int64_t count,
+                                                        const double* __restrict__ k, int c,
+                                                        double* __restrict__ corr, int ldc) {
+    constexpr int TC = 16 * RC;
+    __shared__ double sig_t[kCorrDepth][kCorrVoxels + 1];
+    __shared__ double k_t[kCorrDepth][TC];
+    __shared__ int64_t vox[kCorrVoxels];
+    const int tid = threadIdx.x, tv = tid & 7, tc = tid >> 3;
+    const int64_t p0 = int64_t(blockIdx.x) * kCorrVoxels;
+    const int col0 = blockIdx.y * TC;
+    const int m = S.m;
+    if (tid < kCorrVoxels) vox[tid] = p0 + tid < count ? listed(list, p0 + tid) : -1;
+    double acc[4][RC];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < RC; ++b) acc[a][b] = 0.0;
+    __syncthreads();
+    for (int i0 = 0; i0 < m; i0 += kCorrDepth) {
+        const int depth = min(kCorrDepth, m - i0);
+        for (int e = tid; e < kCorrVoxels * kCorrDepth; e += 128) {
+            const int vv = e / kCorrDepth, ii = e % kCorrDepth;
+            const int64_t voxel = vox[vv];
+            sig_t[ii][vv] = (voxel >= 0 && ii < depth) ? S(voxel, i0 + ii) : 0.0;
+        }
+        for (int e = tid; e < kCorrDepth * TC; e += 128) {
+            const int ii = e / TC, cc = e % TC;
+            const int col = col0 + cc;
+            k_t[ii][cc] = (ii < depth && col < c) ? k[size_t(i0 + ii) * c + col] : 0.0;
+        }
+        __syncthreads();
+        for (int ii = 0; ii < depth; ++ii) {
+            double sv[4], kv[RC];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) sv[a] = sig_t[ii][tv + 8 * a];
+#pragma unroll
+            for (int b = 0; b < RC; ++b) kv[b] = k_t[ii][tc + 16 * b];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < RC; ++b) acc[a][b] = fma(kv[b], sv[a], acc[a][b]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int64_t voxel = vox[tv + 8 * a];
+        if (voxel < 0) continue;
+#pragma unroll
+        for (int b = 0; b < RC; ++b) {
+            const int col = col0 + tc + 16 * b;
+            if (col < c) corr[voxel * ldc + col] = acc[a][b];
+        }
+    }
 }
 
-__device__ Slot carve(double* base, int m, int cmax, int ng) {
-    Slot s;
+// ---- ridge NNLS ------------------------------------------------------------------------
+
+// A warp's NNLS workspace. Shared memory: the solution x, its candidate z, the factor's vectors
+// h, w and y (InvFactor), the active and in-factor flags. Global slot: the packed inverse
+// factor, the signal (for the QR fallback) and the QR workspace.
+struct NnlsSlot {
+    double *x, *z, *h, *w, *y, *M, *sig, *qsub, *qd, *qrv;
+    uint8_t *flag, *inf;
+};
+
+inline size_t nnls_slot_doubles(int m, int cap) {
+    return size_t(tri_row(cap)) + size_t(m) + size_t(m + kQrCap) * kQrCap + 2 * size_t(m + kQrCap) + 8;
+}
+
+__host__ __device__ inline size_t nnls_smem_bytes(int c, int cap) {
+    return ((2 * size_t(c) + 3 * size_t(cap)) * sizeof(double) + 2 * size_t(c) + 15) / 16 * 16;
+}
+
+__device__ NnlsSlot carve_nnls(double* base, unsigned char* smem, int m, int c, int cap) {
+    NnlsSlot s;
     double* p = base;
-    s.s = p; p += m;
-    s.ws = p; p += m;
-    s.as = p; p += m;
-    s.corr = p; p += cmax;
-    s.x = p; p += cmax;
-    s.z = p; p += cmax;
-    s.th = p; p += cmax;
-    s.L = p; p += size_t(kCholCap) * kCholCap;
-    s.cols = p; p += size_t(m) * ng;
-    s.fu = p; p += ng;
-    s.fz = p; p += ng;
-    s.fsub = p; p += size_t(ng) * m;
+    s.M = p; p += tri_row(cap);
+    s.sig = p; p += m;
     s.qsub = p; p += size_t(m + kQrCap) * kQrCap;
     s.qd = p; p += m + kQrCap;
-    s.qrv = p; p += m + kQrCap;
-    s.frv = p; p += m;
-    s.flag = reinterpret_cast<uint8_t*>(p);
-    s.inf = s.flag + cmax;
-    s.fflag = s.inf + cmax;
+    s.qrv = p;
+    double* q = reinterpret_cast<double*>(smem);
+    s.x = q; q += c;
+    s.z = q; q += c;
+    s.h = q; q += cap;
+    s.w = q; q += cap;
+    s.y = q; q += cap;
+    s.flag = reinterpret_cast<uint8_t*>(q);
+    s.inf = s.flag + c;
     return s;
 }
 
-struct WarpState {
-    int cols[kCholCap];    // factor columns, joining order
-    int sorted[kCholCap];  // active columns with x != 0 candidates, increasing (the factor's set)
-    int qact[kQrCap];      // QR fallback active columns, increasing
+template <int CAP, int CMAX>
+struct NnlsState {
+    int cols[CAP];     // factor columns, joining order
+    int sorted[CMAX];  // columns with x != 0, increasing; the columns to append again in a fit
+    int qact[kQrCap];  // QR fallback active columns, increasing
     double qtau[kQrCap], qnu[kQrCap], qnd[kQrCap];
     int qperm[kQrCap];
-    double fres[kMaxGroups];
-    int fact[kMaxGroups], fn_act;
-    double ftau[kMaxGroups], fnu[kMaxGroups], fnd[kMaxGroups];
-    int fperm[kMaxGroups];
-    double fiso[kMaxGroups], prev[kMaxGroups], fr[kMaxGroups];
-    double med[2];
-    double a[kCholCap];
 };
-
-// ---- the active-set Cholesky factor of a Gram matrix (cpp/src/sd/nnls.cpp:237-301) ------
-
-// Appends `col`: L w = G_{A,col}, pivot = G_col,col - w.w; false when the pivot is not clearly
-// positive.
-__device__ bool chol_append(const RidgeDev& R, double* L, int& na, WarpState& st, int col, int lane) {
-    double* w = st.a;
-    for (int r = lane; r < na; r += 32) w[r] = R.gram[size_t(st.cols[r]) * R.c + col];
-    __syncwarp();
-    for (int j = 0; j < na; ++j) {
-        const double wj = w[j] / L[j * kCholCap + j];
-        __syncwarp();
-        if (lane == 0) w[j] = wj;
-        for (int r = j + 1 + lane; r < na; r += 32) w[r] -= L[r * kCholCap + j] * wj;
-        __syncwarp();
-    }
-    double sq = 0.0;
-    for (int r = lane; r < na; r += 32) sq += w[r] * w[r];
-    sq = warp_sum(sq);
-    const double gcc = R.gram[size_t(col) * R.c + col];
-    const double pivot = gcc - sq;
-    if (!(pivot > kMinPivot * gcc) || na >= kCholCap) return false;
-    for (int r = lane; r < na; r += 32) L[na * kCholCap + r] = w[r];
-    __syncwarp();
-    if (lane == 0) {
-        L[na * kCholCap + na] = sqrt(pivot);
-        st.cols[na] = col;
-    }
-    ++na;
-    __syncwarp();
-    return true;
-}
-
-__device__ void chol_remove(double* L, int na, int pos, int lane) {
-    for (int j = lane; j < na; j += 32)
-        for (int row = pos; row < na - 1; ++row) L[row * kCholCap + j] = L[(row + 1) * kCholCap + j];
-    __syncwarp();
-    for (int col = pos; col < na - 1; ++col) {
-        const double diag = L[col * kCholCap + col], above = L[col * kCholCap + col + 1];
-        const double len = hypot(diag, above);
-        const double c = diag / len, s = above / len;
-        for (int row = col + lane; row < na - 1; row += 32) {
-            const double l = L[row * kCholCap + col], r = L[row * kCholCap + col + 1];
-            L[row * kCholCap + col] = c * l + s * r;
-            L[row * kCholCap + col + 1] = c * r - s * l;
-        }
-        __syncwarp();
-    }
-}
-
-// z <- G_AA^-1 rhs_A, zero off the factor's columns.
-__device__ void chol_solve(const double* L, int na, const WarpState& st, const double* rhs, double* z, int c,
-                           double* a, int lane) {
-    for (int j = lane; j < c; j += 32) z[j] = 0.0;
-    for (int p = lane; p < na; p += 32) a[p] = rhs[st.cols[p]];
-    __syncwarp();
-    for (int j = 0; j < na; ++j) {
-        const double aj = a[j] / L[j * kCholCap + j];
-        __syncwarp();
-        if (lane == 0) a[j] = aj;
-        for (int r = j + 1 + lane; r < na; r += 32) a[r] -= L[r * kCholCap + j] * aj;
-        __syncwarp();
-    }
-    for (int j = na - 1; j >= 0; --j) {
-        const double aj = a[j] / L[j * kCholCap + j];
-        __syncwarp();
-        if (lane == 0) a[j] = aj;
-        for (int r = lane; r < j; r += 32) a[r] -= L[j * kCholCap + r] * aj;
-        __syncwarp();
-    }
-    for (int p = lane; p < na; p += 32) z[st.cols[p]] = a[p];
-    __syncwarp();
-}
 
 // The stacked columns [K_A; ridge I] of the ridge QR fallback.
 struct StackedColumns {
@@ -194,12 +208,12 @@ struct StackedColumns {
 
 // Least squares on the active columns by QR (fit_by_qr, cpp/src/sd/nnls.cpp:385-401); false
 // when more columns are active than the QR workspace holds.
-__device__ bool ridge_qr_fit(const RidgeDev& R, const double* sig, const uint8_t* flag, Slot& sl, WarpState& st,
-                             int lane) {
+template <class State>
+__device__ __noinline__ bool ridge_qr_fit(const RidgeDev& R, const double* sig, NnlsSlot& sl, State& st, int lane) {
     int k = 0;
     if (lane == 0) {
         for (int j = 0; j < R.c; ++j)
-            if (flag[j]) {
+            if (sl.flag[j]) {
                 if (k < kQrCap) st.qact[k] = j;
                 ++k;
             }
@@ -218,14 +232,15 @@ __device__ bool ridge_qr_fit(const RidgeDev& R, const double* sig, const uint8_t
 }
 
 // min ||K x - sig||^2 + ridge^2 ||x||^2 over x >= 0 (solve_ridge_nnls with l1 = 0,
-// cpp/src/sd/nnls.cpp:362-418), the result in sl.x. Returns false only when the QR fallback's
-// workspace overflowed (x is then the last fit).
-__device__ bool ridge_nnls(const RidgeDev& R, const double* sig, Slot& sl, WarpState& st, int lane) {
-    const int c = R.c, m = R.m;
+// cpp/src/sd/nnls.cpp:362-418) from corr = K^T sig, the result in sl.x. The signal itself is
+// built only when a QR fit needs it. Returns false only when the QR fallback's workspace
+// overflowed (x is then the last fit). VPL * 32 is the factor's capacity, CPL * 32 >= c.
+template <int VPL, int CPL, class State>
+__device__ __noinline__ bool ridge_nnls(const RidgeDev& R, const SignalDev& S, int64_t voxel,
+                                        const double* __restrict__ corr, NnlsSlot& sl, State& st, int lane) {
+    const int c = R.c;
+    const InvFactor fac{sl.M, sl.h, sl.w, sl.y, st.cols, VPL * 32};
     for (int j = lane; j < c; j += 32) {
-        double acc = 0.0;
-        for (int i = 0; i < m; ++i) acc += R.k[size_t(i) * c + j] * sig[i];
-        sl.corr[j] = acc;
         sl.x[j] = 0.0;
         sl.z[j] = 0.0;
         sl.flag[j] = 0;
@@ -233,66 +248,102 @@ __device__ bool ridge_nnls(const RidgeDev& R, const double* sig, Slot& sl, WarpS
     }
     __syncwarp();
     const bool use_qr_only = !R.normal_equations;
-    bool failed = false, overflow = false;
-    int na = 0, n_sorted = 0, inner = 0;
+    bool failed = false, overflow = false, have_sig = false;
+    int na = 0, inner = 0;
     const int max_inner = 3 * c;
-    // fit_on: the factor brought to the active set, or QR from the first failing pivot on.
-    auto fit_on = [&]() {
+    auto append = [&](int j) {
+        for (int r = lane; r < na; r += 32) sl.h[r] = R.gram[size_t(st.cols[r]) * c + j];
+        __syncwarp();
+        return inv_append<VPL>(fac, na, R.gram[size_t(j) * c + j], corr[j], j, kMinPivot, lane);
+    };
+    // fit_on: the factor brought to the active set (ActiveCholesky::update, :246-262), or QR from
+    // the first failing pivot on. Columns that left the active set leave the factor, the columns
+    // after the first of them are appended again in their order (the factor of the remaining
+    // columns in joining order), then `entering`, the column that joined since the last fit (or
+    // -1; every other active column is in the factor already, so update()'s scan appends only it).
+    auto fit_on = [&](int entering) {
         if (!use_qr_only && !failed) {
-            for (int pos = na - 1; pos >= 0; --pos) {
-                const int col = st.cols[pos];
-                if (sl.flag[col]) continue;
-                chol_remove(sl.L, na, pos, lane);
-                if (lane == 0) {
-                    for (int q = pos; q < na - 1; ++q) st.cols[q] = st.cols[q + 1];
-                    sl.inf[col] = 0;
+            int cut = na;
+            for (int pos = 0; pos < na; ++pos)
+                if (!sl.flag[st.cols[pos]]) {
+                    cut = pos;
+                    break;
                 }
-                --na;
+            if (cut < na) {
+                int keep = 0;
+                if (lane == 0) {
+                    for (int pos = cut; pos < na; ++pos) {
+                        const int col = st.cols[pos];
+                        if (sl.flag[col]) st.sorted[keep++] = col;
+                        else sl.inf[col] = 0;
+                    }
+                }
+                keep = __shfl_sync(0xffffffffu, keep, 0);
                 __syncwarp();
+                na = cut;
+                for (int q = 0; q < keep && !failed; ++q) failed = !append(st.sorted[q]);
             }
-            for (int j = 0; j < c && !failed; ++j) {
-                if (!sl.flag[j] || sl.inf[j]) continue;
-                if (!chol_append(R, sl.L, na, st, j, lane)) {
+            if (!failed && entering >= 0 && sl.flag[entering] && !sl.inf[entering]) {
+                if (!append(entering)) {
                     failed = true;
                 } else {
-                    if (lane == 0) sl.inf[j] = 1;
+                    if (lane == 0) sl.inf[entering] = 1;
                     __syncwarp();
                 }
             }
         }
         if (use_qr_only || failed) {
-            overflow |= !ridge_qr_fit(R, sig, sl.flag, sl, st, lane);
+            if (!have_sig) {
+                for (int i = lane; i < R.m; i += 32) sl.sig[i] = S(voxel, i);
+                __syncwarp();
+                have_sig = true;
+            }
+            overflow |= !ridge_qr_fit(R, sl.sig, sl, st, lane);
         } else {
-            chol_solve(sl.L, na, st, sl.corr, sl.z, c, st.a, lane);
+            inv_solve<VPL>(fac, na, sl.z, c, lane);
         }
     };
     for (;;) {
         // Gradient corr - G x over the non-zero x, columns in increasing order; the steepest
         // inactive entry, the first on a tie.
-        if (lane == 0) {
-            n_sorted = 0;
-            for (int j = 0; j < c; ++j)
-                if (sl.x[j] != 0.0) st.sorted[n_sorted++] = j;
+        int n_sorted = 0;
+        for (int base = 0; base < c; base += 32) {
+            const int j = base + lane;
+            const bool nz = j < c && sl.x[j] != 0.0;
+            const unsigned ballot = __ballot_sync(0xffffffffu, nz);
+            if (nz) st.sorted[n_sorted + __popc(ballot & ((1u << lane) - 1u))] = j;
+            n_sorted += __popc(ballot);
         }
-        n_sorted = __shfl_sync(0xffffffffu, n_sorted, 0);
         __syncwarp();
+        double g[CPL];
+#pragma unroll
+        for (int t = 0; t < CPL; ++t) {
+            const int j = lane + 32 * t;
+            g[t] = j < c ? corr[j] : 0.0;
+        }
+        for (int q = 0; q < n_sorted; ++q) {
+            const int col = st.sorted[q];
+            const double xc = sl.x[col];
+            const double* row = R.gram + size_t(col) * c;
+#pragma unroll
+            for (int t = 0; t < CPL; ++t) {
+                const int j = lane + 32 * t;
+                if (j < c) g[t] -= xc * row[j];
+            }
+        }
         double bv = 0.0;
         int bi = -1;
-        for (int j = lane; j < c; j += 32) {
-            if (sl.flag[j]) continue;
-            double g = sl.corr[j];
-            for (int q = 0; q < n_sorted; ++q) {
-                const int col = st.sorted[q];
-                g -= sl.x[col] * R.gram[size_t(col) * c + j];
-            }
-            if (bi < 0 || g > bv) { bv = g; bi = j; }
+#pragma unroll
+        for (int t = 0; t < CPL; ++t) {
+            const int j = lane + 32 * t;
+            if (j < c && !sl.flag[j] && (bi < 0 || g[t] > bv)) { bv = g[t]; bi = j; }
         }
         const int e = warp_argmax_first(bv, bi);
         const double ge = e >= 0 ? __shfl_sync(0xffffffffu, bv, e & 31) : 0.0;
         if (e < 0 || ge <= R.tol) break;
         if (lane == 0) sl.flag[e] = 1;
         __syncwarp();
-        fit_on();
+        fit_on(e);
         for (;;) {
             bool any = false;
             for (int j = lane; j < c; j += 32) any |= sl.flag[j] && sl.z[j] <= 0.0;
@@ -323,7 +374,7 @@ __device__ bool ridge_nnls(const RidgeDev& R, const double* sig, Slot& sl, WarpS
             for (int j = lane; j < c; j += 32)
                 if (sl.flag[j] && !(fabs(sl.x[j]) >= R.tol)) sl.flag[j] = 0;
             __syncwarp();
-            fit_on();
+            fit_on(-1);
         }
         for (int j = lane; j < c; j += 32) sl.x[j] = sl.z[j];
         __syncwarp();
@@ -331,9 +382,71 @@ __device__ bool ridge_nnls(const RidgeDev& R, const double* sig, Slot& sl, WarpS
     return !overflow;
 }
 
+// One warp per listed voxel, pulled from a device counter: x(v) <- the ridge NNLS of corr(v);
+// bad(v) <- 1 when the QR fallback overflowed.
+template <int VPL, int CPL>
+__global__ void __launch_bounds__(kMtWarps * 32, (CPL <= 2 ? 8 : 4)) ridge_nnls_kernel(
+    RidgeDev R, SignalDev S, const int* __restrict__ list, int64_t count, const double* __restrict__ corr, int ldc,
+    double* __restrict__ x_out, int ldx, uint8_t* __restrict__ bad, int* queue, double* __restrict__ workspace,
+    size_t slot_size) {
+    using State = NnlsState<VPL * 32, CPL * 32>;
+    __shared__ State states[kMtWarps];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    State& st = states[warp];
+    NnlsSlot sl = carve_nnls(workspace + (size_t(blockIdx.x) * kMtWarps + warp) * slot_size,
+                             smem_raw + warp * nnls_smem_bytes(R.c, VPL * 32), R.m, R.c, VPL * 32);
+    for (;;) {
+        int64_t p = 0;
+        if (lane == 0) p = atomicAdd(queue, 1);
+        p = __shfl_sync(0xffffffffu, p, 0);
+        if (p >= count) break;
+        const int64_t voxel = listed(list, p);
+        const bool ok = ridge_nnls<VPL, CPL>(R, S, voxel, corr + voxel * ldc, sl, st, lane);
+        for (int j = lane; j < R.c; j += 32) x_out[voxel * ldx + j] = sl.x[j];
+        if (lane == 0 && !ok && bad) bad[voxel] = 1;
+        __syncwarp();
+    }
+}
+
+// ---- fractions -------------------------------------------------------------------------
+
+// A warp's fraction workspace in its global slot: the thresholded FOD, the fraction columns
+// (row-major) and the NNLS / QR workspace.
+struct FracSlot {
+    double *th, *cols, *fu, *fz, *fsub, *frv, *res;
+    uint8_t* fflag;
+};
+
+inline size_t frac_slot_doubles(int m, int ca, int ng) {
+    return size_t(ca) + size_t(m) * ng + 2 * size_t(ng) + size_t(ng) * m + 2 * size_t(m) + (size_t(ng) + 7) / 8 + 8;
+}
+
+__device__ FracSlot carve_frac(double* base, int m, int ca, int ng) {
+    FracSlot s;
+    double* p = base;
+    s.th = p; p += ca;
+    s.cols = p; p += size_t(m) * ng;
+    s.fu = p; p += ng;
+    s.fz = p; p += ng;
+    s.fsub = p; p += size_t(ng) * m;
+    s.frv = p; p += m;
+    s.res = p; p += m;
+    s.fflag = reinterpret_cast<uint8_t*>(p);
+    return s;
+}
+
+struct FracState {
+    int fact[kMaxGroups], fn_act;
+    double ftau[kMaxGroups], fnu[kMaxGroups], fnd[kMaxGroups];
+    int fperm[kMaxGroups];
+    double fr[kMaxGroups];
+    double med[2];
+};
+
 // Median of v[0..n), the mean of the two middle values for even n (cpp/src/sd/fractions.cpp:56-68),
 // by ranks: the element of stable rank r is the r-th smallest.
-__device__ double warp_median(const double* v, int n, WarpState& st, int lane) {
+__device__ double warp_median(const double* v, int n, FracState& st, int lane) {
     const int hi = n / 2, lo = n % 2 ? n / 2 : n / 2 - 1;
     for (int i = lane; i < n; i += 32) {
         const double vi = v[i];
@@ -352,7 +465,7 @@ __device__ double warp_median(const double* v, int n, WarpState& st, int lane) {
 // compute_fractions (cpp/src/sd/fractions.cpp:70-101): tol < 0 uses the default tolerance of the
 // fraction columns. Writes the fractions (groups, then isotropic tissues) to st.fr.
 __device__ void fractions(const TissueDev& T, const double* fod, const double* sig, bool per_block, double tol,
-                          Slot& sl, WarpState& st, int lane) {
+                          FracSlot& sl, FracState& st, int lane) {
     const int m = T.m, ca = T.ca, ci = T.ci;
     const double threshold = warp_median(fod, ca, st, lane) * (1.0 - kMedianTie);
     for (int j = lane; j < ca; j += 32) sl.th[j] = fod[j] < threshold ? 0.0 : fod[j];
@@ -398,103 +511,131 @@ __device__ void fractions(const TissueDev& T, const double* fod, const double* s
         }
         tol = 10.0 * kEps64 * colmax * double(max(m, ncol));
     }
-    NnlsScratch ns{sl.fu, sl.fz, sl.fflag, st.fact, &st.fn_act, sl.frv,
+    NnlsScratch ns{sl.fu, sl.fz, sl.fflag, st.fact, &st.fn_act, sl.res,
                    QrScratch{sl.fsub, st.ftau, st.fnu, st.fnd, st.fperm, sl.frv}, kMaxGroups};
-    // The residual and the QR's rotated data must not share memory.
-    ns.res = sl.qrv;
     warp_nnls_explicit(sl.cols, m, ncol, sig, tol, 3 * ncol, ns, lane);
     for (int g = lane; g < ncol; g += 32) st.fr[g] = sl.fu[g];
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(kMtWarps * 32) multi_tissue_kernel(
-    const double* __restrict__ signals, int64_t v, const double* __restrict__ weights, TissueDev lr,
-    RidgeDev lr_solver, TissueDev hr, RidgeDev hr_solver, int max_rounds, double fraction_tol, double final_tol,
-    int* queue, double* __restrict__ workspace, size_t slot_size, int cmax, int ng_max,
-    double* __restrict__ fods, double* __restrict__ fractions_out, int32_t* __restrict__ rounds_out,
-    uint8_t* __restrict__ status) {
-    __shared__ WarpState states[kMtWarps];
+// One round's fractions of the listed voxels (cpp/src/sd/multi_tissue.cpp:100-125): f_iso(v)
+// takes the isotropic fractions; a voxel whose fractions all moved by less than fraction_tol, or
+// that used its last round, records its round count, the others join the next round's list
+// with their fractions kept for the next comparison.
+__global__ void __launch_bounds__(kMtWarps * 32, 8) lr_fractions_kernel(
+    TissueDev T, const double* __restrict__ signals, const double* __restrict__ fods, int ldf,
+    const int* __restrict__ list, int64_t count, int round, int max_rounds, double fraction_tol,
+    double* __restrict__ fiso, double* __restrict__ prev, int32_t* __restrict__ rounds, int* __restrict__ next,
+    int* next_count, int* queue, double* __restrict__ workspace, size_t slot_size) {
+    __shared__ FracState states[kMtWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    WarpState& st = states[warp];
-    Slot sl = carve(workspace + (size_t(blockIdx.x) * kMtWarps + warp) * slot_size, lr.m, cmax, ng_max);
-    const int m = lr.m, ci = lr.ci;
+    FracState& st = states[warp];
+    FracSlot sl = carve_frac(workspace + (size_t(blockIdx.x) * kMtWarps + warp) * slot_size, T.m, T.ca, 1 + T.ci);
+    const int ci = T.ci;
     for (;;) {
-        int64_t voxel = 0;
-        if (lane == 0) voxel = atomicAdd(queue, 1);
-        voxel = __shfl_sync(0xffffffffu, voxel, 0);
-        if (voxel >= v) break;
-        for (int i = lane; i < m; i += 32) {
-            const double s = signals[voxel * m + i];
-            sl.s[i] = s;
-            sl.ws[i] = s * weights[i];
-        }
-        if (lane < kMaxGroups) {
-            st.fiso[lane] = 0.0;
-            st.prev[lane] = INFINITY;
-        }
+        int64_t p = 0;
+        if (lane == 0) p = atomicAdd(queue, 1);
+        p = __shfl_sync(0xffffffffu, p, 0);
+        if (p >= count) break;
+        const int64_t voxel = listed(list, p);
+        fractions(T, fods + voxel * ldf, signals + voxel * T.m, false, -1.0, sl, st, lane);
+        // The first round has nothing to compare with (its previous fractions are infinite).
+        bool converged = round > 0;
+        for (int j = 0; j <= ci; ++j) converged &= fabs(st.fr[j] - prev[voxel * (ci + 1) + j]) < fraction_tol;
         __syncwarp();
-        bool ok = true;
-        int rounds = 0;
-        for (int round = 0; round < max_rounds; ++round) {
-            ++rounds;
-            for (int i = lane; i < m; i += 32) {
-                double r = 0.0;
-                for (int j = 0; j < ci; ++j) r += lr.wiso[size_t(i) * ci + j] * st.fiso[j];
-                sl.as[i] = fmax(sl.ws[i] - r, 0.0);
-            }
-            __syncwarp();
-            ok &= ridge_nnls(lr_solver, sl.as, sl, st, lane);
-            fractions(lr, sl.x, sl.s, false, -1.0, sl, st, lane);
-            bool converged = true;
-            for (int j = 0; j <= ci; ++j) converged &= fabs(st.fr[j] - st.prev[j]) < fraction_tol;
-            __syncwarp();
-            if (lane < ci) st.fiso[lane] = st.fr[1 + lane];
-            __syncwarp();
-            if (converged) break;
-            if (lane <= ci) st.prev[lane] = st.fr[lane];
-            __syncwarp();
-        }
-        for (int i = lane; i < m; i += 32) {
-            double r = 0.0;
-            for (int j = 0; j < ci; ++j) r += hr.wiso[size_t(i) * ci + j] * st.fiso[j];
-            sl.as[i] = fmax(sl.ws[i] - r, 0.0);
-        }
-        __syncwarp();
-        ok &= ridge_nnls(hr_solver, sl.as, sl, st, lane);
-        for (int j = lane; j < hr.ca; j += 32) fods[voxel * hr.ca + j] = sl.x[j];
-        __syncwarp();
-        fractions(hr, sl.x, sl.s, true, final_tol, sl, st, lane);
-        const int nf = hr.nb + ci;
-        double total = kFractionSumOffset;
-        for (int g = 0; g < nf; ++g) total += st.fr[g];
-        for (int g = lane; g < nf; g += 32) fractions_out[voxel * nf + g] = st.fr[g] / total;
-        if (lane == 0) {
-            if (rounds_out) rounds_out[voxel] = rounds;
-            if (status) status[voxel] = ok ? 0 : 1;
+        if (lane < ci) fiso[voxel * ci + lane] = st.fr[1 + lane];
+        if (converged || round + 1 >= max_rounds) {
+            if (lane == 0) rounds[voxel] = round + 1;
+        } else {
+            if (lane <= ci) prev[voxel * (ci + 1) + lane] = st.fr[lane];
+            if (lane == 0) next[atomicAdd(next_count, 1)] = int(voxel);
         }
         __syncwarp();
     }
 }
 
-__global__ void __launch_bounds__(kMtWarps * 32) single_tissue_kernel(
-    const double* __restrict__ signals, int64_t v, RidgeDev solver, int* queue, double* __restrict__ workspace,
-    size_t slot_size, int cmax, double* __restrict__ fods, uint8_t* __restrict__ status) {
-    __shared__ WarpState states[kMtWarps];
+// The final per-block fractions of every voxel, normalised to sum to 1 (+1e-16), with the round
+// counts and statuses (cpp/src/sd/multi_tissue.cpp:127-148).
+__global__ void __launch_bounds__(kMtWarps * 32, 8) hr_fractions_kernel(
+    TissueDev T, const double* __restrict__ signals, const double* __restrict__ fods, int64_t count,
+    double final_tol, const int32_t* __restrict__ rounds_in, const uint8_t* __restrict__ bad,
+    double* __restrict__ fractions_out, int32_t* __restrict__ rounds_out, uint8_t* __restrict__ status, int* queue,
+    double* __restrict__ workspace, size_t slot_size) {
+    __shared__ FracState states[kMtWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    WarpState& st = states[warp];
-    Slot sl = carve(workspace + (size_t(blockIdx.x) * kMtWarps + warp) * slot_size, solver.m, cmax, 1);
+    FracState& st = states[warp];
+    FracSlot sl = carve_frac(workspace + (size_t(blockIdx.x) * kMtWarps + warp) * slot_size, T.m, T.ca,
+                             T.nb + T.ci);
+    const int nf = T.nb + T.ci;
     for (;;) {
         int64_t voxel = 0;
         if (lane == 0) voxel = atomicAdd(queue, 1);
         voxel = __shfl_sync(0xffffffffu, voxel, 0);
-        if (voxel >= v) break;
-        for (int i = lane; i < solver.m; i += 32) sl.s[i] = signals[voxel * solver.m + i];
-        __syncwarp();
-        const bool ok = ridge_nnls(solver, sl.s, sl, st, lane);
-        for (int j = lane; j < solver.c; j += 32) fods[voxel * solver.c + j] = sl.x[j];
-        if (lane == 0 && status) status[voxel] = ok ? 0 : 1;
+        if (voxel >= count) break;
+        fractions(T, fods + voxel * T.ca, signals + voxel * T.m, true, final_tol, sl, st, lane);
+        double total = kFractionSumOffset;
+        for (int g = 0; g < nf; ++g) total += st.fr[g];
+        for (int g = lane; g < nf; g += 32) fractions_out[voxel * nf + g] = st.fr[g] / total;
+        if (lane == 0) {
+            if (rounds_out) rounds_out[voxel] = rounds_in[voxel];
+            if (status) status[voxel] = bad[voxel];
+        }
         __syncwarp();
     }
+}
+
+// ---- host side -------------------------------------------------------------------------
+
+// The warps of a persistent grid: as many as the SMs hold at once (or one per item), in whole
+// CTAs of kMtWarps.
+template <class Kernel>
+int64_t resident_slots(Kernel kernel, size_t smem, int64_t items) {
+    require(smem <= 200 * 1024, "the kernel has too many columns for the shared-memory solver");
+    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+               "cudaFuncSetAttribute");
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kMtWarps * 32, smem),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((items + kMtWarps - 1) / kMtWarps,
+                                                                  int64_t(sm_count()) * std::max(per_sm, 1)));
+    return blocks * kMtWarps;
+}
+
+// A bump allocator over one device buffer, 256-byte aligned pieces.
+struct Carver {
+    char* base;
+    size_t used = 0;
+    template <class T>
+    T* take(size_t n) {
+        T* p = reinterpret_cast<T*>(base ? base + used : nullptr);
+        used += (n * sizeof(T) + 255) / 256 * 256;
+        return p;
+    }
+};
+
+// Launches the ridge NNLS of `count` listed voxels on the instantiation that fits the solver.
+struct NnlsLaunch {
+    void (*kernel)(RidgeDev, SignalDev, const int*, int64_t, const double*, int, double*, int, uint8_t*, int*,
+                   double*, size_t);
+    int cap;
+};
+
+inline NnlsLaunch nnls_variant(int c) {
+    if (c <= 64) return {ridge_nnls_kernel<2, 2>, 64};
+    if (c <= 320) return {ridge_nnls_kernel<kCholCap / 32, 10>, kCholCap};
+    return {ridge_nnls_kernel<kCholCap / 32, kMaxColumns / 32>, kCholCap};
+}
+
+inline void launch_correlate(const SignalDev& S, const int* list, int64_t count, const RidgeDev& R, double* corr,
+                             int ldc, cudaStream_t st) {
+    if (count == 0) return;
+    const unsigned gx = unsigned((count + kCorrVoxels - 1) / kCorrVoxels);
+    if (R.c <= 48) {
+        correlate_kernel<3><<<dim3(gx, 1), 128, 0, st>>>(S, list, count, R.k, R.c, corr, ldc);
+    } else {
+        correlate_kernel<4><<<dim3(gx, unsigned((R.c + 63) / 64)), 128, 0, st>>>(S, list, count, R.k, R.c, corr, ldc);
+    }
+    cuda_check(cudaGetLastError(), "correlate_kernel launch");
 }
 
 }  // namespace
@@ -508,8 +649,14 @@ struct lar_fod_solver_s {
     lar::DeviceArray<double> k, gram;
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
+    int* pinned = nullptr;  // one host int the round loop reads the next round's count into
     ~lar_fod_solver_s() {
         if (scratch) cudaFree(scratch);
+        if (pinned) cudaFreeHost(pinned);
+    }
+    int* count_buffer() {
+        if (!pinned) lar::cuda_check(cudaMallocHost(&pinned, sizeof(int)), "cudaMallocHost");
+        return pinned;
     }
     lar::RidgeDev view() const {
         return lar::RidgeDev{int(host.m), int(host.c), host.ridge, tol, host.normal_equations ? 1 : 0, k.ptr, gram.ptr};
@@ -546,7 +693,7 @@ int lar_l2nnls_create(const double* k, int64_t m, int64_t c, double reg, double 
         require(reg >= 0.0, "reg must be at least 0");
         require(tol_x > 0.0, "tol_x must be positive");
         require(k != nullptr && m > 0 && c > 0, "k must be a non-empty (m, c) array");
-        require(c <= (int64_t(1) << 16) && m <= 4096, "the kernel is too large");
+        require(c <= 640 && m <= 4096, "the kernel has more than 640 directions or 4096 measurements");
         auto h = std::make_unique<lar_fod_solver_s>();
         h->host = host::prepare_ridge_design(k, m, c, reg);
         h->tol = tol_x;
@@ -612,23 +759,104 @@ int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights
         require(v >= 0, "v must be at least 0");
         if (v == 0) return;
         require(signals && fods && fractions, "signals, fods and fractions must not be NULL");
-        const int cmax = int(std::max(lr->ca, hr->ca));
-        const int ng = int(hr->nb + hr->ci);
-        const size_t slot = slot_doubles(int(m), cmax, std::max(ng, 2));
-        const int slots = int(std::max<int64_t>(kMtWarps, std::min<int64_t>((v + kMtWarps - 1) / kMtWarps * kMtWarps,
-                                                                            int64_t(sm_count()) * 8)));
-        const size_t head = 256 + ((size_t(m) * sizeof(double) + 255) / 256) * 256;
-        char* base = static_cast<char*>(hr_solver->reserve(head + size_t(slots) * slot * sizeof(double)));
+        const int mi = int(m), ci = int(lr->ci), c_lr = int(lr->ca), c_hr = int(hr->ca);
+        const int nf = int(hr->nb + hr->ci);
+        const int max_rounds = int(std::min<int64_t>(max_outer, 1 << 20));
+        const RidgeDev lrs = lr_solver->view(), hrs = hr_solver->view();
+        const TissueDev lrt = lr->view(), hrt = hr->view();
+        const NnlsLaunch lr_nnls = nnls_variant(c_lr), hr_nnls = nnls_variant(c_hr);
+        const size_t lr_smem = nnls_smem_bytes(c_lr, lr_nnls.cap) * kMtWarps;
+        const size_t hr_smem = nnls_smem_bytes(c_hr, hr_nnls.cap) * kMtWarps;
+        // Voxels per pass: the per-voxel state of a pass (correlations, the low-resolution FOD,
+        // f_iso and the previous fractions, two list entries, the round count and status) within
+        // 4 GiB.
+        const size_t per_voxel = (size_t(std::max(c_lr, c_hr)) + size_t(c_lr) + 2 * size_t(ci) + 1) * sizeof(double) +
+                                 3 * sizeof(int) + 1;
+        const int64_t n_max = std::min<int64_t>(v, std::max<int64_t>(4096, int64_t((size_t(4) << 30) / per_voxel)));
+        const int64_t lr_slots = resident_slots(lr_nnls.kernel, lr_smem, n_max);
+        const int64_t hr_slots = resident_slots(hr_nnls.kernel, hr_smem, n_max);
+        const int64_t lf_slots = resident_slots(lr_fractions_kernel, 0, n_max);
+        const int64_t hf_slots = resident_slots(hr_fractions_kernel, 0, n_max);
+        const size_t lr_slot = nnls_slot_doubles(mi, lr_nnls.cap), hr_slot = nnls_slot_doubles(mi, hr_nnls.cap);
+        const size_t lf_slot = frac_slot_doubles(mi, c_lr, 1 + ci), hf_slot = frac_slot_doubles(mi, c_hr, nf);
+        const size_t slot_doubles =
+            std::max(std::max(size_t(lr_slots) * lr_slot, size_t(hr_slots) * hr_slot),
+                     std::max(size_t(lf_slots) * lf_slot, size_t(hf_slots) * hf_slot));
+        struct Pieces {
+            int* counters;  // [0] the persistent kernels' work counter, [1] the next round's count
+            double* weights;
+            int* list[2];
+            double *fiso, *prev, *corr, *xlr, *slots;
+            int32_t* rounds;
+            uint8_t* bad;
+        };
+        auto carve_all = [&](Carver& cv) {
+            Pieces p;
+            p.counters = cv.take<int>(8);
+            p.weights = cv.take<double>(size_t(m));
+            p.list[0] = cv.take<int>(size_t(n_max));
+            p.list[1] = cv.take<int>(size_t(n_max));
+            p.fiso = cv.take<double>(size_t(n_max) * std::max(ci, 1));
+            p.prev = cv.take<double>(size_t(n_max) * (ci + 1));
+            p.corr = cv.take<double>(size_t(n_max) * std::max(c_lr, c_hr));
+            p.xlr = cv.take<double>(size_t(n_max) * c_lr);
+            p.rounds = cv.take<int32_t>(size_t(n_max));
+            p.bad = cv.take<uint8_t>(size_t(n_max));
+            p.slots = cv.take<double>(slot_doubles);
+            return p;
+        };
+        Carver sizing{nullptr};
+        carve_all(sizing);
+        Carver cv{static_cast<char*>(hr_solver->reserve(sizing.used))};
+        const Pieces P = carve_all(cv);
+        int* host_count = hr_solver->count_buffer();
         auto st = static_cast<cudaStream_t>(stream);
-        cuda_check(cudaMemsetAsync(base, 0, sizeof(int), st), "cudaMemsetAsync");
-        double* dweights = reinterpret_cast<double*>(base + 256);
-        cuda_check(cudaMemcpyAsync(dweights, weights, size_t(m) * sizeof(double), cudaMemcpyHostToDevice, st),
+        cuda_check(cudaMemcpyAsync(P.weights, weights, size_t(m) * sizeof(double), cudaMemcpyHostToDevice, st),
                    "cudaMemcpyAsync (weights)");
-        multi_tissue_kernel<<<slots / kMtWarps, kMtWarps * 32, 0, st>>>(
-            signals, v, dweights, lr->view(), lr_solver->view(), hr->view(), hr_solver->view(),
-            int(std::min<int64_t>(max_outer, 1 << 20)), fraction_tol, final_tol_x, reinterpret_cast<int*>(base),
-            reinterpret_cast<double*>(base + head), slot, cmax, std::max(ng, 2), fods, fractions, rounds, status);
-        cuda_check(cudaGetLastError(), "multi_tissue_kernel launch");
+        auto blocks = [](int64_t slots, int64_t count) {
+            return unsigned(std::max<int64_t>(1, std::min<int64_t>(slots / kMtWarps, (count + kMtWarps - 1) / kMtWarps)));
+        };
+        auto reset_queue = [&] { cuda_check(cudaMemsetAsync(P.counters, 0, sizeof(int), st), "cudaMemsetAsync"); };
+        for (int64_t v0 = 0; v0 < v; v0 += n_max) {
+            const int64_t n = std::min(n_max, v - v0);
+            const double* sig = signals + v0 * m;
+            if (ci > 0) cuda_check(cudaMemsetAsync(P.fiso, 0, size_t(n) * ci * sizeof(double), st), "cudaMemsetAsync");
+            cuda_check(cudaMemsetAsync(P.rounds, 0, size_t(n) * sizeof(int32_t), st), "cudaMemsetAsync");
+            cuda_check(cudaMemsetAsync(P.bad, 0, size_t(n), st), "cudaMemsetAsync");
+            const SignalDev lr_sig{sig, P.weights, lrt.wiso, P.fiso, mi, ci};
+            const int* cur = nullptr;  // the first round takes every voxel
+            int* nxt = P.list[0];
+            int64_t count = n;
+            for (int round = 0; round < max_rounds && count > 0; ++round) {
+                launch_correlate(lr_sig, cur, count, lrs, P.corr, c_lr, st);
+                cuda_check(cudaMemsetAsync(P.counters, 0, 2 * sizeof(int), st), "cudaMemsetAsync");
+                lr_nnls.kernel<<<blocks(lr_slots, count), kMtWarps * 32, lr_smem, st>>>(
+                    lrs, lr_sig, cur, count, P.corr, c_lr, P.xlr, c_lr, P.bad, P.counters, P.slots, lr_slot);
+                cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
+                reset_queue();
+                lr_fractions_kernel<<<blocks(lf_slots, count), kMtWarps * 32, 0, st>>>(
+                    lrt, sig, P.xlr, c_lr, cur, count, round, max_rounds, fraction_tol, P.fiso, P.prev, P.rounds, nxt,
+                    P.counters + 1, P.counters, P.slots, lf_slot);
+                cuda_check(cudaGetLastError(), "lr_fractions_kernel launch");
+                cuda_check(cudaMemcpyAsync(host_count, P.counters + 1, sizeof(int), cudaMemcpyDeviceToHost, st),
+                           "cudaMemcpyAsync (round count)");
+                cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+                count = *host_count;
+                cur = nxt;
+                nxt = nxt == P.list[0] ? P.list[1] : P.list[0];
+            }
+            const SignalDev hr_sig{sig, P.weights, hrt.wiso, P.fiso, mi, ci};
+            launch_correlate(hr_sig, nullptr, n, hrs, P.corr, c_hr, st);
+            reset_queue();
+            hr_nnls.kernel<<<blocks(hr_slots, n), kMtWarps * 32, hr_smem, st>>>(
+                hrs, hr_sig, nullptr, n, P.corr, c_hr, fods + v0 * c_hr, c_hr, P.bad, P.counters, P.slots, hr_slot);
+            cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
+            reset_queue();
+            hr_fractions_kernel<<<blocks(hf_slots, n), kMtWarps * 32, 0, st>>>(
+                hrt, sig, fods + v0 * c_hr, n, final_tol_x, P.rounds, P.bad, fractions + v0 * nf,
+                rounds ? rounds + v0 : nullptr, status ? status + v0 : nullptr, P.counters, P.slots, hf_slot);
+            cuda_check(cudaGetLastError(), "hr_fractions_kernel launch");
+        }
         // The weights' host buffer is the caller's; the copy must finish before it returns.
         cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
     });
@@ -642,16 +870,35 @@ int lar_fit_single_tissue(const double* signals, int64_t v, lar_fod_solver solve
         if (v == 0) return;
         require(signals && fods, "signals and fods must not be NULL");
         const int m = int(solver->host.m), c = int(solver->host.c);
-        const size_t slot = slot_doubles(m, c, 2);
-        const int slots = int(std::max<int64_t>(kMtWarps, std::min<int64_t>((v + kMtWarps - 1) / kMtWarps * kMtWarps,
-                                                                            int64_t(sm_count()) * 8)));
-        char* base = static_cast<char*>(solver->reserve(256 + size_t(slots) * slot * sizeof(double)));
+        const RidgeDev R = solver->view();
+        const NnlsLaunch nn = nnls_variant(c);
+        const size_t smem = nnls_smem_bytes(c, nn.cap) * kMtWarps;
+        const int64_t n_max = std::min<int64_t>(v, std::max<int64_t>(4096, int64_t((size_t(2) << 30) / (size_t(c) * 8))));
+        const int64_t slots = resident_slots(nn.kernel, smem, n_max);
+        const size_t slot = nnls_slot_doubles(m, nn.cap);
+        auto carve_all = [&](Carver& cv, int*& counters, double*& corr, double*& work) {
+            counters = cv.take<int>(8);
+            corr = cv.take<double>(size_t(n_max) * c);
+            work = cv.take<double>(size_t(slots) * slot);
+        };
+        int* counters = nullptr;
+        double *corr = nullptr, *work = nullptr;
+        Carver sizing{nullptr};
+        carve_all(sizing, counters, corr, work);
+        Carver cv{static_cast<char*>(solver->reserve(sizing.used))};
+        carve_all(cv, counters, corr, work);
         auto st = static_cast<cudaStream_t>(stream);
-        cuda_check(cudaMemsetAsync(base, 0, sizeof(int), st), "cudaMemsetAsync");
-        single_tissue_kernel<<<slots / kMtWarps, kMtWarps * 32, 0, st>>>(
-            signals, v, solver->view(), reinterpret_cast<int*>(base), reinterpret_cast<double*>(base + 256), slot, c,
-            fods, status);
-        cuda_check(cudaGetLastError(), "single_tissue_kernel launch");
+        for (int64_t v0 = 0; v0 < v; v0 += n_max) {
+            const int64_t n = std::min(n_max, v - v0);
+            const SignalDev S{signals + v0 * m, nullptr, nullptr, nullptr, m, 0};
+            launch_correlate(S, nullptr, n, R, corr, c, st);
+            if (status) cuda_check(cudaMemsetAsync(status + v0, 0, size_t(n), st), "cudaMemsetAsync");
+            cuda_check(cudaMemsetAsync(counters, 0, sizeof(int), st), "cudaMemsetAsync");
+            const unsigned nb = unsigned(std::max<int64_t>(1, std::min<int64_t>(slots / kMtWarps, (n + kMtWarps - 1) / kMtWarps)));
+            nn.kernel<<<nb, kMtWarps * 32, smem, st>>>(R, S, nullptr, n, corr, c, fods + v0 * c, c,
+                                                       status ? status + v0 : nullptr, counters, work, slot);
+            cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
+        }
     });
 }
 

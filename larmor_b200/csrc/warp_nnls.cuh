@@ -246,16 +246,28 @@ __device__ inline int warp_nnls_explicit(const double* __restrict__ c, int rows,
         __syncwarp();
         double bv = 0.0;
         int bi = -1;
-        for (int j = lane; j < m; j += 32) {
-            if (s.flag[j]) continue;
-            double g = 0.0;
-            for (int r = 0; r < rows; ++r) g += c[size_t(r) * m + j] * s.res[r];
-            if (bi < 0 || g > bv) { bv = g; bi = j; }
-        }
-        const int e = warp_argmax_first(bv, bi);
+        int e = -1;
         double ge = 0.0;
-        if (e >= 0)
-            for (int r = 0; r < rows; ++r) ge += c[size_t(r) * m + e] * s.res[r];
+        if (m <= 8) {
+            // Few columns of many rows: lanes split the rows, one reduction per column.
+            for (int j = 0; j < m; ++j) {
+                double g = 0.0;
+                for (int r = lane; r < rows; r += 32) g += c[size_t(r) * m + j] * s.res[r];
+                g = warp_sum(g);
+                if (!s.flag[j] && (bi < 0 || g > bv)) { bv = g; bi = j; }
+            }
+            e = bi;
+            ge = bv;
+        } else {
+            for (int j = lane; j < m; j += 32) {
+                if (s.flag[j]) continue;
+                double g = 0.0;
+                for (int r = 0; r < rows; ++r) g += c[size_t(r) * m + j] * s.res[r];
+                if (bi < 0 || g > bv) { bv = g; bi = j; }
+            }
+            e = warp_argmax_first(bv, bi);
+            ge = e >= 0 ? __shfl_sync(0xffffffffu, bv, e & 31) : 0.0;
+        }
         if (e < 0 || ge <= tol) return 1;
         if (na >= s.acap) return -1;
         __syncwarp();

@@ -158,3 +158,35 @@ def mfod_volume(seed: int = 3, shape=(110, 110, 70), radius: float = 1.0435) -> 
     gtab = mfod_table(rng)
     signals = mfod_signals(rng, gtab, int(mask.sum()))
     return Workload(Volume(_fill(shape, mask, signals), np.eye(4)), gtab, mask, "mfod")
+
+
+def mfod_responses(s0: float = 1000.0):
+    """ZonalSHRF responses (WM, GM, CSF) of the mFOD generator's tissues on its shells: the WM
+    profile of one stick-zeppelin fibre projected on the zonal SH by Gauss-Legendre quadrature,
+    as the reference's tests build a tensor response (tests/sd/test_msmt.py:41-58)."""
+    from larmor_b200.sd.rf import ZonalSHRF
+    from larmor_b200.sd.sh import build_basis_matrix
+
+    shells = np.array([0.0, 1000.0, 2000.0, 3000.0])
+    nodes, weights = np.polynomial.legendre.leggauss(64)
+    theta = np.arccos(nodes)
+    zonal = build_basis_matrix(theta, np.zeros_like(theta), 8)[:, [0, 3, 10, 21, 36]]
+    rows = []
+    for b in shells:
+        cos2 = nodes**2
+        stick = np.exp(-b * 1.7e-3 * cos2)
+        zep = np.exp(-b * (0.5e-3 + (1.7e-3 - 0.5e-3) * cos2))
+        profile = s0 * (0.6 * stick + 0.4 * zep)
+        rows.append(2 * np.pi * (weights * profile) @ zonal)
+    wm = ZonalSHRF(bvals=shells, coefficients=np.array(rows))
+    gm = ZonalSHRF(bvals=shells, coefficients=np.sqrt(4 * np.pi) * (s0 * np.exp(-shells * 0.8e-3))[:, None])
+    csf = ZonalSHRF(bvals=shells, coefficients=np.sqrt(4 * np.pi) * (s0 * np.exp(-shells * 3e-3))[:, None])
+    return [wm, gm, csf]
+
+
+def mfod_model_responses():
+    """The SDModel responses of the mFOD workload: the WM tensor of the single fibre
+    (AnisotropicRF), GM and CSF isotropic."""
+    from larmor_b200.sd.rf import AnisotropicRF, IsotropicRF
+
+    return [AnisotropicRF([1.7e-3, 0.2e-3, 0.2e-3], 0.0), IsotropicRF(0.8e-3), IsotropicRF(3e-3)]

@@ -65,7 +65,16 @@ def test_single_tissue_l2nnls_matches_the_oracle(cuda, oracle, mfod_fixture, rid
     fods = _core.fit_single_tissue(np.ascontiguousarray(signals), solver, 1)
     ref = oracle.ridge_nnls(k, ridge, 1e-6, signals, n_threads=4)
     np.testing.assert_array_equal(fods != 0, ref != 0)
-    assert (np.abs(fods - ref) <= 1e-9 * np.abs(ref).max(axis=1, keepdims=True)).all()
+    # Values to the forward error of an FP64 normal-equations solve, 10 cond(G_AA) eps of the
+    # largest coefficient (cond(G_AA) reaches 8e6 here without the ridge; both fits carry that
+    # error, in different rounding).
+    gram = k.T @ k + ridge**2 * np.eye(k.shape[1])
+    for v in range(signals.shape[0]):
+        act = np.nonzero(ref[v])[0]
+        if len(act) == 0:
+            continue
+        tol = 10 * np.linalg.cond(gram[np.ix_(act, act)]) * np.finfo(np.float64).eps
+        assert np.abs(fods[v] - ref[v]).max() <= max(tol, 1e-9) * np.abs(ref[v]).max()
 
 
 def test_sd_model_three_tissue_matches_the_oracle(cuda, oracle):
