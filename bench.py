@@ -120,7 +120,7 @@ class DtiWorkload:
     """Config 1: DTI WLLS on the 64x64x40 volume (79,912 voxels, 1 b0 + 30 directions)."""
 
     name = "dti_wlls_64x64x40"
-    kernel = "fit_dti_maps_kernel"
+    kernels = ("fit_dti_maps_kernel",)
     has_fp32 = True
     # Algorithmic bytes per voxel: 31 float32 samples in, 16 float32 maps + 1 byte out
     # (the 8-byte floor per voxel is host-prepared input too).
@@ -161,6 +161,10 @@ class DtiWorkload:
         _core.fit_dti_maps_device(self.handle, self.d_signals, self.d_floor, True, self.d_maps,
                                   self.d_npd, precision=precision)
 
+    def kernel_bytes(self) -> dict:
+        """Algorithmic DRAM bytes of one step, per kernel (all its launches in the step)."""
+        return {"fit_dti_maps_kernel": self.bytes_per_voxel * self.v}
+
     def step_e2e(self):
         from larmor_b200 import _core
 
@@ -187,7 +191,7 @@ class DkiWorkload:
     """Config 2: constrained DKI WLLS on the 96x96x60 volume (199,768 voxels, 6 b0 + 2 x 64)."""
 
     name = "dki_wlls_96x96x60"
-    kernel = "fit_log_warp_kernel"
+    kernels = ("fit_log_warp_kernel", "constrained_fit_kernel", "dki_maps_kernel")
     has_fp32 = True
     # 134 float32 samples + S0 and floor (double) in; 36 float32 maps + npd + broke out.
     bytes_per_voxel = 4 * 134 + 16 + 36 * 4 + 2
@@ -234,6 +238,18 @@ class DkiWorkload:
             self.handle.handle, _lib.ptr(self.d_signals), _lib.ptr(self.d_s0), _lib.ptr(self.d_floor),
             _lib.ptr(self.d_b0), self.v, 1, 20, 1e-6, precision, _lib.ptr(self.d_maps), _lib.ptr(self.d_npd),
             _lib.ptr(self.d_broke), _lib.ptr(self.d_params), _core._stream(self.torch)))
+
+    def kernel_bytes(self) -> dict:
+        """Algorithmic DRAM bytes of one step, per kernel: the IRLS fit reads the float32
+        signals, S0 and floor and writes the parameters and broke flags; the constrained re-fit
+        reads the same inputs and the listed parameters of each violator and writes its
+        parameters; the maps read the parameters and write 36 float32 maps and npd."""
+        self.torch.cuda.synchronize()
+        n_viol = self.handle.violators()
+        inputs = 4 * 134 + 16
+        return {"fit_log_warp_kernel": self.v * (inputs + 22 * 8 + 1),
+                "constrained_fit_kernel": n_viol * (inputs + 2 * 22 * 8),
+                "dki_maps_kernel": self.v * (22 * 8 + 36 * 4 + 1)}
 
     def step_e2e(self):
         self.d_signals.copy_(self.h_signals, non_blocking=True)
@@ -283,7 +299,8 @@ class MfodWorkload(_SdWorkloadBase):
     (44 in the loop) + GM + CSF, up to 50 rounds, on S0-normalised signals."""
 
     name = "mfod_3tissue_110x110x70"
-    kernel = "multi_tissue_kernel"
+    kernels = ("correlate_kernel", "ridge_nnls_kernel<2,2>", "lr_fractions_kernel", "ridge_nnls_kernel<8,10>",
+               "hr_fractions_kernel")
     has_fp32 = False
     # 280 double samples in, 300 double amplitudes + 3 fractions out.
     bytes_per_voxel = 8 * 280 + 8 * 303
@@ -328,6 +345,25 @@ class MfodWorkload(_SdWorkloadBase):
         _core.fit_multi_tissue_device(self.d_signals, self.lr.weights, self.k_lr, self.lr_solver, self.k_hr,
                                       self.hr_solver, 50, 1e-7, 1e-2, self.d_fods, self.d_fr)
 
+    def kernel_bytes(self) -> dict:
+        """Algorithmic DRAM bytes of one step, per kernel. A voxel-round of the low-resolution
+        loop correlates the 280 signals (read) into 44 correlations (written), whose NNLS reads
+        them and writes 44 amplitudes, whose fractions read those and the signals and write 3
+        fractions; the high-resolution pass does the same with 300 directions once per voxel."""
+        from larmor_b200 import _core
+
+        torch = self.torch
+        rounds = torch.zeros((self.v,), dtype=torch.int32, device=self.d_signals.device)
+        _core.fit_multi_tissue_device(self.d_signals, self.lr.weights, self.k_lr, self.lr_solver, self.k_hr,
+                                      self.hr_solver, 50, 1e-7, 1e-2, self.d_fods, self.d_fr, rounds=rounds)
+        vr = int(rounds.sum().item())
+        m, c_lr, c_hr = 280, self.k_lr.ca, self.k_hr.ca
+        return {"correlate_kernel": vr * 8 * (m + c_lr) + self.v * 8 * (m + c_hr),
+                "ridge_nnls_kernel<2,2>": vr * 8 * 2 * c_lr,
+                "lr_fractions_kernel": vr * 8 * (c_lr + m + 3),
+                "ridge_nnls_kernel<8,10>": self.v * 8 * 2 * c_hr,
+                "hr_fractions_kernel": self.v * 8 * (c_hr + m + 3)}
+
     def step_e2e(self):
         self.d_signals.copy_(self.h_signals, non_blocking=True)
         self.step_device()
@@ -353,7 +389,7 @@ class MsmtWorkload(_SdWorkloadBase):
     constraints (300 directions + 2) per voxel."""
 
     name = "msmt_csd_lsi_110x110x70"
-    kernel = "lsi_kernel"
+    kernels = ("lsi_kernel",)
     has_fp32 = False
     bytes_per_voxel = 8 * 280 + 8 * 47 + 1
 
@@ -382,6 +418,10 @@ class MsmtWorkload(_SdWorkloadBase):
         from larmor_b200 import _core
 
         _core.fit_lsi_device(self.design, self.d_signals, self.d_x, self.d_conv)
+
+    def kernel_bytes(self) -> dict:
+        """Algorithmic DRAM bytes of one step: 280 signals in, 47 coefficients and a flag out."""
+        return {"lsi_kernel": self.bytes_per_voxel * self.v}
 
     def step_e2e(self):
         self.d_signals.copy_(self.h_signals, non_blocking=True)
@@ -511,9 +551,16 @@ def main() -> int:
     gpu_index = dev.index if dev.index is not None else 0
     visible = os.environ.get("CUDA_VISIBLE_DEVICES")
     smi_index = int(visible.split(",")[gpu_index]) if visible and visible.split(",")[gpu_index].isdigit() else gpu_index
+    from larmor_b200 import _core
+
+    _core.kernel_timing(True)
+    launches0 = _core.launch_count()
     with ClockSampler(smi_index) as clocks:
         dev_ms = timed(wl.step_device, args.steps)
     barrier()
+    launches = _core.launch_count() - launches0
+    kernel_ms = {name: _core.kernel_time(name) for name in wl.kernels}
+    _core.kernel_timing(False)
     dev_ms = max_over_ranks(dev_ms)
 
     # The plain FP32 kernel, for comparison.
@@ -532,10 +579,16 @@ def main() -> int:
 
     voxels_all = wl.v * world
     value = voxels_all * args.steps / (dev_ms / 1e3)
-    avg_launch_s = dev_ms / args.steps / 1e3
     pk, pk_kind = peaks()
-    achieved_gbs = wl.bytes_per_voxel * wl.v / avg_launch_s / 1e9
-    traffic = committed_traffic(wl.kernel, wl.name)
+    # The dominant kernel: the most device time in the timed region (CUDA events on its stream).
+    step_bytes = wl.kernel_bytes()
+    top = max(kernel_ms, key=lambda k: kernel_ms[k][0])
+    top_ms, top_launches = kernel_ms[top]
+    avg_launch_s = top_ms / max(top_launches, 1) / 1e3
+    bytes_per_launch = step_bytes[top] * args.steps / max(top_launches, 1)
+    achieved_gbs = bytes_per_launch / avg_launch_s / 1e9
+    traffic = committed_traffic(top, wl.name)
+    total_kernel_ms = max(sum(t for t, _ in kernel_ms.values()), 1e-30)
 
     cpu = None
     if rank == 0:
@@ -551,15 +604,17 @@ def main() -> int:
         "data": "synthetic", "config": wl.config,
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved_gbs / pk["hbm_gbs"], "traffic": traffic,
-                     "kernel": wl.kernel, "peak_source": pk_kind,
-                     "algorithmic_bytes_per_voxel": wl.bytes_per_voxel},
+                     "kernel": top, "peak_source": pk_kind,
+                     "algorithmic_bytes_per_launch": bytes_per_launch,
+                     "avg_launch_ms": avg_launch_s * 1e3, "launches": top_launches,
+                     "kernel_share": {k: round(t / total_kernel_ms, 4) for k, (t, _) in kernel_ms.items()}},
         "cpu_baseline": cpu,
         "e2e": {"value": voxels_all * args.steps / (e2e_ms / 1e3), "unit": "voxel fits/s",
                 "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes},
         "plain_fp32": None if fp32_ms is None else {
             "value": voxels_all * args.steps / (fp32_ms / 1e3), "unit": "voxel fits/s",
             "ms_per_step": fp32_ms / args.steps},
-        "gpu_launches": args.steps,
+        "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
     if rank == 0:

@@ -52,6 +52,21 @@ const char* lar_last_error(void);
 /* Library version string. */
 const char* lar_version(void);
 
+/* ---- Launch accounting ----------------------------------------------------------------
+ * No counterpart in the reference (its fits run on host threads). Every kernel launch of the
+ * library is counted; with timing on, each is bracketed by CUDA events on its stream so that a
+ * benchmark can time one kernel of a multi-kernel call. */
+
+/* Kernels the library has launched since it was loaded. */
+int64_t lar_launch_count(void);
+
+/* Turns per-kernel event timing on (enable != 0) or off; either way clears the records. */
+int lar_kernel_timing(int enable);
+
+/* Total device time (ms) and number of the timed launches of kernel `name` (as the library
+ * names it, e.g. "lsi_kernel", "ridge_nnls_kernel<2,2>"); waits for their events. */
+int lar_kernel_time(const char* name, double* total_ms, int64_t* launches);
+
 /* ---- Log-signal fits (DTI, DKI) ------------------------------------------------------- */
 
 typedef struct lar_log_design_s* lar_log_design;
@@ -62,6 +77,11 @@ typedef struct lar_log_design_s* lar_log_design;
 int lar_log_design_create(const double* x, int64_t n, int64_t p, const double* g, int64_t m,
                           lar_log_design* out);
 void lar_log_design_destroy(lar_log_design design);
+
+/* The number of voxels of the last constrained fit on this design whose fit broke a
+ * constraint and took the constrained re-fit (0 without constraints). Read it after that
+ * call's stream has finished. A diagnostic with no counterpart in the reference. */
+int lar_log_design_violators(lar_log_design design, int64_t* count);
 
 /* Fits each row of log_s (v, n) (device) by least squares on the design: ordinary, or
  * weighted by the predicted signal iterated until no predicted log signal changes by more than

@@ -118,6 +118,13 @@ class LogDesign:
             except Exception:  # interpreter shutdown
                 pass
 
+    def violators(self) -> int:
+        """Voxels of the last constrained fit on this design that took the constrained re-fit
+        (read after that fit's stream has finished)."""
+        n = ctypes.c_int64(0)
+        _lib.check(_lib.lib().lar_log_design_violators(self._handle, ctypes.byref(n)))
+        return n.value
+
     @classmethod
     def cached(cls, x: np.ndarray, g: np.ndarray) -> LogDesign:
         x = np.ascontiguousarray(x, dtype=np.float64)
@@ -410,3 +417,22 @@ def fit_single_tissue(signals, solver: FodSolver, n_threads):
         _lib.check(_lib.lib().lar_fit_single_tissue(_lib.ptr(s), v, solver.handle, _lib.ptr(fods), None,
                                                     _stream(torch)))
     return fods.cpu().numpy()
+
+
+# ---- launch accounting (benchmarks) ------------------------------------------------------
+
+def launch_count() -> int:
+    """Kernels the library has launched since it was loaded."""
+    return int(_lib.lib().lar_launch_count())
+
+
+def kernel_timing(enable: bool) -> None:
+    """Turns per-kernel CUDA-event timing on or off (clearing the records either way)."""
+    _lib.check(_lib.lib().lar_kernel_timing(int(bool(enable))))
+
+
+def kernel_time(name: str) -> tuple[float, int]:
+    """(total ms, launches) of the timed launches of one kernel; waits for their events."""
+    ms, n = ctypes.c_double(0.0), ctypes.c_int64(0)
+    _lib.check(_lib.lib().lar_kernel_time(name.encode(), ctypes.byref(ms), ctypes.byref(n)))
+    return ms.value, n.value

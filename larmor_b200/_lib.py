@@ -20,8 +20,12 @@ _f64 = _c.c_double
 SIGNATURES: dict[str, tuple] = {
     "lar_last_error": (_c.c_char_p, []),
     "lar_version": (_c.c_char_p, []),
+    "lar_launch_count": (_i64, []),
+    "lar_kernel_timing": (_i32, [_i32]),
+    "lar_kernel_time": (_i32, [_c.c_char_p, _p, _p]),
     "lar_log_design_create": (_i32, [_p, _i64, _i64, _p, _i64, _p]),
     "lar_log_design_destroy": (None, [_p]),
+    "lar_log_design_violators": (_i32, [_p, _p]),
     "lar_fit_log_signal": (_i32, [_p, _p, _i64, _i32, _i64, _f64, _i32, _p, _p, _p, _p]),
     "lar_fit_dti_maps": (_i32, [_p, _p, _p, _i64, _i32, _i64, _f64, _i32, _p, _p, _p, _p]),
     "lar_dki_maps": (_i32, [_p, _i64, _p, _p, _p]),

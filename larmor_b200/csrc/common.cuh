@@ -70,6 +70,19 @@ struct DeviceArray {
     }
 };
 
+// Launch accounting: every kernel launch of the library is made inside a LaunchScope, which
+// counts it and, while kernel timing is on (lar_kernel_timing), brackets it with CUDA events
+// on its stream.
+struct LaunchScope {
+    LaunchScope(const char* name, cudaStream_t stream);
+    ~LaunchScope();
+    LaunchScope(const LaunchScope&) = delete;
+    LaunchScope& operator=(const LaunchScope&) = delete;
+    const char* name;
+    cudaStream_t stream;
+    cudaEvent_t start = nullptr;
+};
+
 inline int sm_count() {
     int dev = 0, n = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");

@@ -243,6 +243,7 @@ void launch_constrained(const LogDesignDevice<double>& d, const Src& src, int we
                         double* workspace, int slots, double* params, cudaStream_t stream) {
     require(d.p + 1 <= 32, "the constrained fit takes at most 31 parameters");
     const int blocks = std::max(1, slots / kCWarps);
+    LaunchScope scope("constrained_fit_kernel", stream);
     constrained_fit_kernel<Src><<<blocks, kCWarps * 32, 0, stream>>>(
         d, src, weighted, list, queue, workspace, constrained_slot_doubles(d.n, d.p, d.m), params);
     cuda_check(cudaGetLastError(), "constrained_fit_kernel launch");

@@ -237,6 +237,7 @@ void launch_dki_maps(const double* params, int64_t v, float* maps, uint8_t* npd,
     if (v == 0) return;
     const KaQuadrature quad = ka_quadrature();
     const int64_t grid = (v + 127) / 128;
+    LaunchScope scope("dki_maps_kernel", stream);
     dki_maps_kernel<<<unsigned(grid), 128, 0, stream>>>(params, v, quad, maps, npd);
     cuda_check(cudaGetLastError(), "dki_maps_kernel launch");
 }

@@ -346,6 +346,7 @@ void launch_fit(lar_log_design_s* h, const double* log_s, int64_t v, int weighte
         auto kernel = fit_log_small_kernel<T, 7, kSmallBlock, LogSource>;
         set_smem(kernel, sm);
         const int64_t grid = (v + kSmallBlock - 1) / kSmallBlock;
+        LaunchScope scope("fit_log_small_kernel", stream);
         kernel<<<unsigned(grid), kSmallBlock, sm, stream>>>(d, src, v, weighted, max_rw, T(tol), params,
                                                             broke, iterations);
         cuda_check(cudaGetLastError(), "fit_log_small_kernel launch");
@@ -364,6 +365,7 @@ void launch_dti_maps(const lar_log_design_s* h, const float* s, const double* fl
     auto kernel = fit_dti_maps_kernel<T, kSmallBlock>;
     set_smem(kernel, sm);
     const int64_t grid = (v + kSmallBlock - 1) / kSmallBlock;
+    LaunchScope scope("fit_dti_maps_kernel", stream);
     kernel<<<unsigned(grid), kSmallBlock, sm, stream>>>(d, src, v, weighted, max_rw, T(tol), maps, npd, params);
     cuda_check(cudaGetLastError(), "fit_dti_maps_kernel launch");
 }
@@ -430,6 +432,17 @@ int lar_log_design_create(const double* x, int64_t n, int64_t p, const double* g
 }
 
 void lar_log_design_destroy(lar_log_design design) { delete design; }
+
+int lar_log_design_violators(lar_log_design design, int64_t* count) {
+    return guarded([&] {
+        require(design != nullptr && count != nullptr, "design and count must not be NULL");
+        int n = 0;
+        if (design->host.m > 0 && design->scratch.base != nullptr)
+            cuda_check(cudaMemcpy(&n, design->scratch.base, sizeof(int), cudaMemcpyDeviceToHost),
+                       "cudaMemcpy (violator count)");
+        *count = n;
+    });
+}
 
 int lar_fit_log_signal(lar_log_design design, const double* log_s, int64_t v, int weighted,
                        int64_t max_iter, double tol, int precision, double* params,

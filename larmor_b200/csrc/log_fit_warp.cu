@@ -233,6 +233,7 @@ void launch_warp_impl(const LogDesignDevice<T>& d, const Src& src, int64_t v, in
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     const int64_t need = (v + kWarps - 1) / kWarps;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sm_count()) * std::max(per_sm, 1) * 4));
+    LaunchScope scope("fit_log_warp_kernel", stream);
     kernel<<<unsigned(grid), kWarps * 32, smem, stream>>>(d, src, v, weighted, max_rw, T(tol), params, broke,
                                                           iterations, violators);
     cuda_check(cudaGetLastError(), "fit_log_warp_kernel launch");

@@ -445,7 +445,8 @@ int lar_fit_lsi(lar_lsi_design design, const double* signals, int64_t v, int onl
         cuda_check(cudaMemsetAsync(base, 0, sizeof(int), st), "cudaMemsetAsync");
         LsiDevice D{int(h.m), int(h.n), int(h.k), design->qt.ptr, design->back.ptr, design->et.ptr,
                     design->e.ptr, design->gram.ptr, design->abs_sums.ptr};
-        lsi_kernel<<<unsigned(blocks), kLsiWarps * 32, smem, st>>>(
+        LaunchScope scope("lsi_kernel", st);
+    lsi_kernel<<<unsigned(blocks), kLsiWarps * 32, smem, st>>>(
             D, signals, v, only_qr, reinterpret_cast<int*>(base), cap, reinterpret_cast<double*>(base + 256), slot,
             x, converged, status, outer, active);
         cuda_check(cudaGetLastError(), "lsi_kernel launch");

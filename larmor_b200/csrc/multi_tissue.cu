@@ -618,18 +618,20 @@ struct NnlsLaunch {
     void (*kernel)(RidgeDev, SignalDev, const int*, int64_t, const double*, int, double*, int, uint8_t*, int*,
                    double*, size_t);
     int cap;
+    const char* name;
 };
 
 inline NnlsLaunch nnls_variant(int c) {
-    if (c <= 64) return {ridge_nnls_kernel<2, 2>, 64};
-    if (c <= 320) return {ridge_nnls_kernel<kCholCap / 32, 10>, kCholCap};
-    return {ridge_nnls_kernel<kCholCap / 32, kMaxColumns / 32>, kCholCap};
+    if (c <= 64) return {ridge_nnls_kernel<2, 2>, 64, "ridge_nnls_kernel<2,2>"};
+    if (c <= 320) return {ridge_nnls_kernel<kCholCap / 32, 10>, kCholCap, "ridge_nnls_kernel<8,10>"};
+    return {ridge_nnls_kernel<kCholCap / 32, kMaxColumns / 32>, kCholCap, "ridge_nnls_kernel<8,20>"};
 }
 
 inline void launch_correlate(const SignalDev& S, const int* list, int64_t count, const RidgeDev& R, double* corr,
                              int ldc, cudaStream_t st) {
     if (count == 0) return;
     const unsigned gx = unsigned((count + kCorrVoxels - 1) / kCorrVoxels);
+    LaunchScope scope("correlate_kernel", st);
     if (R.c <= 48) {
         correlate_kernel<3><<<dim3(gx, 1), 128, 0, st>>>(S, list, count, R.k, R.c, corr, ldc);
     } else {
@@ -830,14 +832,20 @@ int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights
             for (int round = 0; round < max_rounds && count > 0; ++round) {
                 launch_correlate(lr_sig, cur, count, lrs, P.corr, c_lr, st);
                 cuda_check(cudaMemsetAsync(P.counters, 0, 2 * sizeof(int), st), "cudaMemsetAsync");
-                lr_nnls.kernel<<<blocks(lr_slots, count), kMtWarps * 32, lr_smem, st>>>(
-                    lrs, lr_sig, cur, count, P.corr, c_lr, P.xlr, c_lr, P.bad, P.counters, P.slots, lr_slot);
-                cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
+                {
+                    LaunchScope scope(lr_nnls.name, st);
+                    lr_nnls.kernel<<<blocks(lr_slots, count), kMtWarps * 32, lr_smem, st>>>(
+                        lrs, lr_sig, cur, count, P.corr, c_lr, P.xlr, c_lr, P.bad, P.counters, P.slots, lr_slot);
+                    cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
+                }
                 reset_queue();
-                lr_fractions_kernel<<<blocks(lf_slots, count), kMtWarps * 32, 0, st>>>(
-                    lrt, sig, P.xlr, c_lr, cur, count, round, max_rounds, fraction_tol, P.fiso, P.prev, P.rounds, nxt,
-                    P.counters + 1, P.counters, P.slots, lf_slot);
-                cuda_check(cudaGetLastError(), "lr_fractions_kernel launch");
+                {
+                    LaunchScope scope("lr_fractions_kernel", st);
+                    lr_fractions_kernel<<<blocks(lf_slots, count), kMtWarps * 32, 0, st>>>(
+                        lrt, sig, P.xlr, c_lr, cur, count, round, max_rounds, fraction_tol, P.fiso, P.prev, P.rounds,
+                        nxt, P.counters + 1, P.counters, P.slots, lf_slot);
+                    cuda_check(cudaGetLastError(), "lr_fractions_kernel launch");
+                }
                 cuda_check(cudaMemcpyAsync(host_count, P.counters + 1, sizeof(int), cudaMemcpyDeviceToHost, st),
                            "cudaMemcpyAsync (round count)");
                 cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
@@ -848,10 +856,14 @@ int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights
             const SignalDev hr_sig{sig, P.weights, hrt.wiso, P.fiso, mi, ci};
             launch_correlate(hr_sig, nullptr, n, hrs, P.corr, c_hr, st);
             reset_queue();
-            hr_nnls.kernel<<<blocks(hr_slots, n), kMtWarps * 32, hr_smem, st>>>(
-                hrs, hr_sig, nullptr, n, P.corr, c_hr, fods + v0 * c_hr, c_hr, P.bad, P.counters, P.slots, hr_slot);
-            cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
+            {
+                LaunchScope scope(hr_nnls.name, st);
+                hr_nnls.kernel<<<blocks(hr_slots, n), kMtWarps * 32, hr_smem, st>>>(
+                    hrs, hr_sig, nullptr, n, P.corr, c_hr, fods + v0 * c_hr, c_hr, P.bad, P.counters, P.slots, hr_slot);
+                cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
+            }
             reset_queue();
+            LaunchScope scope("hr_fractions_kernel", st);
             hr_fractions_kernel<<<blocks(hf_slots, n), kMtWarps * 32, 0, st>>>(
                 hrt, sig, fods + v0 * c_hr, n, final_tol_x, P.rounds, P.bad, fractions + v0 * nf,
                 rounds ? rounds + v0 : nullptr, status ? status + v0 : nullptr, P.counters, P.slots, hf_slot);
@@ -895,6 +907,7 @@ int lar_fit_single_tissue(const double* signals, int64_t v, lar_fod_solver solve
             if (status) cuda_check(cudaMemsetAsync(status + v0, 0, size_t(n), st), "cudaMemsetAsync");
             cuda_check(cudaMemsetAsync(counters, 0, sizeof(int), st), "cudaMemsetAsync");
             const unsigned nb = unsigned(std::max<int64_t>(1, std::min<int64_t>(slots / kMtWarps, (n + kMtWarps - 1) / kMtWarps)));
+            LaunchScope scope(nn.name, st);
             nn.kernel<<<nb, kMtWarps * 32, smem, st>>>(R, S, nullptr, n, corr, c, fods + v0 * c, c,
                                                        status ? status + v0 : nullptr, counters, work, slot);
             cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
