@@ -45,73 +45,70 @@ def peaks() -> tuple[dict, str]:
     return {"hbm_gbs": FALLBACK_HBM_GBS, "bf16_tflops": 1590.0}, "fallback"
 
 
-def committed_traffic(kernel: str, workload: str) -> float | None:
-    """Per-launch DRAM bytes of a kernel from the committed ncu summary, if any."""
+def committed_traffic(kernel: str, workload: str, algorithmic_bytes: float) -> float | None:
+    """Per-launch DRAM bytes of a kernel: the measured DRAM bytes per algorithmic byte of its
+    committed ncu capture (profiles/traffic.json, a smaller case of the same workload) times
+    this launch's algorithmic bytes."""
     path = ROOT / "profiles" / "traffic.json"
     if not path.exists():
         return None
-    table = json.loads(path.read_text())
-    entry = table.get(f"{workload}:{kernel}")
-    return None if entry is None else float(entry["bytes_per_launch"])
+    entry = json.loads(path.read_text()).get("kernels", {}).get(f"{workload}:{kernel}")
+    return None if entry is None else float(entry["dram_per_algorithmic_byte"]) * algorithmic_bytes
 
 
 # ---- clocks ------------------------------------------------------------------------------
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons of one GPU while running."""
+    """Samples one GPU's SM clock and throttle reasons through NVML every 2 ms while running
+    (nvidia-smi's 100 ms period misses timed regions of a few milliseconds)."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
     def __init__(self, index: int) -> None:
         self.index = index
-        self.proc = None
-        self.lines: list[str] = []
+        self.samples: list[tuple[float, float, int]] = []
+        self.stop = threading.Event()
+        self.thread = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except OSError:
-            self.proc = None
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        except Exception:  # noqa: BLE001 - no NVML: no clock record
+            self.nvml = None
+            return self
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv, h = self.nvml, self.handle
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(mx), int(reasons)))
+            except Exception:  # noqa: BLE001
+                pass
+            time.sleep(0.002)
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self.stop.set()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
 
     def summary(self) -> dict:
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 7:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx.append(float(parts[1]))
-            except ValueError:
-                continue
-            for name, flag in zip(names, parts[3:7]):
-                if flag.lower() == "active":
-                    reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "source": "nvml"}
+        reasons = sorted({name for _, _, r in self.samples for name, bit in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(x[0] for x in self.samples),
+                "sm_max_mhz": max(x[1] for x in self.samples), "reasons": reasons,
+                "samples": len(self.samples), "source": "nvml"}
 
 
 # ---- workloads ---------------------------------------------------------------------------
@@ -139,6 +136,11 @@ class DtiWorkload:
         self.signals = masked_signals(w.volume, np.nonzero(w.mask))
         self.floor = sample_floors(s0, None, len(self.signals))
         self.v = len(self.signals)
+
+    def subset(self, n: int) -> None:
+        self.signals, self.floor = self.signals[:n], self.floor[:n]
+        self.v = len(self.signals)
+        self.config["voxels"] = self.v
 
     def device_setup(self, torch, dev):
         from larmor_b200 import _core
@@ -212,6 +214,11 @@ class DkiWorkload:
         self.v = len(self.signals)
         self.config = {"workload": self.name, "grid": [96, 96, 60], "voxels": self.v, "measurements": 134,
                        "fit": "wls, constrained (768 constraints)", "l2": "flushed (256 MiB write) before each step"}
+
+    def subset(self, n: int) -> None:
+        self.signals, self.s0, self.floor = self.signals[:n], self.s0[:n], self.floor[:n]
+        self.v = len(self.signals)
+        self.config["voxels"] = self.v
 
     def device_setup(self, torch, dev):
         from larmor_b200 import _core
@@ -292,6 +299,13 @@ class _SdWorkloadBase:
         self.signals = masked_signals(w.volume, np.nonzero(w.mask)).astype(np.float64)
         self.s0 = estimate_s0(w.volume, w.gtab, w.mask)[w.mask]
         self.v = len(self.signals)
+
+    def subset(self, n: int) -> None:
+        self.signals, self.s0 = self.signals[:n], self.s0[:n]
+        if hasattr(self, "norm"):
+            self.norm = self.norm[:n]
+        self.v = len(self.signals)
+        self.config["voxels"] = self.v
 
 
 class MfodWorkload(_SdWorkloadBase):
@@ -485,6 +499,11 @@ def main() -> int:
                     help="seconds of CPU work per reference step")
     ap.add_argument("--cpu-budget", type=float, default=10.0,
                     help="seconds of CPU baseline work on rank 0")
+    ap.add_argument("--voxels", type=int, default=0,
+                    help="fit only the first N voxels of the volume (small cases for ncu)")
+    ap.add_argument("--profile", action="store_true",
+                    help="warm-up and K device-resident steps only, timed per step on stdout (for ncu); "
+                         "prints no bench line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -513,7 +532,17 @@ def main() -> int:
     torch.cuda.set_device(dev)
 
     wl = WORKLOADS[args.workload](seed=1 + rank)
+    if args.voxels:
+        wl.subset(args.voxels)
     wl.device_setup(torch, dev)
+    if args.profile:
+        for i in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            wl.step_device()
+            torch.cuda.synchronize()
+            print(f"{wl.name} voxels {wl.v} step {i} {1e3 * (time.perf_counter() - t0):.3f} ms")
+        return 0
     flush = torch.empty(256 * 2**20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
 
@@ -538,11 +567,9 @@ def main() -> int:
         return total
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        from larmor_b200.sharding import max_over_ranks as slowest
+
+        return slowest(x, device=dev)
 
     # Warm-up, then the timed device-resident steps.
     for _ in range(args.warmup):
@@ -587,7 +614,7 @@ def main() -> int:
     avg_launch_s = top_ms / max(top_launches, 1) / 1e3
     bytes_per_launch = step_bytes[top] * args.steps / max(top_launches, 1)
     achieved_gbs = bytes_per_launch / avg_launch_s / 1e9
-    traffic = committed_traffic(top, wl.name)
+    traffic = committed_traffic(top, wl.name, bytes_per_launch)
     total_kernel_ms = max(sum(t for t, _ in kernel_ms.values()), 1e-30)
 
     cpu = None

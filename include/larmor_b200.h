@@ -193,6 +193,22 @@ int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights
 int lar_fit_single_tissue(const double* signals, int64_t v, lar_fod_solver solver, double* fods,
                           uint8_t* status, void* stream);
 
+/* ---- FOD amplitudes to spherical harmonics ----------------------------------------------
+ * The SD fit's _to_sh (src/larmor/sd/model.py:412-440, fit_sh src/larmor/sd/sh.py:134): the
+ * least-squares SH fit of amplitudes on a sphere grid, as the product with a projector
+ * P = density pinv(B) (ncoef, ca) that the caller forms once per (grid, lmax, basis). */
+typedef struct lar_sh_projector_s* lar_sh_projector;
+
+/* Copies the projector (ncoef, ca) (host, row-major) to the device. */
+int lar_sh_projector_create(const double* projector, int64_t ncoef, int64_t ca, lar_sh_projector* out);
+
+void lar_sh_projector_destroy(lar_sh_projector projector);
+
+/* out (v, ncoef; row stride ldo) = amplitudes (v, ca; row stride lda) P^T, all device double;
+ * with exact_integral the l = 0 coefficient is the amplitudes' sum / sqrt(4 pi) instead. */
+int lar_project_sh(lar_sh_projector projector, const double* amplitudes, int64_t v, int64_t lda,
+                   int exact_integral, double* out, int64_t ldo, void* stream);
+
 /* ---- A fit that allocates no device memory ------------------------------------------- */
 
 /* No counterpart in the reference: an entry point for callers that cannot allocate device

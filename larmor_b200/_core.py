@@ -379,6 +379,14 @@ def fit_multi_tissue(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, 
     _require_threads(n_threads)
     if max_outer < 0:
         raise ValueError("max_outer must be at least 0")
+    fods, fractions = _fit_multi_tissue_on_device(signals, weights, lr, lr_solver, hr, hr_solver, max_outer,
+                                                  fraction_tol, final_tol_x)
+    return fods.cpu().numpy(), fractions.cpu().numpy()
+
+
+def _fit_multi_tissue_on_device(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol,
+                                final_tol_x):
+    """fit_multi_tissue of checked host arrays, the results left on the device (torch tensors)."""
     torch = _torch()
     dev = torch.device("cuda", torch.cuda.current_device())
     v = signals.shape[0]
@@ -388,7 +396,7 @@ def fit_multi_tissue(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, 
         s = torch.from_numpy(signals).to(dev)
         fit_multi_tissue_device(s, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol, final_tol_x,
                                 fods, fractions)
-    return fods.cpu().numpy(), fractions.cpu().numpy()
+    return fods, fractions
 
 
 def fit_multi_tissue_device(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol,
@@ -408,6 +416,11 @@ def fit_single_tissue(signals, solver: FodSolver, n_threads):
     if signals.shape[1] != solver.n_meas:
         raise ValueError(f"signals {signals.shape} do not have the solver's {solver.n_meas} measurements")
     _require_threads(n_threads)
+    return _fit_single_tissue_on_device(signals, solver).cpu().numpy()
+
+
+def _fit_single_tissue_on_device(signals, solver: FodSolver):
+    """fit_single_tissue of a checked host array, the FODs left on the device (a torch tensor)."""
     torch = _torch()
     dev = torch.device("cuda", torch.cuda.current_device())
     v = signals.shape[0]
@@ -416,7 +429,36 @@ def fit_single_tissue(signals, solver: FodSolver, n_threads):
         s = torch.from_numpy(signals).to(dev)
         _lib.check(_lib.lib().lar_fit_single_tissue(_lib.ptr(s), v, solver.handle, _lib.ptr(fods), None,
                                                     _stream(torch)))
-    return fods.cpu().numpy()
+    return fods
+
+
+class ShProjector(_Handle):
+    """The least-squares projector of amplitudes on a sphere grid onto an SH basis, scaled by
+    the grid's density, on the device (the _to_sh step, src/larmor/sd/model.py:412-440)."""
+
+    _destroy = "lar_sh_projector_destroy"
+
+    def __init__(self, projector) -> None:
+        super().__init__()
+        p = _array(projector, "projector", 2)
+        self.ncoef, self.ca = p.shape
+        _lib.check(_lib.lib().lar_sh_projector_create(_lib.ptr(p), self.ncoef, self.ca, ctypes.byref(self._handle)))
+
+
+def project_sh_device(projector: ShProjector, amplitudes, exact_integral: bool):
+    """SH coefficients (v, ncoef) of device amplitudes (v, ca), a column slice of a row-major
+    tensor allowed; a new device tensor."""
+    torch = _torch()
+    if amplitudes.dim() != 2 or amplitudes.shape[1] != projector.ca or amplitudes.stride(1) != 1:
+        raise ValueError(f"amplitudes {tuple(amplitudes.shape)} do not have the projector's {projector.ca} "
+                         "directions in unit-stride rows")
+    v = amplitudes.shape[0]
+    out = torch.empty((v, projector.ncoef), dtype=torch.float64, device=amplitudes.device)
+    if v:
+        _lib.check(_lib.lib().lar_project_sh(projector.handle, _lib.ptr(amplitudes), v, amplitudes.stride(0),
+                                             int(bool(exact_integral)), _lib.ptr(out), projector.ncoef,
+                                             _stream(torch)))
+    return out
 
 
 # ---- launch accounting (benchmarks) ------------------------------------------------------

@@ -40,6 +40,9 @@ SIGNATURES: dict[str, tuple] = {
     "lar_deconv_kernel_destroy": (None, [_p]),
     "lar_fit_multi_tissue": (_i32, [_p, _i64, _p, _p, _p, _p, _p, _i64, _f64, _f64, _p, _p, _p, _p, _p]),
     "lar_fit_single_tissue": (_i32, [_p, _i64, _p, _p, _p, _p]),
+    "lar_sh_projector_create": (_i32, [_p, _i64, _i64, _p]),
+    "lar_sh_projector_destroy": (None, [_p]),
+    "lar_project_sh": (_i32, [_p, _p, _i64, _i64, _i32, _p, _i64, _p]),
     "lar_fit_log_signal_noalloc": (_i32, [_p, _i64, _i64, _p, _i64, _p, _i64, _i32, _i64, _f64, _p, _p, _p]),
 }
 

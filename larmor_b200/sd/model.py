@@ -2,6 +2,7 @@
 
 from __future__ import annotations
 
+import functools
 from dataclasses import dataclass
 
 import numpy as np
@@ -28,8 +29,9 @@ from larmor_b200.dwi.inputs import as_mask, check_dwi, estimate_s0, masked_signa
 from larmor_b200.dwi.mask import unmask  # noqa: E402
 from larmor_b200.sd.kernel import Kernel, order_rfs  # noqa: E402
 from larmor_b200.sd.rf import IsotropicRF  # noqa: E402
-from larmor_b200.sd.sh import BASES, fit_sh  # noqa: E402
-from larmor_b200.sd.sphere import DIRS_300, get_dirs  # noqa: E402
+from larmor_b200 import _core  # noqa: E402
+from larmor_b200.sd.sh import BASES, build_basis_matrix, fit_sh  # noqa: E402
+from larmor_b200.sd.sphere import DIRS_300, get_dirs, get_theta_phi  # noqa: E402
 
 SHELL_TOLERANCE = 100.0
 # The relative peak threshold of SDModel's FODs (their truncation leaves side lobes).
@@ -62,6 +64,18 @@ def low_resolution_dirs(rfs, n_meas: int) -> list[np.ndarray]:
     """Each anisotropic response's coarse directions: the spiral of min(n_meas, its count)
     points without its last, which repeats the first (src/larmor/sd/model.py:394-409)."""
     return [get_dirs(min(n_meas, rf.low_resolution_dirs))[:-1] for rf in rfs if not isinstance(rf, IsotropicRF)]
+
+
+@functools.lru_cache(maxsize=16)
+def sh_projector(lmax: int, basis: str):
+    """The device projector of amplitudes on DIRS_300 onto the SH basis of lmax: the
+    least-squares fit of fit_sh (pinv of the full-rank basis matrix) times 300 / (4 pi)."""
+    from larmor_b200 import _core
+
+    theta, phi = get_theta_phi(np.asarray(DIRS_300, dtype=np.float64))
+    matrix = build_basis_matrix(theta, phi, lmax, basis)
+    density = len(DIRS_300) / (4.0 * np.pi)
+    return _core.ShProjector(np.ascontiguousarray(np.linalg.pinv(matrix) * density))
 
 
 def to_sh(fods: np.ndarray, lmax: int, basis: str, *, exact_integral: bool = False) -> np.ndarray:
@@ -127,10 +141,12 @@ class SDModel:
         normalised = np.minimum(normalised[finite], 1.0)
         amplitudes, fitted_fractions, hr = self._fit_normalised(normalised, gtab, solver, threads)
         n_coeffs = (lmax + 1) * (lmax + 2) // 2
+        projector = sh_projector(lmax, self.basis)
         fods = []
         for block in hr.aniso_blocks:
             sh = np.full((len(finite), n_coeffs), np.nan)
-            sh[finite] = to_sh(amplitudes[:, block], lmax, self.basis, exact_integral=True)
+            if len(normalised):
+                sh[finite] = _core.project_sh_device(projector, amplitudes[:, block], True).cpu().numpy()
             fods.append(unmask(sh, mask))
         fractions = None
         if fitted_fractions is not None:
@@ -153,11 +169,13 @@ class SDModel:
         return hr, lr, solver._prepare(hr, bvals, Stage.HIGH_RES), solver._prepare(lr, bvals, Stage.LOW_RES)
 
     def _fit_normalised(self, signals, gtab, solver, threads):
-        from larmor_b200.sd.solvers import fit_multi_tissue, fit_single_tissue
+        """The high-resolution amplitudes (on the device) and fractions (host) of the
+        S0-normalised signals."""
+        from larmor_b200.sd.solvers import fit_multi_tissue_on_device, fit_single_tissue_on_device
 
         hr, lr, hr_solver, lr_solver = self._prepare(solver, gtab.bvals, gtab.bvecs)
         if lr is None:
-            return fit_single_tissue(signals, hr_solver, threads), None, hr
-        fods, fractions = fit_multi_tissue(signals, lr, hr, lr_solver, hr_solver, threads,
-                                           fraction_tol=self.method._fraction_tolerance)
-        return fods, fractions, hr
+            return fit_single_tissue_on_device(signals, hr_solver), None, hr
+        fods, fractions = fit_multi_tissue_on_device(signals, lr, hr, lr_solver, hr_solver,
+                                                     fraction_tol=self.method._fraction_tolerance)
+        return fods, fractions.cpu().numpy(), hr

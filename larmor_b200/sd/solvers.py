@@ -57,6 +57,21 @@ def fit_single_tissue(signals, solver, n_threads):
     return _core.fit_single_tissue(np.ascontiguousarray(signals, dtype=np.float64), solver, n_threads=n_threads)
 
 
+def fit_single_tissue_on_device(signals, solver):
+    """fit_single_tissue with the FODs left on the device (a torch tensor)."""
+    return _core._fit_single_tissue_on_device(_core._array(np.ascontiguousarray(signals, dtype=np.float64),
+                                                           "signals", 2), solver)
+
+
+def fit_multi_tissue_on_device(signals, lr_kernel: Kernel, hr_kernel: Kernel, lr_solver, hr_solver,
+                               fraction_tol: float = FRACTION_TOL):
+    """fit_multi_tissue with the amplitudes and fractions left on the device (torch tensors)."""
+    return _core._fit_multi_tissue_on_device(
+        np.ascontiguousarray(signals, dtype=np.float64), np.ascontiguousarray(lr_kernel.weights, dtype=np.float64),
+        _deconv_kernel(lr_kernel), lr_solver, _deconv_kernel(hr_kernel), hr_solver, MAX_ROUNDS, fraction_tol,
+        FINAL_FRACTION_TOL_X)
+
+
 def fit_multi_tissue(signals, lr_kernel: Kernel, hr_kernel: Kernel, lr_solver, hr_solver, n_threads: int = 1,
                      fraction_tol: float = FRACTION_TOL):
     """The high-resolution FOD amplitudes (n, ca_hr) and the fractions (n, n_rfs)

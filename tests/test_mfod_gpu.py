@@ -105,3 +105,25 @@ def test_sd_model_three_tissue_matches_the_oracle(cuda, oracle):
     # The maps are float32, as the reference's.
     np.testing.assert_allclose(fit.fods[0].reshape(-1, ref_sh.shape[1]), ref_sh, rtol=1e-5, atol=1e-6)
     np.testing.assert_allclose(fit.tissue_fractions.reshape(-1, 3), rfr, rtol=0, atol=1e-6)
+
+
+@pytest.mark.parametrize("lmax", [8, 12])
+@pytest.mark.parametrize("exact_integral", [True, False])
+def test_sh_projection_matches_the_least_squares_fit(cuda, lmax, exact_integral):
+    """The device _to_sh (amplitudes on DIRS_300 to SH) against numpy's lstsq restatement, on
+    column blocks of a two-block amplitude array (a strided source) and with more than one
+    48-coefficient tile (lmax 12: 91 coefficients)."""
+    import torch
+
+    from larmor_b200 import _core
+    from larmor_b200.sd.model import sh_projector, to_sh
+
+    rng = np.random.default_rng(11)
+    amps = np.abs(rng.normal(size=(1000, 600)))
+    amps[rng.random(amps.shape) < 0.8] = 0.0
+    d = torch.from_numpy(amps).to("cuda")
+    projector = sh_projector(lmax, "tournier")
+    for block in (slice(0, 300), slice(300, 600)):
+        ref = to_sh(amps[:, block], lmax, "tournier", exact_integral=exact_integral)
+        got = _core.project_sh_device(projector, d[:, block], exact_integral).cpu().numpy()
+        assert (np.abs(got - ref) <= 1e-12 * np.abs(ref).max(axis=1, keepdims=True)).all()
