@@ -460,11 +460,221 @@ class MsmtWorkload(_SdWorkloadBase):
         return done, time.perf_counter() - t0, f"first {n} voxels of the volume, repeated for ~{budget_s:.0f} s"
 
 
-WORKLOADS = {"dti": DtiWorkload, "dki": DkiWorkload, "mfod": MfodWorkload, "msmt": MsmtWorkload}
+def _job_kernel_bytes(job) -> dict:
+    """Algorithmic DRAM bytes of one job of a batch, per kernel (as the single workloads count
+    them); the DKI violator count and the mFOD rounds come from the job's last fit."""
+    v, n = job.voxels, job.signals.shape[1]
+    if job.kind == "dti":
+        return {"fit_dti_maps_kernel": v * (4 * n + 8 + 16 * 4 + 1)}
+    if job.kind == "dki":
+        viol = job.handles["design"].violators()
+        return {"fit_log_warp_kernel": v * (4 * n + 16 + 22 * 8 + 1),
+                "constrained_fit_kernel": viol * (4 * n + 16 + 2 * 22 * 8),
+                "dki_maps_kernel": v * (22 * 8 + 36 * 4 + 1)}
+    vr = int(job.out["rounds"].sum().item())
+    c_lr, c_hr = job.handles["k_lr"].ca, job.handles["k_hr"].ca
+    return {"correlate_kernel": vr * 8 * (n + c_lr) + v * 8 * (n + c_hr),
+            "ridge_nnls_kernel<2,2>": vr * 8 * 2 * c_lr,
+            "lr_fractions_kernel": vr * 8 * (c_lr + n + 3),
+            "ridge_nnls_kernel<8,10>": v * 8 * 2 * c_hr,
+            "hr_fractions_kernel": v * 8 * (c_hr + n + 3)}
+
+
+class BatchWorkload:
+    """Config 4: 64 seeded volumes of uneven size (10k-400k voxels), gradient table (1-3 shells
+    of 30-90 directions) and model (DTI/DKI/mFOD 40/20/40), all fitted by one replay of one
+    CUDA graph whose parallel branches run the volumes side by side."""
+
+    name = "batch_uneven_64_volumes"
+    kernels = ("fit_dti_maps_kernel", "fit_log_warp_kernel", "constrained_fit_kernel", "dki_maps_kernel",
+               "correlate_kernel", "ridge_nnls_kernel<2,2>", "lr_fractions_kernel", "ridge_nnls_kernel<8,10>",
+               "hr_fractions_kernel")
+    has_fp32 = False
+
+    def __init__(self, seed: int) -> None:
+        from larmor_b200.batch import generate_jobs
+
+        self.jobs = generate_jobs(seed=4 + 10 * (seed - 1))
+        self.v = sum(j.voxels for j in self.jobs)
+        kinds = {k: sum(1 for j in self.jobs if j.kind == k) for k in ("dti", "dki", "mfod")}
+        self.config = {"workload": self.name, "volumes": len(self.jobs), "voxels": self.v, "jobs": kinds,
+                       "voxels_per_volume": [min(j.voxels for j in self.jobs), max(j.voxels for j in self.jobs)],
+                       "launch": "one CUDA graph replay per step (4 parallel branches)",
+                       "l2": "inputs (4.8 GB) larger than L2"}
+
+    def subset(self, n: int) -> None:
+        self.jobs = self.jobs[:max(1, n)]
+        self.v = sum(j.voxels for j in self.jobs)
+        self.config["volumes"], self.config["voxels"] = len(self.jobs), self.v
+
+    def device_setup(self, torch, dev):
+        from larmor_b200.batch import Batch
+
+        self.torch = torch
+        self.batch = Batch(self.jobs, branches=4)
+        self.batch.capture()
+        self.h_in = [tuple(torch.from_numpy(np.ascontiguousarray(t.cpu().numpy())).pin_memory() for t in j.d_in)
+                     for j in self.jobs]
+        self.h_out = [{k: torch.empty(t.shape, dtype=t.dtype).pin_memory() for k, t in j.out.items()}
+                      for j in self.jobs]
+        self.h2d_bytes = sum(t.numel() * t.element_size() for ts in self.h_in for t in ts)
+        self.d2h_bytes = sum(t.numel() * t.element_size() for o in self.h_out for t in o.values())
+
+    def step_device(self, precision=0):
+        self.batch.run()
+
+    def step_eager(self):
+        """The same work launched kernel by kernel (for per-kernel event timing)."""
+        self.batch.run_eager()
+
+    def graph_launches(self) -> int:
+        return self.batch.graph_kernels
+
+    def step_e2e(self):
+        for j, hin in zip(self.jobs, self.h_in):
+            for d, h in zip(j.d_in, hin):
+                d.copy_(h, non_blocking=True)
+        self.batch.run()
+        for j, hout in zip(self.jobs, self.h_out):
+            for k, t in j.out.items():
+                hout[k].copy_(t, non_blocking=True)
+
+    def kernel_bytes(self) -> dict:
+        self.torch.cuda.synchronize()
+        total: dict = {}
+        for j in self.jobs:
+            for k, b in _job_kernel_bytes(j).items():
+                total[k] = total.get(k, 0) + b
+        return total
+
+    def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
+        from larmor_b200.dwi.dki import dki_constraints, dki_design
+        from larmor_b200.dwi.dti import dti_design
+        from larmor_b200.sd.kernel import Kernel
+        from larmor_b200.sd.model import compute_shell_weights, low_resolution_dirs
+        from larmor_b200.sd.sphere import DIRS_300
+        from oracle import oracle as o
+
+        calls = []
+        for j in self.jobs:
+            n = min(j.voxels, 128)
+            if j.kind in ("dti", "dki"):
+                log_s = np.log(np.maximum(j.signals[:n].astype(np.float64), j.floor[:n, None]))
+                x = dti_design(j.gtab) if j.kind == "dti" else dki_design(j.gtab)
+                g = None if j.kind == "dti" else dki_constraints(j.gtab)
+                calls.append((n, lambda x=x, g=g, s=log_s: o.fit_log_signal(x, g, s, True, n_threads=threads)))
+            else:
+                b, g = j.gtab.bvals, j.gtab.bvecs
+                w = compute_shell_weights(b, 1.0)
+                hr = Kernel(j.responses, b, g, dirs=DIRS_300, weights=w)
+                lr = Kernel(j.responses, b, g, dirs=low_resolution_dirs(j.responses, len(b)), weights=w)
+                lrd = dict(k_aniso=lr.k_aniso, k_iso=lr.k_iso, w_k_iso=lr.w_k_iso, w_k_aniso=lr.w_k_aniso)
+                hrd = dict(k_aniso=hr.k_aniso, k_iso=hr.k_iso, w_k_iso=hr.w_k_iso, w_k_aniso=hr.w_k_aniso,
+                           blocks=[(bb.start, bb.stop) for bb in hr.aniso_blocks])
+                sig = np.ascontiguousarray(j.signals[:n])
+                calls.append((n, lambda s=sig, lw=lr.weights, a=lrd, h=hrd: o.fit_multi_tissue(
+                    s, lw, a, h, n_threads=threads)))
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget_s:
+            for n, call in calls:
+                call()
+                done += n
+        return done, time.perf_counter() - t0, (f"the first 128 voxels of each of the {len(self.jobs)} volumes "
+                                                f"(fits only), repeated for ~{budget_s:.0f} s")
+
+
+WORKLOADS = {"dti": DtiWorkload, "dki": DkiWorkload, "mfod": MfodWorkload, "msmt": MsmtWorkload,
+             "batch": BatchWorkload}
 
 
 
 # ---- runs --------------------------------------------------------------------------------
+
+def _serve_jobs(seed: int, count: int):
+    """Fit requests drawn from the config-3 distribution: contiguous runs of voxels of the
+    110x110x70 three-tissue volume (S0-normalised), their lengths log-uniform in [4096, 65536]."""
+    from larmor_b200.batch import MfodJob
+    from larmor_b200.synthetic import mfod_model_responses
+
+    wl = MfodWorkload(seed=1)
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for _ in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(4096), np.log(65536)))))
+        start = int(rng.integers(0, wl.v - n))
+        jobs.append(MfodJob(wl.gtab, np.ascontiguousarray(wl.norm[start:start + n]), mfod_model_responses()))
+    return jobs
+
+
+def run_serving(args) -> dict:
+    """Config 5: Poisson arrivals of mFOD fit requests at rates swept up to saturation through
+    the continuous-batching server, against the plain per-request fit (one request at a time).
+    Latency is arrival to result on the host (wall clock), the quantity a client sees."""
+    import torch
+
+    from larmor_b200 import _core
+    from larmor_b200.serve import FitServer
+
+    jobs = _serve_jobs(5, args.serve_requests)
+    voxels = sum(j.voxels for j in jobs)
+    # Warm-up: the handles of every slot and the kernels' first launches.
+    server = FitServer(budget_bytes=80 << 30, slots=args.serve_slots)
+    for f in [server.submit(j) for j in jobs[:args.serve_slots]]:
+        f.result()
+    # Plain per-request fits: one request at a time, back to back.
+    t0 = time.perf_counter()
+    for j in jobs:
+        server.submit(j).result()
+    plain_s = time.perf_counter() - t0
+    plain_rate = len(jobs) / plain_s
+    rng = np.random.default_rng(55)
+    sweep = {}
+    _core.kernel_timing(True)
+    launches0 = _core.launch_count()
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        for factor in args.serve_load:
+            lam = factor * plain_rate
+            gaps = rng.exponential(1.0 / lam, len(jobs))
+            first = len(server.completed)
+            t_start = time.perf_counter()
+            futures = []
+            for j, gap in zip(jobs, gaps):
+                time.sleep(gap)
+                futures.append(server.submit(j))
+            for f in futures:
+                f.result()
+            t_end = time.perf_counter()
+            lat = sorted(1e3 * (r.finished - r.arrival) for r in server.completed[first:])
+            sweep[f"{factor:g}x"] = {"arrival_rate_per_s": lam, "p50_ms": float(np.percentile(lat, 50)),
+                                     "p99_ms": float(np.percentile(lat, 99)),
+                                     "throughput_voxels_per_s": voxels / (t_end - t_start)}
+    launches = _core.launch_count() - launches0
+    kernel_ms = {k: _core.kernel_time(k) for k in MfodWorkload.kernels}
+    _core.kernel_timing(False)
+    peak_running = server.peak_running
+    server.close()
+    top_load = f"{args.serve_load[-1]:g}x"
+    best = max(v["throughput_voxels_per_s"] for v in sweep.values())
+    top = max(kernel_ms, key=lambda k: kernel_ms[k][0])
+    return {
+        "metric": METRIC, "value": best, "unit": "voxel fits/s", "n_gpus": 1, "steps": len(args.serve_load),
+        "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "serve_mfod_poisson", "requests_per_rate": len(jobs), "voxels_per_rate": voxels,
+                   "request_voxels": "log-uniform 4096-65536 (config-3 volume)", "slots": args.serve_slots,
+                   "hbm_budget_gb": 80, "rates": "multiples of the plain per-request rate",
+                   "timing": "host wall clock, arrival to result"},
+        "serving": sweep,
+        "plain_per_request": {"value": voxels / plain_s, "unit": "voxel fits/s", "requests_per_s": plain_rate},
+        "saturation": {"load": top_load, "peak_concurrent_requests": peak_running},
+        "e2e": {"value": best, "unit": "voxel fits/s", "h2d_bytes_per_step": sum(j.signals.nbytes for j in jobs),
+                "d2h_bytes_per_step": sum(j.voxels * 8 * 308 for j in jobs)},
+        "roofline": None, "dominant_kernel": top,
+        "kernel_share": {k: round(t / max(sum(x for x, _ in kernel_ms.values()), 1e-30), 4)
+                         for k, (t, _) in kernel_ms.items()},
+        "cpu_baseline": None, "gpu_launches": launches, "clocks": clocks.summary(),
+    }
+
 
 def run_reference(args, wl) -> dict:
     threads = os.cpu_count() or 1
@@ -493,7 +703,7 @@ def main() -> int:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="mfod", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="mfod", choices=sorted(WORKLOADS) + ["serve"])
     ap.add_argument("--impl", default="larmor_b200", choices=["larmor_b200", "reference"])
     ap.add_argument("--reference-budget", type=float, default=3.0,
                     help="seconds of CPU work per reference step")
@@ -501,6 +711,10 @@ def main() -> int:
                     help="seconds of CPU baseline work on rank 0")
     ap.add_argument("--voxels", type=int, default=0,
                     help="fit only the first N voxels of the volume (small cases for ncu)")
+    ap.add_argument("--serve-requests", type=int, default=24, help="requests per arrival rate (serve)")
+    ap.add_argument("--serve-slots", type=int, default=6, help="requests on the GPU at once (serve)")
+    ap.add_argument("--serve-load", type=float, nargs="+", default=[0.5, 1.0, 2.0, 4.0],
+                    help="arrival rates as multiples of the plain per-request rate (serve)")
     ap.add_argument("--profile", action="store_true",
                     help="warm-up and K device-resident steps only, timed per step on stdout (for ncu); "
                          "prints no bench line")
@@ -510,6 +724,18 @@ def main() -> int:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.workload == "serve":
+        if rank != 0:
+            return 0
+        if args.impl == "reference":
+            wl = MfodWorkload(seed=1)
+            line = run_reference(args, wl)
+            line["config"] = {"workload": "serve_mfod_poisson", "reference": "the mFOD fit of config-3 voxels"}
+            print(json.dumps(line))
+            return 0
+        print(json.dumps(run_serving(args)))
+        return 0
 
     if args.impl == "reference":
         if rank != 0:
@@ -588,6 +814,16 @@ def main() -> int:
     launches = _core.launch_count() - launches0
     kernel_ms = {name: _core.kernel_time(name) for name in wl.kernels}
     _core.kernel_timing(False)
+    if hasattr(wl, "graph_launches"):
+        # Graph replays launch the library's kernels without a host call: count the recorded
+        # kernels, and time each kernel in the same work launched eagerly.
+        launches = wl.graph_launches() * args.steps
+        _core.kernel_timing(True)
+        for _ in range(args.steps):
+            wl.step_eager()
+        torch.cuda.synchronize()
+        kernel_ms = {name: _core.kernel_time(name) for name in wl.kernels}
+        _core.kernel_timing(False)
     dev_ms = max_over_ranks(dev_ms)
 
     # The plain FP32 kernel, for comparison.
@@ -613,7 +849,7 @@ def main() -> int:
     top_ms, top_launches = kernel_ms[top]
     avg_launch_s = top_ms / max(top_launches, 1) / 1e3
     bytes_per_launch = step_bytes[top] * args.steps / max(top_launches, 1)
-    achieved_gbs = bytes_per_launch / avg_launch_s / 1e9
+    achieved_gbs = bytes_per_launch / avg_launch_s / 1e9 if avg_launch_s > 0 else 0.0
     traffic = committed_traffic(top, wl.name, bytes_per_launch)
     total_kernel_ms = max(sum(t for t, _ in kernel_ms.values()), 1e-30)
 

@@ -95,6 +95,7 @@ constexpr int kCorrDepth = 16;   // measurements per shared-memory stage
 // 8 voxel lanes x 16 column lanes, each with 4 voxels x RC columns of the tile.
 template <int RC>
 __global__ void __launch_bounds__(128) correlate_kernel(SignalDev S, const int* __restrict__ list, int64_t count,
+                                                        const int* __restrict__ count_dev,
                                                         const double* __restrict__ k, int c,
                                                         double* __restrict__ corr, int ldc) {
     constexpr int TC = 16 * RC;
@@ -105,6 +106,8 @@ __global__ void __launch_bounds__(128) correlate_kernel(SignalDev S, const int* 
     const int64_t p0 = int64_t(blockIdx.x) * kCorrVoxels;
     const int col0 = blockIdx.y * TC;
     const int m = S.m;
+    if (count_dev) count = min(count, int64_t(*count_dev));
+    if (p0 >= count) return;
     if (tid < kCorrVoxels) vox[tid] = p0 + tid < count ? listed(list, p0 + tid) : -1;
     double acc[4][RC];
 #pragma unroll
@@ -386,10 +389,11 @@ __device__ __noinline__ bool ridge_nnls(const RidgeDev& R, const SignalDev& S, i
 // bad(v) <- 1 when the QR fallback overflowed.
 template <int VPL, int CPL>
 __global__ void __launch_bounds__(kMtWarps * 32, (CPL <= 2 ? 8 : 4)) ridge_nnls_kernel(
-    RidgeDev R, SignalDev S, const int* __restrict__ list, int64_t count, const double* __restrict__ corr, int ldc,
-    double* __restrict__ x_out, int ldx, uint8_t* __restrict__ bad, int* queue, double* __restrict__ workspace,
-    size_t slot_size) {
+    RidgeDev R, SignalDev S, const int* __restrict__ list, int64_t count, const int* __restrict__ count_dev,
+    const double* __restrict__ corr, int ldc, double* __restrict__ x_out, int ldx, uint8_t* __restrict__ bad,
+    int* queue, double* __restrict__ workspace, size_t slot_size) {
     using State = NnlsState<VPL * 32, CPL * 32>;
+    if (count_dev) count = min(count, int64_t(*count_dev));
     __shared__ State states[kMtWarps];
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -524,9 +528,10 @@ __device__ void fractions(const TissueDev& T, const double* fod, const double* s
 // with their fractions kept for the next comparison.
 __global__ void __launch_bounds__(kMtWarps * 32, 8) lr_fractions_kernel(
     TissueDev T, const double* __restrict__ signals, const double* __restrict__ fods, int ldf,
-    const int* __restrict__ list, int64_t count, int round, int max_rounds, double fraction_tol,
-    double* __restrict__ fiso, double* __restrict__ prev, int32_t* __restrict__ rounds, int* __restrict__ next,
-    int* next_count, int* queue, double* __restrict__ workspace, size_t slot_size) {
+    const int* __restrict__ list, int64_t count, const int* __restrict__ count_dev, int round, int max_rounds,
+    double fraction_tol, double* __restrict__ fiso, double* __restrict__ prev, int32_t* __restrict__ rounds,
+    int* __restrict__ next, int* next_count, int* queue, double* __restrict__ workspace, size_t slot_size) {
+    if (count_dev) count = min(count, int64_t(*count_dev));
     __shared__ FracState states[kMtWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     FracState& st = states[warp];
@@ -615,8 +620,8 @@ struct Carver {
 
 // Launches the ridge NNLS of `count` listed voxels on the instantiation that fits the solver.
 struct NnlsLaunch {
-    void (*kernel)(RidgeDev, SignalDev, const int*, int64_t, const double*, int, double*, int, uint8_t*, int*,
-                   double*, size_t);
+    void (*kernel)(RidgeDev, SignalDev, const int*, int64_t, const int*, const double*, int, double*, int, uint8_t*,
+                   int*, double*, size_t);
     int cap;
     const char* name;
 };
@@ -627,15 +632,16 @@ inline NnlsLaunch nnls_variant(int c) {
     return {ridge_nnls_kernel<kCholCap / 32, kMaxColumns / 32>, kCholCap, "ridge_nnls_kernel<8,20>"};
 }
 
-inline void launch_correlate(const SignalDev& S, const int* list, int64_t count, const RidgeDev& R, double* corr,
-                             int ldc, cudaStream_t st) {
+inline void launch_correlate(const SignalDev& S, const int* list, int64_t count, const int* count_dev,
+                             const RidgeDev& R, double* corr, int ldc, cudaStream_t st) {
     if (count == 0) return;
     const unsigned gx = unsigned((count + kCorrVoxels - 1) / kCorrVoxels);
     LaunchScope scope("correlate_kernel", st);
     if (R.c <= 48) {
-        correlate_kernel<3><<<dim3(gx, 1), 128, 0, st>>>(S, list, count, R.k, R.c, corr, ldc);
+        correlate_kernel<3><<<dim3(gx, 1), 128, 0, st>>>(S, list, count, count_dev, R.k, R.c, corr, ldc);
     } else {
-        correlate_kernel<4><<<dim3(gx, unsigned((R.c + 63) / 64)), 128, 0, st>>>(S, list, count, R.k, R.c, corr, ldc);
+        correlate_kernel<4><<<dim3(gx, unsigned((R.c + 63) / 64)), 128, 0, st>>>(S, list, count, count_dev, R.k, R.c,
+                                                                                 corr, ldc);
     }
     cuda_check(cudaGetLastError(), "correlate_kernel launch");
 }
@@ -659,6 +665,19 @@ struct lar_fod_solver_s {
     int* count_buffer() {
         if (!pinned) lar::cuda_check(cudaMallocHost(&pinned, sizeof(int)), "cudaMallocHost");
         return pinned;
+    }
+    // The shell weights on the device, uploaded when they differ from the last call's. Under
+    // stream capture nothing may be uploaded, so they must match an earlier uncaptured call.
+    std::vector<double> weights_host;
+    lar::DeviceArray<double> weights_dev;
+    const double* device_weights(const double* w, int64_t m, bool capturing) {
+        if (weights_host.size() != size_t(m) || !std::equal(w, w + m, weights_host.begin())) {
+            lar::require(!capturing, "under stream capture the weights must be those of an earlier uncaptured "
+                                     "call with this solver");
+            weights_host.assign(w, w + m);
+            weights_dev.upload(weights_host.data(), weights_host.size());
+        }
+        return weights_dev.ptr;
     }
     lar::RidgeDev view() const {
         return lar::RidgeDev{int(host.m), int(host.c), host.ridge, tol, host.normal_equations ? 1 : 0, k.ptr, gram.ptr};
@@ -785,8 +804,7 @@ int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights
             std::max(std::max(size_t(lr_slots) * lr_slot, size_t(hr_slots) * hr_slot),
                      std::max(size_t(lf_slots) * lf_slot, size_t(hf_slots) * hf_slot));
         struct Pieces {
-            int* counters;  // [0] the persistent kernels' work counter, [1] the next round's count
-            double* weights;
+            int* counters;  // [0] the persistent kernels' work counter, [2], [3] the two lists' counts
             int* list[2];
             double *fiso, *prev, *corr, *xlr, *slots;
             int32_t* rounds;
@@ -795,7 +813,6 @@ int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights
         auto carve_all = [&](Carver& cv) {
             Pieces p;
             p.counters = cv.take<int>(8);
-            p.weights = cv.take<double>(size_t(m));
             p.list[0] = cv.take<int>(size_t(n_max));
             p.list[1] = cv.take<int>(size_t(n_max));
             p.fiso = cv.take<double>(size_t(n_max) * std::max(ci, 1));
@@ -811,10 +828,14 @@ int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights
         carve_all(sizing);
         Carver cv{static_cast<char*>(hr_solver->reserve(sizing.used))};
         const Pieces P = carve_all(cv);
-        int* host_count = hr_solver->count_buffer();
         auto st = static_cast<cudaStream_t>(stream);
-        cuda_check(cudaMemcpyAsync(P.weights, weights, size_t(m) * sizeof(double), cudaMemcpyHostToDevice, st),
-                   "cudaMemcpyAsync (weights)");
+        // Under stream capture (a CUDA graph) nothing may wait on the host: every round is
+        // enqueued and reads its voxel count on the device, exiting at once when it is 0.
+        cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+        cuda_check(cudaStreamIsCapturing(st, &capture), "cudaStreamIsCapturing");
+        const bool graph = capture != cudaStreamCaptureStatusNone;
+        const double* dweights = hr_solver->device_weights(weights, m, graph);
+        int* host_count = graph ? nullptr : hr_solver->count_buffer();
         auto blocks = [](int64_t slots, int64_t count) {
             return unsigned(std::max<int64_t>(1, std::min<int64_t>(slots / kMtWarps, (count + kMtWarps - 1) / kMtWarps)));
         };
@@ -825,41 +846,53 @@ int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights
             if (ci > 0) cuda_check(cudaMemsetAsync(P.fiso, 0, size_t(n) * ci * sizeof(double), st), "cudaMemsetAsync");
             cuda_check(cudaMemsetAsync(P.rounds, 0, size_t(n) * sizeof(int32_t), st), "cudaMemsetAsync");
             cuda_check(cudaMemsetAsync(P.bad, 0, size_t(n), st), "cudaMemsetAsync");
-            const SignalDev lr_sig{sig, P.weights, lrt.wiso, P.fiso, mi, ci};
-            const int* cur = nullptr;  // the first round takes every voxel
-            int* nxt = P.list[0];
+            const SignalDev lr_sig{sig, dweights, lrt.wiso, P.fiso, mi, ci};
+            // The first round takes every voxel; later rounds the list the previous one wrote,
+            // with its count read back on the host (or, under capture, on the device).
+            const int* cur = nullptr;
+            const int* cur_count = nullptr;
+            int side = 0;
             int64_t count = n;
             for (int round = 0; round < max_rounds && count > 0; ++round) {
-                launch_correlate(lr_sig, cur, count, lrs, P.corr, c_lr, st);
-                cuda_check(cudaMemsetAsync(P.counters, 0, 2 * sizeof(int), st), "cudaMemsetAsync");
+                int* nxt = P.list[side];
+                int* nxt_count = P.counters + 2 + side;
+                launch_correlate(lr_sig, cur, count, cur_count, lrs, P.corr, c_lr, st);
+                reset_queue();
+                cuda_check(cudaMemsetAsync(nxt_count, 0, sizeof(int), st), "cudaMemsetAsync");
                 {
                     LaunchScope scope(lr_nnls.name, st);
                     lr_nnls.kernel<<<blocks(lr_slots, count), kMtWarps * 32, lr_smem, st>>>(
-                        lrs, lr_sig, cur, count, P.corr, c_lr, P.xlr, c_lr, P.bad, P.counters, P.slots, lr_slot);
+                        lrs, lr_sig, cur, count, cur_count, P.corr, c_lr, P.xlr, c_lr, P.bad, P.counters, P.slots,
+                        lr_slot);
                     cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
                 }
                 reset_queue();
                 {
                     LaunchScope scope("lr_fractions_kernel", st);
                     lr_fractions_kernel<<<blocks(lf_slots, count), kMtWarps * 32, 0, st>>>(
-                        lrt, sig, P.xlr, c_lr, cur, count, round, max_rounds, fraction_tol, P.fiso, P.prev, P.rounds,
-                        nxt, P.counters + 1, P.counters, P.slots, lf_slot);
+                        lrt, sig, P.xlr, c_lr, cur, count, cur_count, round, max_rounds, fraction_tol, P.fiso, P.prev,
+                        P.rounds, nxt, nxt_count, P.counters, P.slots, lf_slot);
                     cuda_check(cudaGetLastError(), "lr_fractions_kernel launch");
                 }
-                cuda_check(cudaMemcpyAsync(host_count, P.counters + 1, sizeof(int), cudaMemcpyDeviceToHost, st),
-                           "cudaMemcpyAsync (round count)");
-                cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
-                count = *host_count;
+                if (!graph) {
+                    cuda_check(cudaMemcpyAsync(host_count, nxt_count, sizeof(int), cudaMemcpyDeviceToHost, st),
+                               "cudaMemcpyAsync (round count)");
+                    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+                    count = *host_count;
+                } else {
+                    cur_count = nxt_count;
+                }
                 cur = nxt;
-                nxt = nxt == P.list[0] ? P.list[1] : P.list[0];
+                side ^= 1;
             }
-            const SignalDev hr_sig{sig, P.weights, hrt.wiso, P.fiso, mi, ci};
-            launch_correlate(hr_sig, nullptr, n, hrs, P.corr, c_hr, st);
+            const SignalDev hr_sig{sig, dweights, hrt.wiso, P.fiso, mi, ci};
+            launch_correlate(hr_sig, nullptr, n, nullptr, hrs, P.corr, c_hr, st);
             reset_queue();
             {
                 LaunchScope scope(hr_nnls.name, st);
                 hr_nnls.kernel<<<blocks(hr_slots, n), kMtWarps * 32, hr_smem, st>>>(
-                    hrs, hr_sig, nullptr, n, P.corr, c_hr, fods + v0 * c_hr, c_hr, P.bad, P.counters, P.slots, hr_slot);
+                    hrs, hr_sig, nullptr, n, nullptr, P.corr, c_hr, fods + v0 * c_hr, c_hr, P.bad, P.counters, P.slots,
+                    hr_slot);
                 cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
             }
             reset_queue();
@@ -869,8 +902,6 @@ int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights
                 rounds ? rounds + v0 : nullptr, status ? status + v0 : nullptr, P.counters, P.slots, hf_slot);
             cuda_check(cudaGetLastError(), "hr_fractions_kernel launch");
         }
-        // The weights' host buffer is the caller's; the copy must finish before it returns.
-        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
     });
 }
 
@@ -903,12 +934,12 @@ int lar_fit_single_tissue(const double* signals, int64_t v, lar_fod_solver solve
         for (int64_t v0 = 0; v0 < v; v0 += n_max) {
             const int64_t n = std::min(n_max, v - v0);
             const SignalDev S{signals + v0 * m, nullptr, nullptr, nullptr, m, 0};
-            launch_correlate(S, nullptr, n, R, corr, c, st);
+            launch_correlate(S, nullptr, n, nullptr, R, corr, c, st);
             if (status) cuda_check(cudaMemsetAsync(status + v0, 0, size_t(n), st), "cudaMemsetAsync");
             cuda_check(cudaMemsetAsync(counters, 0, sizeof(int), st), "cudaMemsetAsync");
             const unsigned nb = unsigned(std::max<int64_t>(1, std::min<int64_t>(slots / kMtWarps, (n + kMtWarps - 1) / kMtWarps)));
             LaunchScope scope(nn.name, st);
-            nn.kernel<<<nb, kMtWarps * 32, smem, st>>>(R, S, nullptr, n, corr, c, fods + v0 * c, c,
+            nn.kernel<<<nb, kMtWarps * 32, smem, st>>>(R, S, nullptr, n, nullptr, corr, c, fods + v0 * c, c,
                                                        status ? status + v0 : nullptr, counters, work, slot);
             cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
         }
