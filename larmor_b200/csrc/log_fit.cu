@@ -274,7 +274,16 @@ const LogDesignDevice<double>& device_view<double>(const lar_log_design_s* h) { 
 template <>
 const LogDesignDevice<float>& device_view<float>(const lar_log_design_s* h) { return h->d32; }
 
-constexpr int kSmallBlock = 64;
+// Voxels per CTA of the shared-memory fits: 64, or 32 / 16 when the design and a CTA's signals
+// of 64 voxels do not fit in shared memory (tables of more than about 200 measurements).
+inline int small_block(int n, int raw_bytes, size_t per_value) {
+    for (int block : {64, 32, 16}) {
+        const size_t bytes = size_t(n) * (2 * 7 + 28) * per_value + size_t(n) * block * per_value +
+                             size_t(n) * block * raw_bytes + 16;
+        if (bytes <= 227 * 1024) return block;
+    }
+    return 16;
+}
 
 template <class Kernel>
 void set_smem(Kernel kernel, size_t bytes) {
@@ -342,14 +351,19 @@ void launch_fit(lar_log_design_s* h, const double* log_s, int64_t v, int weighte
     const int p = int(h->host.p);
     LogSource src{log_s, h->host.n};
     if (p == 7 && h->host.m == 0) {
-        const size_t sm = SmallFit<T, 7>::bytes(d.n, kSmallBlock, LogSource::raw_bytes);
-        auto kernel = fit_log_small_kernel<T, 7, kSmallBlock, LogSource>;
-        set_smem(kernel, sm);
-        const int64_t grid = (v + kSmallBlock - 1) / kSmallBlock;
-        LaunchScope scope("fit_log_small_kernel", stream);
-        kernel<<<unsigned(grid), kSmallBlock, sm, stream>>>(d, src, v, weighted, max_rw, T(tol), params,
-                                                            broke, iterations);
-        cuda_check(cudaGetLastError(), "fit_log_small_kernel launch");
+        auto run = [&](auto kernel, int block) {
+            const size_t sm = SmallFit<T, 7>::bytes(d.n, block, LogSource::raw_bytes);
+            set_smem(kernel, sm);
+            const int64_t grid = (v + block - 1) / block;
+            LaunchScope scope("fit_log_small_kernel", stream);
+            kernel<<<unsigned(grid), block, sm, stream>>>(d, src, v, weighted, max_rw, T(tol), params, broke,
+                                                          iterations);
+            cuda_check(cudaGetLastError(), "fit_log_small_kernel launch");
+        };
+        const int block = small_block(d.n, LogSource::raw_bytes, sizeof(T));
+        if (block == 64) run(fit_log_small_kernel<T, 7, 64, LogSource>, 64);
+        else if (block == 32) run(fit_log_small_kernel<T, 7, 32, LogSource>, 32);
+        else run(fit_log_small_kernel<T, 7, 16, LogSource>, 16);
         return;
     }
     launch_general<T>(h, src, v, weighted, max_rw, tol, params, broke, iterations, stream);
@@ -361,13 +375,18 @@ void launch_dti_maps(const lar_log_design_s* h, const float* s, const double* fl
                      double* params, cudaStream_t stream) {
     const auto& d = device_view<T>(h);
     FlooredSource src{s, floor, h->host.n};
-    const size_t sm = SmallFit<T, 7>::bytes(d.n, kSmallBlock, FlooredSource::raw_bytes);
-    auto kernel = fit_dti_maps_kernel<T, kSmallBlock>;
-    set_smem(kernel, sm);
-    const int64_t grid = (v + kSmallBlock - 1) / kSmallBlock;
-    LaunchScope scope("fit_dti_maps_kernel", stream);
-    kernel<<<unsigned(grid), kSmallBlock, sm, stream>>>(d, src, v, weighted, max_rw, T(tol), maps, npd, params);
-    cuda_check(cudaGetLastError(), "fit_dti_maps_kernel launch");
+    auto run = [&](auto kernel, int block) {
+        const size_t sm = SmallFit<T, 7>::bytes(d.n, block, FlooredSource::raw_bytes);
+        set_smem(kernel, sm);
+        const int64_t grid = (v + block - 1) / block;
+        LaunchScope scope("fit_dti_maps_kernel", stream);
+        kernel<<<unsigned(grid), block, sm, stream>>>(d, src, v, weighted, max_rw, T(tol), maps, npd, params);
+        cuda_check(cudaGetLastError(), "fit_dti_maps_kernel launch");
+    };
+    const int block = small_block(d.n, FlooredSource::raw_bytes, sizeof(T));
+    if (block == 64) run(fit_dti_maps_kernel<T, 64>, 64);
+    else if (block == 32) run(fit_dti_maps_kernel<T, 32>, 32);
+    else run(fit_dti_maps_kernel<T, 16>, 16);
 }
 
 template <class T>

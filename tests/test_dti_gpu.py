@@ -106,3 +106,31 @@ def test_fp32_variant_stays_near_the_fp64_fit(cuda, oracle):
     f32 = DTIModel(fit_method="wls", precision="fp32").fit(w.volume, w.gtab, w.mask)
     assert np.abs(f32.fa - f64.fa).max() < 1e-3
     assert np.abs(f32.md - f64.md).max() < 1e-6
+
+
+@pytest.mark.parametrize("shells", [2, 3])
+def test_large_tables_use_smaller_ctas_and_match_the_oracle(cuda, oracle, shells):
+    """Tables of 200-290 measurements (2-3 shells of 90 directions) do not fit 64 voxels per CTA
+    in shared memory; the fit takes 32 or 16 voxels per CTA and still matches the oracle."""
+    from larmor_b200 import _core
+    from larmor_b200.dwi.dti import dti_design
+    from larmor_b200.synthetic import random_rotations, unit_directions
+    from larmor_b200.types import GradientTable
+
+    rng = np.random.default_rng(40 + shells)
+    dirs = [unit_directions(rng, 90) for _ in range(shells)]
+    bvals = np.concatenate([np.zeros(18)] + [np.full(90, 1000.0 * (k + 1)) for k in range(shells)])
+    bvecs = np.vstack([np.zeros((18, 3))] + dirs)
+    design = dti_design(GradientTable(bvals, bvecs))
+    v = 700
+    rot = random_rotations(rng, v)
+    ev = np.stack([rng.uniform(1.2e-3, 2e-3, v), *(2 * [rng.uniform(0.2e-3, 0.6e-3, v)])], axis=1)
+    tensors = np.einsum("vij,vj,vkj->vik", rot, ev, rot)
+    g = GradientTable(bvals, bvecs)
+    s = 1000.0 * np.exp(-g.bvals[None, :] * np.einsum("ni,vij,nj->vn", g.bvecs, tensors, g.bvecs))
+    s = np.abs(s + rng.normal(0, 20.0, s.shape) + 1j * rng.normal(0, 20.0, s.shape))
+    log_s = np.ascontiguousarray(np.log(s))
+    params, broke = _core.fit_log_signal(design, np.zeros((0, 7)), log_s, True, 20, 1e-6, 1)
+    ref, _ = oracle.fit_log_signal(design, None, log_s, True)
+    sc = np.linalg.norm(design, axis=0)
+    np.testing.assert_allclose(params * sc, ref * sc, rtol=0, atol=1e-10)
