@@ -313,7 +313,7 @@ class MfodWorkload(_SdWorkloadBase):
     (44 in the loop) + GM + CSF, up to 50 rounds, on S0-normalised signals."""
 
     name = "mfod_3tissue_110x110x70"
-    kernels = ("correlate_kernel", "ridge_nnls_kernel<2,2>", "lr_fractions_kernel", "ridge_nnls_kernel<8,10>",
+    kernels = ("correlate_kernel", "ridge_nnls_kernel<1,2>", "lr_fractions_kernel", "ridge_nnls_kernel<8,10>",
                "hr_fractions_kernel")
     has_fp32 = False
     # 280 double samples in, 300 double amplitudes + 3 fractions out.
@@ -373,7 +373,7 @@ class MfodWorkload(_SdWorkloadBase):
         vr = int(rounds.sum().item())
         m, c_lr, c_hr = 280, self.k_lr.ca, self.k_hr.ca
         return {"correlate_kernel": vr * 8 * (m + c_lr) + self.v * 8 * (m + c_hr),
-                "ridge_nnls_kernel<2,2>": vr * 8 * 2 * c_lr,
+                "ridge_nnls_kernel<1,2>": vr * 8 * 2 * c_lr,
                 "lr_fractions_kernel": vr * 8 * (c_lr + m + 3),
                 "ridge_nnls_kernel<8,10>": self.v * 8 * 2 * c_hr,
                 "hr_fractions_kernel": self.v * 8 * (c_hr + m + 3)}
@@ -474,7 +474,7 @@ def _job_kernel_bytes(job) -> dict:
     vr = int(job.out["rounds"].sum().item())
     c_lr, c_hr = job.handles["k_lr"].ca, job.handles["k_hr"].ca
     return {"correlate_kernel": vr * 8 * (n + c_lr) + v * 8 * (n + c_hr),
-            "ridge_nnls_kernel<2,2>": vr * 8 * 2 * c_lr,
+            "ridge_nnls_kernel<1,2>": vr * 8 * 2 * c_lr,
             "lr_fractions_kernel": vr * 8 * (c_lr + n + 3),
             "ridge_nnls_kernel<8,10>": v * 8 * 2 * c_hr,
             "hr_fractions_kernel": v * 8 * (c_hr + n + 3)}
@@ -487,7 +487,7 @@ class BatchWorkload:
 
     name = "batch_uneven_64_volumes"
     kernels = ("fit_dti_maps_kernel", "fit_log_warp_kernel", "constrained_fit_kernel", "dki_maps_kernel",
-               "correlate_kernel", "ridge_nnls_kernel<2,2>", "lr_fractions_kernel", "ridge_nnls_kernel<8,10>",
+               "correlate_kernel", "ridge_nnls_kernel<1,2>", "lr_fractions_kernel", "ridge_nnls_kernel<8,10>",
                "hr_fractions_kernel")
     has_fp32 = False
 
@@ -617,9 +617,12 @@ def run_serving(args) -> dict:
 
     jobs = _serve_jobs(5, args.serve_requests)
     voxels = sum(j.voxels for j in jobs)
-    # Warm-up: the handles of every slot and the kernels' first launches.
+    # Warm-up: the largest request on every slot at once, so that each slot's handles and
+    # scratch are built and sized before the timed arrivals (growing scratch later would free
+    # and allocate device memory, which waits for the whole GPU).
     server = FitServer(budget_bytes=80 << 30, slots=args.serve_slots)
-    for f in [server.submit(j) for j in jobs[:args.serve_slots]]:
+    largest = max(jobs, key=lambda j: j.voxels)
+    for f in [server.submit(largest) for _ in range(args.serve_slots)]:
         f.result()
     # Plain per-request fits: one request at a time, back to back.
     t0 = time.perf_counter()

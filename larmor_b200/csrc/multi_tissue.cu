@@ -156,15 +156,15 @@ __global__ void __launch_bounds__(128) correlate_kernel(SignalDev S, const int* 
 // ---- ridge NNLS ------------------------------------------------------------------------
 
 // A warp's NNLS workspace. Shared memory: the solution x, its candidate z, the factor's vectors
-// h, w and y (InvFactor), the active and in-factor flags. Global slot: the packed inverse
-// factor, the signal (for the QR fallback) and the QR workspace.
+// h, w and y (InvFactor), the active and in-factor flags. Global slot: the packed factor and
+// its inverse, the signal (for the QR fallback) and the QR workspace.
 struct NnlsSlot {
-    double *x, *z, *h, *w, *y, *M, *sig, *qsub, *qd, *qrv;
+    double *x, *z, *h, *w, *y, *L, *M, *sig, *qsub, *qd, *qrv;
     uint8_t *flag, *inf;
 };
 
 inline size_t nnls_slot_doubles(int m, int cap) {
-    return size_t(tri_row(cap)) + size_t(m) + size_t(m + kQrCap) * kQrCap + 2 * size_t(m + kQrCap) + 8;
+    return 2 * size_t(packed_size(cap)) + size_t(m) + size_t(m + kQrCap) * kQrCap + 2 * size_t(m + kQrCap) + 8;
 }
 
 __host__ __device__ inline size_t nnls_smem_bytes(int c, int cap) {
@@ -174,7 +174,8 @@ __host__ __device__ inline size_t nnls_smem_bytes(int c, int cap) {
 __device__ NnlsSlot carve_nnls(double* base, unsigned char* smem, int m, int c, int cap) {
     NnlsSlot s;
     double* p = base;
-    s.M = p; p += tri_row(cap);
+    s.L = p; p += packed_size(cap);
+    s.M = p; p += packed_size(cap);
     s.sig = p; p += m;
     s.qsub = p; p += size_t(m + kQrCap) * kQrCap;
     s.qd = p; p += m + kQrCap;
@@ -212,7 +213,7 @@ struct StackedColumns {
 // Least squares on the active columns by QR (fit_by_qr, cpp/src/sd/nnls.cpp:385-401); false
 // when more columns are active than the QR workspace holds.
 template <class State>
-__device__ __noinline__ bool ridge_qr_fit(const RidgeDev& R, const double* sig, NnlsSlot& sl, State& st, int lane) {
+__device__ __noinline__ bool ridge_qr_fit(const RidgeDev R, const double* sig, const NnlsSlot sl, State& st, int lane) {
     int k = 0;
     if (lane == 0) {
         for (int j = 0; j < R.c; ++j)
@@ -238,11 +239,17 @@ __device__ __noinline__ bool ridge_qr_fit(const RidgeDev& R, const double* sig, 
 // cpp/src/sd/nnls.cpp:362-418) from corr = K^T sig, the result in sl.x. The signal itself is
 // built only when a QR fit needs it. Returns false only when the QR fallback's workspace
 // overflowed (x is then the last fit). VPL * 32 is the factor's capacity, CPL * 32 >= c.
+//
+// Inlined into its kernel with every argument by value, so that its state (the active count,
+// the flags, the workspace pointers) stays in registers; the outer (entering column) and inner
+// (blocking step) iterations of Lawson-Hanson share one loop with one fit, so the factor code
+// is emitted once.
 template <int VPL, int CPL, class State>
-__device__ __noinline__ bool ridge_nnls(const RidgeDev& R, const SignalDev& S, int64_t voxel,
-                                        const double* __restrict__ corr, NnlsSlot& sl, State& st, int lane) {
+__device__ __forceinline__ bool ridge_nnls(const RidgeDev R, const SignalDev S, int64_t voxel,
+                                           const double* __restrict__ corr, const NnlsSlot sl, State& st,
+                                           int lane) {
     const int c = R.c;
-    const InvFactor fac{sl.M, sl.h, sl.w, sl.y, st.cols, VPL * 32};
+    const InvFactor fac{sl.L, sl.M, sl.h, sl.w, sl.y, st.cols, VPL * 32};
     for (int j = lane; j < c; j += 32) {
         sl.x[j] = 0.0;
         sl.z[j] = 0.0;
@@ -254,103 +261,53 @@ __device__ __noinline__ bool ridge_nnls(const RidgeDev& R, const SignalDev& S, i
     bool failed = false, overflow = false, have_sig = false;
     int na = 0, inner = 0;
     const int max_inner = 3 * c;
-    auto append = [&](int j) {
-        for (int r = lane; r < na; r += 32) sl.h[r] = R.gram[size_t(st.cols[r]) * c + j];
-        __syncwarp();
-        return inv_append<VPL>(fac, na, R.gram[size_t(j) * c + j], corr[j], j, kMinPivot, lane);
-    };
-    // fit_on: the factor brought to the active set (ActiveCholesky::update, :246-262), or QR from
-    // the first failing pivot on. Columns that left the active set leave the factor, the columns
-    // after the first of them are appended again in their order (the factor of the remaining
-    // columns in joining order), then `entering`, the column that joined since the last fit (or
-    // -1; every other active column is in the factor already, so update()'s scan appends only it).
-    auto fit_on = [&](int entering) {
-        if (!use_qr_only && !failed) {
-            int cut = na;
-            for (int pos = 0; pos < na; ++pos)
-                if (!sl.flag[st.cols[pos]]) {
-                    cut = pos;
-                    break;
-                }
-            if (cut < na) {
-                int keep = 0;
-                if (lane == 0) {
-                    for (int pos = cut; pos < na; ++pos) {
-                        const int col = st.cols[pos];
-                        if (sl.flag[col]) st.sorted[keep++] = col;
-                        else sl.inf[col] = 0;
-                    }
-                }
-                keep = __shfl_sync(0xffffffffu, keep, 0);
-                __syncwarp();
-                na = cut;
-                for (int q = 0; q < keep && !failed; ++q) failed = !append(st.sorted[q]);
-            }
-            if (!failed && entering >= 0 && sl.flag[entering] && !sl.inf[entering]) {
-                if (!append(entering)) {
-                    failed = true;
-                } else {
-                    if (lane == 0) sl.inf[entering] = 1;
-                    __syncwarp();
-                }
-            }
-        }
-        if (use_qr_only || failed) {
-            if (!have_sig) {
-                for (int i = lane; i < R.m; i += 32) sl.sig[i] = S(voxel, i);
-                __syncwarp();
-                have_sig = true;
-            }
-            overflow |= !ridge_qr_fit(R, sl.sig, sl, st, lane);
-        } else {
-            inv_solve<VPL>(fac, na, sl.z, c, lane);
-        }
-    };
+    bool blocked = false;  // the last fit left an active column at or below zero: an inner step
     for (;;) {
-        // Gradient corr - G x over the non-zero x, columns in increasing order; the steepest
-        // inactive entry, the first on a tie.
-        int n_sorted = 0;
-        for (int base = 0; base < c; base += 32) {
-            const int j = base + lane;
-            const bool nz = j < c && sl.x[j] != 0.0;
-            const unsigned ballot = __ballot_sync(0xffffffffu, nz);
-            if (nz) st.sorted[n_sorted + __popc(ballot & ((1u << lane) - 1u))] = j;
-            n_sorted += __popc(ballot);
-        }
-        __syncwarp();
-        double g[CPL];
-#pragma unroll
-        for (int t = 0; t < CPL; ++t) {
-            const int j = lane + 32 * t;
-            g[t] = j < c ? corr[j] : 0.0;
-        }
-        for (int q = 0; q < n_sorted; ++q) {
-            const int col = st.sorted[q];
-            const double xc = sl.x[col];
-            const double* row = R.gram + size_t(col) * c;
+        int entering = -1;
+        if (!blocked) {
+            // Outer step: the gradient corr - G x over the non-zero x, columns in increasing
+            // order; the steepest inactive entry, the first on a tie.
+            int n_sorted = 0;
+            for (int base = 0; base < c; base += 32) {
+                const int j = base + lane;
+                const bool nz = j < c && sl.x[j] != 0.0;
+                const unsigned ballot = __ballot_sync(0xffffffffu, nz);
+                if (nz) st.sorted[n_sorted + __popc(ballot & ((1u << lane) - 1u))] = j;
+                n_sorted += __popc(ballot);
+            }
+            __syncwarp();
+            double g[CPL];
 #pragma unroll
             for (int t = 0; t < CPL; ++t) {
                 const int j = lane + 32 * t;
-                if (j < c) g[t] -= xc * row[j];
+                g[t] = j < c ? corr[j] : 0.0;
             }
-        }
-        double bv = 0.0;
-        int bi = -1;
+            for (int q = 0; q < n_sorted; ++q) {
+                const int col = st.sorted[q];
+                const double xc = sl.x[col];
+                const double* row = R.gram + size_t(col) * c;
 #pragma unroll
-        for (int t = 0; t < CPL; ++t) {
-            const int j = lane + 32 * t;
-            if (j < c && !sl.flag[j] && (bi < 0 || g[t] > bv)) { bv = g[t]; bi = j; }
-        }
-        const int e = warp_argmax_first(bv, bi);
-        const double ge = e >= 0 ? __shfl_sync(0xffffffffu, bv, e & 31) : 0.0;
-        if (e < 0 || ge <= R.tol) break;
-        if (lane == 0) sl.flag[e] = 1;
-        __syncwarp();
-        fit_on(e);
-        for (;;) {
-            bool any = false;
-            for (int j = lane; j < c; j += 32) any |= sl.flag[j] && sl.z[j] <= 0.0;
-            if (!__any_sync(0xffffffffu, any)) break;
+                for (int t = 0; t < CPL; ++t) {
+                    const int j = lane + 32 * t;
+                    if (j < c) g[t] -= xc * row[j];
+                }
+            }
+            double bv = 0.0;
+            int bi = -1;
+#pragma unroll
+            for (int t = 0; t < CPL; ++t) {
+                const int j = lane + 32 * t;
+                if (j < c && !sl.flag[j] && (bi < 0 || g[t] > bv)) { bv = g[t]; bi = j; }
+            }
+            const int e = warp_argmax_first(bv, bi);
+            const double ge = e >= 0 ? __shfl_sync(0xffffffffu, bv, e & 31) : 0.0;
+            if (e < 0 || ge <= R.tol) break;
+            if (lane == 0) sl.flag[e] = 1;
+            __syncwarp();
+            entering = e;
+        } else {
+            // Inner step: move towards the fit until the first active column reaches zero,
+            // drop it and every active column below the tolerance.
             if (++inner > max_inner) {
                 // The last least-squares fit is the answer (cpp/src/sd/nnls.cpp:204-207).
                 for (int j = lane; j < c; j += 32) sl.x[j] = sl.z[j];
@@ -377,10 +334,49 @@ __device__ __noinline__ bool ridge_nnls(const RidgeDev& R, const SignalDev& S, i
             for (int j = lane; j < c; j += 32)
                 if (sl.flag[j] && !(fabs(sl.x[j]) >= R.tol)) sl.flag[j] = 0;
             __syncwarp();
-            fit_on(-1);
         }
-        for (int j = lane; j < c; j += 32) sl.x[j] = sl.z[j];
-        __syncwarp();
+        // The fit on the active set (ActiveCholesky::update, :246-262), or QR from the first
+        // failing pivot on: the columns that left the active set leave the factor (from the
+        // last position down), then the entering column joins (every other active column is
+        // in the factor already, so update()'s scan appends only it).
+        if (!use_qr_only && !failed) {
+            for (int pos = na - 1; pos >= 0; --pos) {
+                const int col = st.cols[pos];
+                if (sl.flag[col]) continue;
+                inv_remove(fac, na, pos, lane);
+                if (lane == 0) sl.inf[col] = 0;
+                --na;
+                __syncwarp();
+            }
+            if (entering >= 0) {
+                for (int r = lane; r < na; r += 32) sl.h[r] = R.gram[size_t(st.cols[r]) * c + entering];
+                __syncwarp();
+                if (!inv_append<VPL>(fac, na, R.gram[size_t(entering) * c + entering], corr[entering], entering,
+                                     kMinPivot, lane)) {
+                    failed = true;
+                } else {
+                    if (lane == 0) sl.inf[entering] = 1;
+                    __syncwarp();
+                }
+            }
+        }
+        if (use_qr_only || failed) {
+            if (!have_sig) {
+                for (int i = lane; i < R.m; i += 32) sl.sig[i] = S(voxel, i);
+                __syncwarp();
+                have_sig = true;
+            }
+            overflow |= !ridge_qr_fit(R, sl.sig, sl, st, lane);
+        } else {
+            inv_solve<VPL>(fac, na, sl.z, c, lane);
+        }
+        bool any = false;
+        for (int j = lane; j < c; j += 32) any |= sl.flag[j] && sl.z[j] <= 0.0;
+        blocked = __any_sync(0xffffffffu, any);
+        if (!blocked) {
+            for (int j = lane; j < c; j += 32) sl.x[j] = sl.z[j];
+            __syncwarp();
+        }
     }
     return !overflow;
 }
@@ -627,7 +623,9 @@ struct NnlsLaunch {
 };
 
 inline NnlsLaunch nnls_variant(int c) {
-    if (c <= 64) return {ridge_nnls_kernel<2, 2>, 64, "ridge_nnls_kernel<2,2>"};
+    // Up to 64 directions (the low-resolution kernels): a 32-column factor, the active sets
+    // being far smaller (past 32 active columns the fit continues by QR).
+    if (c <= 64) return {ridge_nnls_kernel<1, 2>, 32, "ridge_nnls_kernel<1,2>"};
     if (c <= 320) return {ridge_nnls_kernel<kCholCap / 32, 10>, kCholCap, "ridge_nnls_kernel<8,10>"};
     return {ridge_nnls_kernel<kCholCap / 32, kMaxColumns / 32>, kCholCap, "ridge_nnls_kernel<8,20>"};
 }

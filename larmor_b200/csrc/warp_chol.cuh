@@ -157,16 +157,25 @@ __device__ __noinline__ void factor_solve(const WarpFactor& f, int na, const dou
 namespace lar {
 
 // The inverse M = L^-1 of a growing Cholesky factor L of a Gram matrix on an active set, held by
-// one warp, with y = M rhs_A: the active-set solve z_A = G_AA^-1 rhs_A = M^T y becomes one
-// triangular matrix-vector product (lanes over the columns of M, its rows read whole), and an
-// appended column two such products and a reduction, instead of serial substitutions.
+// one warp next to L itself, with y = M rhs_A: the active-set solve z_A = G_AA^-1 rhs_A = M^T y
+// becomes one triangular matrix-vector product (lanes over the columns of M, its rows read
+// whole), and an appended column two such products and a reduction, instead of serial
+// substitutions.
 //
 // Appending column e with cross entries h = G(A, e) and diagonal g_ee: w = M h, the pivot
-// d^2 = g_ee - w.w, the new row of M is -(w^T M) / d with 1 / d on the diagonal, and
+// d^2 = g_ee - w.w, L's new row is [w^T d], M's is [-(w^T M) / d, 1 / d], and
 // y_e = (rhs_e - w.y) / d, since L_new = [L 0; w^T d].
 //
-// Storage: M as packed rows (row r at r (r + 1) / 2); h, w and y in shared memory.
+// Removing the column at position p (ActiveCholesky's downdate, cpp/src/sd/nnls.cpp:305-324):
+// L's rows below p move up and Givens rotations G_k of its columns (k, k+1), k = p..na-2, clear
+// the entries left above the diagonal: L~ Q = [L' 0] with Q = G_p ... G_{na-2}. Then
+// L'^-1 is Q^T M without its last row and without column p (which Q^T M holds as zeros there):
+// the same rotations, transposed, act on the rows (k, k+1) of M and on y.
+//
+// Storage: L and M as packed rows (row r at r (r + 3) / 2 with r + 2 slots: the columns 0..r
+// and the one a rotation fills transiently); h, w and y in shared memory.
 struct InvFactor {
+    double* L;    // packed rows
     double* M;    // packed rows
     double* h;    // (cap,) the cross entries of the column being appended
     double* w;    // (cap,) M h
@@ -175,13 +184,11 @@ struct InvFactor {
     int cap;
 };
 
-__host__ __device__ constexpr int tri_row(int r) { return r * (r + 1) / 2; }
-
 // Appends column `col` (cross entries already in f.h[0..na)): false, leaving the factor as it
 // was, when the pivot is not above min_relative * h_cc or the factor is full.
 template <int VPL>
-__device__ __noinline__ bool inv_append(const InvFactor& f, int& na, double h_cc, double rhs_c, int col,
-                                        double min_relative, int lane) {
+__device__ __forceinline__ bool inv_append(const InvFactor f, int& na, double h_cc, double rhs_c, int col,
+                                           double min_relative, int lane) {
     if (na >= f.cap) return false;
     const int nt = (na + 31) >> 5;
     double w[VPL];
@@ -193,7 +200,7 @@ __device__ __noinline__ bool inv_append(const InvFactor& f, int& na, double h_cc
 #pragma unroll
         for (int t = 0; t < VPL; ++t) {
             const int r = lane + 32 * t;
-            if (t < nt && r >= j && r < na) w[t] = fma(f.M[tri_row(r) + j], hj, w[t]);
+            if (t < nt && r >= j && r < na) w[t] = fma(f.M[packed_row(r) + j], hj, w[t]);
         }
     }
     double sq = 0.0, wy = 0.0;
@@ -212,27 +219,33 @@ __device__ __noinline__ bool inv_append(const InvFactor& f, int& na, double h_cc
     if (!(pivot > min_relative * h_cc)) return false;
     const double d = sqrt(pivot), inv_d = 1.0 / d;
     __syncwarp();
-    // Row na of the new M: -(w^T M)_j / d for j < na (rows of M read whole), 1 / d on the diagonal.
+    // Row na of M: -(w^T M)_j / d for j < na (rows of M read whole), 1 / d on the diagonal;
+    // row na of L: w, d.
     double u[VPL];
 #pragma unroll
     for (int t = 0; t < VPL; ++t) u[t] = 0.0;
     for (int r = 0; r < na; ++r) {
         const double wr = f.w[r];
-        const double* row = f.M + tri_row(r);
+        const double* row = f.M + packed_row(r);
 #pragma unroll
         for (int t = 0; t < VPL; ++t) {
             const int j = lane + 32 * t;
             if (t < nt && j <= r) u[t] = fma(wr, row[j], u[t]);
         }
     }
-    double* nrow = f.M + tri_row(na);
+    double* mrow = f.M + packed_row(na);
+    double* lrow = f.L + packed_row(na);
 #pragma unroll
     for (int t = 0; t < VPL; ++t) {
         const int j = lane + 32 * t;
-        if (t < nt && j < na) nrow[j] = -u[t] * inv_d;
+        if (t < nt && j < na) {
+            mrow[j] = -u[t] * inv_d;
+            lrow[j] = f.w[j];
+        }
     }
     if (lane == 0) {
-        nrow[na] = inv_d;
+        mrow[na] = inv_d;
+        lrow[na] = d;
         f.y[na] = (rhs_c - wy) * inv_d;
         f.cols[na] = col;
     }
@@ -241,16 +254,65 @@ __device__ __noinline__ bool inv_append(const InvFactor& f, int& na, double h_cc
     return true;
 }
 
+// Removes the factor column at position pos of na (see above).
+__device__ __forceinline__ void inv_remove(const InvFactor f, int na, int pos, int lane) {
+    auto at = [&](double* base, int r, int c) -> double& { return base[packed_row(r) + c]; };
+    // L~: the rows below pos move up (row r + 1 has r + 2 entries, row r has r + 2 slots).
+    for (int row = pos; row < na - 1; ++row) {
+        for (int c = lane; c <= row + 1; c += 32) at(f.L, row, c) = at(f.L, row + 1, c);
+        __syncwarp();
+    }
+    if (lane == 0)
+        for (int q = pos; q < na - 1; ++q) f.cols[q] = f.cols[q + 1];
+    for (int k = pos; k < na - 1; ++k) {
+        const double diag = at(f.L, k, k), above = at(f.L, k, k + 1);
+        const double len = hypot(diag, above);
+        const double c = diag / len, s = above / len;
+        __syncwarp();
+        for (int row = k + lane; row < na - 1; row += 32) {
+            const double l = at(f.L, row, k), r = at(f.L, row, k + 1);
+            at(f.L, row, k) = c * l + s * r;
+            at(f.L, row, k + 1) = c * r - s * l;
+        }
+        // Rows (k, k + 1) of M and entries (k, k + 1) of y by G_k^T; row k's slot k + 1 is
+        // filled here (zero before).
+        for (int j = lane; j <= k + 1; j += 32) {
+            const double a = j <= k ? at(f.M, k, j) : 0.0, b = at(f.M, k + 1, j);
+            at(f.M, k, j) = c * a + s * b;
+            at(f.M, k + 1, j) = c * b - s * a;
+        }
+        if (lane == 0) {
+            const double a = f.y[k], b = f.y[k + 1];
+            f.y[k] = c * a + s * b;
+            f.y[k + 1] = c * b - s * a;
+        }
+        __syncwarp();
+    }
+    // Column pos leaves M's rows pos..na-2 (the columns after it move left); the last row goes.
+    for (int row = pos; row < na - 1; ++row) {
+        double* mr = f.M + packed_row(row);
+        // In chunks of 32 in increasing column order: each chunk reads its sources (one column
+        // to the right) before any lane writes, and later chunks read columns not yet written.
+        for (int base = pos; base <= row; base += 32) {
+            const int j = base + lane;
+            const double v = j <= row ? mr[j + 1] : 0.0;
+            __syncwarp();
+            if (j <= row) mr[j] = v;
+            __syncwarp();
+        }
+    }
+}
+
 // z (zlen, zero off the factor's columns) <- M^T y = G_AA^-1 rhs_A.
 template <int VPL>
-__device__ __noinline__ void inv_solve(const InvFactor& f, int na, double* z, int zlen, int lane) {
+__device__ __forceinline__ void inv_solve(const InvFactor f, int na, double* z, int zlen, int lane) {
     const int nt = (na + 31) >> 5;
     double acc[VPL];
 #pragma unroll
     for (int t = 0; t < VPL; ++t) acc[t] = 0.0;
     for (int r = 0; r < na; ++r) {
         const double yr = f.y[r];
-        const double* row = f.M + tri_row(r);
+        const double* row = f.M + packed_row(r);
 #pragma unroll
         for (int t = 0; t < VPL; ++t) {
             const int j = lane + 32 * t;
