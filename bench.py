@@ -765,12 +765,20 @@ def main() -> int:
         wl.subset(args.voxels)
     wl.device_setup(torch, dev)
     if args.profile:
+        from larmor_b200 import _core
+
         for i in range(args.warmup + args.steps):
+            last = i == args.warmup + args.steps - 1
+            _core.kernel_timing(last)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             wl.step_device()
             torch.cuda.synchronize()
             print(f"{wl.name} voxels {wl.v} step {i} {1e3 * (time.perf_counter() - t0):.3f} ms")
+        times = {k: _core.kernel_time(k) for k in wl.kernels}
+        _core.kernel_timing(False)
+        print("kernels (ms, launches) of the last step:",
+              ", ".join(f"{k} {t:.2f} ({n})" for k, (t, n) in times.items() if n))
         return 0
     flush = torch.empty(256 * 2**20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()

@@ -384,7 +384,7 @@ __device__ __forceinline__ bool ridge_nnls(const RidgeDev R, const SignalDev S, 
 // One warp per listed voxel, pulled from a device counter: x(v) <- the ridge NNLS of corr(v);
 // bad(v) <- 1 when the QR fallback overflowed.
 template <int VPL, int CPL>
-__global__ void __launch_bounds__(kMtWarps * 32, (CPL <= 2 ? 8 : 4)) ridge_nnls_kernel(
+__global__ void __launch_bounds__(kMtWarps * 32, (CPL <= 2 ? 6 : 4)) ridge_nnls_kernel(
     RidgeDev R, SignalDev S, const int* __restrict__ list, int64_t count, const int* __restrict__ count_dev,
     const double* __restrict__ corr, int ldc, double* __restrict__ x_out, int ldx, uint8_t* __restrict__ bad,
     int* queue, double* __restrict__ workspace, size_t slot_size) {
@@ -446,7 +446,7 @@ struct FracState {
 
 // Median of v[0..n), the mean of the two middle values for even n (cpp/src/sd/fractions.cpp:56-68),
 // by ranks: the element of stable rank r is the r-th smallest.
-__device__ double warp_median(const double* v, int n, FracState& st, int lane) {
+__device__ __forceinline__ double warp_median(const double* v, int n, FracState& st, int lane) {
     const int hi = n / 2, lo = n % 2 ? n / 2 : n / 2 - 1;
     for (int i = lane; i < n; i += 32) {
         const double vi = v[i];
@@ -462,16 +462,228 @@ __device__ double warp_median(const double* v, int n, FracState& st, int lane) {
     return n % 2 ? st.med[0] : (st.med[1] + st.med[0]) / 2.0;
 }
 
+constexpr int kFastRowsPerLane = 10;  // measurements per lane of the register fraction fit (m <= 320)
+
+// Lawson-Hanson (cpp/src/sd/nnls.cpp:187-221) on the normal equations G u = b of at most four
+// columns, every lane running the same scalar steps: the gradient b - G u over the active
+// columns, the steepest inactive column (the first on a tie), the least-squares fit of the
+// active block by Cholesky, the blocking step and the drops below tol, at most max_inner inner
+// steps. Inactive rows of the active block's system are the identity, so each solve runs on
+// compile-time indices. False when a pivot is not positive (the caller then fits by QR).
+__device__ __forceinline__ bool small_nnls(const double (&G)[4][4], const double (&b)[4], int n, double tol,
+                                           int max_inner, double (&u)[4]) {
+    bool flag[4];
+    double z[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        flag[j] = false;
+        u[j] = 0.0;
+        z[j] = 0.0;
+    }
+    auto solve = [&]() -> bool {
+        double L[4][4], y[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+#pragma unroll
+            for (int c = 0; c <= a; ++c) {
+                double sum = flag[a] && flag[c] ? G[a][c] : (a == c ? 1.0 : 0.0);
+#pragma unroll
+                for (int k = 0; k < c; ++k) sum -= L[a][k] * L[c][k];
+                if (a == c) {
+                    if (!(sum > 0.0)) return false;
+                    L[a][a] = sqrt(sum);
+                } else {
+                    L[a][c] = sum / L[c][c];
+                }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            double sum = flag[a] ? b[a] : 0.0;
+#pragma unroll
+            for (int k = 0; k < a; ++k) sum -= L[a][k] * y[k];
+            y[a] = sum / L[a][a];
+        }
+#pragma unroll
+        for (int a = 3; a >= 0; --a) {
+            double sum = y[a];
+#pragma unroll
+            for (int k = a + 1; k < 4; ++k) sum -= L[k][a] * z[k];
+            z[a] = flag[a] ? sum / L[a][a] : 0.0;
+        }
+        return true;
+    };
+    int inner = 0;
+    for (;;) {
+        int e = -1;
+        double best = 0.0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (j >= n) continue;
+            double w = b[j];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (flag[q]) w -= G[j][q] * u[q];
+            if (!flag[j] && (e < 0 || w > best)) {
+                best = w;
+                e = j;
+            }
+        }
+        if (e < 0 || best <= tol) return true;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (j == e) flag[j] = true;
+        if (!solve()) return false;
+        for (;;) {
+            bool any = false;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) any |= flag[j] && z[j] <= 0.0;
+            if (!any) break;
+            if (++inner > max_inner) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) u[j] = flag[j] ? z[j] : 0.0;
+                return true;
+            }
+            double sv = 0.0;
+            int si = -1;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (!flag[j] || z[j] > 0.0) continue;
+                const double dist = u[j] - z[j];
+                const double stp = dist > 0.0 ? u[j] / dist : 0.0;
+                if (si < 0 || stp < sv) {
+                    sv = stp;
+                    si = j;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double zj = flag[j] ? z[j] : 0.0;
+                u[j] += sv * (zj - u[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (j == si) u[j] = 0.0;
+                if (flag[j] && (j == si || !(fabs(u[j]) >= tol))) flag[j] = false;
+            }
+            if (!solve()) return false;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) u[j] = flag[j] ? z[j] : 0.0;
+    }
+}
+
+// compute_fractions for one anisotropic column next to at most three isotropic ones and at most
+// 320 measurements: the column K th scaled to a maximum of 1 in registers, then C^T C, C^T s and
+// the columns' norm1 in one reduction, and the NNLS on those (small_nnls). False when that
+// needs the QR fit.
+__device__ __forceinline__ bool fractions_small(const TissueDev T, const double* sig, int gb, int ge, double tol,
+                                                const FracSlot sl, FracState& st, int lane) {
+    const int m = T.m, ci = T.ci, n = 1 + ci;
+    double col[kFastRowsPerLane];
+#pragma unroll
+    for (int t = 0; t < kFastRowsPerLane; ++t) col[t] = 0.0;
+    for (int j = gb; j < ge; ++j) {
+        const double tj = sl.th[j];
+        if (tj == 0.0) continue;
+        const double* kr = T.kt + size_t(j) * m;
+#pragma unroll
+        for (int t = 0; t < kFastRowsPerLane; ++t) {
+            const int i = lane + 32 * t;
+            if (i < m) col[t] += kr[i] * tj;
+        }
+    }
+    double largest = -INFINITY;
+    bool any = false;
+#pragma unroll
+    for (int t = 0; t < kFastRowsPerLane; ++t) {
+        const int i = lane + 32 * t;
+        if (i < m && !isnan(col[t])) {
+            largest = any ? fmax(largest, col[t]) : col[t];
+            any = true;
+        }
+    }
+    // The largest non-NaN value over the lanes (Eigen's maxCoeff<PropagateNumbers>).
+    largest = warp_max(any ? largest : -INFINITY);
+    const bool all_nan = !__any_sync(0xffffffffu, any);
+    if (!all_nan && largest > 0.0) {
+#pragma unroll
+        for (int t = 0; t < kFastRowsPerLane; ++t) col[t] /= largest;
+    }
+    // Partial sums: G (upper triangle, 10), C^T s (4), norm1 (4).
+    double part[18];
+#pragma unroll
+    for (int k = 0; k < 18; ++k) part[k] = 0.0;
+#pragma unroll
+    for (int t = 0; t < kFastRowsPerLane; ++t) {
+        const int i = lane + 32 * t;
+        if (i >= m) continue;
+        double v[4];
+        v[0] = col[t];
+#pragma unroll
+        for (int q = 1; q < 4; ++q) v[q] = q <= ci ? T.iso[size_t(i) * ci + q - 1] : 0.0;
+        const double si = sig[i];
+        int k = 0;
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int c = a; c < 4; ++c) part[k++] += v[a] * v[c];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            part[10 + a] += v[a] * si;
+            part[14 + a] += fabs(v[a]);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+        for (int k = 0; k < 18; ++k) part[k] += __shfl_xor_sync(0xffffffffu, part[k], off);
+    double G[4][4], b[4], u[4];
+    {
+        int k = 0;
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int c = a; c < 4; ++c) {
+                G[a][c] = part[k];
+                G[c][a] = part[k];
+                ++k;
+            }
+    }
+    double colmax = 0.0;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        b[a] = part[10 + a];
+        if (a < n) colmax = fmax(colmax, part[14 + a]);
+    }
+    if (tol < 0.0) tol = 10.0 * kEps64 * colmax * double(max(m, n));
+    if (!small_nnls(G, b, n, tol, 3 * n, u)) return false;
+    if (lane < n) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (q == lane) st.fr[q] = u[q];
+    }
+    __syncwarp();
+    return true;
+}
+
 // compute_fractions (cpp/src/sd/fractions.cpp:70-101): tol < 0 uses the default tolerance of the
-// fraction columns. Writes the fractions (groups, then isotropic tissues) to st.fr.
-__device__ void fractions(const TissueDev& T, const double* fod, const double* sig, bool per_block, double tol,
-                          FracSlot& sl, FracState& st, int lane) {
+// fraction columns. Writes the fractions (groups, then isotropic tissues) to st.fr. One
+// anisotropic group, at most three isotropic tissues and at most 320 measurements take the
+// register fit (fractions_small); otherwise, or when its normal equations are not positive
+// definite, the columns are built in the warp's slot and fitted by QR.
+__device__ __forceinline__ void fractions(const TissueDev T, const double* fod, const double* sig, bool per_block,
+                                          double tol, const FracSlot sl, FracState& st, int lane) {
     const int m = T.m, ca = T.ca, ci = T.ci;
     const double threshold = warp_median(fod, ca, st, lane) * (1.0 - kMedianTie);
     for (int j = lane; j < ca; j += 32) sl.th[j] = fod[j] < threshold ? 0.0 : fod[j];
     __syncwarp();
     const int ng = per_block ? T.nb : 1;
     const int ncol = ng + ci;
+    if (ng == 1 && ci <= 3 && m <= 32 * kFastRowsPerLane) {
+        const int gb = per_block ? T.blocks[0] : 0, ge = per_block ? T.blocks[1] : ca;
+        if (fractions_small(T, sig, gb, ge, tol, sl, st, lane)) return;
+    }
     double colmax = 0.0;
     for (int g = 0; g < ng; ++g) {
         const int b = per_block ? T.blocks[2 * g] : 0, e = per_block ? T.blocks[2 * g + 1] : ca;
@@ -522,7 +734,7 @@ __device__ void fractions(const TissueDev& T, const double* fod, const double* s
 // takes the isotropic fractions; a voxel whose fractions all moved by less than fraction_tol, or
 // that used its last round, records its round count, the others join the next round's list
 // with their fractions kept for the next comparison.
-__global__ void __launch_bounds__(kMtWarps * 32, 8) lr_fractions_kernel(
+__global__ void __launch_bounds__(kMtWarps * 32, 4) lr_fractions_kernel(
     TissueDev T, const double* __restrict__ signals, const double* __restrict__ fods, int ldf,
     const int* __restrict__ list, int64_t count, const int* __restrict__ count_dev, int round, int max_rounds,
     double fraction_tol, double* __restrict__ fiso, double* __restrict__ prev, int32_t* __restrict__ rounds,
@@ -557,7 +769,7 @@ __global__ void __launch_bounds__(kMtWarps * 32, 8) lr_fractions_kernel(
 
 // The final per-block fractions of every voxel, normalised to sum to 1 (+1e-16), with the round
 // counts and statuses (cpp/src/sd/multi_tissue.cpp:127-148).
-__global__ void __launch_bounds__(kMtWarps * 32, 8) hr_fractions_kernel(
+__global__ void __launch_bounds__(kMtWarps * 32, 4) hr_fractions_kernel(
     TissueDev T, const double* __restrict__ signals, const double* __restrict__ fods, int64_t count,
     double final_tol, const int32_t* __restrict__ rounds_in, const uint8_t* __restrict__ bad,
     double* __restrict__ fractions_out, int32_t* __restrict__ rounds_out, uint8_t* __restrict__ status, int* queue,

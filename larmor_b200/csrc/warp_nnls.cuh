@@ -70,7 +70,7 @@ struct RowMajorColumns {
 // loader gives: writes the coefficients of those columns into z (indexed by column; other
 // entries untouched).
 template <class Columns>
-__device__ inline void warp_qr_least_squares_cols(const Columns& cols, int rows, const int* act, int k,
+__device__ __forceinline__ void warp_qr_least_squares_cols(const Columns cols, int rows, const int* act, int k,
                                                   const double* d, QrScratch s, double* z, int lane) {
     if (k == 0) return;
     for (int q = 0; q < k; ++q) {
@@ -204,7 +204,7 @@ __device__ inline void warp_qr_least_squares_cols(const Columns& cols, int rows,
 }
 
 // Least squares of d on the columns act[0..k) of c (rows x ldc, row-major).
-__device__ inline void warp_qr_least_squares(const double* __restrict__ c, int rows, int ldc,
+__device__ __forceinline__ void warp_qr_least_squares(const double* __restrict__ c, int rows, int ldc,
                                              const int* act, int k, const double* d, QrScratch s,
                                              double* z, int lane) {
     warp_qr_least_squares_cols(RowMajorColumns{c, ldc}, rows, act, k, d, s, z, lane);
@@ -226,7 +226,7 @@ struct NnlsScratch {
 // (cpp/src/sd/nnls.cpp:187-221, :332-346). Returns 1 when the method ended by its rule, 0 when
 // the inner-step limit ran out (u is then the last fit), -1 when more than acap columns became
 // active (u undefined). u is in s.u.
-__device__ inline int warp_nnls_explicit(const double* __restrict__ c, int rows, int m, const double* d,
+__device__ __forceinline__ int warp_nnls_explicit(const double* __restrict__ c, int rows, int m, const double* d,
                                          double tol, int max_inner, NnlsScratch s, int lane) {
     for (int j = lane; j < m; j += 32) {
         s.u[j] = 0.0;
