@@ -49,20 +49,22 @@ struct LsiDevice {
     const double* abs_sums;  // (k,)
 };
 
-// Global scratch of one warp: the QR-based fallback's explicit matrix and workspaces.
+// Global scratch of one warp: the Cholesky factor and its inverse, the QR-based fallback's
+// explicit matrix and workspaces.
 inline size_t lsi_slot_doubles(int n, int k) {
-    return 2 * size_t(k)                    // fallback u, z
+    return 2 * size_t(packed_size(kFactorCap))  // L, M
+           + 2 * size_t(k)                  // fallback u, z
            + size_t(n + 1) * k              // fallback matrix
            + size_t(kFactorCap) * (n + 1)   // fallback QR columns
            + (size_t(k) + 7) / 8            // fallback flags
            + 64;
 }
 
-// Shared memory of one warp: bounds f, multipliers u, candidate z (k each), the packed factor and
-// its reciprocal diagonal (cap), small vectors, then the int and byte arrays.
+// Shared memory of one warp: bounds f, multipliers u, candidate z (k each), the factor's vectors
+// h, w, y (cap each), small vectors, then the int and byte arrays.
 struct LsiWarpLayout {
     int k, cap;
-    __host__ __device__ size_t doubles() const { return 3 * size_t(k) + packed_size(cap) + cap + 4 * 64; }
+    __host__ __device__ size_t doubles() const { return 3 * size_t(k) + 3 * size_t(cap) + 4 * 64; }
     __host__ __device__ size_t ints() const { return 2 * size_t(cap) + 2 * 64 + 8; }
     __host__ __device__ size_t bytes() const {
         return (doubles() * sizeof(double) + ints() * sizeof(int) + size_t(k) + 15) / 16 * 16;
@@ -70,7 +72,7 @@ struct LsiWarpLayout {
 };
 
 struct LsiWarp {
-    double *f, *u, *z, *L, *inv, *rot, *t, *d, *res;
+    double *f, *u, *z, *h, *wv, *y, *L, *M, *rot, *t, *d, *res;
     int *cols, *sorted, *act, *perm;
     int* n_act;
     uint8_t* flag;
@@ -82,8 +84,11 @@ __device__ LsiWarp carve_lsi(unsigned char* base, const LsiWarpLayout& lay) {
     w.f = p; p += lay.k;
     w.u = p; p += lay.k;
     w.z = p; p += lay.k;
-    w.L = p; p += packed_size(lay.cap);
-    w.inv = p; p += lay.cap;
+    w.h = p; p += lay.cap;
+    w.wv = p; p += lay.cap;
+    w.y = p; p += lay.cap;
+    w.L = nullptr;  // in the warp's global slot
+    w.M = nullptr;
     w.rot = p; p += 64;
     w.t = p; p += 64;
     w.d = p; p += 64;
@@ -104,12 +109,16 @@ struct LsiQrShared {
 };
 
 // The LDP multipliers (cpp/src/sd/lsi.cpp:253-297) in w.u. Returns false when a Cholesky pivot
-// fails or the inner steps run out (the caller falls back to the QR-based NNLS).
-__device__ __noinline__ bool ldp_multipliers(const LsiDevice& D, const LsiWarp& w, int cap, int* outer_steps,
-                                             int lane) {
+// fails or the inner steps run out (the caller falls back to the QR-based NNLS). The factor of
+// H_AA is kept with its inverse (warp_chol.cuh, InvFactor): y = M f_A grows with each append, a
+// solve is one triangular matrix-vector product, and a removal is the Givens downdate of both.
+// Inlined into the kernel with every argument by value, so that its state stays in registers.
+template <int CPL>
+__device__ __forceinline__ bool ldp_multipliers(const LsiDevice D, const LsiWarp w, int cap, int* outer_steps,
+                                                int lane) {
     constexpr int VPL = kFactorCap / 32;
     const int k = D.k;
-    const WarpFactor fac{w.L, w.inv, w.cols, cap};
+    const InvFactor fac{w.L, w.M, w.h, w.wv, w.y, w.cols, cap};
     double norm1 = 0.0;
     for (int j = lane; j < k; j += 32) {
         norm1 = fmax(norm1, D.abs_sums[j] + fabs(w.f[j]));
@@ -122,15 +131,19 @@ __device__ __noinline__ bool ldp_multipliers(const LsiDevice& D, const LsiWarp& 
     const int max_inner = 3 * k;
     int na = 0, inner = 0, outer = 0;
     __syncwarp();
+    auto solve = [&]() {
+        if (na <= 32) inv_solve<1>(fac, na, w.z, k, lane);
+        else inv_solve<VPL>(fac, na, w.z, k, lane);
+    };
     for (;;) {
         double fu = 0.0;
         for (int j = lane; j < k; j += 32) fu += w.f[j] * w.u[j];
         fu = warp_sum(fu);
         // Steepest inactive gradient f (1 - f.u) - sum_c u_c (E E^T)_c over the active columns in
         // increasing order (u is zero elsewhere), the first on a tie.
-        double g[kColsPerLane];
+        double g[CPL];
 #pragma unroll
-        for (int t = 0; t < kColsPerLane; ++t) {
+        for (int t = 0; t < CPL; ++t) {
             const int j = lane + 32 * t;
             g[t] = j < k ? w.f[j] * (1.0 - fu) : 0.0;
         }
@@ -140,7 +153,7 @@ __device__ __noinline__ bool ldp_multipliers(const LsiDevice& D, const LsiWarp& 
             if (uc == 0.0) continue;
             const double* row = D.gram + size_t(c) * k;
 #pragma unroll
-            for (int t = 0; t < kColsPerLane; ++t) {
+            for (int t = 0; t < CPL; ++t) {
                 const int j = lane + 32 * t;
                 if (j < k) g[t] -= uc * row[j];
             }
@@ -148,7 +161,7 @@ __device__ __noinline__ bool ldp_multipliers(const LsiDevice& D, const LsiWarp& 
         double bv = 0.0;
         int bi = -1;
 #pragma unroll
-        for (int t = 0; t < kColsPerLane; ++t) {
+        for (int t = 0; t < CPL; ++t) {
             const int j = lane + 32 * t;
             if (j < k && !w.flag[j] && (bi < 0 || g[t] > bv)) { bv = g[t]; bi = j; }
         }
@@ -158,18 +171,15 @@ __device__ __noinline__ bool ldp_multipliers(const LsiDevice& D, const LsiWarp& 
         ++outer;
         // H(cols[r], e) = (E E^T)(cols[r], e) + f_cols[r] f_e, then append.
         const double fe = w.f[e];
-        double h[VPL];
-#pragma unroll
-        for (int t = 0; t < VPL; ++t) {
-            const int r = lane + 32 * t;
-            h[t] = 0.0;
-            if (r < na) {
-                const int c = w.cols[r];
-                h[t] = D.gram[size_t(c) * k + e] + w.f[c] * fe;
-            }
+        for (int r = lane; r < na; r += 32) {
+            const int c = w.cols[r];
+            w.h[r] = D.gram[size_t(c) * k + e] + w.f[c] * fe;
         }
+        __syncwarp();
         const double hee = D.gram[size_t(e) * k + e] + fe * fe;
-        if (!factor_append<VPL>(fac, na, h, hee, e, kMinRelativePivot, lane)) {
+        const bool appended = na < 32 ? inv_append<1>(fac, na, hee, fe, e, kMinRelativePivot, lane)
+                                      : inv_append<VPL>(fac, na, hee, fe, e, kMinRelativePivot, lane);
+        if (!appended) {
             *outer_steps = outer;
             return false;
         }
@@ -180,7 +190,7 @@ __device__ __noinline__ bool ldp_multipliers(const LsiDevice& D, const LsiWarp& 
             w.sorted[q] = e;
         }
         __syncwarp();
-        factor_solve<VPL>(fac, na, w.f, w.z, k, lane);
+        solve();
         for (;;) {
             // Blocking step over active columns with z <= 0, the first on a tie.
             double sv = 0.0;
@@ -222,10 +232,11 @@ __device__ __noinline__ bool ldp_multipliers(const LsiDevice& D, const LsiWarp& 
             // keep(): drop the factor columns that left, from the last position to the first.
             for (int pos = na - 1; pos >= 0; --pos) {
                 if (w.flag[w.cols[pos]]) continue;
-                factor_remove(fac, na, pos, lane);
+                inv_remove(fac, na, pos, lane);
                 --na;
+                __syncwarp();
             }
-            factor_solve<VPL>(fac, na, w.f, w.z, k, lane);
+            solve();
         }
         for (int j = lane; j < k; j += 32) w.u[j] = w.z[j];
         __syncwarp();
@@ -234,7 +245,8 @@ __device__ __noinline__ bool ldp_multipliers(const LsiDevice& D, const LsiWarp& 
     return true;
 }
 
-__global__ void __launch_bounds__(kLsiWarps * 32) lsi_kernel(LsiDevice D, const double* __restrict__ signals,
+template <int CPL>
+__global__ void __launch_bounds__(kLsiWarps * 32, 4) lsi_kernel(LsiDevice D, const double* __restrict__ signals,
                                                              int64_t v, int only_qr, int* queue, int cap,
                                                              double* __restrict__ workspace, size_t slot_doubles,
                                                              double* __restrict__ x, uint8_t* __restrict__ converged,
@@ -245,11 +257,13 @@ __global__ void __launch_bounds__(kLsiWarps * 32) lsi_kernel(LsiDevice D, const 
     __shared__ LsiQrShared qr_shared[kLsiWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const LsiWarpLayout lay{D.k, cap};
-    const LsiWarp w = carve_lsi(smem_raw + warp * lay.bytes(), lay);
     LsiQrShared& qsh = qr_shared[warp];
     const int m = D.m, n = D.n, k = D.k, rows = n + 1;
     double* slot = workspace + (size_t(blockIdx.x) * kLsiWarps + warp) * slot_doubles;
-    double* u2 = slot;
+    LsiWarp w = carve_lsi(smem_raw + warp * lay.bytes(), lay);
+    w.L = slot;
+    w.M = slot + packed_size(kFactorCap);
+    double* u2 = w.M + packed_size(kFactorCap);
     double* z2 = u2 + k;
     double* cmat = z2 + k;                        // (rows, k)
     double* sub = cmat + size_t(rows) * k;        // (kFactorCap, rows)
@@ -293,7 +307,7 @@ __global__ void __launch_bounds__(kLsiWarps * 32) lsi_kernel(LsiDevice D, const 
             for (int j = lane; j < k; j += 32) w.f[j] /= scale;
             __syncwarp();
             const double* mult = w.u;
-            const bool fast = !only_qr && ldp_multipliers(D, w, cap, &outer, lane);
+            const bool fast = !only_qr && ldp_multipliers<CPL>(D, w, cap, &outer, lane);
             if (!fast) {
                 // QR-based NNLS on the explicit [E^T; f^T] (cpp/src/sd/lsi.cpp:321-332).
                 double colmax = 0.0;
@@ -423,10 +437,13 @@ int lar_fit_lsi(lar_lsi_design design, const double* signals, int64_t v, int onl
         const LsiWarpLayout lay{int(h.k), cap};
         const size_t smem = lay.bytes() * kLsiWarps;
         require(smem <= 200 * 1024, "the LSI problem has too many constraints for the shared-memory solver");
-        cuda_check(cudaFuncSetAttribute(lsi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+        // Constraint columns per lane: 10 up to 320 constraints (302 with the 300-direction grid),
+        // else kColsPerLane.
+        auto kernel = h.k <= 320 ? lsi_kernel<10> : lsi_kernel<kColsPerLane>;
+        cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                    "cudaFuncSetAttribute");
         int per_sm = 0;
-        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lsi_kernel, kLsiWarps * 32, smem),
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kLsiWarps * 32, smem),
                    "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((v + kLsiWarps - 1) / kLsiWarps,
                                                                       int64_t(sm_count()) * std::max(per_sm, 1)));
@@ -446,7 +463,7 @@ int lar_fit_lsi(lar_lsi_design design, const double* signals, int64_t v, int onl
         LsiDevice D{int(h.m), int(h.n), int(h.k), design->qt.ptr, design->back.ptr, design->et.ptr,
                     design->e.ptr, design->gram.ptr, design->abs_sums.ptr};
         LaunchScope scope("lsi_kernel", st);
-    lsi_kernel<<<unsigned(blocks), kLsiWarps * 32, smem, st>>>(
+        kernel<<<unsigned(blocks), kLsiWarps * 32, smem, st>>>(
             D, signals, v, only_qr, reinterpret_cast<int*>(base), cap, reinterpret_cast<double*>(base + 256), slot,
             x, converged, status, outer, active);
         cuda_check(cudaGetLastError(), "lsi_kernel launch");

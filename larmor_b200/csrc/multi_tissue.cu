@@ -351,8 +351,14 @@ __device__ __forceinline__ bool ridge_nnls(const RidgeDev R, const SignalDev S, 
             if (entering >= 0) {
                 for (int r = lane; r < na; r += 32) sl.h[r] = R.gram[size_t(st.cols[r]) * c + entering];
                 __syncwarp();
-                if (!inv_append<VPL>(fac, na, R.gram[size_t(entering) * c + entering], corr[entering], entering,
-                                     kMinPivot, lane)) {
+                // Below 32 active columns one row slice per lane holds the factor's rows: the
+                // one-slice code skips the unrolled empty slices of the larger capacity.
+                const double gee = R.gram[size_t(entering) * c + entering];
+                const bool appended =
+                    (VPL == 1 || na < 32)
+                        ? inv_append<1>(fac, na, gee, corr[entering], entering, kMinPivot, lane)
+                        : inv_append<VPL>(fac, na, gee, corr[entering], entering, kMinPivot, lane);
+                if (!appended) {
                     failed = true;
                 } else {
                     if (lane == 0) sl.inf[entering] = 1;
@@ -367,6 +373,8 @@ __device__ __forceinline__ bool ridge_nnls(const RidgeDev R, const SignalDev S, 
                 have_sig = true;
             }
             overflow |= !ridge_qr_fit(R, sl.sig, sl, st, lane);
+        } else if (VPL == 1 || na <= 32) {
+            inv_solve<1>(fac, na, sl.z, c, lane);
         } else {
             inv_solve<VPL>(fac, na, sl.z, c, lane);
         }

@@ -72,9 +72,22 @@ def test_lsi_matches_the_oracle_with_identical_active_sets(cuda, oracle, msmt_fi
     np.testing.assert_array_equal(active, ractive)
     if not only_qr:
         np.testing.assert_array_equal(outer, router)
-    scale = np.abs(rx).max(axis=1, keepdims=True)
     np.testing.assert_allclose(x, rx, rtol=0, atol=1e-9)
-    assert (np.abs(x - rx) <= 1e-10 * scale).all()
+    # Values to the forward error of the active-set solve, 10 cond(H_AA) eps of the voxel's
+    # largest coefficient (at least 1e-10 of it): both fits solve H_AA u_A = f_A, with H = E E^T + f f^T
+    # reaching cond 3e8 here, in different rounding.
+    m = oracle.lsi_design(msmt_fixture["forward"], msmt_fixture["constraints"], float(msmt_fixture["ridge"]))
+    for v in range(len(signals)):
+        scale = np.abs(rx[v]).max()
+        tol = 1e-10
+        act = np.nonzero(ractive[v])[0]
+        if rstatus[v] == 0 and len(act):
+            rot = m["q_t"] @ signals[v]
+            f = -m["e"] @ rot
+            f /= np.abs(f).max()
+            h = (m["gram"] + np.outer(f, f))[np.ix_(act, act)]
+            tol = max(tol, 10 * np.linalg.cond(h) * np.finfo(np.float64).eps)
+        assert np.abs(x[v] - rx[v]).max() <= tol * scale
     assert active.sum(axis=1).max() > 5
 
 
