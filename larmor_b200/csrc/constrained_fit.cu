@@ -19,6 +19,7 @@
 // reflections, the m constraint columns for gradients and steps, and the active columns for
 // the small QR.
 
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 
@@ -236,6 +237,14 @@ __global__ void __launch_bounds__(kCWarps * 32) constrained_fit_kernel(
 }
 
 }  // namespace
+
+int constrained_resident_warps() {
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, constrained_fit_kernel<CappedSource>,
+                                                             kCWarps * 32, 0),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    return sm_count() * std::max(per_sm, 1) * kCWarps;
+}
 
 template <class Src>
 void launch_constrained(const LogDesignDevice<double>& d, const Src& src, int weighted,
