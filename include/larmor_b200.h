@@ -181,12 +181,26 @@ void lar_deconv_kernel_destroy(lar_deconv_kernel kernel);
  * tolerance final_tol_x), normalised to sum to 1. weights (m,) (host) are the shell weights of
  * the FOD fits. Writes fods (v, ca_hr) and fractions (v, nb_hr + ci) (device double); rounds
  * (v,) int32 and status (v,) uint8 (1 where an active set outgrew the QR workspace) may be
- * NULL. Waits for its stream. Calls sharing hr_solver must not overlap on the GPU.
+ * NULL. Without stream capture it reads each round's voxel count back on the host (waiting for
+ * its stream once per round); under capture it enqueues max_outer rounds that read their counts
+ * on the device (an earlier uncaptured call on these solvers must have used the same weights
+ * and no fewer voxels). Calls sharing hr_solver must not overlap on the GPU.
  * Replaces larmor._core.fit_multi_tissue (cpp/src/python/sd.cpp:310-358). */
 int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights, lar_deconv_kernel lr,
                          lar_fod_solver lr_solver, lar_deconv_kernel hr, lar_fod_solver hr_solver,
                          int64_t max_outer, double fraction_tol, double final_tol_x, double* fods,
                          double* fractions, int32_t* rounds, uint8_t* status, void* stream);
+
+/* lar_fit_multi_tissue without host waits (no counterpart in the reference, whose rounds run on
+ * host threads): every one of max_outer rounds is enqueued and reads its voxel count on the
+ * device, exiting at once when it is 0, so the call returns as soon as the work is enqueued and
+ * concurrent fits on other streams are not held up by host round trips. Results are those of
+ * lar_fit_multi_tissue. The weights are copied at the call (the host buffer may be reused after
+ * it returns). */
+int lar_fit_multi_tissue_async(const double* signals, int64_t v, const double* weights, lar_deconv_kernel lr,
+                               lar_fod_solver lr_solver, lar_deconv_kernel hr, lar_fod_solver hr_solver,
+                               int64_t max_outer, double fraction_tol, double final_tol_x, double* fods,
+                               double* fractions, int32_t* rounds, uint8_t* status, void* stream);
 
 /* The FOD (v, c) of every row of signals (v, m) (device double) with one L2NNLS solver.
  * Replaces larmor._core.fit_single_tissue (cpp/src/python/sd.cpp, cpp/src/sd/solver.cpp:422). */

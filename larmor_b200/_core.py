@@ -400,11 +400,14 @@ def _fit_multi_tissue_on_device(signals, weights, lr, lr_solver, hr, hr_solver, 
 
 
 def fit_multi_tissue_device(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol,
-                            final_tol_x, fods, fractions, rounds=None, status=None) -> None:
-    """The device-resident fit_multi_tissue (torch CUDA tensors; weights a host array)."""
+                            final_tol_x, fods, fractions, rounds=None, status=None, asynchronous=False) -> None:
+    """The device-resident fit_multi_tissue (torch CUDA tensors; weights a host array). With
+    asynchronous, every round is enqueued with its voxel count read on the device, and the call
+    returns without waiting for the GPU (lar_fit_multi_tissue_async)."""
     torch = _torch()
     weights = np.ascontiguousarray(weights, dtype=np.float64)
-    _lib.check(_lib.lib().lar_fit_multi_tissue(
+    entry = _lib.lib().lar_fit_multi_tissue_async if asynchronous else _lib.lib().lar_fit_multi_tissue
+    _lib.check(entry(
         _lib.ptr(signals), signals.shape[0], _lib.ptr(weights), lr.handle, lr_solver.handle, hr.handle,
         hr_solver.handle, int(max_outer), float(fraction_tol), float(final_tol_x), _lib.ptr(fods),
         _lib.ptr(fractions), _lib.ptr(rounds), _lib.ptr(status), _stream(torch)))

@@ -165,9 +165,9 @@ def job_inputs_host(job) -> tuple:
     return (np.ascontiguousarray(job.signals, dtype=np.float64),)
 
 
-def launch_job(job, handles: dict, d_in: tuple, out: dict) -> None:
+def launch_job(job, handles: dict, d_in: tuple, out: dict, asynchronous: bool = False) -> None:
     """Enqueues one job's fit on the current stream (the mFOD fit waits on the host for each
-    round's voxel count unless the stream is being captured)."""
+    round's voxel count unless the stream is being captured or `asynchronous` is set)."""
     import torch
 
     if job.kind == "dti":
@@ -185,7 +185,7 @@ def launch_job(job, handles: dict, d_in: tuple, out: dict) -> None:
         h = handles
         _core.fit_multi_tissue_device(d_in[0], h["weights"], h["k_lr"], h["lr_solver"], h["k_hr"], h["hr_solver"],
                                       MAX_ROUNDS, 1e-7, FINAL_FRACTION_TOL_X, out["fods"], out["fractions"],
-                                      out["rounds"], out["status"])
+                                      out["rounds"], out["status"], asynchronous=asynchronous)
 
 
 def job_device_bytes(job) -> int:

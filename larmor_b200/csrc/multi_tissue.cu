@@ -924,67 +924,13 @@ struct lar_deconv_kernel_s {
 
 using namespace lar;
 
-extern "C" {
-
-int lar_l2nnls_create(const double* k, int64_t m, int64_t c, double reg, double tol_x, lar_fod_solver* out) {
-    return guarded([&] {
-        require(out != nullptr, "out must not be NULL");
-        require(reg >= 0.0, "reg must be at least 0");
-        require(tol_x > 0.0, "tol_x must be positive");
-        require(k != nullptr && m > 0 && c > 0, "k must be a non-empty (m, c) array");
-        require(c <= 640 && m <= 4096, "the kernel has more than 640 directions or 4096 measurements");
-        auto h = std::make_unique<lar_fod_solver_s>();
-        h->host = host::prepare_ridge_design(k, m, c, reg);
-        h->tol = tol_x;
-        h->k.upload(h->host.kernel.data(), h->host.kernel.size());
-        h->gram.upload(h->host.gram.data(), h->host.gram.size());
-        *out = h.release();
-    });
-}
-
-void lar_fod_solver_destroy(lar_fod_solver solver) { delete solver; }
-
-int lar_deconv_kernel_create(const double* k_aniso, int64_t m, int64_t ca, const double* k_iso,
-                             const double* w_k_iso, int64_t ci, const int64_t* blocks, int64_t nb,
-                             lar_deconv_kernel* out) {
-    return guarded([&] {
-        require(out != nullptr, "out must not be NULL");
-        require(k_aniso != nullptr && m > 0 && ca > 0, "k_aniso must be a non-empty (m, ca) array");
-        require(ci >= 0 && (ci == 0 || (k_iso && w_k_iso)), "k_iso and w_k_iso must be (m, ci) arrays");
-        require(nb >= 1 && blocks != nullptr, "aniso_blocks must hold at least one block");
-        require(nb + ci <= kMaxGroups, "at most 16 tissues");
-        std::string text;
-        for (int64_t b = 0; b < nb; ++b) {
-            const int64_t s = blocks[2 * b], e = blocks[2 * b + 1];
-            require(s >= 0 && s < e && e <= ca, "aniso_blocks must be non-empty ranges within 0.." +
-                                                    std::to_string(ca));
-        }
-        auto h = std::make_unique<lar_deconv_kernel_s>();
-        h->m = m; h->ca = ca; h->ci = ci; h->nb = nb;
-        std::vector<double> kt(size_t(ca * m));
-        for (int64_t i = 0; i < m; ++i)
-            for (int64_t j = 0; j < ca; ++j) kt[size_t(j * m + i)] = k_aniso[i * ca + j];
-        h->kt.upload(kt.data(), kt.size());
-        std::vector<double> iso(size_t(std::max<int64_t>(1, m * ci)), 0.0), wiso(iso.size(), 0.0);
-        if (ci > 0) {
-            std::copy(k_iso, k_iso + m * ci, iso.begin());
-            std::copy(w_k_iso, w_k_iso + m * ci, wiso.begin());
-        }
-        h->iso.upload(iso.data(), iso.size());
-        h->wiso.upload(wiso.data(), wiso.size());
-        std::vector<int> bl(size_t(2 * nb));
-        for (int64_t b = 0; b < 2 * nb; ++b) bl[size_t(b)] = int(blocks[b]);
-        h->blocks.upload(bl.data(), bl.size());
-        *out = h.release();
-    });
-}
-
-void lar_deconv_kernel_destroy(lar_deconv_kernel kernel) { delete kernel; }
-
-int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights, lar_deconv_kernel lr,
-                         lar_fod_solver lr_solver, lar_deconv_kernel hr, lar_fod_solver hr_solver,
-                         int64_t max_outer, double fraction_tol, double final_tol_x, double* fods,
-                         double* fractions, int32_t* rounds, uint8_t* status, void* stream) {
+// The multi-tissue fit behind both entry points. device_rounds: enqueue every round with its
+// voxel count read on the device (as under stream capture) instead of reading each count back.
+static int fit_multi_tissue(const double* signals, int64_t v, const double* weights, lar_deconv_kernel lr,
+                            lar_fod_solver lr_solver, lar_deconv_kernel hr, lar_fod_solver hr_solver,
+                            int64_t max_outer, double fraction_tol, double final_tol_x, double* fods,
+                            double* fractions, int32_t* rounds, uint8_t* status, void* stream,
+                            bool device_rounds) {
     return guarded([&] {
         require(lr && hr && lr_solver && hr_solver, "kernels and solvers must not be NULL");
         require(weights != nullptr, "weights must not be NULL");
@@ -1051,8 +997,9 @@ int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights
         // enqueued and reads its voxel count on the device, exiting at once when it is 0.
         cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
         cuda_check(cudaStreamIsCapturing(st, &capture), "cudaStreamIsCapturing");
-        const bool graph = capture != cudaStreamCaptureStatusNone;
-        const double* dweights = hr_solver->device_weights(weights, m, graph);
+        const bool capturing = capture != cudaStreamCaptureStatusNone;
+        const bool graph = capturing || device_rounds;
+        const double* dweights = hr_solver->device_weights(weights, m, capturing);
         int* host_count = graph ? nullptr : hr_solver->count_buffer();
         auto blocks = [](int64_t slots, int64_t count) {
             return unsigned(std::max<int64_t>(1, std::min<int64_t>(slots / kMtWarps, (count + kMtWarps - 1) / kMtWarps)));
@@ -1122,6 +1069,80 @@ int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights
         }
     });
 }
+
+extern "C" {
+
+int lar_fit_multi_tissue(const double* signals, int64_t v, const double* weights, lar_deconv_kernel lr,
+                         lar_fod_solver lr_solver, lar_deconv_kernel hr, lar_fod_solver hr_solver,
+                         int64_t max_outer, double fraction_tol, double final_tol_x, double* fods,
+                         double* fractions, int32_t* rounds, uint8_t* status, void* stream) {
+    return fit_multi_tissue(signals, v, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol, final_tol_x,
+                            fods, fractions, rounds, status, stream, false);
+}
+
+int lar_fit_multi_tissue_async(const double* signals, int64_t v, const double* weights, lar_deconv_kernel lr,
+                               lar_fod_solver lr_solver, lar_deconv_kernel hr, lar_fod_solver hr_solver,
+                               int64_t max_outer, double fraction_tol, double final_tol_x, double* fods,
+                               double* fractions, int32_t* rounds, uint8_t* status, void* stream) {
+    return fit_multi_tissue(signals, v, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol, final_tol_x,
+                            fods, fractions, rounds, status, stream, true);
+}
+
+
+int lar_l2nnls_create(const double* k, int64_t m, int64_t c, double reg, double tol_x, lar_fod_solver* out) {
+    return guarded([&] {
+        require(out != nullptr, "out must not be NULL");
+        require(reg >= 0.0, "reg must be at least 0");
+        require(tol_x > 0.0, "tol_x must be positive");
+        require(k != nullptr && m > 0 && c > 0, "k must be a non-empty (m, c) array");
+        require(c <= 640 && m <= 4096, "the kernel has more than 640 directions or 4096 measurements");
+        auto h = std::make_unique<lar_fod_solver_s>();
+        h->host = host::prepare_ridge_design(k, m, c, reg);
+        h->tol = tol_x;
+        h->k.upload(h->host.kernel.data(), h->host.kernel.size());
+        h->gram.upload(h->host.gram.data(), h->host.gram.size());
+        *out = h.release();
+    });
+}
+
+void lar_fod_solver_destroy(lar_fod_solver solver) { delete solver; }
+
+int lar_deconv_kernel_create(const double* k_aniso, int64_t m, int64_t ca, const double* k_iso,
+                             const double* w_k_iso, int64_t ci, const int64_t* blocks, int64_t nb,
+                             lar_deconv_kernel* out) {
+    return guarded([&] {
+        require(out != nullptr, "out must not be NULL");
+        require(k_aniso != nullptr && m > 0 && ca > 0, "k_aniso must be a non-empty (m, ca) array");
+        require(ci >= 0 && (ci == 0 || (k_iso && w_k_iso)), "k_iso and w_k_iso must be (m, ci) arrays");
+        require(nb >= 1 && blocks != nullptr, "aniso_blocks must hold at least one block");
+        require(nb + ci <= kMaxGroups, "at most 16 tissues");
+        std::string text;
+        for (int64_t b = 0; b < nb; ++b) {
+            const int64_t s = blocks[2 * b], e = blocks[2 * b + 1];
+            require(s >= 0 && s < e && e <= ca, "aniso_blocks must be non-empty ranges within 0.." +
+                                                    std::to_string(ca));
+        }
+        auto h = std::make_unique<lar_deconv_kernel_s>();
+        h->m = m; h->ca = ca; h->ci = ci; h->nb = nb;
+        std::vector<double> kt(size_t(ca * m));
+        for (int64_t i = 0; i < m; ++i)
+            for (int64_t j = 0; j < ca; ++j) kt[size_t(j * m + i)] = k_aniso[i * ca + j];
+        h->kt.upload(kt.data(), kt.size());
+        std::vector<double> iso(size_t(std::max<int64_t>(1, m * ci)), 0.0), wiso(iso.size(), 0.0);
+        if (ci > 0) {
+            std::copy(k_iso, k_iso + m * ci, iso.begin());
+            std::copy(w_k_iso, w_k_iso + m * ci, wiso.begin());
+        }
+        h->iso.upload(iso.data(), iso.size());
+        h->wiso.upload(wiso.data(), wiso.size());
+        std::vector<int> bl(size_t(2 * nb));
+        for (int64_t b = 0; b < 2 * nb; ++b) bl[size_t(b)] = int(blocks[b]);
+        h->blocks.upload(bl.data(), bl.size());
+        *out = h.release();
+    });
+}
+
+void lar_deconv_kernel_destroy(lar_deconv_kernel kernel) { delete kernel; }
 
 int lar_fit_single_tissue(const double* signals, int64_t v, lar_fod_solver solver, double* fods, uint8_t* status,
                           void* stream) {

@@ -5,9 +5,9 @@ which returns a future. A dispatcher admits them in arrival order whenever a slo
 stream with its worker thread) is free and the request fits in the HBM budget next to the
 requests already running; a request that arrives while others are on the GPU starts as soon as
 one of them releases its slot and memory, and its kernels run beside theirs on its own stream.
-Each worker uploads its request's inputs, runs the fit, copies the results to the host and
-then frees its slot (the mFOD fit waits on the host once per round, which is why every slot
-has a thread of its own; the waits release the GIL).
+Each worker uploads its request's inputs, enqueues the fit (the mFOD fit without host waits:
+lar_fit_multi_tissue_async), copies the results to the host once the stream finishes and then
+frees its slot; every slot has a thread of its own, and its waits release the GIL.
 
 Design handles (log-fit designs, deconvolution kernels and solvers) are built once per
 (model, gradient table, responses) and slot and kept resident; a handle's scratch belongs to
@@ -174,7 +174,7 @@ class FitServer:
         with torch.cuda.stream(stream):
             d_in = tuple(torch.from_numpy(a).to(dev, non_blocking=True) for a in job_inputs_host(job))
             out = job_outputs(job, handles, dev)
-            launch_job(job, handles, d_in, out)
+            launch_job(job, handles, d_in, out, asynchronous=True)
             host = {k: t.to("cpu", non_blocking=True) for k, t in out.items()}
         stream.synchronize()
         return {k: t.numpy() for k, t in host.items()}

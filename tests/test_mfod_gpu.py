@@ -127,3 +127,34 @@ def test_sh_projection_matches_the_least_squares_fit(cuda, lmax, exact_integral)
         ref = to_sh(amps[:, block], lmax, "tournier", exact_integral=exact_integral)
         got = _core.project_sh_device(projector, d[:, block], exact_integral).cpu().numpy()
         assert (np.abs(got - ref) <= 1e-12 * np.abs(ref).max(axis=1, keepdims=True)).all()
+
+
+def test_async_multi_tissue_equals_the_waiting_call(cuda, mfod_fixture):
+    """lar_fit_multi_tissue_async (every round enqueued, counts read on the device) gives the
+    waiting call's results bit for bit, including the round counts."""
+    import torch
+
+    from larmor_b200 import _core
+
+    z = mfod_fixture
+    signals, _, _ = mfod_inputs(z)
+    fods, fr, rd, st = _gpu_fit(z, signals)
+    lr = _core.DeconvKernel(np.ascontiguousarray(z["lr_k_aniso"]), np.ascontiguousarray(z["lr_k_iso"]),
+                            np.ascontiguousarray(z["lr_w_k_iso"]), [(0, z["lr_k_aniso"].shape[1])])
+    hr = _core.DeconvKernel(np.ascontiguousarray(z["hr_k_aniso"]), np.ascontiguousarray(z["hr_k_iso"]),
+                            np.ascontiguousarray(z["hr_w_k_iso"]), [tuple(b) for b in z["hr_blocks"]])
+    lr_solver = _core.FodSolver.l2nnls(np.ascontiguousarray(z["lr_w_k_aniso"]), 0.0, 1e-6)
+    hr_solver = _core.FodSolver.l2nnls(np.ascontiguousarray(z["hr_w_k_aniso"]), 0.1, 1e-6)
+    dev = torch.device("cuda")
+    v = len(signals)
+    s = torch.from_numpy(np.ascontiguousarray(signals)).to(dev)
+    out = dict(fods=torch.zeros((v, hr.ca), dtype=torch.float64, device=dev),
+               fr=torch.zeros((v, hr.nb + hr.ci), dtype=torch.float64, device=dev),
+               rd=torch.zeros((v,), dtype=torch.int32, device=dev), st=torch.ones((v,), dtype=torch.uint8, device=dev))
+    _core.fit_multi_tissue_device(s, z["weights"], lr, lr_solver, hr, hr_solver, 50, 1e-7, 1e-2, out["fods"],
+                                  out["fr"], out["rd"], out["st"], asynchronous=True)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out["fods"].cpu().numpy(), fods)
+    np.testing.assert_array_equal(out["fr"].cpu().numpy(), fr)
+    np.testing.assert_array_equal(out["rd"].cpu().numpy(), rd)
+    np.testing.assert_array_equal(out["st"].cpu().numpy(), st)
