@@ -511,7 +511,8 @@ class BatchWorkload:
         from larmor_b200.batch import Batch
 
         self.torch = torch
-        self.batch = Batch(self.jobs, branches=4)
+        self.batch = Batch(self.jobs, branches=4, tune=True)
+        self.config["launch_settings"] = self.batch.launch_settings
         self.batch.capture()
         self.h_in = [tuple(torch.from_numpy(np.ascontiguousarray(t.cpu().numpy())).pin_memory() for t in j.d_in)
                      for j in self.jobs]

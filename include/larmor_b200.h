@@ -60,6 +60,15 @@ const char* lar_version(void);
 /* Kernels the library has launched since it was loaded. */
 int64_t lar_launch_count(void);
 
+/* Launch settings a tuner may set (no counterpart in the reference): "dti.voxels_per_cta"
+ * (16, 32 or 64; used when the table fits), "log.warp.waves" (resident-CTA waves of the
+ * warp-per-voxel log fit's grid, default 4), and the resident CTAs per SM of the persistent
+ * grids, "dki.refit.ctas_per_sm", "lsi.ctas_per_sm", "sd.nnls.ctas_per_sm" and
+ * "sd.fractions.ctas_per_sm" (at most the occupancy limit). 0 restores the library's choice.
+ * Results do not depend on them; an unknown name or a value out of range is LAR_ERR_INVALID. */
+int lar_set_launch_setting(const char* name, int64_t value);
+int lar_get_launch_setting(const char* name, int64_t* value);
+
 /* Turns per-kernel event timing on (enable != 0) or off; either way clears the records. */
 int lar_kernel_timing(int enable);
 

@@ -21,6 +21,8 @@ SIGNATURES: dict[str, tuple] = {
     "lar_last_error": (_c.c_char_p, []),
     "lar_version": (_c.c_char_p, []),
     "lar_launch_count": (_i64, []),
+    "lar_set_launch_setting": (_i32, [_c.c_char_p, _i64]),
+    "lar_get_launch_setting": (_i32, [_c.c_char_p, _p]),
     "lar_kernel_timing": (_i32, [_i32]),
     "lar_kernel_time": (_i32, [_c.c_char_p, _p, _p]),
     "lar_log_design_create": (_i32, [_p, _i64, _i64, _p, _i64, _p]),

@@ -6,7 +6,8 @@ two jobs never share one). `Batch.capture()` runs every job once eagerly, which 
 handle's scratch and uploads its shell weights, then records all of them into one CUDA graph:
 the jobs are spread over parallel branches of the graph (longest first onto the least-loaded
 branch), so that a volume too small to fill the GPU runs beside others. `Batch.run()` replays
-the graph: one launch for the whole batch. The results stay on the device in each job's output
+the graph: one launch for the whole batch. With `tune=True` the launch shapes of each model's
+kernels are first chosen by measurement (larmor_b200.autotune). The results stay on the device in each job's output
 tensors.
 
 The per-model work is the same kernels as the single fits (larmor_b200._core), so a job's
@@ -205,11 +206,18 @@ def job_device_bytes(job) -> int:
 class Batch:
     """Jobs fitted together, replayed as one CUDA graph (see the module docstring)."""
 
-    def __init__(self, jobs, branches: int = 4) -> None:
+    def __init__(self, jobs, branches: int = 4, tune: bool = False, tuner=None) -> None:
+        """tune: first pick each model's launch settings on a sample of its largest volume
+        (larmor_b200.autotune; the choice is cached per GPU and workload signature)."""
         import torch
 
         self.torch = torch
         self.jobs = list(jobs)
+        self.launch_settings = {}
+        if tune:
+            from larmor_b200.autotune import tune_jobs
+
+            self.launch_settings = tune_jobs(self.jobs, tuner)
         self.dev = torch.device("cuda", torch.cuda.current_device())
         self.streams = [torch.cuda.Stream(self.dev) for _ in range(max(1, branches))]
         self.assignment = assign_branches([j.cost() for j in self.jobs], len(self.streams))

@@ -83,6 +83,18 @@ struct LaunchScope {
     cudaEvent_t start = nullptr;
 };
 
+// Launch settings (lar_set_launch_setting): 0 when a setting is unset, which keeps the
+// library's own choice. A tuner sets them; results never depend on them.
+int64_t launch_setting(const char* name);
+
+// Resident CTAs per SM of a persistent grid: the occupancy limit, or less when the named setting
+// asks for fewer.
+inline int ctas_per_sm(int occupancy, const char* setting) {
+    const int64_t want = launch_setting(setting);
+    const int occ = occupancy > 0 ? occupancy : 1;
+    return want > 0 && want < occ ? int(want) : occ;
+}
+
 inline int sm_count() {
     int dev = 0, n = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");

@@ -243,7 +243,7 @@ int constrained_resident_warps() {
     cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, constrained_fit_kernel<CappedSource>,
                                                              kCWarps * 32, 0),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    return sm_count() * std::max(per_sm, 1) * kCWarps;
+    return sm_count() * ctas_per_sm(per_sm, "dki.refit.ctas_per_sm") * kCWarps;
 }
 
 template <class Src>

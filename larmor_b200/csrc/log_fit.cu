@@ -277,6 +277,12 @@ const LogDesignDevice<float>& device_view<float>(const lar_log_design_s* h) { re
 // Voxels per CTA of the shared-memory fits: 64, or 32 / 16 when the design and a CTA's signals
 // of 64 voxels do not fit in shared memory (tables of more than about 200 measurements).
 inline int small_block(int n, int raw_bytes, size_t per_value) {
+    auto fits = [&](int block) {
+        return size_t(n) * (2 * 7 + 28) * per_value + size_t(n) * block * per_value + size_t(n) * block * raw_bytes +
+                   16 <= 227 * 1024;
+    };
+    const int64_t want = launch_setting("dti.voxels_per_cta");
+    if ((want == 16 || want == 32 || want == 64) && fits(int(want))) return int(want);
     for (int block : {64, 32, 16}) {
         const size_t bytes = size_t(n) * (2 * 7 + 28) * per_value + size_t(n) * block * per_value +
                              size_t(n) * block * raw_bytes + 16;

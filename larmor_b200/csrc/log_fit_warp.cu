@@ -232,7 +232,8 @@ void launch_warp_impl(const LogDesignDevice<T>& d, const Src& src, int64_t v, in
     cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kWarps * 32, smem),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     const int64_t need = (v + kWarps - 1) / kWarps;
-    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sm_count()) * std::max(per_sm, 1) * 4));
+    const int64_t waves = launch_setting("log.warp.waves") > 0 ? launch_setting("log.warp.waves") : 4;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sm_count()) * std::max(per_sm, 1) * waves));
     LaunchScope scope("fit_log_warp_kernel", stream);
     kernel<<<unsigned(grid), kWarps * 32, smem, stream>>>(d, src, v, weighted, max_rw, T(tol), params, broke,
                                                           iterations, violators);

@@ -446,7 +446,7 @@ int lar_fit_lsi(lar_lsi_design design, const double* signals, int64_t v, int onl
         cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kLsiWarps * 32, smem),
                    "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((v + kLsiWarps - 1) / kLsiWarps,
-                                                                      int64_t(sm_count()) * std::max(per_sm, 1)));
+                                                                      int64_t(sm_count()) * ctas_per_sm(per_sm, "lsi.ctas_per_sm")));
         const int slots = int(blocks) * kLsiWarps;
         const size_t slot = lsi_slot_doubles(int(h.n), int(h.k));
         const size_t need = 256 + size_t(slots) * slot * sizeof(double);

@@ -810,7 +810,7 @@ __global__ void __launch_bounds__(kMtWarps * 32, 4) hr_fractions_kernel(
 // The warps of a persistent grid: as many as the SMs hold at once (or one per item), in whole
 // CTAs of kMtWarps.
 template <class Kernel>
-int64_t resident_slots(Kernel kernel, size_t smem, int64_t items) {
+int64_t resident_slots(Kernel kernel, size_t smem, int64_t items, const char* setting) {
     require(smem <= 200 * 1024, "the kernel has too many columns for the shared-memory solver");
     cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                "cudaFuncSetAttribute");
@@ -818,7 +818,7 @@ int64_t resident_slots(Kernel kernel, size_t smem, int64_t items) {
     cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kMtWarps * 32, smem),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((items + kMtWarps - 1) / kMtWarps,
-                                                                  int64_t(sm_count()) * std::max(per_sm, 1)));
+                                                                  int64_t(sm_count()) * ctas_per_sm(per_sm, setting)));
     return blocks * kMtWarps;
 }
 
@@ -958,10 +958,10 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
         const size_t per_voxel = (size_t(std::max(c_lr, c_hr)) + size_t(c_lr) + 2 * size_t(ci) + 1) * sizeof(double) +
                                  3 * sizeof(int) + 1;
         const int64_t n_max = std::min<int64_t>(v, std::max<int64_t>(4096, int64_t((size_t(4) << 30) / per_voxel)));
-        const int64_t lr_slots = resident_slots(lr_nnls.kernel, lr_smem, n_max);
-        const int64_t hr_slots = resident_slots(hr_nnls.kernel, hr_smem, n_max);
-        const int64_t lf_slots = resident_slots(lr_fractions_kernel, 0, n_max);
-        const int64_t hf_slots = resident_slots(hr_fractions_kernel, 0, n_max);
+        const int64_t lr_slots = resident_slots(lr_nnls.kernel, lr_smem, n_max, "sd.nnls.ctas_per_sm");
+        const int64_t hr_slots = resident_slots(hr_nnls.kernel, hr_smem, n_max, "sd.nnls.ctas_per_sm");
+        const int64_t lf_slots = resident_slots(lr_fractions_kernel, 0, n_max, "sd.fractions.ctas_per_sm");
+        const int64_t hf_slots = resident_slots(hr_fractions_kernel, 0, n_max, "sd.fractions.ctas_per_sm");
         const size_t lr_slot = nnls_slot_doubles(mi, lr_nnls.cap), hr_slot = nnls_slot_doubles(mi, hr_nnls.cap);
         const size_t lf_slot = frac_slot_doubles(mi, c_lr, 1 + ci), hf_slot = frac_slot_doubles(mi, c_hr, nf);
         const size_t slot_doubles =
@@ -1156,7 +1156,7 @@ int lar_fit_single_tissue(const double* signals, int64_t v, lar_fod_solver solve
         const NnlsLaunch nn = nnls_variant(c);
         const size_t smem = nnls_smem_bytes(c, nn.cap) * kMtWarps;
         const int64_t n_max = std::min<int64_t>(v, std::max<int64_t>(4096, int64_t((size_t(2) << 30) / (size_t(c) * 8))));
-        const int64_t slots = resident_slots(nn.kernel, smem, n_max);
+        const int64_t slots = resident_slots(nn.kernel, smem, n_max, "sd.nnls.ctas_per_sm");
         const size_t slot = nnls_slot_doubles(m, nn.cap);
         auto carve_all = [&](Carver& cv, int*& counters, double*& corr, double*& work) {
             counters = cv.take<int>(8);
