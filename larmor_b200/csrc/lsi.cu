@@ -232,7 +232,8 @@ __device__ __forceinline__ bool ldp_multipliers(const LsiDevice D, const LsiWarp
             // keep(): drop the factor columns that left, from the last position to the first.
             for (int pos = na - 1; pos >= 0; --pos) {
                 if (w.flag[w.cols[pos]]) continue;
-                inv_remove(fac, na, pos, lane);
+                if (na <= 32) inv_remove<1>(fac, na, pos, lane);
+                else inv_remove<VPL>(fac, na, pos, lane);
                 --na;
                 __syncwarp();
             }

@@ -343,7 +343,8 @@ __device__ __forceinline__ bool ridge_nnls(const RidgeDev R, const SignalDev S, 
             for (int pos = na - 1; pos >= 0; --pos) {
                 const int col = st.cols[pos];
                 if (sl.flag[col]) continue;
-                inv_remove(fac, na, pos, lane);
+                if (VPL == 1 || na <= 32) inv_remove<1>(fac, na, pos, lane);
+                else inv_remove<VPL>(fac, na, pos, lane);
                 if (lane == 0) sl.inf[col] = 0;
                 --na;
                 __syncwarp();

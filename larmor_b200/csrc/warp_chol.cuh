@@ -254,52 +254,57 @@ __device__ __forceinline__ bool inv_append(const InvFactor f, int& na, double h_
     return true;
 }
 
-// Removes the factor column at position pos of na (see above).
+// Removes the factor column at position pos of na (see above), VPL * 32 >= na. One pass over the
+// rotations: L~'s row r is read where L's row r + 1 lies until rotation r, its last, moves it up
+// into row r; M's row k is final after rotation k and is written there without column pos.
+// Each rotation: c = diag / hypot(diag, above), s = above / hypot, by one reciprocal hypot.
+template <int VPL>
 __device__ __forceinline__ void inv_remove(const InvFactor f, int na, int pos, int lane) {
-    auto at = [&](double* base, int r, int c) -> double& { return base[packed_row(r) + c]; };
-    // L~: the rows below pos move up (row r + 1 has r + 2 entries, row r has r + 2 slots).
-    for (int row = pos; row < na - 1; ++row) {
-        for (int c = lane; c <= row + 1; c += 32) at(f.L, row, c) = at(f.L, row + 1, c);
-        __syncwarp();
-    }
     if (lane == 0)
         for (int q = pos; q < na - 1; ++q) f.cols[q] = f.cols[q + 1];
     for (int k = pos; k < na - 1; ++k) {
-        const double diag = at(f.L, k, k), above = at(f.L, k, k + 1);
-        const double len = hypot(diag, above);
-        const double c = diag / len, s = above / len;
+        double* lk = f.L + packed_row(k + 1);  // L~ row k
+        const double diag = lk[k], above = lk[k + 1];
+        const double rh = rhypot(diag, above);
+        const double c = diag * rh, s = above * rh;
         __syncwarp();
+        // L~ rows k..na-2 (stored one row down): columns (k, k + 1) by G_k.
         for (int row = k + lane; row < na - 1; row += 32) {
-            const double l = at(f.L, row, k), r = at(f.L, row, k + 1);
-            at(f.L, row, k) = c * l + s * r;
-            at(f.L, row, k + 1) = c * r - s * l;
+            double* lr = f.L + packed_row(row + 1);
+            const double l = lr[k], r = lr[k + 1];
+            lr[k] = c * l + s * r;
+            lr[k + 1] = c * r - s * l;
         }
-        // Rows (k, k + 1) of M and entries (k, k + 1) of y by G_k^T; row k's slot k + 1 is
-        // filled here (zero before).
-        for (int j = lane; j <= k + 1; j += 32) {
-            const double a = j <= k ? at(f.M, k, j) : 0.0, b = at(f.M, k + 1, j);
-            at(f.M, k, j) = c * a + s * b;
-            at(f.M, k + 1, j) = c * b - s * a;
+        // M rows (k, k + 1) by G_k^T (row k's column k + 1 is zero before), y likewise.
+        double a[VPL], b[VPL];
+#pragma unroll
+        for (int t = 0; t < VPL; ++t) {
+            const int j = lane + 32 * t;
+            a[t] = b[t] = 0.0;
+            if (j <= k + 1) {
+                const double ma = j <= k ? f.M[packed_row(k) + j] : 0.0, mb = f.M[packed_row(k + 1) + j];
+                a[t] = c * ma + s * mb;
+                b[t] = c * mb - s * ma;
+            }
         }
         if (lane == 0) {
-            const double a = f.y[k], b = f.y[k + 1];
-            f.y[k] = c * a + s * b;
-            f.y[k + 1] = c * b - s * a;
+            const double ya = f.y[k], yb = f.y[k + 1];
+            f.y[k] = c * ya + s * yb;
+            f.y[k + 1] = c * yb - s * ya;
         }
         __syncwarp();
-    }
-    // Column pos leaves M's rows pos..na-2 (the columns after it move left); the last row goes.
-    for (int row = pos; row < na - 1; ++row) {
-        double* mr = f.M + packed_row(row);
-        // In chunks of 32 in increasing column order: each chunk reads its sources (one column
-        // to the right) before any lane writes, and later chunks read columns not yet written.
-        for (int base = pos; base <= row; base += 32) {
-            const int j = base + lane;
-            const double v = j <= row ? mr[j + 1] : 0.0;
-            __syncwarp();
-            if (j <= row) mr[j] = v;
-            __syncwarp();
+        // Row k of L~ is final: move it up (columns 0..k; its column k + 1 is now zero).
+        for (int j = lane; j <= k; j += 32) f.L[packed_row(k) + j] = lk[j];
+        // Row k of M is final: without column pos. Row k + 1 stays whole for the next rotation.
+#pragma unroll
+        for (int t = 0; t < VPL; ++t) {
+            const int j = lane + 32 * t;
+            if (j <= k + 1) {
+                if (j != pos) f.M[packed_row(k) + (j < pos ? j : j - 1)] = a[t];
+                f.M[packed_row(k + 1) + j] = b[t];
+            }
         }
+        __syncwarp();
     }
 }
 
