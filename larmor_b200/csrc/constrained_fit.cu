@@ -52,7 +52,7 @@ struct WarpShared {
 };
 
 template <class Src>
-__global__ void __launch_bounds__(kCWarps * 32) constrained_fit_kernel(
+__global__ void __launch_bounds__(kCWarps * 32, 4) constrained_fit_kernel(
     LogDesignDevice<double> d, Src src, int weighted, ViolatorList<double> list, int* queue,
     double* __restrict__ workspace, size_t slot_doubles, double* __restrict__ params) {
     __shared__ WarpShared shared[kCWarps];
@@ -121,21 +121,46 @@ __global__ void __launch_bounds__(kCWarps * 32) constrained_fit_kernel(
             }
             __syncwarp();
             if (tk != 0.0) {
-                // Columns j > k and the data: dot products by warp reductions over rows.
-                for (int j = k + 1; j <= p; ++j) {
-                    double dot = 0.0;
-                    if (j < p) {
-                        for (int r = k + 1 + lane; r < n; r += 32) dot += qr[size_t(r) * p + k] * qr[size_t(r) * p + j];
-                        dot = wsum(dot) + qr[size_t(k) * p + j];
-                        __syncwarp();
-                        if (lane == 0) qr[size_t(k) * p + j] -= tk * dot;
-                        for (int r = k + 1 + lane; r < n; r += 32) qr[size_t(r) * p + j] -= tk * qr[size_t(r) * p + k] * dot;
-                    } else {
-                        for (int r = k + 1 + lane; r < n; r += 32) dot += qr[size_t(r) * p + k] * ys[r];
-                        dot = wsum(dot) + ys[k];
-                        __syncwarp();
-                        if (lane == 0) ys[k] -= tk * dot;
-                        for (int r = k + 1 + lane; r < n; r += 32) ys[r] -= tk * qr[size_t(r) * p + k] * dot;
+                // Columns j > k and the data (column p), eight at a time: the dot products of a
+                // group in one pass over the rows and independent warp reductions, then the
+                // updates. Each dot keeps its rows' order and its reduction's.
+                for (int j0 = k + 1; j0 <= p; j0 += 8) {
+                    double dv[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) dv[q] = 0.0;
+                    for (int r = k + 1 + lane; r < n; r += 32) {
+                        const double vr = qr[size_t(r) * p + k];
+                        const double* row = qr + size_t(r) * p;
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const int j = j0 + q;
+                            if (j < p) dv[q] += vr * row[j];
+                            else if (j == p) dv[q] += vr * ys[r];
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int j = j0 + q;
+                        if (j <= p) dv[q] = wsum(dv[q]) + (j < p ? qr[size_t(k) * p + j] : ys[k]);
+                    }
+                    __syncwarp();
+                    if (lane == 0) {
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const int j = j0 + q;
+                            if (j < p) qr[size_t(k) * p + j] -= tk * dv[q];
+                            else if (j == p) ys[k] -= tk * dv[q];
+                        }
+                    }
+                    for (int r = k + 1 + lane; r < n; r += 32) {
+                        double* row = qr + size_t(r) * p;
+                        const double vr = row[k];
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const int j = j0 + q;
+                            if (j < p) row[j] -= tk * vr * dv[q];
+                            else if (j == p) ys[r] -= tk * vr * dv[q];
+                        }
                     }
                     __syncwarp();
                 }
@@ -158,23 +183,49 @@ __global__ void __launch_bounds__(kCWarps * 32) constrained_fit_kernel(
             }
         }
         __syncwarp();
-        // NNLS matrix: rows 0..p-1 = R^-T G^T, row p = -(G p_free)^T; lanes over constraints.
+        // NNLS matrix: rows 0..p-1 = R^-T G^T, row p = -(G p_free)^T; lanes over constraints, four
+        // columns at a time so that their substitution chains overlap.
         double colsum_max = 0.0;
-        for (int c = lane; c < m; c += 32) {
-            const double* gr = d.g + size_t(c) * p;
-            double acc_abs = 0.0, gf = 0.0;
-            for (int i = 0; i < p; ++i) {
-                double s = gr[i];
-                for (int k = 0; k < i; ++k) s -= qr[size_t(k) * p + i] * cm[size_t(k) * m + c];
-                s /= qr[size_t(i) * p + i];
-                cm[size_t(i) * m + c] = s;
-                acc_abs += fabs(s);
-                gf += gr[i] * pfree[i];
+        for (int c0 = lane; c0 < m; c0 += 4 * 32) {
+            int cc[4];
+            bool in[4];
+            double acc_abs[4], gf[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                cc[q] = c0 + 32 * q;
+                in[q] = cc[q] < m;
+                acc_abs[q] = 0.0;
+                gf[q] = 0.0;
             }
-            cm[size_t(p) * m + c] = -gf;
-            acc_abs += fabs(gf);
-            colsum_max = fmax(colsum_max, acc_abs);
-            u[c] = 0.0;
+            for (int i = 0; i < p; ++i) {
+                double sv[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) sv[q] = in[q] ? d.g[size_t(cc[q]) * p + i] : 0.0;
+                for (int k = 0; k < i; ++k) {
+                    const double rki = qr[size_t(k) * p + i];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (in[q]) sv[q] -= rki * cm[size_t(k) * m + cc[q]];
+                }
+                const double rii = qr[size_t(i) * p + i];
+                const double pf = pfree[i];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (!in[q]) continue;
+                    const double si = sv[q] / rii;
+                    cm[size_t(i) * m + cc[q]] = si;
+                    acc_abs[q] += fabs(si);
+                    gf[q] += d.g[size_t(cc[q]) * p + i] * pf;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (!in[q]) continue;
+                cm[size_t(p) * m + cc[q]] = -gf[q];
+                acc_abs[q] += fabs(gf[q]);
+                colsum_max = fmax(colsum_max, acc_abs[q]);
+                u[cc[q]] = 0.0;
+            }
         }
         colsum_max = wmax(colsum_max);
         const double tol = 10.0 * kEps * colsum_max * double(max(rows, m));

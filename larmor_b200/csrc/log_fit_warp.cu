@@ -141,11 +141,27 @@ __global__ void __launch_bounds__(kWarps * 32) fit_log_warp_kernel(
                     ws[j] = dev_exp<T>(T(2) * (pred - mx));
                 }
                 __syncwarp();
-                for (int e = lane; e < pp; e += 32) {
-                    const int a = ea[e], b = eb[e];
-                    T acc = T(0);
-                    for (int j = 0; j < n; ++j) acc = fma(ws[j] * xs[j * px + a], xs[j * px + b], acc);
-                    gm[b * px + a] = acc;  // lower triangle
+                // Four entries per lane at a time, so that their sums over the measurements
+                // overlap (each in its own order).
+                for (int e0 = lane; e0 < pp; e0 += 4 * 32) {
+                    int ia[4], ib[4];
+                    T acc[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int e = e0 + 32 * q;
+                        ia[q] = e < pp ? ea[e] : 0;
+                        ib[q] = e < pp ? eb[e] : 0;
+                        acc[q] = T(0);
+                    }
+                    for (int j = 0; j < n; ++j) {
+                        const T wj = ws[j];
+                        const T* xr = xs + j * px;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc[q] = fma(wj * xr[ia[q]], xr[ib[q]], acc[q]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (e0 + 32 * q < pp) gm[ib[q] * px + ia[q]] = acc[q];  // lower triangle
                 }
                 if (lane < p) {
                     T acc = T(0);

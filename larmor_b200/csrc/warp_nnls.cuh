@@ -259,11 +259,23 @@ __device__ __forceinline__ int warp_nnls_explicit(const double* __restrict__ c, 
             e = bi;
             ge = bv;
         } else {
-            for (int j = lane; j < m; j += 32) {
-                if (s.flag[j]) continue;
-                double g = 0.0;
-                for (int r = 0; r < rows; ++r) g += c[size_t(r) * m + j] * s.res[r];
-                if (bi < 0 || g > bv) { bv = g; bi = j; }
+            // Lanes over the columns, four at a time so that their dot products overlap; each
+            // lane takes its columns in increasing order (the first on a tie).
+            for (int j0 = lane; j0 < m; j0 += 4 * 32) {
+                double g[4] = {0.0, 0.0, 0.0, 0.0};
+                bool open[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) open[q] = j0 + 32 * q < m && !s.flag[j0 + 32 * q];
+                for (int r = 0; r < rows; ++r) {
+                    const double rr = s.res[r];
+                    const double* cr = c + size_t(r) * m;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (open[q]) g[q] += cr[j0 + 32 * q] * rr;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (open[q] && (bi < 0 || g[q] > bv)) { bv = g[q]; bi = j0 + 32 * q; }
             }
             e = warp_argmax_first(bv, bi);
             ge = e >= 0 ? __shfl_sync(0xffffffffu, bv, e & 31) : 0.0;
