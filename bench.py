@@ -313,8 +313,8 @@ class MfodWorkload(_SdWorkloadBase):
     (44 in the loop) + GM + CSF, up to 50 rounds, on S0-normalised signals."""
 
     name = "mfod_3tissue_110x110x70"
-    kernels = ("correlate_kernel", "ridge_nnls_kernel<1,2>", "lr_fractions_kernel", "ridge_nnls_kernel<8,10>",
-               "hr_fractions_kernel")
+    kernels = ("correlate_kernel", "ridge_nnls_half_kernel<3>", "ridge_nnls_kernel<1,2>", "lr_fractions_kernel",
+               "ridge_nnls_kernel<8,10>", "hr_fractions_kernel")
     has_fp32 = False
     # 280 double samples in, 300 double amplitudes + 3 fractions out.
     bytes_per_voxel = 8 * 280 + 8 * 303
@@ -372,8 +372,11 @@ class MfodWorkload(_SdWorkloadBase):
                                       self.hr_solver, 50, 1e-7, 1e-2, self.d_fods, self.d_fr, rounds=rounds)
         vr = int(rounds.sum().item())
         m, c_lr, c_hr = 280, self.k_lr.ca, self.k_hr.ca
+        # The low-resolution NNLS runs two voxels per warp; the one-warp kernel refits only the
+        # few voxels that need its QR fallback (counted with the two-voxel kernel's).
         return {"correlate_kernel": vr * 8 * (m + c_lr) + self.v * 8 * (m + c_hr),
-                "ridge_nnls_kernel<1,2>": vr * 8 * 2 * c_lr,
+                "ridge_nnls_half_kernel<3>": vr * 8 * 2 * c_lr,
+                "ridge_nnls_kernel<1,2>": 0,
                 "lr_fractions_kernel": vr * 8 * (c_lr + m + 3),
                 "ridge_nnls_kernel<8,10>": self.v * 8 * 2 * c_hr,
                 "hr_fractions_kernel": self.v * 8 * (c_hr + m + 3)}
@@ -474,7 +477,8 @@ def _job_kernel_bytes(job) -> dict:
     vr = int(job.out["rounds"].sum().item())
     c_lr, c_hr = job.handles["k_lr"].ca, job.handles["k_hr"].ca
     return {"correlate_kernel": vr * 8 * (n + c_lr) + v * 8 * (n + c_hr),
-            "ridge_nnls_kernel<1,2>": vr * 8 * 2 * c_lr,
+            "ridge_nnls_half_kernel<3>": vr * 8 * 2 * c_lr,
+            "ridge_nnls_kernel<1,2>": 0,
             "lr_fractions_kernel": vr * 8 * (c_lr + n + 3),
             "ridge_nnls_kernel<8,10>": v * 8 * 2 * c_hr,
             "hr_fractions_kernel": v * 8 * (c_hr + n + 3)}
@@ -487,8 +491,8 @@ class BatchWorkload:
 
     name = "batch_uneven_64_volumes"
     kernels = ("fit_dti_maps_kernel", "fit_log_warp_kernel", "constrained_fit_kernel", "dki_maps_kernel",
-               "correlate_kernel", "ridge_nnls_kernel<1,2>", "lr_fractions_kernel", "ridge_nnls_kernel<8,10>",
-               "hr_fractions_kernel")
+               "correlate_kernel", "ridge_nnls_half_kernel<3>", "ridge_nnls_kernel<1,2>", "lr_fractions_kernel",
+               "ridge_nnls_kernel<8,10>", "hr_fractions_kernel")
     has_fp32 = False
 
     def __init__(self, seed: int) -> None:

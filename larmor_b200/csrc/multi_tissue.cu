@@ -33,6 +33,7 @@
 
 #include "common.cuh"
 #include "host_la.hpp"
+#include "group_nnls.cuh"
 #include "warp_chol.cuh"
 #include "warp_nnls.cuh"
 
@@ -415,6 +416,189 @@ __global__ void __launch_bounds__(kMtWarps * 32, (CPL <= 2 ? 6 : 4)) ridge_nnls_
         for (int j = lane; j < R.c; j += 32) x_out[voxel * ldx + j] = sl.x[j];
         if (lane == 0 && !ok && bad) bad[voxel] = 1;
         __syncwarp();
+    }
+}
+
+// ---- ridge NNLS, two voxels per warp (at most 48 directions) ---------------------------------
+
+// A half-warp's workspace: x, z (c each), the factor's vectors h, w, y (32 each) and the two
+// flag arrays in shared memory; the factor and its inverse (32 columns) in its global slot.
+struct HalfSlot {
+    double *x, *z, *h, *w, *y, *L, *M;
+    uint8_t *flag, *inf;
+};
+
+inline size_t half_slot_doubles() { return 2 * size_t(packed_size(2 * kHalf)) + 8; }
+
+__host__ __device__ inline size_t half_smem_bytes(int c) {
+    return ((2 * size_t(c) + 3 * 2 * kHalf) * sizeof(double) + 2 * size_t(c) + 15) / 16 * 16;
+}
+
+__device__ HalfSlot carve_half(double* base, unsigned char* smem, int c) {
+    HalfSlot s;
+    s.L = base;
+    s.M = base + packed_size(2 * kHalf);
+    double* q = reinterpret_cast<double*>(smem);
+    s.x = q; q += c;
+    s.z = q; q += c;
+    s.h = q; q += 2 * kHalf;
+    s.w = q; q += 2 * kHalf;
+    s.y = q; q += 2 * kHalf;
+    s.flag = reinterpret_cast<uint8_t*>(q);
+    s.inf = s.flag + c;
+    return s;
+}
+
+template <int CPL>
+struct HalfState {
+    int cols[2 * kHalf];      // factor columns, joining order
+    int sorted[kHalf * CPL];  // columns with x != 0, increasing
+};
+
+// ridge_nnls for one voxel on a half-warp (see group_nnls.cuh): the same steps, rules and
+// tolerances. False when the voxel needs the QR fallback (a pivot below the tolerance or more
+// than 32 active columns); the caller then hands it to the one-warp kernel.
+template <int CPL>
+__device__ __forceinline__ bool ridge_nnls_half(const RidgeDev R, const double* __restrict__ corr, const HalfSlot sl,
+                                                HalfState<CPL>& st, const HalfWarp hw) {
+    const int c = R.c;
+    const InvFactor fac{sl.L, sl.M, sl.h, sl.w, sl.y, st.cols, 2 * kHalf};
+    for (int j = hw.lane; j < c; j += kHalf) {
+        sl.x[j] = 0.0;
+        sl.z[j] = 0.0;
+        sl.flag[j] = 0;
+        sl.inf[j] = 0;
+    }
+    hw.sync();
+    int na = 0, inner = 0;
+    const int max_inner = 3 * c;
+    bool blocked = false;
+    for (;;) {
+        int entering = -1;
+        if (!blocked) {
+            int n_sorted = 0;
+            for (int base = 0; base < c; base += kHalf) {
+                const int j = base + hw.lane;
+                const bool nz = j < c && sl.x[j] != 0.0;
+                const unsigned ballot = hw.ballot(nz);
+                if (nz) st.sorted[n_sorted + __popc(ballot & ((1u << hw.lane) - 1u))] = j;
+                n_sorted += __popc(ballot);
+            }
+            hw.sync();
+            double g[CPL];
+#pragma unroll
+            for (int t = 0; t < CPL; ++t) {
+                const int j = hw.lane + kHalf * t;
+                g[t] = j < c ? corr[j] : 0.0;
+            }
+            for (int q = 0; q < n_sorted; ++q) {
+                const int col = st.sorted[q];
+                const double xc = sl.x[col];
+                const double* row = R.gram + size_t(col) * c;
+#pragma unroll
+                for (int t = 0; t < CPL; ++t) {
+                    const int j = hw.lane + kHalf * t;
+                    if (j < c) g[t] -= xc * row[j];
+                }
+            }
+            double bv = 0.0;
+            int bi = -1;
+#pragma unroll
+            for (int t = 0; t < CPL; ++t) {
+                const int j = hw.lane + kHalf * t;
+                if (j < c && !sl.flag[j] && (bi < 0 || g[t] > bv)) { bv = g[t]; bi = j; }
+            }
+            const int e = hw.argmax_first(bv, bi);
+            const double ge = e >= 0 ? hw.from(bv, e & (kHalf - 1)) : 0.0;
+            if (e < 0 || ge <= R.tol) break;
+            if (hw.lane == 0) sl.flag[e] = 1;
+            hw.sync();
+            entering = e;
+        } else {
+            if (++inner > max_inner) {
+                for (int j = hw.lane; j < c; j += kHalf) sl.x[j] = sl.z[j];
+                hw.sync();
+                return true;
+            }
+            double sv = 0.0;
+            int si = -1;
+            for (int j = hw.lane; j < c; j += kHalf) {
+                if (!sl.flag[j] || sl.z[j] > 0.0) continue;
+                const double dist = sl.x[j] - sl.z[j];
+                const double stp = dist > 0.0 ? sl.x[j] / dist : 0.0;
+                if (si < 0 || stp < sv) { sv = stp; si = j; }
+            }
+            double step;
+            const int b = hw.argmin_first(sv, si, &step);
+            for (int j = hw.lane; j < c; j += kHalf) sl.x[j] += step * (sl.z[j] - sl.x[j]);
+            hw.sync();
+            if (hw.lane == 0) {
+                sl.x[b] = 0.0;
+                sl.flag[b] = 0;
+            }
+            hw.sync();
+            for (int j = hw.lane; j < c; j += kHalf)
+                if (sl.flag[j] && !(fabs(sl.x[j]) >= R.tol)) sl.flag[j] = 0;
+            hw.sync();
+        }
+        for (int pos = na - 1; pos >= 0; --pos) {
+            const int col = st.cols[pos];
+            if (sl.flag[col]) continue;
+            half_remove(fac, na, pos, hw);
+            if (hw.lane == 0) sl.inf[col] = 0;
+            --na;
+            hw.sync();
+        }
+        if (entering >= 0) {
+            if (na >= 2 * kHalf) return false;
+            for (int r = hw.lane; r < na; r += kHalf) sl.h[r] = R.gram[size_t(st.cols[r]) * c + entering];
+            hw.sync();
+            if (!half_append(fac, na, R.gram[size_t(entering) * c + entering], corr[entering], entering, kMinPivot,
+                             hw))
+                return false;
+            if (hw.lane == 0) sl.inf[entering] = 1;
+            hw.sync();
+        }
+        half_solve(fac, na, sl.z, c, hw);
+        bool any = false;
+        for (int j = hw.lane; j < c; j += kHalf) any |= sl.flag[j] && sl.z[j] <= 0.0;
+        blocked = hw.any(any);
+        if (!blocked) {
+            for (int j = hw.lane; j < c; j += kHalf) sl.x[j] = sl.z[j];
+            hw.sync();
+        }
+    }
+    return true;
+}
+
+// Two listed voxels per warp, one per half, pulled from a device counter: x(v) <- the ridge
+// NNLS of corr(v), or v appended to `redo` when it needs the QR fallback.
+template <int CPL>
+__global__ void __launch_bounds__(kMtWarps * 32, 6) ridge_nnls_half_kernel(
+    RidgeDev R, const int* __restrict__ list, int64_t count, const int* __restrict__ count_dev,
+    const double* __restrict__ corr, int ldc, double* __restrict__ x_out, int ldx, int* __restrict__ redo,
+    int* redo_count, int* queue, double* __restrict__ workspace, size_t slot_size) {
+    if (count_dev) count = min(count, int64_t(*count_dev));
+    __shared__ HalfState<CPL> states[2 * kMtWarps];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const HalfWarp hw(threadIdx.x & 31);
+    const int gid = int(threadIdx.x >> 4);  // half-warp within the CTA
+    HalfState<CPL>& st = states[gid];
+    const HalfSlot sl = carve_half(workspace + (size_t(blockIdx.x) * 2 * kMtWarps + gid) * slot_size,
+                                   smem_raw + gid * half_smem_bytes(R.c), R.c);
+    for (;;) {
+        long long p = 0;
+        if (hw.lane == 0) p = atomicAdd(queue, 1);
+        p = hw.from(p, 0);
+        if (p >= count) break;
+        const int64_t voxel = listed(list, p);
+        const bool done = ridge_nnls_half<CPL>(R, corr + voxel * ldc, sl, st, hw);
+        if (done) {
+            for (int j = hw.lane; j < R.c; j += kHalf) x_out[voxel * ldx + j] = sl.x[j];
+        } else if (hw.lane == 0) {
+            redo[atomicAdd(redo_count, 1)] = int(voxel);
+        }
+        hw.sync();
     }
 }
 
@@ -960,17 +1144,27 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
                                  3 * sizeof(int) + 1;
         const int64_t n_max = std::min<int64_t>(v, std::max<int64_t>(4096, int64_t((size_t(4) << 30) / per_voxel)));
         const int64_t lr_slots = resident_slots(lr_nnls.kernel, lr_smem, n_max, "sd.nnls.ctas_per_sm");
+        // Low-resolution kernels of at most 48 directions with normal equations: two voxels per
+        // warp (ridge_nnls_half_kernel), the voxels that need the QR fallback then refitted by
+        // the one-warp kernel.
+        const bool half = lrs.normal_equations && c_lr <= 48;
+        auto half_kernel = ridge_nnls_half_kernel<3>;
+        const size_t half_smem = half_smem_bytes(c_lr) * 2 * kMtWarps;
+        const int64_t half_warps = half ? resident_slots(half_kernel, half_smem, n_max, "sd.nnls.ctas_per_sm") : 0;
         const int64_t hr_slots = resident_slots(hr_nnls.kernel, hr_smem, n_max, "sd.nnls.ctas_per_sm");
         const int64_t lf_slots = resident_slots(lr_fractions_kernel, 0, n_max, "sd.fractions.ctas_per_sm");
         const int64_t hf_slots = resident_slots(hr_fractions_kernel, 0, n_max, "sd.fractions.ctas_per_sm");
         const size_t lr_slot = nnls_slot_doubles(mi, lr_nnls.cap), hr_slot = nnls_slot_doubles(mi, hr_nnls.cap);
         const size_t lf_slot = frac_slot_doubles(mi, c_lr, 1 + ci), hf_slot = frac_slot_doubles(mi, c_hr, nf);
         const size_t slot_doubles =
-            std::max(std::max(size_t(lr_slots) * lr_slot, size_t(hr_slots) * hr_slot),
-                     std::max(size_t(lf_slots) * lf_slot, size_t(hf_slots) * hf_slot));
+            std::max(std::max(std::max(size_t(lr_slots) * lr_slot, size_t(hr_slots) * hr_slot),
+                              std::max(size_t(lf_slots) * lf_slot, size_t(hf_slots) * hf_slot)),
+                     size_t(2 * half_warps) * half_slot_doubles());
         struct Pieces {
-            int* counters;  // [0] the persistent kernels' work counter, [2], [3] the two lists' counts
+            int* counters;  // [0] the persistent kernels' work counter, [2], [3] the two lists' counts,
+                            // [4] the voxels to refit by the one-warp NNLS
             int* list[2];
+            int* redo;
             double *fiso, *prev, *corr, *xlr, *slots;
             int32_t* rounds;
             uint8_t* bad;
@@ -980,6 +1174,7 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
             p.counters = cv.take<int>(8);
             p.list[0] = cv.take<int>(size_t(n_max));
             p.list[1] = cv.take<int>(size_t(n_max));
+            p.redo = cv.take<int>(size_t(n_max));
             p.fiso = cv.take<double>(size_t(n_max) * std::max(ci, 1));
             p.prev = cv.take<double>(size_t(n_max) * (ci + 1));
             p.corr = cv.take<double>(size_t(n_max) * std::max(c_lr, c_hr));
@@ -1025,7 +1220,22 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
                 launch_correlate(lr_sig, cur, count, cur_count, lrs, P.corr, c_lr, st);
                 reset_queue();
                 cuda_check(cudaMemsetAsync(nxt_count, 0, sizeof(int), st), "cudaMemsetAsync");
-                {
+                if (half) {
+                    cuda_check(cudaMemsetAsync(P.counters + 4, 0, sizeof(int), st), "cudaMemsetAsync");
+                    {
+                        LaunchScope scope("ridge_nnls_half_kernel<3>", st);
+                        half_kernel<<<blocks(half_warps, (count + 1) / 2), kMtWarps * 32, half_smem, st>>>(
+                            lrs, cur, count, cur_count, P.corr, c_lr, P.xlr, c_lr, P.redo, P.counters + 4, P.counters,
+                            P.slots, half_slot_doubles());
+                        cuda_check(cudaGetLastError(), "ridge_nnls_half_kernel launch");
+                    }
+                    reset_queue();
+                    LaunchScope scope(lr_nnls.name, st);
+                    lr_nnls.kernel<<<blocks(lr_slots, count), kMtWarps * 32, lr_smem, st>>>(
+                        lrs, lr_sig, P.redo, count, P.counters + 4, P.corr, c_lr, P.xlr, c_lr, P.bad, P.counters,
+                        P.slots, lr_slot);
+                    cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
+                } else {
                     LaunchScope scope(lr_nnls.name, st);
                     lr_nnls.kernel<<<blocks(lr_slots, count), kMtWarps * 32, lr_smem, st>>>(
                         lrs, lr_sig, cur, count, cur_count, P.corr, c_lr, P.xlr, c_lr, P.bad, P.counters, P.slots,
