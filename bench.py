@@ -588,8 +588,98 @@ class BatchWorkload:
                                                 f"(fits only), repeated for ~{budget_s:.0f} s")
 
 
+class PeaksWorkload:
+    """FOD peaks (find_peaks, src/larmor/sd/peaks.py) of lmax-8 FODs on the config-3 mask
+    (110x110x70, 500,040 voxels): the amplitudes of each FOD on the 642-vertex icosphere, then
+    the climbs from their local maxima, merged into at most 3 peaks above 0.1 of the largest.
+    The FODs are seeded synthetic SH series of 1-3 fibres (Dirichlet(2) fractions, random
+    directions, the lmax-8 fibre profile exp(-0.02 l(l+1))) plus N(0, 0.02) noise on every
+    coefficient."""
+
+    name = "peaks_lmax8_110x110x70"
+    kernels = ("project_sh_kernel", "peaks_kernel")
+    has_fp32 = False
+    unit = "voxel peak searches/s"
+
+    def __init__(self, seed: int) -> None:
+        from larmor_b200.sd.sh import build_basis_matrix, get_sh_indices
+        from larmor_b200.sd.sphere import get_theta_phi
+        from larmor_b200.synthetic import ellipsoid_mask
+
+        mask = ellipsoid_mask((110, 110, 70), 1.0435)
+        self.v = int(mask.sum())
+        rng = np.random.default_rng(7 + 10 * (seed - 1))
+        ls, _ = get_sh_indices(8)
+        profile = np.exp(-0.02 * ls * (ls + 1))
+        n_fib = rng.integers(1, 4, size=self.v)
+        fr = rng.dirichlet([2.0, 2.0, 2.0], size=self.v) * (np.arange(3)[None] < n_fib[:, None])
+        fr /= fr.sum(axis=1, keepdims=True)
+        coeffs = 0.02 * rng.normal(size=(self.v, 45))
+        for f in range(3):
+            d = rng.normal(size=(self.v, 3))
+            d /= np.linalg.norm(d, axis=1, keepdims=True)
+            theta, phi = get_theta_phi(d)
+            coeffs += fr[:, f:f + 1] * build_basis_matrix(theta, phi, 8) * profile
+        self.coeffs = np.ascontiguousarray(coeffs)
+        self.config = {"workload": self.name, "grid": [110, 110, 70], "voxels": self.v, "lmax": 8,
+                       "sphere": "642-vertex icosphere", "num_peaks": 3, "relative_threshold": 0.1,
+                       "l2": "amplitudes (2.6 GB) larger than L2"}
+
+    def subset(self, n: int) -> None:
+        self.coeffs = self.coeffs[:n]
+        self.v = len(self.coeffs)
+        self.config["voxels"] = self.v
+
+    def device_setup(self, torch, dev):
+        from larmor_b200 import _core
+        from larmor_b200.sd.peaks import _amplitude_projector, _build_icosphere
+
+        self.torch = torch
+        vertices, neighbours = _build_icosphere()
+        self.sphere = _core.PeakSphere.cached(vertices, neighbours)
+        self.projector = _amplitude_projector(8, False)
+        self.d_coeffs = torch.from_numpy(self.coeffs).to(dev)
+        self.h_coeffs = torch.from_numpy(self.coeffs).pin_memory()
+        self.h_dirs = torch.empty((self.v, 3, 3), dtype=torch.float64).pin_memory()
+        self.h_amps = torch.empty((self.v, 3), dtype=torch.float64).pin_memory()
+        self.h2d_bytes = self.coeffs.nbytes
+        self.d2h_bytes = self.v * 12 * 8
+
+    def step_device(self, precision=0):
+        from larmor_b200 import _core
+
+        on_sphere = _core.project_sh_device(self.projector, self.d_coeffs, exact_integral=False)
+        self.d_dirs, self.d_amps = _core.find_peaks_device(self.sphere, self.d_coeffs, 8, False, on_sphere, 3, 0.1,
+                                                           0.0)
+
+    def kernel_bytes(self) -> dict:
+        """Algorithmic DRAM bytes of one step: 45 coefficients in and 642 amplitudes out for the
+        projection; the coefficients, the amplitudes and 12 outputs for the search."""
+        return {"project_sh_kernel": self.v * 8 * (45 + 642), "peaks_kernel": self.v * 8 * (45 + 642 + 12)}
+
+    def step_e2e(self):
+        self.d_coeffs.copy_(self.h_coeffs, non_blocking=True)
+        self.step_device()
+        self.h_dirs.copy_(self.d_dirs, non_blocking=True)
+        self.h_amps.copy_(self.d_amps, non_blocking=True)
+
+    def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
+        from larmor_b200.sd.peaks import _build_icosphere, _get_amplitudes
+        from oracle import oracle as o
+
+        vertices, neighbours = _build_icosphere()
+        n = min(self.v, 8192)
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget_s:
+            on = np.ascontiguousarray(_get_amplitudes(self.coeffs[:n], 8, False))
+            o.peaks_chunk(self.coeffs[:n], 8, on, vertices, neighbours, 3, 0.1, 0.0, n_threads=threads)
+            done += n
+        return done, time.perf_counter() - t0, (f"first {n} voxels (numpy amplitudes + the oracle's search), "
+                                                f"repeated for ~{budget_s:.0f} s")
+
+
 WORKLOADS = {"dti": DtiWorkload, "dki": DkiWorkload, "mfod": MfodWorkload, "msmt": MsmtWorkload,
-             "batch": BatchWorkload}
+             "batch": BatchWorkload, "peaks": PeaksWorkload}
 
 
 
@@ -696,13 +786,14 @@ def run_reference(args, wl) -> dict:
     secs = sum(s for _, s in per_step)
     value = voxels / secs
     return {
-        "metric": METRIC, "value": value, "unit": "voxel fits/s", "impl": "reference",
+        "metric": METRIC, "value": value, "unit": getattr(wl, "unit", "voxel fits/s"), "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * secs / len(per_step), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": wl.config,
-        "cpu_baseline": {"value": value, "unit": "voxel fits/s", "cores": threads, "kind": "port",
-                         "sample": sample},
-        "e2e": {"value": value, "unit": "voxel fits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": getattr(wl, "unit", "voxel fits/s"), "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": getattr(wl, "unit", "voxel fits/s"), "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
     }
 
 
@@ -873,11 +964,11 @@ def main() -> int:
     if rank == 0:
         threads = os.cpu_count() or 1
         done, secs, sample = wl.cpu_sample(threads, args.cpu_budget)
-        cpu = {"value": done / secs, "unit": "voxel fits/s", "cores": threads, "kind": "port",
+        cpu = {"value": done / secs, "unit": getattr(wl, "unit", "voxel fits/s"), "cores": threads, "kind": "port",
                "sample": sample}
 
     line = {
-        "metric": METRIC, "value": value, "unit": "voxel fits/s", "n_gpus": world,
+        "metric": METRIC, "value": value, "unit": getattr(wl, "unit", "voxel fits/s"), "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": wl.config,
@@ -888,7 +979,7 @@ def main() -> int:
                      "avg_launch_ms": avg_launch_s * 1e3, "launches": top_launches,
                      "kernel_share": {k: round(t / total_kernel_ms, 4) for k, (t, _) in kernel_ms.items()}},
         "cpu_baseline": cpu,
-        "e2e": {"value": voxels_all * args.steps / (e2e_ms / 1e3), "unit": "voxel fits/s",
+        "e2e": {"value": voxels_all * args.steps / (e2e_ms / 1e3), "unit": getattr(wl, "unit", "voxel fits/s"),
                 "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes},
         "plain_fp32": None if fp32_ms is None else {
             "value": voxels_all * args.steps / (fp32_ms / 1e3), "unit": "voxel fits/s",

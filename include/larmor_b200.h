@@ -232,6 +232,46 @@ void lar_sh_projector_destroy(lar_sh_projector projector);
 int lar_project_sh(lar_sh_projector projector, const double* amplitudes, int64_t v, int64_t lda,
                    int exact_integral, double* out, int64_t ldo, void* stream);
 
+/* ---- FOD peaks ------------------------------------------------------------------------ */
+
+/* Series in the tournier basis: n_coeffs(lmax, full) = (lmax + 1)(lmax + 2) / 2 even degrees, or
+ * (lmax + 1)^2 all degrees when full; lmax <= 20, even unless full. Each entry point returns
+ * LAR_ERR_INVALID for another lmax, a row stride below the coefficient count or a negative
+ * count, before any device work. */
+
+/* A sphere for the peak search: nv unit vertices (nv, 3) and the indices of the 6 neighbours of
+ * each (nv, 6; a vertex with 5 lists itself), host arrays copied to the device. Replaces the
+ * sphere the reference builds per call in _core.peaks_chunk (cpp/src/python/sh.cpp:130-147):
+ * LAR_ERR_INVALID when a neighbour index is outside [0, nv). */
+typedef struct lar_peak_sphere_s* lar_peak_sphere;
+
+int lar_peak_sphere_create(const double* vertices, const int64_t* neighbours, int64_t nv, lar_peak_sphere* out);
+
+void lar_peak_sphere_destroy(lar_peak_sphere sphere);
+
+/* _core.sh_derivatives (cpp/src/python/sh.cpp:69-82, cpp/src/sh/harmonics.cpp:139-196) for n
+ * points: out (n, 6) = f, df/dtheta, df/dphi / sin theta, d2f/dtheta2, d2f/dtheta dphi / sin theta,
+ * d2f/dphi2 / sin^2 theta of series i (row i of coeffs, stride ldc) at (theta[i], phi[i]). All
+ * device arrays. */
+int lar_sh_derivatives(const double* coeffs, int64_t n, int64_t ldc, int lmax, int full, const double* theta,
+                       const double* phi, double* out, void* stream);
+
+/* _core.climb (cpp/src/python/sh.cpp:84-108, cpp/src/sh/peaks.cpp:31-78) for n climbs: series i
+ * from the unit vector starts[i] (n, 3) to directions (n, 3) and amplitudes (n), NaN where the
+ * climb has not stopped within max_iters (>= 0) steps. All device arrays. */
+int lar_climb(const double* coeffs, int64_t n, int64_t ldc, int lmax, int full, const double* starts, int max_iters,
+              double tol, double max_step, double* directions, double* amplitudes, void* stream);
+
+/* _core.peaks_chunk (cpp/src/python/sh.cpp:112-176, cpp/src/sh/peaks.cpp:80-133): the peaks of
+ * n voxels' series (row stride ldc) from their amplitudes on the sphere's vertices (on_sphere,
+ * row stride lds >= nv), largest first, into directions (n, n_peaks, 3) and amplitudes
+ * (n, n_peaks), NaN where a voxel has fewer; symmetric series' peaks turned to z >= 0. n_peaks
+ * >= 1. All device arrays except the sphere. Allocates a stream-ordered workspace of 128 nv
+ * bytes per resident warp. */
+int lar_find_peaks(lar_peak_sphere sphere, const double* coeffs, int64_t n, int64_t ldc, int lmax, int full,
+                   const double* on_sphere, int64_t lds, int n_peaks, double relative_threshold, double threshold,
+                   double* directions, double* amplitudes, void* stream);
+
 /* ---- A fit that allocates no device memory ------------------------------------------- */
 
 /* No counterpart in the reference: an entry point for callers that cannot allocate device

@@ -435,6 +435,12 @@ def _fit_single_tissue_on_device(signals, solver: FodSolver):
     return fods
 
 
+def _row_stride(t) -> int:
+    """The row stride of a 2D tensor with unit-stride rows; a one-row tensor's stride along the
+    rows is arbitrary (numpy and torch keep 0 for a view like a[None]), so its row length."""
+    return t.stride(0) if t.shape[0] > 1 else t.shape[1]
+
+
 class ShProjector(_Handle):
     """The least-squares projector of amplitudes on a sphere grid onto an SH basis, scaled by
     the grid's density, on the device (the _to_sh step, src/larmor/sd/model.py:412-440)."""
@@ -452,16 +458,182 @@ def project_sh_device(projector: ShProjector, amplitudes, exact_integral: bool):
     """SH coefficients (v, ncoef) of device amplitudes (v, ca), a column slice of a row-major
     tensor allowed; a new device tensor."""
     torch = _torch()
-    if amplitudes.dim() != 2 or amplitudes.shape[1] != projector.ca or amplitudes.stride(1) != 1:
+    if (amplitudes.dim() != 2 or amplitudes.shape[1] != projector.ca
+            or (amplitudes.shape[0] and amplitudes.stride(1) != 1)):
         raise ValueError(f"amplitudes {tuple(amplitudes.shape)} do not have the projector's {projector.ca} "
                          "directions in unit-stride rows")
     v = amplitudes.shape[0]
     out = torch.empty((v, projector.ncoef), dtype=torch.float64, device=amplitudes.device)
     if v:
-        _lib.check(_lib.lib().lar_project_sh(projector.handle, _lib.ptr(amplitudes), v, amplitudes.stride(0),
+        _lib.check(_lib.lib().lar_project_sh(projector.handle, _lib.ptr(amplitudes), v, _row_stride(amplitudes),
                                              int(bool(exact_integral)), _lib.ptr(out), projector.ncoef,
                                              _stream(torch)))
     return out
+
+
+# ---- FOD peaks (cpp/src/python/sh.cpp) ---------------------------------------------------
+
+MAX_LMAX = 20
+
+
+def _check_lmax(lmax: int, full: bool, n_coeffs_given: int) -> None:
+    """cpp/src/python/sh.cpp:40-53: lmax within 0..20, even unless full, matching the count."""
+    if lmax < 0 or lmax > MAX_LMAX or (not full and lmax % 2 != 0):
+        raise ValueError(f"lmax must be at most {MAX_LMAX}, and even unless full, got {lmax}")
+    expected = (lmax + 1) ** 2 if full else (lmax + 1) * (lmax + 2) // 2
+    if expected != n_coeffs_given:
+        raise ValueError(f"lmax {lmax} has {expected} coefficients, got {n_coeffs_given}")
+
+
+def _series(sh) -> np.ndarray:
+    """A 1D float64 series of any strides, copied (the bindings' copy_series)."""
+    if not isinstance(sh, np.ndarray) or sh.dtype != np.float64:
+        got = type(sh).__name__ if not isinstance(sh, np.ndarray) else str(sh.dtype)
+        raise TypeError(f"sh must be a float64 numpy array, got {got}")
+    if sh.ndim != 1:
+        raise ValueError(f"sh must have 1 dimension, got shape {sh.shape}")
+    return np.ascontiguousarray(sh)
+
+
+def sh_derivatives(sh, lmax: int, theta: float, phi: float, full: bool = False) -> tuple[float, ...]:
+    """The amplitude f of a series and df/dtheta, df/dphi / sin theta, d2f/dtheta2,
+    d2f/dtheta dphi / sin theta, d2f/dphi2 / sin^2 theta at (theta, phi)
+    (cpp/src/python/sh.cpp:69-82), computed on the device.
+
+    Raises:
+        ValueError: If lmax is above 20, odd without full, or does not match sh.
+    """
+    series = _series(sh)
+    _check_lmax(lmax, full, series.shape[0])
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    s = torch.from_numpy(series).to(dev)
+    angles = torch.tensor([float(theta), float(phi)], dtype=torch.float64, device=dev)
+    out = torch.empty(6, dtype=torch.float64, device=dev)
+    _lib.check(_lib.lib().lar_sh_derivatives(_lib.ptr(s), 1, series.shape[0], lmax, int(bool(full)),
+                                             _lib.ptr(angles), ctypes.c_void_p(angles.data_ptr() + 8),
+                                             _lib.ptr(out), _stream(torch)))
+    return tuple(float(x) for x in out.cpu().numpy())
+
+
+def climb(sh, lmax: int, start, max_iters: int = 50, tol: float = 1e-4, max_step: float = 0.2,
+          full: bool = False) -> tuple[np.ndarray, float]:
+    """Climbs from start to the peak whose basin it lies in (cpp/src/python/sh.cpp:84-108),
+    on the device: the peak's direction (3,) and amplitude, both NaN if the climb does not
+    converge within max_iters.
+
+    Raises:
+        ValueError: If lmax is above 20, odd without full, or does not match sh, or max_iters
+            is negative.
+    """
+    series = _series(sh)
+    _check_lmax(lmax, full, series.shape[0])
+    if max_iters < 0:
+        raise ValueError("max_iters must be at least 0")
+    st = np.asarray(start, dtype=np.float64).reshape(-1)
+    if st.shape != (3,):
+        raise ValueError(f"start must hold three numbers, got {st.shape[0]}")
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    s = torch.from_numpy(series).to(dev)
+    d_start = torch.from_numpy(np.ascontiguousarray(st)).to(dev)
+    dirs = torch.empty(3, dtype=torch.float64, device=dev)
+    amps = torch.empty(1, dtype=torch.float64, device=dev)
+    _lib.check(_lib.lib().lar_climb(_lib.ptr(s), 1, series.shape[0], lmax, int(bool(full)), _lib.ptr(d_start),
+                                    int(max_iters), float(tol), float(max_step), _lib.ptr(dirs), _lib.ptr(amps),
+                                    _stream(torch)))
+    return dirs.cpu().numpy(), float(amps.cpu().numpy()[0])
+
+
+class PeakSphere(_Handle):
+    """A sphere for the peak search on the device: unit vertices (nv, 3) and the 6 neighbours of
+    each (nv, 6), copied (the reference copies its sphere per call, cpp/src/python/sh.cpp:130-147).
+
+    Raises:
+        ValueError: If a neighbour index is outside the sphere.
+    """
+
+    _destroy = "lar_peak_sphere_destroy"
+
+    def __init__(self, vertices, neighbours) -> None:
+        super().__init__()
+        v = np.ascontiguousarray(vertices, dtype=np.float64)
+        nb = np.ascontiguousarray(neighbours, dtype=np.int64)
+        self.nv = v.shape[0]
+        _lib.check(_lib.lib().lar_peak_sphere_create(_lib.ptr(v), _lib.ptr(nb), self.nv,
+                                                     ctypes.byref(self._handle)))
+
+    @classmethod
+    def cached(cls, vertices: np.ndarray, neighbours: np.ndarray) -> "PeakSphere":
+        return _designs.get(_digest(vertices, neighbours, extra=b"peak-sphere"), lambda: cls(vertices, neighbours))
+
+
+def find_peaks_device(sphere: PeakSphere, coeffs, lmax: int, full: bool, on_sphere, n_peaks: int,
+                      relative_threshold: float, threshold: float):
+    """The peaks of device series (n, C) from their device amplitudes on the sphere (n, nv):
+    directions (n, n_peaks, 3) and amplitudes (n, n_peaks), new device tensors."""
+    torch = _torch()
+    n = coeffs.shape[0]
+    if coeffs.dim() != 2 or on_sphere.dim() != 2 or (n and (coeffs.stride(1) != 1 or on_sphere.stride(1) != 1)):
+        raise ValueError("coeffs and on_sphere must be 2D tensors with unit-stride rows")
+    if on_sphere.shape[0] != n or on_sphere.shape[1] != sphere.nv:
+        raise ValueError(f"on_sphere {tuple(on_sphere.shape)} does not have {n} voxels x {sphere.nv} vertices")
+    _check_lmax(lmax, full, coeffs.shape[1])
+    dirs = torch.empty((n, n_peaks, 3), dtype=torch.float64, device=coeffs.device)
+    amps = torch.empty((n, n_peaks), dtype=torch.float64, device=coeffs.device)
+    if n:
+        _lib.check(_lib.lib().lar_find_peaks(
+            sphere.handle, _lib.ptr(coeffs), n, _row_stride(coeffs), lmax, int(bool(full)), _lib.ptr(on_sphere),
+            _row_stride(on_sphere), int(n_peaks), float(relative_threshold), float(threshold), _lib.ptr(dirs),
+            _lib.ptr(amps), _stream(torch)))
+    return dirs, amps
+
+
+def _shape(a: np.ndarray) -> str:
+    return "(" + ", ".join(str(x) for x in a.shape) + ")"
+
+
+def peaks_chunk(coeffs, lmax: int, on_sphere, vertices, neighbours, n_peaks: int, relative_threshold: float,
+                threshold: float, n_threads: int, full: bool = False) -> tuple[np.ndarray, np.ndarray]:
+    """Finds the peaks of every voxel of a chunk (cpp/src/python/sh.cpp:112-198), on the device.
+
+    coeffs is (n, C) in the tournier basis, with all degrees if full. on_sphere (n, V) holds the
+    amplitudes at the vertices (V, 3), and neighbours (V, 6) the 6 neighbours of each vertex.
+    Returns directions (n, n_peaks, 3) and amplitudes (n, n_peaks), largest first, with z >= 0
+    unless full, and NaN where a voxel has fewer peaks.
+
+    Raises:
+        TypeError: If an array does not have the dtype the reference binds (float64; neighbours
+            int64).
+        ValueError: If lmax is above 20, odd without full or does not match C, the shapes do
+            not match, a neighbour is outside the sphere, n_peaks or n_threads is 0.
+    """
+    coeffs = _array(coeffs, "coeffs", 2)
+    on_sphere = _array(on_sphere, "on_sphere", 2)
+    for name, a, dtype in (("vertices", vertices, np.float64), ("neighbours", neighbours, np.int64)):
+        if not isinstance(a, np.ndarray) or a.dtype != dtype:
+            got = type(a).__name__ if not isinstance(a, np.ndarray) else str(a.dtype)
+            raise TypeError(f"{name} must be a {np.dtype(dtype)} numpy array, got {got}")
+        if a.ndim != 2:
+            raise ValueError(f"{name} must have 2 dimensions, got shape {a.shape}")
+    _check_lmax(lmax, full, coeffs.shape[1])
+    nv = vertices.shape[0]
+    if (vertices.shape[1] != 3 or neighbours.shape[0] != nv or neighbours.shape[1] != 6
+            or on_sphere.shape[0] != coeffs.shape[0] or on_sphere.shape[1] != nv):
+        raise ValueError(f"shapes do not match: coeffs {_shape(coeffs)}, on_sphere {_shape(on_sphere)}, "
+                         f"vertices {_shape(vertices)}, neighbours {_shape(neighbours)}")
+    if nv and (neighbours.min() < 0 or neighbours.max() >= nv):
+        raise ValueError("a neighbour index is outside the sphere")
+    if n_peaks < 1:
+        raise ValueError("n_peaks must be at least 1")
+    _require_threads(n_threads)
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    sphere = PeakSphere.cached(np.ascontiguousarray(vertices), np.ascontiguousarray(neighbours))
+    c = torch.from_numpy(coeffs).to(dev)
+    o = torch.from_numpy(on_sphere).to(dev)
+    dirs, amps = find_peaks_device(sphere, c, lmax, full, o, n_peaks, relative_threshold, threshold)
+    return dirs.cpu().numpy(), amps.cpu().numpy()
 
 
 # ---- launch accounting (benchmarks) ------------------------------------------------------

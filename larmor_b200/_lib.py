@@ -46,6 +46,11 @@ SIGNATURES: dict[str, tuple] = {
     "lar_sh_projector_create": (_i32, [_p, _i64, _i64, _p]),
     "lar_sh_projector_destroy": (None, [_p]),
     "lar_project_sh": (_i32, [_p, _p, _i64, _i64, _i32, _p, _i64, _p]),
+    "lar_peak_sphere_create": (_i32, [_p, _p, _i64, _p]),
+    "lar_peak_sphere_destroy": (None, [_p]),
+    "lar_sh_derivatives": (_i32, [_p, _i64, _i64, _i32, _i32, _p, _p, _p, _p]),
+    "lar_climb": (_i32, [_p, _i64, _i64, _i32, _i32, _p, _i32, _f64, _f64, _p, _p, _p]),
+    "lar_find_peaks": (_i32, [_p, _p, _i64, _i64, _i32, _i32, _p, _i64, _i32, _f64, _f64, _p, _p, _p]),
     "lar_fit_log_signal_noalloc": (_i32, [_p, _i64, _i64, _p, _i64, _p, _i64, _i32, _i64, _f64, _p, _p, _p]),
 }
 

@@ -42,6 +42,7 @@ const std::map<std::string, int64_t> kSettings = {
     {"lsi.ctas_per_sm", 32},        // CTAs per SM of the LSI
     {"sd.nnls.ctas_per_sm", 32},    // CTAs per SM of the ridge NNLS
     {"sd.fractions.ctas_per_sm", 32},  // CTAs per SM of the fraction kernels
+    {"peaks.ctas_per_sm", 32},      // CTAs per SM of the peak search
 };
 }  // namespace
 

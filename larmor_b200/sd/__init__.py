@@ -4,6 +4,8 @@ from larmor_b200.sd.method import SDMethod
 from larmor_b200.sd.model import SDFit, SDModel
 from larmor_b200.sd.solvers import L2NNLS
 from larmor_b200.sd.msmt_csd import MSMTCSDModel
+from larmor_b200.sd.peaks import Peaks, find_peaks
 from larmor_b200.sd.rf import AnisotropicRF, IsotropicRF, ZonalSHRF
 
-__all__ = ["AnisotropicRF", "IsotropicRF", "L2NNLS", "MSMTCSDModel", "SDFit", "SDMethod", "SDModel", "ZonalSHRF"]
+__all__ = ["AnisotropicRF", "IsotropicRF", "L2NNLS", "MSMTCSDModel", "Peaks", "SDFit", "SDMethod", "SDModel",
+           "ZonalSHRF", "find_peaks"]

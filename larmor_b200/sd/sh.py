@@ -74,7 +74,8 @@ def sh_layout(num_coeffs: int) -> tuple[int, bool]:
     lmax = math.isqrt(num_coeffs) - 1
     if num_coeffs >= 1 and (lmax + 1) ** 2 == num_coeffs:
         return lmax, True
-    raise ValueError(f"{num_coeffs} SH coefficients fit no layout")
+    raise ValueError(f"{num_coeffs} SH coefficients fit no layout: a symmetric FOD has (lmax + 1)(lmax + 2) / 2 "
+                     "(1, 6, 15, 28, 45, ...), an asymmetric one (lmax + 1)^2 (4, 9, 16, 25, ...).")
 
 
 def _perm_sign(lmax: int, full: bool, basis: str):

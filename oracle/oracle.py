@@ -11,6 +11,9 @@ Each function mirrors the reference call it restates:
     nnls               larmor._core.lsqnonneg        cpp/src/sd/nnls.cpp:332
     ridge_nnls         FodSolver.l2nnls + fit_single_tissue  cpp/src/sd/solver.cpp:422
     fit_multi_tissue   larmor._core.fit_multi_tissue cpp/src/python/sd.cpp:310
+    sh_derivatives     larmor._core.sh_derivatives   cpp/src/python/sh.cpp:69
+    climb              larmor._core.climb            cpp/src/python/sh.cpp:84
+    peaks_chunk        larmor._core.peaks_chunk      cpp/src/python/sh.cpp:112
 """
 
 from __future__ import annotations
@@ -178,3 +181,43 @@ def fit_multi_tissue(signals, weights, lr, hr, lr_ridge=0.0, hr_ridge=0.1, tol_x
 def median(values) -> float:
     values = _c64(values)
     return float(lib().oracle_median(_p(values), _i64(len(values))))
+
+
+# ---- FOD peaks (peaks.cpp) ---------------------------------------------------------------
+
+
+def sh_derivatives(sh, lmax, theta, phi, full=False) -> tuple[float, ...]:
+    """larmor._core.sh_derivatives (cpp/src/python/sh.cpp:69-82)."""
+    sh = _c64(sh)
+    out = np.empty(6)
+    lib().oracle_sh_derivatives(_p(sh), _i64(lmax), int(full), _dbl(theta), _dbl(phi), _p(out))
+    return tuple(float(x) for x in out)
+
+
+def climb(sh, lmax, start, max_iters=50, tol=1e-4, max_step=0.2, full=False):
+    """larmor._core.climb (cpp/src/python/sh.cpp:84-108): (direction (3,), amplitude), NaN when
+    the climb does not stop within max_iters."""
+    sh = _c64(sh)
+    start = _c64(start)
+    d = np.empty(3)
+    a = np.empty(1)
+    lib().oracle_climb(_p(sh), _i64(lmax), int(full), _p(start), _i64(max_iters), _dbl(tol), _dbl(max_step),
+                       _p(d), _p(a))
+    return d, float(a[0])
+
+
+def peaks_chunk(coeffs, lmax, on_sphere, vertices, neighbours, n_peaks, relative_threshold, threshold,
+                n_threads=1, full=False):
+    """larmor._core.peaks_chunk (cpp/src/python/sh.cpp:112-176): directions (n, n_peaks, 3) and
+    amplitudes (n, n_peaks). The arguments are assumed valid."""
+    coeffs = _c64(coeffs)
+    on_sphere = _c64(on_sphere)
+    vertices = _c64(vertices)
+    neighbours = np.ascontiguousarray(neighbours, dtype=np.int64)
+    n = coeffs.shape[0]
+    dirs = np.empty((n, n_peaks, 3))
+    amps = np.empty((n, n_peaks))
+    lib().oracle_peaks_chunk(_p(coeffs), _i64(n), _i64(coeffs.shape[1]), _i64(lmax), int(full), _p(on_sphere),
+                             _p(vertices), _p(neighbours), _i64(len(vertices)), _i64(n_peaks),
+                             _dbl(relative_threshold), _dbl(threshold), _i64(n_threads), _p(dirs), _p(amps))
+    return dirs, amps

@@ -33,6 +33,11 @@ def msmt_fixture():
 
 
 @pytest.fixture(scope="session")
+def peaks_fixture():
+    return dict(np.load(GOLDEN / "peaks.npz"))
+
+
+@pytest.fixture(scope="session")
 def oracle():
     from oracle import oracle as o
 

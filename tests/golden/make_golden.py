@@ -24,6 +24,10 @@ What the fixtures hold, all from the reference's own code and data:
   shell weights and the SH projection matrices of sd/model.py:_to_sh.
 - msmt.npz: the forward and constraint matrices and ridge of MSMT-CSD (sd/msmt.py) for the
   responses of tests/data/msmt on a seeded three-shell table, as tests/sd/test_msmt.py builds them.
+- peaks.npz: the FOD block of the reference's peak tests with MRtrix sh2peaks' peaks of it, the
+  642-vertex icosphere of find_peaks and the outputs of the reference's numpy peak oracle
+  (tests/sd/reference_peaks.py) on the cases of tests/sd/test_peaks_compiled.py; the icosphere
+  is also written to larmor_b200/data/icosphere642.npz, where the package reads it.
 - dirs300.npy: the reference's 300 FOD directions (src/larmor/data/dir300.txt), a table the
   SD models must share exactly; also written to larmor_b200/data/dirs300.npy, where the
   package reads it.
@@ -85,6 +89,90 @@ def _install_stubs() -> None:
     skimage.morphology = morphology
     sys.modules["skimage"] = skimage
     sys.modules["skimage.morphology"] = morphology
+
+
+def _peaks_fixture(reference: Path) -> None:
+    """peaks.npz: the FOD block of the reference's peak tests (tests/data/peaks/fod.mif, 8x8x8,
+    lmax 8) with MRtrix sh2peaks' peaks of it (peaks_ref.mif), the 642-vertex icosphere and the
+    block's amplitudes on it (src/larmor/sd/peaks.py:_build_icosphere, _get_amplitudes), and the
+    outputs of the reference's numpy peak oracle (tests/sd/reference_peaks.py) on the cases of
+    tests/sd/test_peaks_compiled.py: derivatives at random and polar angles, climbs from random
+    starts on the block and on random series, climbs under other settings, and the peak search
+    of every voxel under three threshold settings."""
+    sys.path.insert(0, str(reference / "tests" / "sd"))
+    import reference_peaks as rp
+
+    from larmor.io import load_volume
+    from larmor.sd.peaks import _build_icosphere, _get_amplitudes
+    from larmor.sd.sh import get_sh_indices
+
+    data = reference / "tests" / "data" / "peaks"
+    fod = load_volume(data / "fod.mif")
+    fod.to_closest_canonical()
+    block = np.ascontiguousarray(fod.as_float(dtype=np.float64).reshape(-1, fod.data.shape[-1]))
+    ref = load_volume(data / "peaks_ref.mif")
+    ref.to_closest_canonical()
+    mrtrix = ref.as_float(dtype=np.float64).reshape(len(block), -1)
+    vertices, neighbours = _build_icosphere()
+    on_sphere = _get_amplitudes(block, 8, full=False)
+    out = dict(fod_block=block, mrtrix_peaks=mrtrix, vertices=vertices,
+               neighbours=neighbours.astype(np.int64), on_sphere=on_sphere)
+
+    def random_sh(lmax, seed):
+        return np.random.default_rng(seed).normal(size=len(get_sh_indices(lmax)[0]))
+
+    def random_starts(n, seed):
+        st = np.random.default_rng(seed).normal(size=(n, 3))
+        return st / np.linalg.norm(st, axis=1, keepdims=True)
+
+    # Derivatives: lmax 0..20, three random series each, at random angles and at the poles.
+    for lmax in range(0, 21, 2):
+        rng = np.random.default_rng(lmax)
+        theta = np.concatenate([rng.uniform(0, np.pi, 40), [0.0, 1e-6, 5e-5, 2e-4, np.pi - 1e-6, np.pi]])
+        phi = rng.uniform(-np.pi, np.pi, len(theta))
+        shs = np.array([random_sh(lmax, seed) for seed in range(3)])
+        vals = np.array([[rp.derivatives(sh, lmax, float(t), float(q)) for t, q in zip(theta, phi)] for sh in shs])
+        out[f"deriv_l{lmax}_sh"], out[f"deriv_l{lmax}_theta"], out[f"deriv_l{lmax}_phi"] = shs, theta, phi
+        out[f"deriv_l{lmax}_values"] = vals
+
+    def climbs(shs, lmax, starts, **settings):
+        dirs = np.empty((len(shs), len(starts), 3))
+        amps = np.empty((len(shs), len(starts)))
+        for i, sh in enumerate(shs):
+            for j, st in enumerate(starts):
+                dirs[i, j], amps[i, j] = rp.climb(sh, lmax, st, **settings)
+        return dirs, amps
+
+    # Climbs from random starts on 20 voxels of the block, and on random series.
+    voxels = np.random.default_rng(0).choice(len(block), 20, replace=False)
+    starts = random_starts(20, 1)
+    out["climb_block_voxels"], out["climb_block_starts"] = voxels, starts
+    out["climb_block_dirs"], out["climb_block_amps"] = climbs(block[voxels], 8, starts)
+    for lmax in (2, 8, 16, 20):
+        shs = np.array([random_sh(lmax, seed) for seed in range(4)])
+        st = random_starts(15, lmax)
+        out[f"climb_l{lmax}_sh"], out[f"climb_l{lmax}_starts"] = shs, st
+        out[f"climb_l{lmax}_dirs"], out[f"climb_l{lmax}_amps"] = climbs(shs, lmax, st)
+    # Other settings: one capped step, a smaller cap, too few iterations, no tolerance.
+    settings = [dict(tol=1.0), dict(tol=1.0, max_step=0.05), dict(max_iters=3), dict(tol=0.0)]
+    starts = random_starts(10, 2)
+    rows = np.arange(0, len(block), 37)
+    out["climb_settings_voxels"], out["climb_settings_starts"] = rows, starts
+    for k, st in enumerate(settings):
+        out[f"climb_settings{k}_dirs"], out[f"climb_settings{k}_amps"] = climbs(block[rows], 8, starts, **st)
+    out["climb_settings"] = np.array([[st.get("max_iters", 50), st.get("tol", 1e-4), st.get("max_step", 0.2)]
+                                      for st in settings])
+    # The peak search of every voxel.
+    for k, (num, rel, thr) in enumerate([(3, 0.1, 0.0), (2, 0.3, 0.2), (6, 0.0, 0.0)]):
+        res = [rp.pep(block[i], 8, on_sphere[i], vertices, neighbours, num, rel, thr) for i in range(len(block))]
+        out[f"pep{k}_dirs"] = np.array([r[0] for r in res])
+        out[f"pep{k}_amps"] = np.array([r[1] for r in res])
+    out["pep_settings"] = np.array([[3, 0.1, 0.0], [2, 0.3, 0.2], [6, 0.0, 0.0]])
+    np.savez_compressed(OUT / "peaks.npz", **out)
+    # The icosphere ships with the package too: find_peaks' start vertices, whose order is the
+    # order in which climbs are merged.
+    np.savez_compressed(OUT.parents[1] / "larmor_b200" / "data" / "icosphere642.npz", vertices=vertices,
+                        neighbours=neighbours.astype(np.int64))
 
 
 def main(reference: Path) -> None:
@@ -226,6 +314,7 @@ def main(reference: Path) -> None:
         bvals=tgtab.bvals, bvecs=tgtab.bvecs, shells=shells,
         wm_coefficients=rfs_msmt[0].coefficients, gm_coefficients=rfs_msmt[1].coefficients,
         csf_coefficients=rfs_msmt[2].coefficients)
+    _peaks_fixture(reference)
     np.save(OUT / "dirs300.npy", np.asarray(DIRS_300, dtype=np.float64))
     # The same table ships with the package: the SD models' FOD directions.
     np.save(OUT.parents[1] / "larmor_b200" / "data" / "dirs300.npy", np.asarray(DIRS_300, dtype=np.float64))
