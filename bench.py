@@ -597,7 +597,8 @@ class PeaksWorkload:
     coefficient."""
 
     name = "peaks_lmax8_110x110x70"
-    kernels = ("project_sh_kernel", "peaks_kernel")
+    kernels = ("project_sh_kernel", "peak_count_kernel", "scan_blocks_kernel", "scan_sums_kernel", "peak_fill_kernel",
+               "climb_pool_kernel", "peak_merge_kernel")
     has_fp32 = False
     unit = "voxel peak searches/s"
 
@@ -652,10 +653,33 @@ class PeaksWorkload:
         self.d_dirs, self.d_amps = _core.find_peaks_device(self.sphere, self.d_coeffs, 8, False, on_sphere, 3, 0.1,
                                                            0.0)
 
+    def climbs(self) -> int:
+        """The climbs of one step: the local maxima with a positive amplitude of every voxel's
+        amplitudes on the icosphere (counted with torch, in chunks)."""
+        from larmor_b200 import _core
+        from larmor_b200.sd.peaks import _build_icosphere
+
+        torch = self.torch
+        _, neighbours = _build_icosphere()
+        nb = torch.from_numpy(neighbours).to(self.d_coeffs.device)
+        total = 0
+        for start in range(0, self.v, 16384):
+            amp = _core.project_sh_device(self.projector, self.d_coeffs[start:start + 16384], exact_integral=False)
+            is_max = (amp > 0) & (amp[:, nb] <= amp[:, :, None]).all(dim=2)
+            total += int(is_max.sum().item())
+        return total
+
     def kernel_bytes(self) -> dict:
-        """Algorithmic DRAM bytes of one step: 45 coefficients in and 642 amplitudes out for the
-        projection; the coefficients, the amplitudes and 12 outputs for the search."""
-        return {"project_sh_kernel": self.v * 8 * (45 + 642), "peaks_kernel": self.v * 8 * (45 + 642 + 12)}
+        """Algorithmic DRAM bytes of one step: the projection reads 45 coefficients and writes
+        642 amplitudes; the count and the fill read the amplitudes (the fill writes an 8-byte
+        start per climb); the pool reads a start and writes a 32-byte result per climb, and reads
+        each voxel's 45 coefficients (shared by its climbs);
+        the merge reads the results and writes 12 outputs."""
+        c = self.climbs()
+        return {"project_sh_kernel": self.v * 8 * (45 + 642), "peak_count_kernel": self.v * (8 * 642 + 4),
+                "scan_blocks_kernel": self.v * 12, "scan_sums_kernel": 0,
+                "peak_fill_kernel": self.v * 8 * 642 + 8 * c,
+                "climb_pool_kernel": self.v * 8 * 45 + c * (8 + 32), "peak_merge_kernel": c * 32 + self.v * (12 * 8 + 12)}
 
     def step_e2e(self):
         self.d_coeffs.copy_(self.h_coeffs, non_blocking=True)

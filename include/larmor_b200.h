@@ -266,8 +266,9 @@ int lar_climb(const double* coeffs, int64_t n, int64_t ldc, int lmax, int full, 
  * n voxels' series (row stride ldc) from their amplitudes on the sphere's vertices (on_sphere,
  * row stride lds >= nv), largest first, into directions (n, n_peaks, 3) and amplitudes
  * (n, n_peaks), NaN where a voxel has fewer; symmetric series' peaks turned to z >= 0. n_peaks
- * >= 1. All device arrays except the sphere. Allocates a stream-ordered workspace of 128 nv
- * bytes per resident warp. */
+ * >= 1, n < 2^31. All device arrays except the sphere. Waits for its stream once, to size the
+ * list of the chunk's climbs; allocates stream-ordered workspaces of 20 bytes per voxel and 40
+ * bytes per climb (one per local maximum of a voxel's amplitudes). */
 int lar_find_peaks(lar_peak_sphere sphere, const double* coeffs, int64_t n, int64_t ldc, int lmax, int full,
                    const double* on_sphere, int64_t lds, int n_peaks, double relative_threshold, double threshold,
                    double* directions, double* amplitudes, void* stream);
