@@ -189,6 +189,109 @@ class DtiWorkload:
         return done, time.perf_counter() - t0, f"whole volume ({self.v} voxels) repeated for ~{budget_s:.0f} s"
 
 
+class DtiModelWorkload:
+    """Config 1 through the model API: DTIModel(fit_method="wls").fit(volume, gtab, mask) on the
+    64x64x40 volume (79,912 mask voxels), from the raw float32 volume to the maps. The device
+    stages the inputs: the mask voxels' samples, S0 with its neighbourhood repair, the
+    per-voxel floors (lar_stage_dwi); then the fused fit and maps. value: staging + fit with the
+    raw volume resident; e2e: the whole model call, host volume in, host maps out; host_staging:
+    the same call with the inputs prepared on the host (numpy) instead."""
+
+    name = "dti_model_wlls_64x64x40"
+    kernels = ("stage_gather_kernel", "stage_index_kernel", "stage_repair_kernel", "stage_floor_kernel",
+               "fit_dti_maps_kernel")
+    has_fp32 = False
+
+    def __init__(self, seed: int) -> None:
+        from larmor_b200.synthetic import dti_volume
+
+        self.w = dti_volume(seed=seed)
+        self.mask = self.w.mask
+        self.v = int(self.mask.sum())
+        self.config = {"workload": self.name, "grid": [64, 64, 40], "voxels": self.v, "measurements": 31,
+                       "fit": "wls", "api": "DTIModel.fit (model level, raw volume in)",
+                       "l2": "flushed (256 MiB write) before each step"}
+
+    def subset(self, n: int) -> None:
+        flat = np.flatnonzero(self.mask)
+        keep = np.zeros(self.mask.size, dtype=bool)
+        keep[flat[:n]] = True
+        self.mask = keep.reshape(self.mask.shape)
+        self.v = int(self.mask.sum())
+        self.config["voxels"] = self.v
+
+    def device_setup(self, torch, dev):
+        from larmor_b200 import _core
+        from larmor_b200.dwi.dti import dti_design
+        from larmor_b200.dwi.inputs import upload_volume
+
+        self.torch = torch
+        self.raw = upload_volume(self.w.volume)
+        self.handle = _core.LogDesign.cached(dti_design(self.w.gtab), np.zeros((0, 7)))
+        self.d_maps = torch.empty((16, self.v), dtype=torch.float32, device=dev)
+        self.d_npd = torch.empty((self.v,), dtype=torch.uint8, device=dev)
+        self.h2d_bytes = self.w.volume.data.nbytes + 8 * self.v
+        self.d2h_bytes = 16 * 4 * self.v + self.v
+
+    def step_device(self, precision=0):
+        from larmor_b200 import _core
+        from larmor_b200.dwi.inputs import stage_dwi
+
+        staged = stage_dwi(self.w.volume, self.w.gtab, self.mask, raw=self.raw)
+        _core.fit_dti_maps_device(self.handle, staged.signals, staged.floor, True, self.d_maps, self.d_npd)
+
+    def kernel_bytes(self) -> dict:
+        """Algorithmic DRAM bytes of one step: the gather reads 31 float32 samples and writes 31
+        float32 signals, the raw S0, a state byte, the row maximum and a finite byte per voxel;
+        the index map write and the repair read 4 + 8 bytes per voxel; the floors 8 + 8; the fit
+        reads the signals and the floor and writes 16 float32 maps and a byte."""
+        v = self.v
+        return {"stage_gather_kernel": v * (31 * 4 * 2 + 8 + 1 + 8 + 1 + 8), "stage_index_kernel": v * 12,
+                "stage_repair_kernel": v * (8 + 1 + 8 + 8), "stage_floor_kernel": v * 24,
+                "fit_dti_maps_kernel": v * (4 * 31 + 8 + 16 * 4 + 1)}
+
+    def step_e2e(self):
+        from larmor_b200.dwi import DTIModel
+
+        DTIModel(fit_method="wls").fit(self.w.volume, self.w.gtab, self.mask)
+
+    def extra(self, timed) -> dict:
+        """The model call with the host (numpy) preparation of the inputs, timed the same way."""
+        from larmor_b200.dwi.dti import dti_design, fit_dti_signals
+        from larmor_b200.dwi.inputs import estimate_s0, largest_finite_signal, masked_signals, sample_floors
+        from larmor_b200.dwi.mask import unmask
+
+        design = dti_design(self.w.gtab)
+
+        def host_staged():
+            s0 = estimate_s0(self.w.volume, self.w.gtab, self.mask)[self.mask]
+            signals = masked_signals(self.w.volume, np.nonzero(self.mask))
+            largest = None if (np.isfinite(s0) & (s0 > 0)).all() else largest_finite_signal(signals)
+            maps, npd = fit_dti_signals(design, signals, sample_floors(s0, largest, len(signals)), True)
+            unmask(maps[6], self.mask)
+
+        ms = timed(host_staged)
+        return {"host_staging": {"value": self.v / (ms / 1e3), "unit": "voxel fits/s", "ms_per_step": ms,
+                                 "what": "the same DTIModel call with S0, the gather and the floors on the host"}}
+
+    def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
+        from larmor_b200.dwi.dti import dti_design
+        from oracle import oracle as o
+        from oracle import staging
+
+        design = dti_design(self.w.gtab)
+        vol = self.w.volume
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget_s:
+            st = staging.stage(vol.data, vol.slope, vol.intercept, self.w.gtab.b0_mask, self.mask)
+            sig = st["signals"].astype(np.float64)
+            log_s = np.log(np.where((sig > 0) & np.isfinite(sig), sig, st["floor"][:, None]))
+            o.fit_log_signal(design, None, log_s, True, n_threads=threads)
+            done += self.v
+        return done, time.perf_counter() - t0, (f"whole volume ({self.v} voxels): the oracle's staging (numpy) and "
+                                                f"FP64 fit, repeated for ~{budget_s:.0f} s")
+
+
 class DkiWorkload:
     """Config 2: constrained DKI WLLS on the 96x96x60 volume (199,768 voxels, 6 b0 + 2 x 64)."""
 
@@ -703,7 +806,7 @@ class PeaksWorkload:
 
 
 WORKLOADS = {"dti": DtiWorkload, "dki": DkiWorkload, "mfod": MfodWorkload, "msmt": MsmtWorkload,
-             "batch": BatchWorkload, "peaks": PeaksWorkload}
+             "batch": BatchWorkload, "peaks": PeaksWorkload, "dti_model": DtiModelWorkload}
 
 
 
@@ -1011,6 +1114,14 @@ def main() -> int:
         "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
+    if hasattr(wl, "extra"):
+        def timed_host(step):
+            for _ in range(args.warmup):
+                step()
+            barrier()
+            return max_over_ranks(timed(step, args.steps)) / args.steps
+
+        line.update(wl.extra(timed_host))
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:

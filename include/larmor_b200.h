@@ -46,6 +46,16 @@ extern "C" {
 #define LAR_FP64 0
 #define LAR_FP32 1
 
+/* Sample types of a raw volume for lar_stage_dwi. */
+#define LAR_DTYPE_F32 0
+#define LAR_DTYPE_F64 1
+#define LAR_DTYPE_I16 2
+#define LAR_DTYPE_U16 3
+#define LAR_DTYPE_I8 4
+#define LAR_DTYPE_U8 5
+#define LAR_DTYPE_I32 6
+#define LAR_DTYPE_U32 7
+
 /* Message of the last failed call on this host thread ("" if none). */
 const char* lar_last_error(void);
 
@@ -231,6 +241,34 @@ void lar_sh_projector_destroy(lar_sh_projector projector);
  * with exact_integral the l = 0 coefficient is the amplitudes' sum / sqrt(4 pi) instead. */
 int lar_project_sh(lar_sh_projector projector, const double* amplitudes, int64_t v, int64_t lda,
                    int exact_integral, double* out, int64_t ldo, void* stream);
+
+/* ---- Device input staging ------------------------------------------------------------- */
+
+/* The inputs of a voxelwise fit from a raw DWI volume on the device, replacing the host steps of
+ * src/larmor/dwi/inputs.py. volume is (nx, ny, nz, n) C-ordered samples of type dtype
+ * (LAR_DTYPE_*), the stored values of Volume.data; voxels (v) the flat grid indices
+ * ((x ny + y) nz + z) of the mask voxels, increasing (np.nonzero order); is_b0 (n) host flags of
+ * the table's b0s. Writes, all device arrays:
+ *   signals (v, n) float32: the samples converted to float32, then scaled by slope and intercept
+ *       in float32 unless that is the identity (Volume.as_float / signal_rows,
+ *       src/larmor/types/volume.py:116-123, src/larmor/dwi/inputs.py:137-172);
+ *   s0 (v): estimate_s0 (src/larmor/dwi/inputs.py:78-134): the mean b0, and for a mask voxel whose
+ *       mean b0 is at or below its mean diffusion-weighted sample, the mean S0 of the plausible mask
+ *       voxels within 3x3x3, else 5x5x5, NaN when there is none. Required with b0s; untouched
+ *       without;
+ *   finite (v): 1 where every sample of the row is finite;
+ *   floor (v) (may be NULL): floor_bad_samples' value for the row (src/larmor/dwi/inputs.py:
+ *       227-252): 1e-3 S0 where S0 is finite and positive, else 1e-3 times largest;
+ *   largest (1) (may be NULL): largest_finite_signal (src/larmor/dwi/inputs.py:212-224).
+ * Allocates a stream-ordered workspace of 17 bytes per mask voxel and 4 per grid voxel. */
+int lar_stage_dwi(const void* volume, int dtype, int64_t nx, int64_t ny, int64_t nz, int64_t n, double slope,
+                  double intercept, const int64_t* voxels, int64_t v, const uint8_t* is_b0, float* signals, double* s0,
+                  uint8_t* finite, double* floor, double* largest, void* stream);
+
+/* The SD models' S0-normalised signals (src/larmor/sd/model.py:184-200): normalised (v, n) =
+ * min(signals / s0, 1) in FP64, finite (v) = 1 where every quotient is finite. Device arrays. */
+int lar_normalise_signals(const float* signals, const double* s0, int64_t v, int64_t n, double* normalised,
+                          uint8_t* finite, void* stream);
 
 /* ---- FOD peaks ------------------------------------------------------------------------ */
 

@@ -54,6 +54,13 @@ def _array(a, name: str, ndim: int, dtype=np.float64) -> np.ndarray:
     return a
 
 
+def _on_device(torch, a, dev):
+    """A C-contiguous device tensor of a host array, or the device tensor itself."""
+    if isinstance(a, np.ndarray):
+        return torch.from_numpy(a).to(dev)
+    return a.contiguous()
+
+
 def _require_threads(n_threads: int) -> None:
     if n_threads < 1:
         raise ValueError("n_threads must be at least 1")
@@ -386,14 +393,15 @@ def fit_multi_tissue(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, 
 
 def _fit_multi_tissue_on_device(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol,
                                 final_tol_x):
-    """fit_multi_tissue of checked host arrays, the results left on the device (torch tensors)."""
+    """fit_multi_tissue of checked host arrays (or a float64 device tensor), the results left on
+    the device (torch tensors)."""
     torch = _torch()
     dev = torch.device("cuda", torch.cuda.current_device())
     v = signals.shape[0]
     fods = torch.empty((v, hr.ca), dtype=torch.float64, device=dev)
     fractions = torch.empty((v, hr.nb + hr.ci), dtype=torch.float64, device=dev)
     if v:
-        s = torch.from_numpy(signals).to(dev)
+        s = _on_device(torch, signals, dev)
         fit_multi_tissue_device(s, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol, final_tol_x,
                                 fods, fractions)
     return fods, fractions
@@ -423,13 +431,14 @@ def fit_single_tissue(signals, solver: FodSolver, n_threads):
 
 
 def _fit_single_tissue_on_device(signals, solver: FodSolver):
-    """fit_single_tissue of a checked host array, the FODs left on the device (a torch tensor)."""
+    """fit_single_tissue of a checked host array (or a float64 device tensor), the FODs left on the
+    device (a torch tensor)."""
     torch = _torch()
     dev = torch.device("cuda", torch.cuda.current_device())
     v = signals.shape[0]
     fods = torch.empty((v, solver.n_dirs), dtype=torch.float64, device=dev)
     if v:
-        s = torch.from_numpy(signals).to(dev)
+        s = _on_device(torch, signals, dev)
         _lib.check(_lib.lib().lar_fit_single_tissue(_lib.ptr(s), v, solver.handle, _lib.ptr(fods), None,
                                                     _stream(torch)))
     return fods

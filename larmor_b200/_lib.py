@@ -46,6 +46,8 @@ SIGNATURES: dict[str, tuple] = {
     "lar_sh_projector_create": (_i32, [_p, _i64, _i64, _p]),
     "lar_sh_projector_destroy": (None, [_p]),
     "lar_project_sh": (_i32, [_p, _p, _i64, _i64, _i32, _p, _i64, _p]),
+    "lar_stage_dwi": (_i32, [_p, _i32, _i64, _i64, _i64, _i64, _f64, _f64, _p, _i64, _p, _p, _p, _p, _p, _p, _p]),
+    "lar_normalise_signals": (_i32, [_p, _p, _i64, _i64, _p, _p, _p]),
     "lar_peak_sphere_create": (_i32, [_p, _p, _i64, _p]),
     "lar_peak_sphere_destroy": (None, [_p]),
     "lar_sh_derivatives": (_i32, [_p, _i64, _i64, _i32, _i32, _p, _p, _p, _p]),
@@ -56,6 +58,8 @@ SIGNATURES: dict[str, tuple] = {
 
 LAR_OK, LAR_ERR_INVALID, LAR_ERR_CUDA, LAR_ERR_MEMORY = 0, 1, 2, 3
 LAR_FP64, LAR_FP32 = 0, 1
+# Sample types of lar_stage_dwi, by numpy dtype.
+LAR_DTYPES = {"float32": 0, "float64": 1, "int16": 2, "uint16": 3, "int8": 4, "uint8": 5, "int32": 6, "uint32": 7}
 
 _lib: ctypes.CDLL | None = None
 

@@ -20,10 +20,7 @@ from larmor_b200.dwi.dti import LOG_SIGNAL_TOL, MAX_REWEIGHTINGS, PRECISIONS
 from larmor_b200.dwi.inputs import (
     as_mask,
     check_dwi,
-    estimate_s0,
-    largest_finite_signal,
-    masked_signals,
-    sample_floors,
+    stage_dwi,
 )
 from larmor_b200.dwi.mask import unmask
 from larmor_b200.types import GradientTable, Volume
@@ -149,20 +146,21 @@ class DKIModel:
         mask = as_mask(volume, mask)
         fitted = mask.copy()
         is_b0 = gtab.b0_mask
-        s0 = None
-        if is_b0.any():
-            s0 = estimate_s0(volume, gtab, mask)[mask]
-            usable = np.isfinite(s0) & (s0 > 0)
+        # The raw volume goes to the device once; S0, the float32 signals and the floors are
+        # staged there (stage_dwi). Without b0s every voxel is fitted and floored from the
+        # largest finite signal.
+        staged = stage_dwi(volume, gtab, mask)
+        signals, s0, floor = staged.signals, staged.s0, staged.floor
+        if s0 is not None:
+            torch = _core._torch()
+            usable = (torch.isfinite(s0) & (s0 > 0)).cpu().numpy()
             if not usable.all():
                 LarmorLogger.warning(
                     "%d mask voxels have no usable S0 (no plausible b0 in them or near them); "
                     "they are not fitted and come out as 0.", int((~usable).sum()))
+                keep = torch.from_numpy(np.flatnonzero(usable)).to(s0.device)
+                signals, s0, floor = signals[keep], s0[keep], floor[keep]
             fitted[mask] = usable
-            s0 = s0[usable]
-        voxels = np.nonzero(fitted)
-        signals = masked_signals(volume, voxels)
-        largest = largest_finite_signal(signals) if s0 is None else None
-        floor = sample_floors(s0, largest, len(signals))
         g = dki_constraints(gtab) if self.constrained else np.zeros((0, design.shape[1]))
         maps, npd, broke = fit_dki_signals(design, g, signals, s0, floor, is_b0,
                                            self.fit_method == "wls", PRECISIONS[self.precision])
@@ -180,7 +178,8 @@ class DKIModel:
 
 
 def fit_dki_signals(design, g, signals, s0, floor, is_b0, weighted, precision=_lib.LAR_FP64):
-    """Fits float32 signals (v, N) on the device; returns maps (36, v), npd (v,), broke (v,)."""
+    """Fits float32 signals (v, N) on the device (host arrays, or device tensors for signals, s0
+    and floor); returns maps (36, v), npd (v,), broke (v,)."""
     torch = _core._torch()
     dev = torch.device("cuda", torch.cuda.current_device())
     handle = _core.LogDesign.cached(design, g)
@@ -190,10 +189,15 @@ def fit_dki_signals(design, g, signals, s0, floor, is_b0, weighted, precision=_l
     broke = torch.empty((v,), dtype=torch.uint8, device=dev)
     params = torch.empty((v, 22), dtype=torch.float64, device=dev)
     if v:
-        s = torch.from_numpy(np.ascontiguousarray(signals, dtype=np.float32)).to(dev)
-        f = torch.from_numpy(np.ascontiguousarray(floor, dtype=np.float64)).to(dev)
+        def dev_array(a, dtype):
+            if a is None or not isinstance(a, np.ndarray):
+                return None if a is None else a.contiguous()
+            return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype)).to(dev)
+
+        s = dev_array(signals, np.float32)
+        f = dev_array(floor, np.float64)
         b0 = torch.from_numpy(np.ascontiguousarray(is_b0, dtype=np.uint8)).to(dev)
-        s0d = None if s0 is None else torch.from_numpy(np.ascontiguousarray(s0, dtype=np.float64)).to(dev)
+        s0d = dev_array(s0, np.float64)
         _lib.check(_lib.lib().lar_fit_dki_maps(
             handle.handle, _lib.ptr(s), _lib.ptr(s0d), _lib.ptr(f), _lib.ptr(b0), v, int(weighted),
             MAX_REWEIGHTINGS, LOG_SIGNAL_TOL, int(precision), _lib.ptr(maps), _lib.ptr(npd),

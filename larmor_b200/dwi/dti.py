@@ -1,8 +1,9 @@
 """Diffusion tensor imaging (DTI) on the GPU, with the API of src/larmor/dwi/dti.py.
 
 `DTIModel(fit_method=...).fit(volume, gtab, mask)` returns the same `DTIFit` maps as the
-reference. The host prepares the inputs (mask, S0, per-voxel sample floor) and gathers the
-masked float32 signals once; one fused sm_100a kernel then floors and logs the samples, fits
+reference. The raw volume goes to the device once; the staging kernels there scale the mask
+voxels' samples, estimate S0 and the per-voxel sample floor (stage_dwi); one fused sm_100a
+kernel then floors and logs the samples, fits
 the tensor (OLS, or WLS iterated to a predicted-log change of 1e-6 or 20 reweightings), and
 writes the 16 maps of compute_dti_metrics (src/larmor/dwi/dti.py:170-235).
 """
@@ -16,14 +17,7 @@ import numpy as np
 from larmor_b200 import _core, _lib
 from larmor_b200._log import LarmorLogger
 from larmor_b200._threads import n_threads
-from larmor_b200.dwi.inputs import (
-    as_mask,
-    check_dwi,
-    estimate_s0,
-    largest_finite_signal,
-    masked_signals,
-    sample_floors,
-)
+from larmor_b200.dwi.inputs import as_mask, check_dwi, stage_dwi
 from larmor_b200.dwi.mask import unmask
 from larmor_b200.types import GradientTable, Volume
 
@@ -90,14 +84,8 @@ class DTIModel:
             raise ValueError("DTIModel.fit needs a mask on the volume's grid.")
         mask = as_mask(volume, mask)
         design = dti_design(gtab)
-        s0 = estimate_s0(volume, gtab, mask)[mask] if gtab.b0_mask.any() else None
-        voxels = np.nonzero(mask)
-        signals = masked_signals(volume, voxels)
-        largest = None
-        if s0 is None or not (np.isfinite(s0) & (s0 > 0)).all():
-            largest = largest_finite_signal(signals)
-        floor = sample_floors(s0, largest, len(signals))
-        maps, npd = fit_dti_signals(design, signals, floor, self.fit_method == "wls",
+        staged = stage_dwi(volume, gtab, mask)
+        maps, npd = fit_dti_signals(design, staged.signals, staged.floor, self.fit_method == "wls",
                                     PRECISIONS[self.precision])
         if npd.any():
             LarmorLogger.warning(
@@ -117,7 +105,8 @@ class DTIModel:
 
 def fit_dti_signals(design: np.ndarray, signals: np.ndarray, floor: np.ndarray, weighted: bool,
                     precision: int = _lib.LAR_FP64) -> tuple[np.ndarray, np.ndarray]:
-    """Fits float32 signals (v, N) on the device; returns maps (16, v) and npd (v,)."""
+    """Fits float32 signals (v, N) (a host array or a device tensor) with per-voxel floors (v,)
+    on the device; returns maps (16, v) and npd (v,)."""
     torch = _core._torch()
     dev = torch.device("cuda", torch.cuda.current_device())
     handle = _core.LogDesign.cached(design, np.zeros((0, design.shape[1])))
@@ -125,8 +114,10 @@ def fit_dti_signals(design: np.ndarray, signals: np.ndarray, floor: np.ndarray, 
     maps = torch.empty((16, v), dtype=torch.float32, device=dev)
     npd = torch.empty((v,), dtype=torch.uint8, device=dev)
     if v:
-        s = torch.from_numpy(np.ascontiguousarray(signals, dtype=np.float32)).to(dev)
-        f = torch.from_numpy(np.ascontiguousarray(floor, dtype=np.float64)).to(dev)
+        s = _core._on_device(torch, np.ascontiguousarray(signals, dtype=np.float32), dev) \
+            if isinstance(signals, np.ndarray) else signals.contiguous()
+        f = _core._on_device(torch, np.ascontiguousarray(floor, dtype=np.float64), dev) \
+            if isinstance(floor, np.ndarray) else floor.contiguous()
         _core.fit_dti_maps_device(handle, s, f, weighted, maps, npd, max_iter=MAX_REWEIGHTINGS,
                                   tol=LOG_SIGNAL_TOL, precision=precision)
     return maps.cpu().numpy(), npd.cpu().numpy().astype(bool)

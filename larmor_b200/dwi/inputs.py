@@ -7,6 +7,8 @@ and the gather of the masked voxels' float32 signals.
 
 from __future__ import annotations
 
+from dataclasses import dataclass
+
 import numpy as np
 from scipy.ndimage import uniform_filter
 
@@ -95,6 +97,92 @@ def sample_floors(s0: np.ndarray | None, largest: float | None, v: int) -> np.nd
         usable = np.isfinite(s0) & (s0 > 0)
         floor[usable] = SIGNAL_FLOOR * s0[usable]
     return floor
+
+
+@dataclass
+class StagedDwi:
+    """The inputs of a fit, staged on the device from the raw volume (lar_stage_dwi).
+
+    voxels are the mask voxels' indices (np.nonzero of the mask); signals (v, N) float32, s0 (v)
+    float64 or None for a table without b0, finite (v) uint8 (every sample finite) and floor (v)
+    float64 are device tensors; largest is a (1,) device tensor."""
+
+    voxels: tuple[np.ndarray, ...]
+    signals: object
+    s0: object
+    finite: object
+    floor: object
+    largest: object
+
+
+def upload_volume(volume: Volume):
+    """The raw samples of a 4D volume on the device as bytes, with their lar_stage_dwi type code.
+
+    Raises:
+        ValueError: If the sample type is not one of the integer or float types the staging reads.
+    """
+    from larmor_b200 import _core, _lib
+
+    data = np.ascontiguousarray(volume.data)
+    code = _lib.LAR_DTYPES.get(str(data.dtype))
+    if code is None:
+        raise ValueError(f"The volume's samples are {data.dtype}; the device staging reads "
+                         f"{', '.join(_lib.LAR_DTYPES)}.")
+    torch = _core._torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    raw = torch.empty(data.nbytes, dtype=torch.uint8, device=dev)
+    raw.copy_(torch.from_numpy(data.reshape(-1).view(np.uint8)))
+    return raw, code
+
+
+def stage_dwi(volume: Volume, gtab: GradientTable, mask: np.ndarray, *, raw=None) -> StagedDwi:
+    """Stages the mask voxels' samples on the device: the raw volume is copied to the device once
+    and the reference's host preparation -- the float32 scaling, estimate_s0 with its
+    neighbourhood repair, largest_finite_signal and the per-voxel floor -- runs there
+    (lar_stage_dwi; src/larmor/dwi/inputs.py:78-252). raw: the volume already on the device, as
+    upload_volume returns it.
+
+    Raises:
+        ValueError: If the volume and table do not match, or the volume's sample type is not
+            one of the integer or float types the staging reads.
+    """
+    from larmor_b200 import _core, _lib
+
+    check_dwi(volume, gtab)
+    if raw is None:
+        raw = upload_volume(volume)
+    data, code = raw
+    torch = _core._torch()
+    dev = data.device
+    nx, ny, nz, n = volume.data.shape
+    flat = np.flatnonzero(mask).astype(np.int64)
+    v = len(flat)
+    d_voxels = torch.from_numpy(flat).to(dev)
+    is_b0 = np.ascontiguousarray(gtab.b0_mask, dtype=np.uint8)
+    signals = torch.empty((v, n), dtype=torch.float32, device=dev)
+    s0 = torch.empty((v,), dtype=torch.float64, device=dev) if is_b0.any() else None
+    finite = torch.empty((v,), dtype=torch.uint8, device=dev)
+    floor = torch.empty((v,), dtype=torch.float64, device=dev)
+    largest = torch.empty((1,), dtype=torch.float64, device=dev)
+    _lib.check(_lib.lib().lar_stage_dwi(
+        _lib.ptr(data), code, nx, ny, nz, n, float(volume.slope), float(volume.intercept), _lib.ptr(d_voxels), v,
+        is_b0.ctypes.data, _lib.ptr(signals), _lib.ptr(s0), _lib.ptr(finite), _lib.ptr(floor), _lib.ptr(largest),
+        _core._stream(torch)))
+    return StagedDwi(np.nonzero(mask), signals, s0, finite, floor, largest)
+
+
+def normalise_signals(signals, s0):
+    """min(signals / s0, 1) in FP64 on the device and whether each row is finite
+    (lar_normalise_signals; the SD models' normalisation, src/larmor/sd/model.py:184-200)."""
+    from larmor_b200 import _core, _lib
+
+    torch = _core._torch()
+    v, n = signals.shape
+    out = torch.empty((v, n), dtype=torch.float64, device=signals.device)
+    finite = torch.empty((v,), dtype=torch.uint8, device=signals.device)
+    _lib.check(_lib.lib().lar_normalise_signals(_lib.ptr(signals), _lib.ptr(s0), v, n, _lib.ptr(out),
+                                                _lib.ptr(finite), _core._stream(torch)))
+    return out, finite
 
 
 def mean_b0(volume: Volume, gtab: GradientTable) -> np.ndarray:

@@ -25,7 +25,7 @@ class SDFit:
 
 from larmor_b200._log import LarmorLogger  # noqa: E402
 from larmor_b200._threads import n_threads  # noqa: E402
-from larmor_b200.dwi.inputs import as_mask, check_dwi, estimate_s0, masked_signals  # noqa: E402
+from larmor_b200.dwi.inputs import as_mask, check_dwi, normalise_signals, stage_dwi  # noqa: E402
 from larmor_b200.dwi.mask import unmask  # noqa: E402
 from larmor_b200.sd.kernel import Kernel, order_rfs  # noqa: E402
 from larmor_b200.sd.rf import IsotropicRF  # noqa: E402
@@ -129,16 +129,19 @@ class SDModel:
             LarmorLogger.warning(f"lmax {self.lmax} needs more directions than the highest shell has, "
                                  f"lowering to {lmax}")
         mask = np.ones(volume.data.shape[:-1], dtype=bool) if mask is None else as_mask(volume, mask)
-        s0 = estimate_s0(volume, gtab, mask)[mask]
-        voxels = np.nonzero(mask)
-        signals = masked_signals(volume, voxels).astype(np.float64)
-        normalised = signals / s0[:, np.newaxis]
-        finite = np.isfinite(normalised).all(axis=1)
+        if not gtab.b0_mask.any():
+            raise ValueError(f"No b0 volume: no b-value is at or below {gtab.b0_threshold} s/mm^2.")
+        # The raw volume goes to the device once: S0 and the signals normalised by it, capped at 1
+        # (diffusion weighting only lowers the signal: a value above S0 is noise), are staged
+        # there (stage_dwi, normalise_signals).
+        staged = stage_dwi(volume, gtab, mask)
+        normalised, finite = normalise_signals(staged.signals, staged.s0)
+        finite = finite.cpu().numpy().astype(bool)
         if not finite.all():
             LarmorLogger.warning(f"{int((~finite).sum())} voxels have a NaN or infinite signal or no S0; "
                                  "their FODs and fractions are NaN.")
-        # Diffusion weighting only lowers the signal: a value above S0 is noise.
-        normalised = np.minimum(normalised[finite], 1.0)
+            keep = _core._torch().from_numpy(np.flatnonzero(finite)).to(normalised.device)
+            normalised = normalised[keep]
         amplitudes, fitted_fractions, hr = self._fit_normalised(normalised, gtab, solver, threads)
         n_coeffs = (lmax + 1) * (lmax + 2) // 2
         projector = sh_projector(lmax, self.basis)

@@ -13,7 +13,7 @@ import numpy as np
 from larmor_b200 import _core
 from larmor_b200._log import LarmorLogger
 from larmor_b200._threads import n_threads
-from larmor_b200.dwi.inputs import as_mask, check_dwi, masked_signals
+from larmor_b200.dwi.inputs import as_mask, check_dwi, stage_dwi
 from larmor_b200.dwi.mask import unmask
 from larmor_b200.sd.model import SDFit
 from larmor_b200.sd.msmt import prepare_msmt
@@ -71,14 +71,22 @@ class MSMTCSDModel:
         sizes = [(d + 1) * (d + 2) // 2 for d in lmaxes]
         starts = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(int)
         design = prepare_msmt(rfs, lmaxes, gtab.bvals, gtab.bvecs, self.directions)
-        voxels = np.nonzero(mask)
-        signals = masked_signals(volume, voxels)
-        finite = np.isfinite(signals).all(axis=1)
+        # The raw volume goes to the device once and the mask voxels' signals are staged there.
+        staged = stage_dwi(volume, gtab, mask)
+        finite = staged.finite.cpu().numpy().astype(bool)
         if not finite.all():
             LarmorLogger.warning(f"{int((~finite).sum())} voxels have a NaN or infinite signal; their "
                                  "FODs and fractions are NaN.")
-        fitted, converged = _core.fit_lsi(np.ascontiguousarray(signals[finite], dtype=np.float64),
-                                          design, threads)
+        torch = _core._torch()
+        signals = staged.signals
+        if not finite.all():
+            signals = signals[torch.from_numpy(np.flatnonzero(finite)).to(signals.device)]
+        signals = signals.to(torch.float64).contiguous()
+        x = torch.empty((signals.shape[0], design.n), dtype=torch.float64, device=signals.device)
+        conv = torch.empty((signals.shape[0],), dtype=torch.uint8, device=signals.device)
+        if signals.shape[0]:
+            _core.fit_lsi_device(design, signals, x, conv)
+        fitted, converged = x.cpu().numpy(), conv.cpu().numpy().astype(bool)
         if not converged.all():
             LarmorLogger.warning(f"The constrained fit of {int((~converged).sum())} voxels stopped at "
                                  "its iteration limit; their FODs may be slightly negative.")

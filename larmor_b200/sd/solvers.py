@@ -58,16 +58,21 @@ def fit_single_tissue(signals, solver, n_threads):
 
 
 def fit_single_tissue_on_device(signals, solver):
-    """fit_single_tissue with the FODs left on the device (a torch tensor)."""
-    return _core._fit_single_tissue_on_device(_core._array(np.ascontiguousarray(signals, dtype=np.float64),
-                                                           "signals", 2), solver)
+    """fit_single_tissue with the FODs left on the device (a torch tensor); signals a host array
+    or a float64 device tensor."""
+    if isinstance(signals, np.ndarray):
+        signals = _core._array(np.ascontiguousarray(signals, dtype=np.float64), "signals", 2)
+    return _core._fit_single_tissue_on_device(signals, solver)
 
 
 def fit_multi_tissue_on_device(signals, lr_kernel: Kernel, hr_kernel: Kernel, lr_solver, hr_solver,
                                fraction_tol: float = FRACTION_TOL):
-    """fit_multi_tissue with the amplitudes and fractions left on the device (torch tensors)."""
+    """fit_multi_tissue with the amplitudes and fractions left on the device (torch tensors);
+    signals a host array or a float64 device tensor."""
+    if isinstance(signals, np.ndarray):
+        signals = np.ascontiguousarray(signals, dtype=np.float64)
     return _core._fit_multi_tissue_on_device(
-        np.ascontiguousarray(signals, dtype=np.float64), np.ascontiguousarray(lr_kernel.weights, dtype=np.float64),
+        signals, np.ascontiguousarray(lr_kernel.weights, dtype=np.float64),
         _deconv_kernel(lr_kernel), lr_solver, _deconv_kernel(hr_kernel), hr_solver, MAX_ROUNDS, fraction_tol,
         FINAL_FRACTION_TOL_X)
 

@@ -28,6 +28,10 @@ What the fixtures hold, all from the reference's own code and data:
   642-vertex icosphere of find_peaks and the outputs of the reference's numpy peak oracle
   (tests/sd/reference_peaks.py) on the cases of tests/sd/test_peaks_compiled.py; the icosphere
   is also written to larmor_b200/data/icosphere642.npz, where the package reads it.
+- staging.npz: the reference's input preparation (estimate_s0, signal_rows,
+  largest_finite_signal, floor_bad_samples) on three seeded volumes: int16 with slope and
+  intercept and dark-b0 voxels to repair, float32 with non-finite and non-positive samples, and a
+  table of b0s only.
 - dirs300.npy: the reference's 300 FOD directions (src/larmor/data/dir300.txt), a table the
   SD models must share exactly; also written to larmor_b200/data/dirs300.npy, where the
   package reads it.
@@ -89,6 +93,73 @@ def _install_stubs() -> None:
     skimage.morphology = morphology
     sys.modules["skimage"] = skimage
     sys.modules["skimage.morphology"] = morphology
+
+
+def _staging_fixture() -> None:
+    """staging.npz: the reference's input preparation (src/larmor/dwi/inputs.py) on three seeded
+    volumes: estimate_s0 over the grid, signal_rows of the mask voxels, largest_finite_signal and
+    floor_bad_samples with the mask voxels' S0.
+    - "int": int16 samples scaled by slope 0.25 and intercept 3. It has dark-b0 voxels that repair
+      from the 3x3x3 neighbourhood, from the 5x5x5 one, or not at all, some on the grid's edge.
+    - "float": float32 samples with NaN, infinite, zero and negative values.
+    - "b0only": float64 samples rounded by the float32 conversion, with a table of b0s only, whose
+      S0 is the plain mean b0."""
+    from larmor.dwi.inputs import estimate_s0, floor_bad_samples, largest_finite_signal, signal_rows
+    from larmor.types import GradientTable, Volume
+
+    rng = np.random.default_rng(11)
+    shape = (14, 12, 10)
+    out = {}
+
+    def table(n_b0, n_dw):
+        dirs = rng.normal(size=(n_dw, 3))
+        dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+        bvals = np.concatenate([np.zeros(n_b0), np.full(n_dw, 1000.0)])
+        bvecs = np.vstack([np.zeros((n_b0, 3)), dirs]) if n_dw else np.zeros((n_b0, 3))
+        return GradientTable(bvals, bvecs)
+
+    grid = np.stack(np.meshgrid(*[np.linspace(-1, 1, k) for k in shape], indexing="ij"), axis=-1)
+    mask = (grid**2).sum(axis=-1) <= 1.15
+    mask[0, 5:8, 3:6] = True  # mask voxels on the grid's edge
+
+    def decays(n_b0, n_dw):
+        s0 = rng.uniform(800, 1200, size=shape)
+        adc = rng.uniform(0.5e-3, 2.5e-3, size=shape + (n_dw,))
+        dw = s0[..., None] * np.exp(-1000.0 * adc)
+        return np.concatenate([np.repeat(s0[..., None], n_b0, axis=-1), dw], axis=-1)
+
+    # "int": dark b0s: one isolated voxel, a 3x3x3 block (its centre repairs from 5x5x5), a
+    # 7x7x7 block (its centre has no plausible voxel within 5x5x5), edge voxels.
+    sig = decays(3, 24)
+    dark = np.zeros(shape, dtype=bool)
+    dark[7, 6, 5] = True
+    dark[3:6, 2:5, 2:5] = True
+    dark[4:11, 3:10, 2:9] |= True
+    dark[0, 6, 4] = True
+    sig[dark, :3] = rng.uniform(0, 60, size=(int(dark.sum()), 3))
+    raw = np.rint((sig - 3.0) / 0.25).astype(np.int16)
+    volumes = {"int": (Volume(raw, np.eye(4), slope=0.25, intercept=3.0), table(3, 24))}
+    # "float": float32 with NaN, inf, zero and negative samples.
+    sig = decays(2, 30).astype(np.float32)
+    bad = rng.random(sig.shape) < 0.01
+    sig[bad] = rng.choice(np.array([np.nan, np.inf, -np.inf, 0.0, -5.0], dtype=np.float32), size=int(bad.sum()))
+    sig[2, 3:5, 2:8, :2] = 1.0  # dark b0s with finite samples
+    volumes["float"] = (Volume(sig, np.eye(4)), table(2, 30))
+    # "b0only": a table of b0s only.
+    sig = decays(4, 0) * (1 + 1e-9 * rng.normal(size=shape + (4,)))
+    volumes["b0only"] = (Volume(sig.astype(np.float64), np.eye(4)), table(4, 0))
+    for name, (vol, gtab) in volumes.items():
+        voxels = np.nonzero(mask)
+        s0 = estimate_s0(vol, gtab, mask)
+        rows = signal_rows(vol, voxels, slice(None))
+        largest = largest_finite_signal(vol, voxels)
+        floored = rows.copy()
+        floor_bad_samples(floored, s0[mask], largest=largest)
+        out.update({f"{name}_data": vol.data, f"{name}_slope": vol.slope, f"{name}_intercept": vol.intercept,
+                    f"{name}_bvals": gtab.bvals, f"{name}_is_b0": gtab.b0_mask, f"{name}_s0": s0,
+                    f"{name}_signals": rows, f"{name}_largest": largest, f"{name}_floored": floored})
+    out["mask"] = mask
+    np.savez_compressed(OUT / "staging.npz", **out)
 
 
 def _peaks_fixture(reference: Path) -> None:
@@ -315,6 +386,7 @@ def main(reference: Path) -> None:
         wm_coefficients=rfs_msmt[0].coefficients, gm_coefficients=rfs_msmt[1].coefficients,
         csf_coefficients=rfs_msmt[2].coefficients)
     _peaks_fixture(reference)
+    _staging_fixture()
     np.save(OUT / "dirs300.npy", np.asarray(DIRS_300, dtype=np.float64))
     # The same table ships with the package: the SD models' FOD directions.
     np.save(OUT.parents[1] / "larmor_b200" / "data" / "dirs300.npy", np.asarray(DIRS_300, dtype=np.float64))
