@@ -691,6 +691,77 @@ class BatchWorkload:
                                                 f"(fits only), repeated for ~{budget_s:.0f} s")
 
 
+class CsdWorkload(_SdWorkloadBase):
+    """Single-shell CSD (CSDModel's solve, src/larmor/sd/csd.py) of the config-3 volume's highest
+    shell: b = 3000, 90 directions, 500,040 voxels, lmax 8 (45 coefficients), 300 constraint
+    directions, the default solver (up to 50 constrained solves per voxel), with the synthetic
+    white matter response of the volume's fibres. The signals are the shell's samples clamped at
+    0, as the model passes them."""
+
+    name = "csd_lmax8_b3000_110x110x70"
+    kernels = ("csd_kernel",)
+    has_fp32 = False
+
+    def __init__(self, seed: int) -> None:
+        from larmor_b200.sd.csd_solver import CSDSolver, csd_problem, csd_shell
+        from larmor_b200.synthetic import mfod_responses
+
+        self._volume(seed)
+        bval = csd_shell(self.gtab)
+        on_shell = self.gtab.shell_index == int(np.argmin(np.abs(self.gtab.shells - bval)))
+        self.problem = csd_problem(self.gtab.bvecs[on_shell], mfod_responses()[0].shell_coefficients(bval), 8,
+                                   CSDSolver())
+        self.shell = np.ascontiguousarray(np.maximum(self.signals[:, on_shell], 0.0))
+        self.config = {"workload": self.name, "grid": [110, 110, 70], "voxels": self.v, "shell": bval,
+                       "measurements": int(on_shell.sum()), "coefficients": 45, "constraints": 300,
+                       "max_iter": 50, "l2": "flushed (256 MiB write) before each step"}
+
+    def subset(self, n: int) -> None:
+        super().subset(n)
+        self.shell = self.shell[:n]
+
+    def device_setup(self, torch, dev):
+        from larmor_b200 import _core
+
+        self.torch = torch
+        p = self.problem
+        self.handle = _core.CsdProblem.cached(p.initial, p.forward, p.constraint, p.norm_weight, p.threshold,
+                                              p.max_iter)
+        self.d_shell = torch.from_numpy(self.shell).to(dev)
+        self.h_shell = torch.from_numpy(self.shell).pin_memory()
+        self.h_fods = torch.empty((self.v, 45), dtype=torch.float64).pin_memory()
+        self.h_conv = torch.empty((self.v,), dtype=torch.uint8).pin_memory()
+        self.h2d_bytes = self.shell.nbytes
+        self.d2h_bytes = self.v * (45 * 8 + 1)
+
+    def step_device(self, precision=0):
+        from larmor_b200 import _core
+
+        self.d_fods, self.d_conv = _core.fit_csd_device(self.handle, self.d_shell)
+
+    def kernel_bytes(self) -> dict:
+        """Algorithmic DRAM bytes of one step: 90 signals in, 45 coefficients and a flag out."""
+        return {"csd_kernel": self.v * (8 * self.shell.shape[1] + 8 * 45 + 1)}
+
+    def step_e2e(self):
+        self.d_shell.copy_(self.h_shell, non_blocking=True)
+        self.step_device()
+        self.h_fods.copy_(self.d_fods, non_blocking=True)
+        self.h_conv.copy_(self.d_conv, non_blocking=True)
+
+    def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
+        from oracle import oracle as o
+
+        p = self.problem
+        n = min(self.v, 4096)
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget_s:
+            o.fit_csd(self.shell[:n], p.initial, p.forward, p.constraint, p.norm_weight, p.threshold, p.max_iter,
+                      n_threads=threads)
+            done += n
+        return done, time.perf_counter() - t0, f"first {n} voxels of the shell, repeated for ~{budget_s:.0f} s"
+
+
 class PeaksWorkload:
     """FOD peaks (find_peaks, src/larmor/sd/peaks.py) of lmax-8 FODs on the config-3 mask
     (110x110x70, 500,040 voxels): the amplitudes of each FOD on the 642-vertex icosphere, then
@@ -806,7 +877,7 @@ class PeaksWorkload:
 
 
 WORKLOADS = {"dti": DtiWorkload, "dki": DkiWorkload, "mfod": MfodWorkload, "msmt": MsmtWorkload,
-             "batch": BatchWorkload, "peaks": PeaksWorkload, "dti_model": DtiModelWorkload}
+             "batch": BatchWorkload, "peaks": PeaksWorkload, "dti_model": DtiModelWorkload, "csd": CsdWorkload}
 
 
 

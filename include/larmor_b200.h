@@ -242,6 +242,27 @@ void lar_sh_projector_destroy(lar_sh_projector projector);
 int lar_project_sh(lar_sh_projector projector, const double* amplitudes, int64_t v, int64_t lda,
                    int exact_integral, double* out, int64_t ldo, void* stream);
 
+/* ---- Single-shell CSD ----------------------------------------------------------------- */
+
+/* The matrices of one shell's constrained spherical deconvolution, copied to the device
+ * (_core.fit_csd's problem, cpp/src/sd/csd.cpp:11-22): initial (c0, m) maps a signal to the
+ * first c0 <= c coefficients of the starting FOD, forward M (m, c), constraint C (k, c) the
+ * weighted SH basis on the constraint directions; the Gram matrix M^T M + norm_weight I is formed
+ * here. c <= 255, k <= 65535, max_iter >= 0; LAR_ERR_INVALID otherwise or when the packed
+ * system does not fit a warp's shared memory. */
+typedef struct lar_csd_s* lar_csd;
+
+int lar_csd_create(const double* initial, int64_t c0, int64_t m, const double* forward, int64_t c,
+                   const double* constraint, int64_t k, double norm_weight, double threshold, int64_t max_iter,
+                   lar_csd* out);
+
+void lar_csd_destroy(lar_csd csd);
+
+/* _core.fit_csd (cpp/src/python/sd.cpp:171-209, cpp/src/sd/csd.cpp:24-65) for v signals (v, m),
+ * device: fods (v, c) and converged (v,) (1 where the set of constrained directions repeated, or
+ * max_iter is 0), device. Signals are fitted as given (the Python layer clamps them at 0). */
+int lar_fit_csd(lar_csd csd, const double* signals, int64_t v, double* fods, uint8_t* converged, void* stream);
+
 /* ---- Device input staging ------------------------------------------------------------- */
 
 /* The inputs of a voxelwise fit from a raw DWI volume on the device, replacing the host steps of

@@ -480,6 +480,87 @@ def project_sh_device(projector: ShProjector, amplitudes, exact_integral: bool):
     return out
 
 
+# ---- single-shell CSD (cpp/src/python/sd.cpp:171-209) -----------------------------------
+
+
+class CsdProblem(_Handle):
+    """The matrices of one shell's CSD fit on the device (lar_csd_create)."""
+
+    _destroy = "lar_csd_destroy"
+
+    def __init__(self, initial, forward, constraint, norm_weight, threshold, max_iter) -> None:
+        super().__init__()
+        self.c0, self.m = initial.shape
+        self.c = forward.shape[1]
+        self.k = constraint.shape[0]
+        _lib.check(_lib.lib().lar_csd_create(_lib.ptr(initial), self.c0, self.m, _lib.ptr(forward), self.c,
+                                             _lib.ptr(constraint), self.k, float(norm_weight), float(threshold),
+                                             int(max_iter), ctypes.byref(self._handle)))
+
+    @classmethod
+    def cached(cls, initial, forward, constraint, norm_weight, threshold, max_iter) -> "CsdProblem":
+        extra = np.array([norm_weight, threshold, max_iter], dtype=np.float64).tobytes() + b"csd"
+        return _designs.get(_digest(initial, forward, constraint, extra=extra),
+                            lambda: cls(initial, forward, constraint, norm_weight, threshold, max_iter))
+
+
+def fit_csd_device(problem: CsdProblem, signals):
+    """The FODs (v, c) and converged flags (v,) of float64 device signals (v, m), left on the
+    device."""
+    torch = _torch()
+    v = signals.shape[0]
+    fods = torch.empty((v, problem.c), dtype=torch.float64, device=signals.device)
+    conv = torch.empty((v,), dtype=torch.uint8, device=signals.device)
+    if v:
+        _lib.check(_lib.lib().lar_fit_csd(problem.handle, _lib.ptr(signals), v, _lib.ptr(fods), _lib.ptr(conv),
+                                          _stream(torch)))
+    return fods, conv
+
+
+def _shape2(rows: int, cols: int) -> str:
+    return f"({rows}, {cols})"
+
+
+def fit_csd(signals, initial, forward, constraint, norm_weight, threshold, max_iter, n_threads):
+    """Fits every row of signals (n, m) by constrained spherical deconvolution
+    (cpp/src/python/sd.cpp:171-209), on the device.
+
+    initial (c0, m) gives the starting FOD's first c0 coefficients, forward (m, c) is the forward
+    model M and constraint (k, c) the weighted SH basis on the constraint directions. Each solve
+    minimises ||M f - s||^2 + norm_weight ||f||^2 plus the squared constraint rows where the FOD is
+    below threshold, until that set of rows repeats or after max_iter solves. Returns the FODs
+    (n, c) and whether each voxel's set repeated (n,).
+
+    Raises:
+        TypeError: If an array is not float64.
+        ValueError: If signals is not C-contiguous, the shapes do not match, max_iter is negative
+            or n_threads is 0.
+    """
+    signals = _array(signals, "signals", 2)
+    mats = []
+    for name, a in (("initial", initial), ("forward", forward), ("constraint", constraint)):
+        if not isinstance(a, np.ndarray) or a.dtype != np.float64:
+            got = type(a).__name__ if not isinstance(a, np.ndarray) else str(a.dtype)
+            raise TypeError(f"{name} must be a float64 numpy array, got {got}")
+        if a.ndim != 2:
+            raise ValueError(f"{name} must have 2 dimensions, got shape {a.shape}")
+        mats.append(np.ascontiguousarray(a))
+    initial, forward, constraint = mats
+    m, c = forward.shape
+    if (signals.shape[1] != m or initial.shape[1] != m or initial.shape[0] > c or constraint.shape[1] != c):
+        raise ValueError(f"shapes do not match: signals {_shape2(*signals.shape)}, initial {_shape2(*initial.shape)}, "
+                         f"forward {_shape2(m, c)}, constraint {_shape2(*constraint.shape)}")
+    if max_iter < 0:
+        raise ValueError("max_iter must be at least 0")
+    _require_threads(n_threads)
+    torch = _torch()
+    problem = CsdProblem.cached(initial, forward, constraint, norm_weight, threshold, max_iter)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    s = torch.from_numpy(signals).to(dev)
+    fods, conv = fit_csd_device(problem, s)
+    return fods.cpu().numpy(), conv.cpu().numpy().astype(bool)
+
+
 # ---- FOD peaks (cpp/src/python/sh.cpp) ---------------------------------------------------
 
 MAX_LMAX = 20

@@ -1,5 +1,7 @@
 """Spherical deconvolution on the GPU: MSMT-CSD (and mFOD), with the API of larmor.sd."""
 
+from larmor_b200.sd.csd import CSDModel
+from larmor_b200.sd.csd_solver import CSDSolver
 from larmor_b200.sd.method import SDMethod
 from larmor_b200.sd.model import SDFit, SDModel
 from larmor_b200.sd.solvers import L2NNLS
@@ -7,5 +9,5 @@ from larmor_b200.sd.msmt_csd import MSMTCSDModel
 from larmor_b200.sd.peaks import Peaks, find_peaks
 from larmor_b200.sd.rf import AnisotropicRF, IsotropicRF, ZonalSHRF
 
-__all__ = ["AnisotropicRF", "IsotropicRF", "L2NNLS", "MSMTCSDModel", "Peaks", "SDFit", "SDMethod", "SDModel",
+__all__ = ["AnisotropicRF", "CSDModel", "CSDSolver", "IsotropicRF", "L2NNLS", "MSMTCSDModel", "Peaks", "SDFit", "SDMethod", "SDModel",
            "ZonalSHRF", "find_peaks"]

@@ -14,6 +14,7 @@ Each function mirrors the reference call it restates:
     sh_derivatives     larmor._core.sh_derivatives   cpp/src/python/sh.cpp:69
     climb              larmor._core.climb            cpp/src/python/sh.cpp:84
     peaks_chunk        larmor._core.peaks_chunk      cpp/src/python/sh.cpp:112
+    fit_csd            larmor._core.fit_csd          cpp/src/python/sd.cpp:171
 """
 
 from __future__ import annotations
@@ -221,3 +222,19 @@ def peaks_chunk(coeffs, lmax, on_sphere, vertices, neighbours, n_peaks, relative
                              _p(vertices), _p(neighbours), _i64(len(vertices)), _i64(n_peaks),
                              _dbl(relative_threshold), _dbl(threshold), _i64(n_threads), _p(dirs), _p(amps))
     return dirs, amps
+
+
+# ---- single-shell CSD (csd.cpp) ------------------------------------------------------------
+
+
+def fit_csd(signals, initial, forward, constraint, norm_weight, threshold, max_iter, n_threads=1):
+    """larmor._core.fit_csd (cpp/src/python/sd.cpp:171-209): FODs (n, c) and converged (n,).
+    The arguments are assumed valid."""
+    signals, initial, forward, constraint = (_c64(a) for a in (signals, initial, forward, constraint))
+    n, c = signals.shape[0], forward.shape[1]
+    fods = np.empty((n, c))
+    conv = np.empty(n, dtype=np.uint8)
+    lib().oracle_fit_csd(_p(signals), _i64(n), _i64(signals.shape[1]), _p(initial), _i64(initial.shape[0]),
+                         _p(forward), _i64(c), _p(constraint), _i64(constraint.shape[0]), _dbl(norm_weight),
+                         _dbl(threshold), _i64(max_iter), _i64(n_threads), _p(fods), _p(conv))
+    return fods, conv.astype(bool)

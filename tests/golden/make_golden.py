@@ -32,6 +32,8 @@ What the fixtures hold, all from the reference's own code and data:
   largest_finite_signal, floor_bad_samples) on three seeded volumes: int16 with slope and
   intercept and dark-b0 voxels to repair, float32 with non-finite and non-positive samples, and a
   table of b0s only.
+- csd.npz: the matrices of single-shell CSD (csd_problem) for four settings on the 60-direction
+  shell of tests/sd/test_csd.py, and that test's synthetic voxels.
 - dirs300.npy: the reference's 300 FOD directions (src/larmor/data/dir300.txt), a table the
   SD models must share exactly; also written to larmor_b200/data/dirs300.npy, where the
   package reads it.
@@ -160,6 +162,42 @@ def _staging_fixture() -> None:
                     f"{name}_signals": rows, f"{name}_largest": largest, f"{name}_floored": floored})
     out["mask"] = mask
     np.savez_compressed(OUT / "staging.npz", **out)
+
+
+def _csd_fixture() -> None:
+    """csd.npz: the matrices of single-shell CSD the reference builds
+    (src/larmor/sd/csd_solver.py:csd_problem) on the 60-direction b=1000 shell and the white matter
+    response of tests/sd/test_csd.py (RESPONSE, _gradients), for four solver settings, and that
+    test's synthetic voxels (_voxels: one fibre, 90 and 60 degree crossings, a noisy crossing)."""
+    from larmor.sd import CSDSolver, ZonalSHRF
+    from larmor.sd.csd_solver import csd_problem
+    from larmor.types import GradientTable
+
+    response = np.array([1800.0, -700.0, 180.0, -35.0, 5.0])
+    rng = np.random.default_rng(1)
+    dirs = rng.normal(size=(60, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    gtab = GradientTable(np.r_[0.0, [1000.0] * 60], np.r_[np.zeros((1, 3)), dirs])
+    out = dict(response=response, bvals=gtab.bvals, bvecs=gtab.bvecs)
+    own = np.random.default_rng(5).normal(size=(120, 3))
+    settings = [(8, CSDSolver()), (8, CSDSolver(init_lmax=2, neg_lambda=0.5, threshold=0.1, max_iter=20)),
+                (10, CSDSolver(norm_lambda=2.0)), (6, CSDSolver(directions=own))]
+    for i, (lmax, solver) in enumerate(settings):
+        pr = csd_problem(gtab.bvecs[1:], response, lmax, solver)
+        out.update({f"p{i}_lmax": lmax, f"p{i}_initial": pr.initial, f"p{i}_forward": pr.forward,
+                    f"p{i}_constraint": pr.constraint, f"p{i}_norm_weight": pr.norm_weight,
+                    f"p{i}_threshold": pr.threshold, f"p{i}_max_iter": pr.max_iter})
+    out["p3_directions"] = own
+    rf = ZonalSHRF(bvals=np.array([1000.0]), coefficients=response[None])
+    rad90, rad60 = np.radians(90.0), np.radians(60.0)
+    fibre_sets = [np.array([[1.0, 0, 0]]), np.array([[1.0, 0, 0], [np.cos(rad90), np.sin(rad90), 0]]),
+                  np.array([[1.0, 0, 0], [np.cos(rad60), np.sin(rad60), 0]]), np.array([[1.0, 0, 0], [0, 1.0, 0]])]
+    rows = np.array([rf.signal(gtab.bvals[1:], gtab.bvecs[1:], f).mean(axis=1) for f in fibre_sets])
+    noisy = rows[3] + np.random.default_rng(2).normal(0, 40.0, rows.shape[1])
+    out["signals"] = np.vstack([rows, noisy[None]])
+    out["fibres"] = np.array([np.pad(f, ((0, 2 - len(f)), (0, 0)), constant_values=np.nan) for f in fibre_sets]
+                             + [np.array([[1.0, 0, 0], [0, 1.0, 0]])])
+    np.savez_compressed(OUT / "csd.npz", **out)
 
 
 def _peaks_fixture(reference: Path) -> None:
@@ -387,6 +425,7 @@ def main(reference: Path) -> None:
         csf_coefficients=rfs_msmt[2].coefficients)
     _peaks_fixture(reference)
     _staging_fixture()
+    _csd_fixture()
     np.save(OUT / "dirs300.npy", np.asarray(DIRS_300, dtype=np.float64))
     # The same table ships with the package: the SD models' FOD directions.
     np.save(OUT.parents[1] / "larmor_b200" / "data" / "dirs300.npy", np.asarray(DIRS_300, dtype=np.float64))
