@@ -227,6 +227,7 @@ class DtiModelWorkload:
 
         self.torch = torch
         self.raw = upload_volume(self.w.volume)
+        self.flat = torch.from_numpy(np.flatnonzero(self.mask).astype(np.int64)).to(dev)
         self.handle = _core.LogDesign.cached(dti_design(self.w.gtab), np.zeros((0, 7)))
         self.d_maps = torch.empty((16, self.v), dtype=torch.float32, device=dev)
         self.d_npd = torch.empty((self.v,), dtype=torch.uint8, device=dev)
@@ -237,7 +238,7 @@ class DtiModelWorkload:
         from larmor_b200 import _core
         from larmor_b200.dwi.inputs import stage_dwi
 
-        staged = stage_dwi(self.w.volume, self.w.gtab, self.mask, raw=self.raw)
+        staged = stage_dwi(self.w.volume, self.w.gtab, self.mask, raw=self.raw, flat=self.flat)
         _core.fit_dti_maps_device(self.handle, staged.signals, staged.floor, True, self.d_maps, self.d_npd)
 
     def kernel_bytes(self) -> dict:

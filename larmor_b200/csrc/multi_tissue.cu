@@ -1230,8 +1230,11 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
                         cuda_check(cudaGetLastError(), "ridge_nnls_half_kernel launch");
                     }
                     reset_queue();
+                    // The voxels the two-voxel kernel handed back are rare (its QR fallback): a
+                    // persistent grid of one CTA per SM takes them.
                     LaunchScope scope(lr_nnls.name, st);
-                    lr_nnls.kernel<<<blocks(lr_slots, count), kMtWarps * 32, lr_smem, st>>>(
+                    const unsigned redo_blocks = std::min<unsigned>(blocks(lr_slots, count), unsigned(sm_count()));
+                    lr_nnls.kernel<<<redo_blocks, kMtWarps * 32, lr_smem, st>>>(
                         lrs, lr_sig, P.redo, count, P.counters + 4, P.corr, c_lr, P.xlr, c_lr, P.bad, P.counters,
                         P.slots, lr_slot);
                     cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");

@@ -103,16 +103,21 @@ def sample_floors(s0: np.ndarray | None, largest: float | None, v: int) -> np.nd
 class StagedDwi:
     """The inputs of a fit, staged on the device from the raw volume (lar_stage_dwi).
 
-    voxels are the mask voxels' indices (np.nonzero of the mask); signals (v, N) float32, s0 (v)
+    mask is the voxels' mask (their order is np.nonzero's); signals (v, N) float32, s0 (v)
     float64 or None for a table without b0, finite (v) uint8 (every sample finite) and floor (v)
     float64 are device tensors; largest is a (1,) device tensor."""
 
-    voxels: tuple[np.ndarray, ...]
+    mask: np.ndarray
     signals: object
     s0: object
     finite: object
     floor: object
     largest: object
+
+    @property
+    def voxels(self) -> tuple[np.ndarray, ...]:
+        """The mask voxels' indices, np.nonzero of the mask."""
+        return np.nonzero(self.mask)
 
 
 def upload_volume(volume: Volume):
@@ -135,12 +140,13 @@ def upload_volume(volume: Volume):
     return raw, code
 
 
-def stage_dwi(volume: Volume, gtab: GradientTable, mask: np.ndarray, *, raw=None) -> StagedDwi:
+def stage_dwi(volume: Volume, gtab: GradientTable, mask: np.ndarray, *, raw=None, flat=None) -> StagedDwi:
     """Stages the mask voxels' samples on the device: the raw volume is copied to the device once
     and the reference's host preparation -- the float32 scaling, estimate_s0 with its
     neighbourhood repair, largest_finite_signal and the per-voxel floor -- runs there
     (lar_stage_dwi; src/larmor/dwi/inputs.py:78-252). raw: the volume already on the device, as
-    upload_volume returns it.
+    upload_volume returns it; flat: the mask voxels' flat grid indices already on the device
+    (int64, np.flatnonzero of the mask).
 
     Raises:
         ValueError: If the volume and table do not match, or the volume's sample type is not
@@ -155,9 +161,8 @@ def stage_dwi(volume: Volume, gtab: GradientTable, mask: np.ndarray, *, raw=None
     torch = _core._torch()
     dev = data.device
     nx, ny, nz, n = volume.data.shape
-    flat = np.flatnonzero(mask).astype(np.int64)
-    v = len(flat)
-    d_voxels = torch.from_numpy(flat).to(dev)
+    d_voxels = torch.from_numpy(np.flatnonzero(mask).astype(np.int64)).to(dev) if flat is None else flat
+    v = d_voxels.shape[0]
     is_b0 = np.ascontiguousarray(gtab.b0_mask, dtype=np.uint8)
     signals = torch.empty((v, n), dtype=torch.float32, device=dev)
     s0 = torch.empty((v,), dtype=torch.float64, device=dev) if is_b0.any() else None
@@ -168,7 +173,7 @@ def stage_dwi(volume: Volume, gtab: GradientTable, mask: np.ndarray, *, raw=None
         _lib.ptr(data), code, nx, ny, nz, n, float(volume.slope), float(volume.intercept), _lib.ptr(d_voxels), v,
         is_b0.ctypes.data, _lib.ptr(signals), _lib.ptr(s0), _lib.ptr(finite), _lib.ptr(floor), _lib.ptr(largest),
         _core._stream(torch)))
-    return StagedDwi(np.nonzero(mask), signals, s0, finite, floor, largest)
+    return StagedDwi(mask, signals, s0, finite, floor, largest)
 
 
 def normalise_signals(signals, s0):
