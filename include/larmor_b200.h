@@ -182,6 +182,14 @@ typedef struct lar_deconv_kernel_s* lar_deconv_kernel;
  * otherwise QR). A coefficient enters only when its gradient exceeds tol_x. Fails with
  * LAR_ERR_INVALID for reg < 0 or tol_x <= 0. Replaces FodSolver.l2nnls
  * (cpp/src/python/sd.cpp:89-102, cpp/src/sd/nnls.cpp:348-360). */
+/* FodSolver.drl (cpp/src/python/sd.cpp:127-145): a damped Richardson-Lucy solver
+ * (cpp/src/sd/drl.cpp:39-100) of K^T (c, m) and K^T K (c, c), host arrays copied: damping
+ * threshold nu, at most n_iter (>= 0) iterations per voxel, every amplitude started at init.
+ * c <= 320, m > 1. lar_fit_single_tissue runs it; lar_fit_multi_tissue refuses it (GRL's
+ * multi-tissue rounds with dRL are not built). */
+int lar_drl_create(const double* k_t, const double* k_t_k, int64_t c, int64_t m, double nu, int64_t n_iter,
+                   double init, lar_fod_solver* out);
+
 int lar_l2nnls_create(const double* k, int64_t m, int64_t c, double reg, double tol_x, lar_fod_solver* out);
 void lar_fod_solver_destroy(lar_fod_solver solver);
 

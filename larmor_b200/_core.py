@@ -303,7 +303,8 @@ class _Handle:
 
 class FodSolver(_Handle):
     """An FOD solver with the matrices it needs from one kernel, copied to the device
-    (cpp/src/python/sd.cpp:399-438). Only the L2NNLS method (mFOD's) is part of this package."""
+    (cpp/src/python/sd.cpp:399-438): the L2NNLS method (mFOD's) and damped Richardson-Lucy (dRL,
+    single-tissue fits only)."""
 
     _destroy = "lar_fod_solver_destroy"
 
@@ -329,8 +330,34 @@ class FodSolver(_Handle):
         return solver
 
     @staticmethod
-    def drl(*_args, **_kwargs):
-        raise NotImplementedError("the damped Richardson-Lucy solver (GRL) is not part of larmor_b200")
+    def drl(k_t, k_t_k, nu, n_iter, init) -> "FodSolver":
+        """Damped Richardson-Lucy (cpp/src/python/sd.cpp:127-145): k_t is K^T (c, m), k_t_k is
+        K^T K (c, c); amplitudes below nu have their updates damped; at most n_iter iterations
+        per voxel, every amplitude started at init. fit_single_tissue runs it on the device
+        (lar_drl_create); the multi-tissue fit does not take it (GRL's rounds are not built).
+
+        Raises:
+            TypeError: If k_t or k_t_k is not a float64 numpy array.
+            ValueError: If the shapes do not match, n_iter is negative, or the solver has more
+                than 320 directions.
+        """
+        for name, a in (("k_t", k_t), ("k_t_k", k_t_k)):
+            if not isinstance(a, np.ndarray) or a.dtype != np.float64:
+                got = type(a).__name__ if not isinstance(a, np.ndarray) else str(a.dtype)
+                raise TypeError(f"{name} must be a float64 numpy array, got {got}")
+            if a.ndim != 2:
+                raise ValueError(f"{name} must have 2 dimensions, got shape {a.shape}")
+        k_t, k_t_k = np.ascontiguousarray(k_t), np.ascontiguousarray(k_t_k)
+        c, m = k_t.shape
+        if k_t_k.shape != (c, c):
+            raise ValueError(f"shapes do not match: k_t ({c}, {m}), k_t_k ({k_t_k.shape[0]}, {k_t_k.shape[1]})")
+        if n_iter < 0:
+            raise ValueError("n_iter must be at least 0")
+        solver = FodSolver()
+        solver.n_meas, solver.n_dirs = m, c
+        _lib.check(_lib.lib().lar_drl_create(_lib.ptr(k_t), _lib.ptr(k_t_k), c, m, float(nu), int(n_iter),
+                                             float(init), ctypes.byref(solver._handle)))
+        return solver
 
     @staticmethod
     def lasso(*_args, **_kwargs):

@@ -46,6 +46,7 @@ SIGNATURES: dict[str, tuple] = {
     "lar_sh_projector_create": (_i32, [_p, _i64, _i64, _p]),
     "lar_sh_projector_destroy": (None, [_p]),
     "lar_project_sh": (_i32, [_p, _p, _i64, _i64, _i32, _p, _i64, _p]),
+    "lar_drl_create": (_i32, [_p, _p, _i64, _i64, _f64, _i64, _f64, _p]),
     "lar_csd_create": (_i32, [_p, _i64, _i64, _p, _i64, _p, _i64, _f64, _f64, _i64, _p]),
     "lar_csd_destroy": (None, [_p]),
     "lar_fit_csd": (_i32, [_p, _p, _i64, _p, _p, _p]),

@@ -44,6 +44,7 @@ const std::map<std::string, int64_t> kSettings = {
     {"sd.fractions.ctas_per_sm", 32},  // CTAs per SM of the fraction kernels
     {"peaks.ctas_per_sm", 32},      // CTAs per SM of the peak search
     {"csd.ctas_per_sm", 32},        // CTAs per SM of the CSD fit
+    {"drl.ctas_per_sm", 32},        // CTAs per SM of damped Richardson-Lucy
 };
 }  // namespace
 

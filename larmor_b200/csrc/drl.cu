@@ -1,0 +1,207 @@
+// Damped Richardson-Lucy (dRL) deconvolution on the GPU: FodSolver.drl + fit_single_tissue
+// (cpp/src/python/sd.cpp:127-145, cpp/src/sd/solver.cpp:9-12) over damped_richardson_lucy
+// (cpp/src/sd/drl.cpp:39-100). Dell'Acqua F et al., NeuroImage 49 (2010) 1446-1458.
+//
+// Each voxel starts every amplitude at `init`. An iteration computes the prediction p = K^T K f
+// and moves each amplitude to max(f (1 + u (K^T s - p) / (p + 1e-16)), 1e-6). The damping is
+// u = 1 - strength (1 - f^8 / (f^8 + nu^8)), with strength = max(1 - 4 std(s), 0). A voxel
+// stops when its amplitudes change in total by no more than 1e-4 of its largest signal value.
+//
+// Mapping: a CTA of 8 warps takes 32 voxels at a time and keeps their FODs F (32, c) and K^T s
+// (32, c) in shared memory for all their iterations. An iteration is one product F K^T K on the
+// FP64 tensor cores: mma.sync m8n8k4 over four 8-voxel row tiles and the 8-direction column
+// tiles, which the warps take round-robin. K^T K (c x c, 720 KB at c = 300) stays in L2 and
+// streams through each CTA once per iteration for its 32 voxels. The update is the epilogue,
+// on the accumulators, after a barrier, since every warp reads all of F. Each voxel's change is
+// reduced in a fixed order, so the stopping test does not depend on the schedule. Converged
+// voxels keep their FOD while the tile's others iterate.
+
+#include <algorithm>
+#include <cmath>
+
+#include <math_constants.h>
+
+#include "common.cuh"
+#include "drl.cuh"
+
+namespace lar {
+namespace {
+
+constexpr int kDrlRows = 32;   // voxels per CTA tile: four 8-row tiles
+constexpr int kDrlWarps = 8;
+constexpr int kDrlMaxCt = 5;   // column tiles per warp: c <= 8 * kDrlWarps * kDrlMaxCt = 320
+
+__device__ __forceinline__ double power_8(double x) {
+    const double x2 = x * x, x4 = x2 * x2;
+    return x4 * x4;
+}
+
+__device__ __forceinline__ void mma_f64(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const double* __restrict__ signals,
+                                                                int64_t v, double* __restrict__ fods) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double part[kDrlWarps][kDrlRows];
+    __shared__ double strength[kDrlRows], threshold[kDrlRows];
+    __shared__ int active[kDrlRows];
+    __shared__ int n_active;
+    const int c = P.c, m = P.m, cp = (c + 7) / 8 * 8, n_ct = cp / 8;
+    double* F = reinterpret_cast<double*>(smem);  // (32, cp)
+    double* KS = F + kDrlRows * cp;               // (32, cp)
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const double nu8 = power_8(P.nu);
+    for (int64_t v0 = int64_t(blockIdx.x) * kDrlRows; v0 < v; v0 += int64_t(gridDim.x) * kDrlRows) {
+        // Each voxel's damping strength (1 - 4 x the sample standard deviation, at least 0) and
+        // stopping threshold (1e-4 x its largest non-NaN signal value).
+        for (int r = warp; r < kDrlRows; r += kDrlWarps) {
+            const int64_t voxel = v0 + r;
+            if (voxel >= v) {
+                if (lane == 0) {
+                    active[r] = 0;
+                    strength[r] = threshold[r] = 0.0;
+                }
+                continue;
+            }
+            const double* s = signals + voxel * m;
+            double sum = 0.0, mx = -CUDART_INF;
+            bool any = false;
+            for (int i = lane; i < m; i += 32) {
+                sum += s[i];
+                if (!isnan(s[i])) {
+                    mx = any ? fmax(mx, s[i]) : s[i];
+                    any = true;
+                }
+            }
+            const double mean = warp_sum(sum) / m;
+            double ss = 0.0;
+            for (int i = lane; i < m; i += 32) ss += (s[i] - mean) * (s[i] - mean);
+            ss = warp_sum(ss);
+            const bool all_nan = !__any_sync(0xffffffffu, any);
+            mx = warp_max(any ? mx : -CUDART_INF);
+            if (lane == 0) {
+                strength[r] = fmax(1.0 - 4.0 * sqrt(ss / double(m - 1)), 0.0);
+                threshold[r] = 1e-4 * (all_nan ? CUDART_NAN : mx);
+                active[r] = 1;
+            }
+        }
+        // K^T s and the start.
+        for (int e = tid; e < kDrlRows * cp; e += blockDim.x) {
+            const int r = e / cp, d = e - r * cp;
+            const int64_t voxel = v0 + r;
+            const bool real = voxel < v && d < c;
+            double ks = 0.0;
+            if (real) {
+                const double* s = signals + voxel * m;
+                const double* kt = P.k_t + size_t(d) * m;
+                for (int i = 0; i < m; ++i) ks = fma(kt[i], s[i], ks);
+            }
+            KS[e] = ks;
+            F[e] = real ? P.init : 0.0;
+        }
+        __syncthreads();
+        for (int it = 0; it < P.n_iter; ++it) {
+            if (tid == 0) {
+                int a = 0;
+                for (int r = 0; r < kDrlRows; ++r) a += active[r];
+                n_active = a;
+            }
+            __syncthreads();
+            if (n_active == 0) break;
+            // The prediction K^T K f of every voxel of the tile (K^T K is symmetric: its column
+            // block is read as rows).
+            double acc[4][kDrlMaxCt][2];
+#pragma unroll
+            for (int rt = 0; rt < 4; ++rt)
+#pragma unroll
+                for (int t = 0; t < kDrlMaxCt; ++t) acc[rt][t][0] = acc[rt][t][1] = 0.0;
+            for (int k0 = 0; k0 < cp; k0 += 4) {
+                const int kk = k0 + (lane & 3);
+                double a[4];
+#pragma unroll
+                for (int rt = 0; rt < 4; ++rt) a[rt] = F[(8 * rt + (lane >> 2)) * cp + kk];
+#pragma unroll
+                for (int t = 0; t < kDrlMaxCt; ++t) {
+                    const int ct = warp + kDrlWarps * t;
+                    if (ct < n_ct) {
+                        const int col = 8 * ct + (lane >> 2);
+                        const double b = (kk < c && col < c) ? __ldg(P.gram + size_t(kk) * c + col) : 0.0;
+#pragma unroll
+                        for (int rt = 0; rt < 4; ++rt) mma_f64(acc[rt][t][0], acc[rt][t][1], a[rt], b);
+                    }
+                }
+            }
+            __syncthreads();
+            // The damped update of the still-active voxels, and each one's total change.
+            double change[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int t = 0; t < kDrlMaxCt; ++t) {
+                const int ct = warp + kDrlWarps * t;
+                if (ct >= n_ct) continue;
+#pragma unroll
+                for (int rt = 0; rt < 4; ++rt) {
+                    const int r = 8 * rt + (lane >> 2);
+                    if (!active[r]) continue;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int d = 8 * ct + 2 * (lane & 3) + h;
+                        if (d >= c) continue;
+                        const double f = F[r * cp + d], f8 = power_8(f);
+                        const double damping = 1.0 - strength[r] * (1.0 - f8 / (f8 + nu8));
+                        const double pred = acc[rt][t][h];
+                        const double ratio = (KS[r * cp + d] - pred) / (pred + 1e-16);
+                        const double updated = fmax(f * (1.0 + damping * ratio), 1e-6);
+                        F[r * cp + d] = updated;
+                        change[rt] += fabs(updated - f);
+                    }
+                }
+            }
+#pragma unroll
+            for (int rt = 0; rt < 4; ++rt) {
+                change[rt] += __shfl_xor_sync(0xffffffffu, change[rt], 1);
+                change[rt] += __shfl_xor_sync(0xffffffffu, change[rt], 2);
+                if ((lane & 3) == 0) part[warp][8 * rt + (lane >> 2)] = change[rt];
+            }
+            __syncthreads();
+            if (tid < kDrlRows && active[tid]) {
+                double total = 0.0;
+                for (int w = 0; w < kDrlWarps; ++w) total += part[w][tid];
+                if (total <= threshold[tid]) active[tid] = 0;
+            }
+            __syncthreads();
+        }
+        for (int e = tid; e < kDrlRows * cp; e += blockDim.x) {
+            const int r = e / cp, d = e - r * cp;
+            const int64_t voxel = v0 + r;
+            if (voxel < v && d < c) fods[voxel * c + d] = F[e];
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+size_t drl_smem_bytes(int c) { return 2 * size_t(kDrlRows) * size_t((c + 7) / 8 * 8) * sizeof(double); }
+
+bool drl_fits(int c) { return c >= 1 && c <= 8 * kDrlWarps * kDrlMaxCt; }
+
+void launch_drl(const DrlDev& P, const double* signals, int64_t v, double* fods, cudaStream_t st) {
+    if (v == 0) return;
+    const size_t smem = drl_smem_bytes(P.c);
+    cuda_check(cudaFuncSetAttribute(drl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+               "cudaFuncSetAttribute");
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, drl_kernel, kDrlWarps * 32, smem),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    const int64_t tiles = (v + kDrlRows - 1) / kDrlRows;
+    const int64_t blocks =
+        std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sm_count()) * ctas_per_sm(per_sm, "drl.ctas_per_sm")));
+    LaunchScope scope("drl_kernel", st);
+    drl_kernel<<<unsigned(blocks), kDrlWarps * 32, smem, st>>>(P, signals, v, fods);
+    cuda_check(cudaGetLastError(), "drl_kernel launch");
+}
+
+}  // namespace lar

@@ -33,6 +33,7 @@
 
 #include "common.cuh"
 #include "host_la.hpp"
+#include "drl.cuh"
 #include "group_nnls.cuh"
 #include "warp_chol.cuh"
 #include "warp_nnls.cuh"
@@ -1055,6 +1056,10 @@ inline void launch_correlate(const SignalDev& S, const int* list, int64_t count,
 
 // FodSolver.l2nnls (cpp/src/python/sd.cpp:89-102, cpp/src/sd/solver.cpp:464-467).
 struct lar_fod_solver_s {
+    // 0: the ridge NNLS (L2NNLS) with its design below; 1: damped Richardson-Lucy (dRL).
+    int kind = 0;
+    lar::DeviceArray<double> drl_kt, drl_gram;
+    lar::DrlDev drl{};
     lar::host::RidgeDesignHost host;
     double tol = 0.0;
     lar::DeviceArray<double> k, gram;
@@ -1118,6 +1123,8 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
                             bool device_rounds) {
     return guarded([&] {
         require(lr && hr && lr_solver && hr_solver, "kernels and solvers must not be NULL");
+        require(lr_solver->kind == 0 && hr_solver->kind == 0,
+                "the multi-tissue fit takes L2NNLS solvers: GRL (dRL solvers in the multi-tissue fit) is not built");
         require(weights != nullptr, "weights must not be NULL");
         const int64_t m = hr->m;
         require(lr->m == m && lr_solver->host.m == m && hr_solver->host.m == m,
@@ -1303,6 +1310,24 @@ int lar_fit_multi_tissue_async(const double* signals, int64_t v, const double* w
 }
 
 
+int lar_drl_create(const double* k_t, const double* k_t_k, int64_t c, int64_t m, double nu, int64_t n_iter,
+                   double init, lar_fod_solver* out) {
+    return guarded([&] {
+        require(out != nullptr, "out must not be NULL");
+        require(k_t != nullptr && k_t_k != nullptr && c > 0 && m > 1, "k_t must be a non-empty (c, m) array, m > 1");
+        require(drl_fits(int(c)), "dRL takes at most 320 directions");
+        require(n_iter >= 0, "n_iter must be at least 0");
+        auto h = std::make_unique<lar_fod_solver_s>();
+        h->kind = 1;
+        h->host.m = m;
+        h->host.c = c;
+        h->drl_kt.upload(k_t, size_t(c * m));
+        h->drl_gram.upload(k_t_k, size_t(c * c));
+        h->drl = DrlDev{h->drl_kt.ptr, h->drl_gram.ptr, int(c), int(m), int(n_iter), nu, init};
+        *out = h.release();
+    });
+}
+
 int lar_l2nnls_create(const double* k, int64_t m, int64_t c, double reg, double tol_x, lar_fod_solver* out) {
     return guarded([&] {
         require(out != nullptr, "out must not be NULL");
@@ -1365,6 +1390,12 @@ int lar_fit_single_tissue(const double* signals, int64_t v, lar_fod_solver solve
         require(v >= 0, "v must be at least 0");
         if (v == 0) return;
         require(signals && fods, "signals and fods must not be NULL");
+        if (solver->kind == 1) {
+            if (status) cuda_check(cudaMemsetAsync(status, 0, size_t(v), static_cast<cudaStream_t>(stream)),
+                                   "cudaMemsetAsync");
+            launch_drl(solver->drl, signals, v, fods, static_cast<cudaStream_t>(stream));
+            return;
+        }
         const int m = int(solver->host.m), c = int(solver->host.c);
         const RidgeDev R = solver->view();
         const NnlsLaunch nn = nnls_variant(c);

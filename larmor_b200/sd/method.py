@@ -5,7 +5,7 @@ from __future__ import annotations
 from enum import StrEnum
 
 from larmor_b200.sd.rf import IsotropicRF
-from larmor_b200.sd.solvers import FRACTION_TOL, L2NNLS
+from larmor_b200.sd.solvers import DRL, FRACTION_TOL, L2NNLS
 
 
 class SDMethod(StrEnum):
@@ -21,9 +21,7 @@ class SDMethod(StrEnum):
         raise ValueError(f"Unknown method {value!r}; valid methods are {', '.join(m.value for m in cls)}.")
 
     def default_solver(self):
-        if self is SDMethod.MFOD:
-            return L2NNLS()
-        raise NotImplementedError("GRL's damped Richardson-Lucy solver is not part of larmor_b200; use mFOD")
+        return L2NNLS() if self is SDMethod.MFOD else DRL()
 
     @property
     def inner_shell_weight(self) -> float:

@@ -91,7 +91,8 @@ def to_sh(fods: np.ndarray, lmax: int, basis: str, *, exact_integral: bool = Fal
 class SDModel:
     """Spherical deconvolution with the mFOD method (L2NNLS FODs, one per anisotropic response,
     all shells weighted equally), on the GPU; the reference's SDModel (src/larmor/sd/model.py:84).
-    GRL (damped Richardson-Lucy) is outside this package."""
+    A single-tissue fit also takes the DRL solver (damped Richardson-Lucy); the GRL method's
+    multi-tissue rounds with dRL are not built yet."""
 
     def __init__(self, rfs, *, method="mFOD", solver=None, inner_shell_weight=None, lmax: int = 8,
                  basis: str = "tournier", progress: bool = False) -> None:
@@ -117,11 +118,14 @@ class SDModel:
     def fit(self, volume, gtab, mask=None, *, n_jobs: int = -1) -> SDFit:
         """The FODs (SH coefficients in the model's basis) and fractions of every voxel of the
         mask (every voxel when None); see src/larmor/sd/model.py:171-260."""
-        from larmor_b200.sd.solvers import L2NNLS
+        from larmor_b200.sd.solvers import DRL, L2NNLS
 
         solver = self.solver if self.solver is not None else self.method.default_solver()
-        if not isinstance(solver, L2NNLS):
-            raise NotImplementedError("larmor_b200 runs the L2NNLS solver only")
+        if not isinstance(solver, (L2NNLS, DRL)):
+            raise NotImplementedError("larmor_b200 runs the L2NNLS and DRL solvers only")
+        if isinstance(solver, DRL) and self.is_multi_tissue:
+            raise NotImplementedError("GRL (the multi-tissue rounds with dRL) is not part of larmor_b200 yet; DRL "
+                                      "runs single-tissue fits")
         threads = n_threads(n_jobs)
         check_dwi(volume, gtab)
         lmax = compute_max_lmax(gtab.bvals, self.lmax)

@@ -1,4 +1,4 @@
-"""The L2NNLS FOD solver and the multi-tissue fit (src/larmor/sd/solvers.py), on the GPU."""
+"""The FOD solvers (L2NNLS, dRL) and the multi-tissue fit (src/larmor/sd/solvers.py), on the GPU."""
 
 from __future__ import annotations
 
@@ -42,6 +42,64 @@ class L2NNLS:
     def _prepare(self, kernel: Kernel, bvals: np.ndarray, stage: Stage) -> _core.FodSolver:
         reg = 0.0 if stage is Stage.LOW_RES else self.reg
         return _core.FodSolver.l2nnls(np.ascontiguousarray(kernel.w_k_aniso), reg, self.tol_x)
+
+
+# The near-zero start of a multi-tissue dRL solve (src/larmor/sd/solvers.py:21).
+MULTI_TISSUE_DRL_INIT = 1e-6
+
+
+def _rl_products(k: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """K^T and K^T K, the matrices of a Richardson-Lucy solve."""
+    return np.ascontiguousarray(k.T), np.ascontiguousarray(k.T @ k)
+
+
+def calibrate_drl_nu(kernel: Kernel, bvals: np.ndarray, target_adc: float = 0.7e-3, scale: float = 0.2,
+                     n_iter: int = 200) -> float:
+    """dRL's damping threshold nu for a kernel (src/larmor/sd/solvers.py:37-69): scale times the
+    largest FOD amplitude an undamped deconvolution with the whole kernel gives for a purely
+    isotropic tissue, exp(-b_max target_adc) on every measurement (run on the device)."""
+    signal = np.full((1, len(bvals)), np.exp(-max(bvals) * target_adc))
+    k_t, k_t_k = _rl_products(kernel.k)
+    solver = _core.FodSolver.drl(k_t, k_t_k, nu=0.0, n_iter=n_iter, init=1.0 / kernel.k.shape[1])
+    fake_fod = _core.fit_single_tissue(signal, solver, n_threads=1)
+    return float(scale * np.max(fake_fod))
+
+
+@dataclass(frozen=True, kw_only=True)
+class DRL:
+    """Damped Richardson-Lucy deconvolution, an FOD solver (src/larmor/sd/solvers.py:72-148):
+    the FOD stays non-negative, and the updates of amplitudes below nu (nu_scale times the
+    largest amplitude an undamped fit gives for an isotropic tissue of diffusivity target_adc) are
+    damped. num_iter caps a single-tissue fit's iterations and hr_num_iter the final solve of a
+    multi-tissue one. Single-tissue fits run on the device; the multi-tissue (GRL) rounds with dRL
+    are not built.
+
+    Raises:
+        ValueError: If an iteration count is below 1, or target_adc or nu_scale is not a
+            positive number.
+    """
+
+    num_iter: int = 200
+    hr_num_iter: int = 600
+    target_adc: float = 0.7e-3
+    nu_scale: float = 0.2
+
+    def __post_init__(self) -> None:
+        if self.num_iter < 1 or self.hr_num_iter < 1:
+            raise ValueError(f"num_iter and hr_num_iter must be at least 1, got {self.num_iter} and "
+                             f"{self.hr_num_iter}")
+        for name in ("target_adc", "nu_scale"):
+            value = getattr(self, name)
+            if not (np.isfinite(value) and value > 0):
+                raise ValueError(f"{name} must be a positive number, got {value}")
+
+    def _prepare(self, kernel: Kernel, bvals: np.ndarray, stage: Stage) -> _core.FodSolver:
+        if stage is not Stage.SINGLE:
+            raise NotImplementedError("GRL (the multi-tissue rounds with dRL) is not part of larmor_b200 yet; dRL "
+                                      "runs single-tissue fits")
+        nu = calibrate_drl_nu(kernel, bvals, self.target_adc, self.nu_scale)
+        k_t, k_t_k = _rl_products(kernel.w_k_aniso)
+        return _core.FodSolver.drl(k_t, k_t_k, nu=nu, n_iter=self.num_iter, init=1.0 / kernel.w_k_aniso.shape[1])
 
 
 def _deconv_kernel(kernel: Kernel) -> _core.DeconvKernel:

@@ -15,6 +15,7 @@ Each function mirrors the reference call it restates:
     climb              larmor._core.climb            cpp/src/python/sh.cpp:84
     peaks_chunk        larmor._core.peaks_chunk      cpp/src/python/sh.cpp:112
     fit_csd            larmor._core.fit_csd          cpp/src/python/sd.cpp:171
+    drl                FodSolver.drl + fit_single_tissue  cpp/src/sd/solver.cpp:9, drl.cpp:39
 """
 
 from __future__ import annotations
@@ -238,3 +239,17 @@ def fit_csd(signals, initial, forward, constraint, norm_weight, threshold, max_i
                          _p(forward), _i64(c), _p(constraint), _i64(constraint.shape[0]), _dbl(norm_weight),
                          _dbl(threshold), _i64(max_iter), _i64(n_threads), _p(fods), _p(conv))
     return fods, conv.astype(bool)
+
+
+# ---- damped Richardson-Lucy (drl.cpp) ----------------------------------------------------
+
+
+def drl(signals, k_t, k_t_k, nu, n_iter, init, n_threads=1):
+    """FodSolver.drl(k_t, k_t_k, nu, n_iter, init) + fit_single_tissue (cpp/src/sd/solver.cpp:9-12,
+    cpp/src/sd/drl.cpp:39-100): the FODs (v, c). The arguments are assumed valid."""
+    signals, k_t, k_t_k = _c64(signals), _c64(k_t), _c64(k_t_k)
+    v, c = signals.shape[0], k_t.shape[0]
+    fods = np.empty((v, c))
+    lib().oracle_drl(_p(signals), _i64(v), _i64(signals.shape[1]), _p(k_t), _p(k_t_k), _i64(c), _dbl(nu),
+                     _i64(n_iter), _dbl(init), _i64(n_threads), _p(fods))
+    return fods

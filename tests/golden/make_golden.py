@@ -34,6 +34,8 @@ What the fixtures hold, all from the reference's own code and data:
   table of b0s only.
 - csd.npz: the matrices of single-shell CSD (csd_problem) for four settings on the 60-direction
   shell of tests/sd/test_csd.py, and that test's synthetic voxels.
+- drl.npz: damped Richardson-Lucy (the reference's numpy drl_solver) on the voxels, kernel and
+  calibrated nu of tests/sd/test_drl.py, for its three settings.
 - dirs300.npy: the reference's 300 FOD directions (src/larmor/data/dir300.txt), a table the
   SD models must share exactly; also written to larmor_b200/data/dirs300.npy, where the
   package reads it.
@@ -198,6 +200,55 @@ def _csd_fixture() -> None:
     out["fibres"] = np.array([np.pad(f, ((0, 2 - len(f)), (0, 0)), constant_values=np.nan) for f in fibre_sets]
                              + [np.array([[1.0, 0, 0], [0, 1.0, 0]])])
     np.savez_compressed(OUT / "csd.npz", **out)
+
+
+def _drl_fixture(reference: Path) -> None:
+    """drl.npz: damped Richardson-Lucy on the cases of tests/sd/test_drl.py. The white matter
+    kernel on the MATLAB gradient table of tests/data/grl_obj.mat (DIRS_300, the shell weights);
+    the test's 300 seeded voxels (noisy one- to three-fibre voxels with CSF, and isotropic ones);
+    nu calibrated as calibrate_drl_nu does (an undamped 200-iteration solve of the isotropic signal
+    exp(-b_max 0.7e-3), nu = 0.2 max(fod)), with the reference's numpy solver in place of the
+    compiled one; and the reference's numpy solver (tests/sd/reference_solvers.py:drl_solver) on
+    the voxels for the test's three settings: calibration (uniform start, undamped), single-tissue
+    (uniform start, damped) and multi-tissue start (1e-6 start, damped), 200 iterations each."""
+    from scipy.io import loadmat
+
+    sys.path.insert(0, str(reference / "tests" / "sd"))
+    from reference_solvers import DRL_INIT, drl_solver
+
+    from larmor.sd import AnisotropicRF
+    from larmor.sd.kernel import Kernel
+    from larmor.sd.sphere import DIRS_300
+
+    grl = loadmat(reference / "tests" / "data" / "grl_obj.mat", simplify_cells=True)["grl_obj"]
+    bvals = np.asarray(grl["bvals"], dtype=np.float64)
+    wm = AnisotropicRF(eigen_vals=[1.7e-3, 0.2e-3, 0.2e-3], mean_kurtosis=0.0)
+    kernel = Kernel([wm], bvals=bvals, bvecs=grl["bvecs"].astype(np.float64), dirs=DIRS_300,
+                    weights=grl["shell_weight"])
+    k = np.ascontiguousarray(kernel.k)
+    k_t, k_t_k = np.ascontiguousarray(k.T), np.ascontiguousarray(k.T @ k)
+    n_cols = k.shape[1]
+    iso = np.full(len(bvals), np.exp(-max(bvals) * 0.7e-3))
+    nu = float(0.2 * np.max(drl_solver(np.full(n_cols, 1.0 / n_cols), iso, k_t, k_t_k, 0.0, 200)))
+    rng = np.random.default_rng(0)
+    n_vox = 300
+    n_fibre = 2 * n_vox // 3
+    fods = np.zeros((n_fibre, n_cols))
+    for fod in fods:
+        cols = rng.choice(n_cols, size=rng.integers(1, 4), replace=False)
+        fod[cols] = rng.dirichlet(np.ones(len(cols)))
+    csf = rng.uniform(0.0, 0.3, size=(n_fibre, 1))
+    fibre = (1 - csf) * fods @ kernel.k_aniso.T + csf * np.exp(-bvals * 3e-3)
+    fibre += rng.uniform(0.0, 0.05, (n_fibre, 1)) * rng.standard_normal(fibre.shape)
+    adc = rng.uniform(0.5e-3, 3e-3, size=(n_vox - n_fibre, 1))
+    signals = np.ascontiguousarray(np.vstack([fibre, np.exp(-bvals * adc)])[rng.permutation(n_vox)])
+    out = dict(bvals=bvals, k=k, signals=signals, nu=nu, drl_init=DRL_INIT)
+    for name, start, damping in (("calibration", 1.0 / n_cols, 0.0), ("single", 1.0 / n_cols, nu),
+                                 ("multi_start", DRL_INIT, nu)):
+        init = np.full(n_cols, start)
+        out[f"{name}_fods"] = np.array([drl_solver(init, sv, k_t, k_t_k, damping, 200) for sv in signals])
+        out[f"{name}_start"], out[f"{name}_nu"] = start, damping
+    np.savez_compressed(OUT / "drl.npz", **out)
 
 
 def _peaks_fixture(reference: Path) -> None:
@@ -426,6 +477,7 @@ def main(reference: Path) -> None:
     _peaks_fixture(reference)
     _staging_fixture()
     _csd_fixture()
+    _drl_fixture(reference)
     np.save(OUT / "dirs300.npy", np.asarray(DIRS_300, dtype=np.float64))
     # The same table ships with the package: the SD models' FOD directions.
     np.save(OUT.parents[1] / "larmor_b200" / "data" / "dirs300.npy", np.asarray(DIRS_300, dtype=np.float64))
