@@ -763,6 +763,69 @@ class CsdWorkload(_SdWorkloadBase):
         return done, time.perf_counter() - t0, f"first {n} voxels of the shell, repeated for ~{budget_s:.0f} s"
 
 
+class DrlWorkload(_SdWorkloadBase):
+    """Damped Richardson-Lucy (the DRL solver, src/larmor/sd/solvers.py:72-148) single-tissue fit
+    of the config-3 volume: 500,040 voxels, their 280 S0-normalised signals, the white matter
+    kernel on the 300 FOD directions (the mFOD workload's fibre response), nu calibrated on it,
+    up to 200 iterations per voxel."""
+
+    name = "drl_single_tissue_110x110x70"
+    kernels = ("drl_kernel",)
+    has_fp32 = False
+
+    def __init__(self, seed: int) -> None:
+        from larmor_b200.sd.kernel import Kernel
+        from larmor_b200.sd.rf import AnisotropicRF
+        from larmor_b200.sd.sphere import DIRS_300
+
+        self._volume(seed)
+        self.norm = np.ascontiguousarray(np.minimum(self.signals / self.s0[:, None], 1.0))
+        self.kernel = Kernel([AnisotropicRF([1.7e-3, 0.2e-3, 0.2e-3], 0.0)], self.gtab.bvals, self.gtab.bvecs,
+                             dirs=DIRS_300)
+        self.config = {"workload": self.name, "grid": [110, 110, 70], "voxels": self.v, "measurements": 280,
+                       "directions": 300, "max_iter": 200, "l2": "inputs (1.1 GB) larger than L2"}
+
+    def device_setup(self, torch, dev):
+        from larmor_b200.sd.solvers import DRL, Stage
+
+        self.torch = torch
+        self.solver = DRL()._prepare(self.kernel, self.gtab.bvals, Stage.SINGLE)
+        self.d_signals = torch.from_numpy(self.norm).to(dev)
+        self.h_signals = torch.from_numpy(self.norm).pin_memory()
+        self.h_fods = torch.empty((self.v, 300), dtype=torch.float64).pin_memory()
+        self.h2d_bytes = self.norm.nbytes
+        self.d2h_bytes = self.v * 300 * 8
+
+    def step_device(self, precision=0):
+        from larmor_b200 import _core
+
+        self.d_fods = _core._fit_single_tissue_on_device(self.d_signals, self.solver)
+
+    def kernel_bytes(self) -> dict:
+        """Algorithmic DRAM bytes of one step: 280 signals in, 300 amplitudes out per voxel."""
+        return {"drl_kernel": self.v * 8 * (280 + 300)}
+
+    def step_e2e(self):
+        self.d_signals.copy_(self.h_signals, non_blocking=True)
+        self.step_device()
+        self.h_fods.copy_(self.d_fods, non_blocking=True)
+
+    def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
+        from larmor_b200.sd.solvers import _rl_products, calibrate_drl_nu
+        from oracle import oracle as o
+
+        k_t, k_t_k = _rl_products(self.kernel.w_k_aniso)
+        nu = getattr(self, "_nu", None)
+        if nu is None:
+            nu = self._nu = calibrate_drl_nu(self.kernel, self.gtab.bvals) if hasattr(self, "solver") else 1e-3
+        n = min(self.v, 512)
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget_s:
+            o.drl(self.norm[:n], k_t, k_t_k, nu, 200, 1.0 / 300, n_threads=threads)
+            done += n
+        return done, time.perf_counter() - t0, f"first {n} voxels of the volume, repeated for ~{budget_s:.0f} s"
+
+
 class PeaksWorkload:
     """FOD peaks (find_peaks, src/larmor/sd/peaks.py) of lmax-8 FODs on the config-3 mask
     (110x110x70, 500,040 voxels): the amplitudes of each FOD on the 642-vertex icosphere, then
@@ -878,7 +941,8 @@ class PeaksWorkload:
 
 
 WORKLOADS = {"dti": DtiWorkload, "dki": DkiWorkload, "mfod": MfodWorkload, "msmt": MsmtWorkload,
-             "batch": BatchWorkload, "peaks": PeaksWorkload, "dti_model": DtiModelWorkload, "csd": CsdWorkload}
+             "batch": BatchWorkload, "peaks": PeaksWorkload, "dti_model": DtiModelWorkload, "csd": CsdWorkload,
+             "drl": DrlWorkload}
 
 
 
