@@ -11,7 +11,10 @@
 // (32, c) in shared memory for all their iterations. An iteration is one product F K^T K on the
 // FP64 tensor cores: mma.sync m8n8k4 over four 8-voxel row tiles and the 8-direction column
 // tiles, which the warps take round-robin. K^T K (c x c, 720 KB at c = 300) stays in L2 and
-// streams through each CTA once per iteration for its 32 voxels. The update is the epilogue,
+// streams through each CTA once per iteration for its 32 voxels, 8 rows at a time, into a
+// double-buffered shared-memory stage by cp.async while the tensor cores work on the previous 8
+// rows. The rows of F, K^T s and the stage are padded, so the fragment loads of a warp fall in
+// distinct banks. The update is the epilogue,
 // on the accumulators, after a barrier, since every warp reads all of F. Each voxel's change is
 // reduced in a fixed order, so the stopping test does not depend on the schedule. Converged
 // voxels keep their FOD while the tile's others iterate.
@@ -30,6 +33,26 @@ namespace {
 constexpr int kDrlRows = 32;   // voxels per CTA tile: four 8-row tiles
 constexpr int kDrlWarps = 8;
 constexpr int kDrlMaxCt = 5;   // column tiles per warp: c <= 8 * kDrlWarps * kDrlMaxCt = 320
+constexpr int kDrlChunk = 8;   // rows of K^T K per stage (two k-steps)
+
+// Row strides (doubles) of F and K^T s, and of the K^T K stage, for cp columns: the padding puts
+// the 8 rows of an A fragment, and the 4 rows of a B fragment, in different banks.
+__host__ __device__ inline int drl_ldf(int cp) { return cp + 4; }
+__host__ __device__ inline int drl_ldg(int cp) { return cp + 8; }
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async16(double* dst, const double* src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N));
+}
 
 __device__ __forceinline__ double power_8(double x) {
     const double x2 = x * x, x4 = x2 * x2;
@@ -49,11 +72,33 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const 
     __shared__ double strength[kDrlRows], threshold[kDrlRows];
     __shared__ int active[kDrlRows];
     __shared__ int n_active;
-    const int c = P.c, m = P.m, cp = (c + 7) / 8 * 8, n_ct = cp / 8;
-    double* F = reinterpret_cast<double*>(smem);  // (32, cp)
-    double* KS = F + kDrlRows * cp;               // (32, cp)
+    const int c = P.c, m = P.m, cp = (c + 7) / 8 * 8, n_ct = cp / 8, ldf = drl_ldf(cp), ldg = drl_ldg(cp);
+    double* F = reinterpret_cast<double*>(smem);  // (32, ldf)
+    double* KS = F + kDrlRows * ldf;              // (32, ldf)
+    double* GS = KS + kDrlRows * ldf;             // (2, kDrlChunk, ldg): the K^T K stage
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const double nu8 = power_8(P.nu);
+    // The stage's columns past c stay 0.
+    for (int e = threadIdx.x; e < 2 * kDrlChunk * ldg; e += blockDim.x)
+        if (e % ldg >= c) GS[e] = 0.0;
+    const int n_chunks = cp / kDrlChunk;
+    // Rows [8 q, 8 q + 8) of K^T K into stage buffer b, one row per 32 threads: cp.async of 16
+    // bytes when the rows are 16-byte aligned (c even; the stage's row stride is a multiple of 16
+    // bytes), else of 8; zeros for the rows past c.
+    const bool wide = c % 2 == 0;
+    auto stage = [&](int q, int b) {
+        const int r = threadIdx.x >> 5, k = q * kDrlChunk + r;
+        double* dst = GS + (b * kDrlChunk + r) * ldg;
+        const double* src = P.gram + size_t(k) * c;
+        if (k >= c) {
+            for (int d = lane; d < c; d += 32) dst[d] = 0.0;
+        } else if (wide) {
+            for (int d = 2 * lane; d < c; d += 64) cp_async16(dst + d, src + d);
+        } else {
+            for (int d = lane; d < c; d += 32) cp_async8(dst + d, src + d);
+        }
+        cp_async_commit();
+    };
     for (int64_t v0 = int64_t(blockIdx.x) * kDrlRows; v0 < v; v0 += int64_t(gridDim.x) * kDrlRows) {
         // Each voxel's damping strength (1 - 4 x the sample standard deviation, at least 0) and
         // stopping threshold (1e-4 x its largest non-NaN signal value).
@@ -89,8 +134,8 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const 
             }
         }
         // K^T s and the start.
-        for (int e = tid; e < kDrlRows * cp; e += blockDim.x) {
-            const int r = e / cp, d = e - r * cp;
+        for (int e = tid; e < kDrlRows * ldf; e += blockDim.x) {
+            const int r = e / ldf, d = e - r * ldf;
             const int64_t voxel = v0 + r;
             const bool real = voxel < v && d < c;
             double ks = 0.0;
@@ -118,23 +163,36 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const 
             for (int rt = 0; rt < 4; ++rt)
 #pragma unroll
                 for (int t = 0; t < kDrlMaxCt; ++t) acc[rt][t][0] = acc[rt][t][1] = 0.0;
-            for (int k0 = 0; k0 < cp; k0 += 4) {
-                const int kk = k0 + (lane & 3);
-                double a[4];
+            stage(0, 0);
+            for (int q = 0; q < n_chunks; ++q) {
+                if (q + 1 < n_chunks) {
+                    stage(q + 1, (q + 1) & 1);
+                    cp_async_wait<1>();
+                } else {
+                    cp_async_wait<0>();
+                }
+                __syncthreads();
+                const double* g = GS + (q & 1) * kDrlChunk * ldg;
 #pragma unroll
-                for (int rt = 0; rt < 4; ++rt) a[rt] = F[(8 * rt + (lane >> 2)) * cp + kk];
+                for (int ks = 0; ks < kDrlChunk; ks += 4) {
+                    const int kk = q * kDrlChunk + ks + (lane & 3);
+                    const double* grow = g + (ks + (lane & 3)) * ldg + (lane >> 2);
+                    double a[4];
 #pragma unroll
-                for (int t = 0; t < kDrlMaxCt; ++t) {
-                    const int ct = warp + kDrlWarps * t;
-                    if (ct < n_ct) {
-                        const int col = 8 * ct + (lane >> 2);
-                        const double b = (kk < c && col < c) ? __ldg(P.gram + size_t(kk) * c + col) : 0.0;
+                    for (int rt = 0; rt < 4; ++rt) a[rt] = F[(8 * rt + (lane >> 2)) * ldf + kk];
 #pragma unroll
-                        for (int rt = 0; rt < 4; ++rt) mma_f64(acc[rt][t][0], acc[rt][t][1], a[rt], b);
+                    for (int t = 0; t < kDrlMaxCt; ++t) {
+                        const int ct = warp + kDrlWarps * t;
+                        if (ct < n_ct) {
+                            const double b = grow[8 * ct];
+#pragma unroll
+                            for (int rt = 0; rt < 4; ++rt) mma_f64(acc[rt][t][0], acc[rt][t][1], a[rt], b);
+                        }
                     }
                 }
+                // The next stage overwrites this buffer: every warp is done with it first.
+                __syncthreads();
             }
-            __syncthreads();
             // The damped update of the still-active voxels, and each one's total change.
             double change[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
@@ -149,12 +207,12 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const 
                     for (int h = 0; h < 2; ++h) {
                         const int d = 8 * ct + 2 * (lane & 3) + h;
                         if (d >= c) continue;
-                        const double f = F[r * cp + d], f8 = power_8(f);
+                        const double f = F[r * ldf + d], f8 = power_8(f);
                         const double damping = 1.0 - strength[r] * (1.0 - f8 / (f8 + nu8));
                         const double pred = acc[rt][t][h];
-                        const double ratio = (KS[r * cp + d] - pred) / (pred + 1e-16);
+                        const double ratio = (KS[r * ldf + d] - pred) / (pred + 1e-16);
                         const double updated = fmax(f * (1.0 + damping * ratio), 1e-6);
-                        F[r * cp + d] = updated;
+                        F[r * ldf + d] = updated;
                         change[rt] += fabs(updated - f);
                     }
                 }
@@ -173,8 +231,8 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const 
             }
             __syncthreads();
         }
-        for (int e = tid; e < kDrlRows * cp; e += blockDim.x) {
-            const int r = e / cp, d = e - r * cp;
+        for (int e = tid; e < kDrlRows * ldf; e += blockDim.x) {
+            const int r = e / ldf, d = e - r * ldf;
             const int64_t voxel = v0 + r;
             if (voxel < v && d < c) fods[voxel * c + d] = F[e];
         }
@@ -184,7 +242,10 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const 
 
 }  // namespace
 
-size_t drl_smem_bytes(int c) { return 2 * size_t(kDrlRows) * size_t((c + 7) / 8 * 8) * sizeof(double); }
+size_t drl_smem_bytes(int c) {
+    const int cp = (c + 7) / 8 * 8;
+    return (2 * size_t(kDrlRows) * drl_ldf(cp) + 2 * size_t(kDrlChunk) * drl_ldg(cp)) * sizeof(double);
+}
 
 bool drl_fits(int c) { return c >= 1 && c <= 8 * kDrlWarps * kDrlMaxCt; }
 
