@@ -185,8 +185,9 @@ typedef struct lar_deconv_kernel_s* lar_deconv_kernel;
 /* FodSolver.drl (cpp/src/python/sd.cpp:127-145): a damped Richardson-Lucy solver
  * (cpp/src/sd/drl.cpp:39-100) of K^T (c, m) and K^T K (c, c), host arrays copied: damping
  * threshold nu, at most n_iter (>= 0) iterations per voxel, every amplitude started at init.
- * c <= 320, m > 1. lar_fit_single_tissue runs it; lar_fit_multi_tissue refuses it (GRL's
- * multi-tissue rounds with dRL are not built). */
+ * c <= 640, m > 1. lar_fit_single_tissue runs it; lar_fit_multi_tissue takes it for either
+ * resolution (GRL: each round's and the final FODs by dRL on the anisotropic signal,
+ * cpp/src/sd/multi_tissue.cpp:40-95). */
 int lar_drl_create(const double* k_t, const double* k_t_k, int64_t c, int64_t m, double nu, int64_t n_iter,
                    double init, lar_fod_solver* out);
 

@@ -333,13 +333,13 @@ class FodSolver(_Handle):
     def drl(k_t, k_t_k, nu, n_iter, init) -> "FodSolver":
         """Damped Richardson-Lucy (cpp/src/python/sd.cpp:127-145): k_t is K^T (c, m), k_t_k is
         K^T K (c, c); amplitudes below nu have their updates damped; at most n_iter iterations
-        per voxel, every amplitude started at init. fit_single_tissue runs it on the device
-        (lar_drl_create); the multi-tissue fit does not take it (GRL's rounds are not built).
+        per voxel, every amplitude started at init. fit_single_tissue and fit_multi_tissue (GRL) run
+        it on the device (lar_drl_create).
 
         Raises:
             TypeError: If k_t or k_t_k is not a float64 numpy array.
             ValueError: If the shapes do not match, n_iter is negative, or the solver has more
-                than 320 directions.
+                than 640 directions.
         """
         for name, a in (("k_t", k_t), ("k_t_k", k_t_k)):
             if not isinstance(a, np.ndarray) or a.dtype != np.float64:

@@ -7,17 +7,20 @@
 // u = 1 - strength (1 - f^8 / (f^8 + nu^8)), with strength = max(1 - 4 std(s), 0). A voxel
 // stops when its amplitudes change in total by no more than 1e-4 of its largest signal value.
 //
-// Mapping: a CTA of 8 warps takes 32 voxels at a time and keeps their FODs F (32, c) and K^T s
-// (32, c) in shared memory for all their iterations. An iteration is one product F K^T K on the
-// FP64 tensor cores: mma.sync m8n8k4 over four 8-voxel row tiles and the 8-direction column
-// tiles, which the warps take round-robin. K^T K (c x c, 720 KB at c = 300) stays in L2 and
-// streams through each CTA once per iteration for its 32 voxels, 8 rows at a time, into a
-// double-buffered shared-memory stage by cp.async while the tensor cores work on the previous 8
-// rows. The rows of F, K^T s and the stage are padded, so the fragment loads of a warp fall in
-// distinct banks. The update is the epilogue,
-// on the accumulators, after a barrier, since every warp reads all of F. Each voxel's change is
-// reduced in a fixed order, so the stopping test does not depend on the schedule. Converged
-// voxels keep their FOD while the tile's others iterate.
+// Mapping: a CTA of 8 warps takes 8 RT voxels at a time (32 up to 320 directions, 8 up to 640)
+// and keeps their FODs F (8 RT, c) and K^T s (8 RT, c) in shared memory for all their
+// iterations. An iteration is one product F K^T K on the FP64 tensor cores: mma.sync m8n8k4
+// over the RT 8-voxel row tiles and the 8-direction column tiles, which the warps take
+// round-robin. K^T K (c x c, 720 KB at c = 300) stays in L2 and streams through each CTA once
+// per iteration for its voxels, 8 rows at a time, into a double-buffered shared-memory stage by
+// cp.async while the tensor cores work on the previous 8 rows. The rows of F, K^T s and the
+// stage are padded, so the fragment loads of a warp fall in distinct banks. The update is the
+// epilogue, on the accumulators, after a barrier, since every warp reads all of F. Each voxel's
+// change is reduced in a fixed order, so the stopping test does not depend on the schedule.
+// Converged voxels keep their FOD while the tile's others iterate.
+//
+// The multi-tissue rounds (GRL, cpp/src/sd/multi_tissue.cpp:40-95) run the same solve on a list
+// of voxels whose signal is the anisotropic part max(s w - W_iso f_iso, 0) of the round.
 
 #include <algorithm>
 #include <cmath>
@@ -30,10 +33,14 @@
 namespace lar {
 namespace {
 
-constexpr int kDrlRows = 32;   // voxels per CTA tile: four 8-row tiles
 constexpr int kDrlWarps = 8;
-constexpr int kDrlMaxCt = 5;   // column tiles per warp: c <= 8 * kDrlWarps * kDrlMaxCt = 320
-constexpr int kDrlChunk = 8;   // rows of K^T K per stage (two k-steps)
+constexpr int kDrlChunk = 8;   // rows of K^T K per stage (two k-steps), one per warp
+// The two tilings: RT 8-voxel row tiles per CTA, MAXCT column tiles per warp, for
+// c <= 8 * kDrlWarps * MAXCT directions.
+constexpr int kNarrowRt = 4, kNarrowCt = 5;   // 32 voxels, c <= 320
+constexpr int kWideRt = 1, kWideCt = 10;      // 8 voxels, c <= 640
+constexpr int kNarrowMaxC = 8 * kDrlWarps * kNarrowCt;
+constexpr int kWideMaxC = 8 * kDrlWarps * kWideCt;
 
 // Row strides (doubles) of F and K^T s, and of the K^T K stage, for cp columns: the padding puts
 // the 8 rows of an A fragment, and the 4 rows of a B fragment, in different banks.
@@ -65,17 +72,34 @@ __device__ __forceinline__ void mma_f64(double& d0, double& d1, double a, double
                  : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const double* __restrict__ signals,
-                                                                int64_t v, double* __restrict__ fods) {
+// Entry i of the signal of `voxel` that dRL deconvolves.
+__device__ __forceinline__ double signal_at(const DrlSignal& S, int64_t voxel, int i) {
+    const double si = S.s[voxel * S.m + i];
+    if (S.w == nullptr) return si;
+    const double ws = __dmul_rn(si, S.w[i]);
+    double r = 0.0;
+    for (int t = 0; t < S.ci; ++t) r = fma(S.wiso[size_t(i) * S.ci + t], S.fiso[voxel * S.ci + t], r);
+    return fmax(ws - r, 0.0);
+}
+
+// x(list[p], :) = the dRL FOD of voxel list[p] for p < count (min(count, *count_dev) when
+// count_dev is given); no list: voxel p itself.
+template <int RT, int MAXCT>
+__global__ void __launch_bounds__(kDrlWarps * 32, 1)
+    drl_kernel(DrlDev P, DrlSignal S, const int* __restrict__ list, int64_t count, const int* __restrict__ count_dev,
+               double* __restrict__ x, int64_t ldx) {
+    constexpr int kRows = 8 * RT;
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ double part[kDrlWarps][kDrlRows];
-    __shared__ double strength[kDrlRows], threshold[kDrlRows];
-    __shared__ int active[kDrlRows];
+    __shared__ double part[kDrlWarps][kRows];
+    __shared__ double strength[kRows], threshold[kRows];
+    __shared__ int active[kRows];
+    __shared__ int64_t vox[kRows];
     __shared__ int n_active;
+    if (count_dev) count = min(count, int64_t(*count_dev));
     const int c = P.c, m = P.m, cp = (c + 7) / 8 * 8, n_ct = cp / 8, ldf = drl_ldf(cp), ldg = drl_ldg(cp);
-    double* F = reinterpret_cast<double*>(smem);  // (32, ldf)
-    double* KS = F + kDrlRows * ldf;              // (32, ldf)
-    double* GS = KS + kDrlRows * ldf;             // (2, kDrlChunk, ldg): the K^T K stage
+    double* F = reinterpret_cast<double*>(smem);  // (kRows, ldf)
+    double* KS = F + kRows * ldf;                 // (kRows, ldf)
+    double* GS = KS + kRows * ldf;                // (2, kDrlChunk, ldg): the K^T K stage
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const double nu8 = power_8(P.nu);
     // The stage's columns past c stay 0.
@@ -99,31 +123,36 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const 
         }
         cp_async_commit();
     };
-    for (int64_t v0 = int64_t(blockIdx.x) * kDrlRows; v0 < v; v0 += int64_t(gridDim.x) * kDrlRows) {
+    for (int64_t p0 = int64_t(blockIdx.x) * kRows; p0 < count; p0 += int64_t(gridDim.x) * kRows) {
+        if (tid < kRows) vox[tid] = p0 + tid < count ? (list ? int64_t(list[p0 + tid]) : p0 + tid) : -1;
+        __syncthreads();
         // Each voxel's damping strength (1 - 4 x the sample standard deviation, at least 0) and
         // stopping threshold (1e-4 x its largest non-NaN signal value).
-        for (int r = warp; r < kDrlRows; r += kDrlWarps) {
-            const int64_t voxel = v0 + r;
-            if (voxel >= v) {
+        for (int r = warp; r < kRows; r += kDrlWarps) {
+            const int64_t voxel = vox[r];
+            if (voxel < 0) {
                 if (lane == 0) {
                     active[r] = 0;
                     strength[r] = threshold[r] = 0.0;
                 }
                 continue;
             }
-            const double* s = signals + voxel * m;
             double sum = 0.0, mx = -CUDART_INF;
             bool any = false;
             for (int i = lane; i < m; i += 32) {
-                sum += s[i];
-                if (!isnan(s[i])) {
-                    mx = any ? fmax(mx, s[i]) : s[i];
+                const double si = signal_at(S, voxel, i);
+                sum += si;
+                if (!isnan(si)) {
+                    mx = any ? fmax(mx, si) : si;
                     any = true;
                 }
             }
             const double mean = warp_sum(sum) / m;
             double ss = 0.0;
-            for (int i = lane; i < m; i += 32) ss += (s[i] - mean) * (s[i] - mean);
+            for (int i = lane; i < m; i += 32) {
+                const double si = signal_at(S, voxel, i);
+                ss += (si - mean) * (si - mean);
+            }
             ss = warp_sum(ss);
             const bool all_nan = !__any_sync(0xffffffffu, any);
             mx = warp_max(any ? mx : -CUDART_INF);
@@ -134,15 +163,14 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const 
             }
         }
         // K^T s and the start.
-        for (int e = tid; e < kDrlRows * ldf; e += blockDim.x) {
+        for (int e = tid; e < kRows * ldf; e += blockDim.x) {
             const int r = e / ldf, d = e - r * ldf;
-            const int64_t voxel = v0 + r;
-            const bool real = voxel < v && d < c;
+            const int64_t voxel = vox[r];
+            const bool real = voxel >= 0 && d < c;
             double ks = 0.0;
             if (real) {
-                const double* s = signals + voxel * m;
                 const double* kt = P.k_t + size_t(d) * m;
-                for (int i = 0; i < m; ++i) ks = fma(kt[i], s[i], ks);
+                for (int i = 0; i < m; ++i) ks = fma(kt[i], signal_at(S, voxel, i), ks);
             }
             KS[e] = ks;
             F[e] = real ? P.init : 0.0;
@@ -151,18 +179,18 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const 
         for (int it = 0; it < P.n_iter; ++it) {
             if (tid == 0) {
                 int a = 0;
-                for (int r = 0; r < kDrlRows; ++r) a += active[r];
+                for (int r = 0; r < kRows; ++r) a += active[r];
                 n_active = a;
             }
             __syncthreads();
             if (n_active == 0) break;
             // The prediction K^T K f of every voxel of the tile (K^T K is symmetric: its column
             // block is read as rows).
-            double acc[4][kDrlMaxCt][2];
+            double acc[RT][MAXCT][2];
 #pragma unroll
-            for (int rt = 0; rt < 4; ++rt)
+            for (int rt = 0; rt < RT; ++rt)
 #pragma unroll
-                for (int t = 0; t < kDrlMaxCt; ++t) acc[rt][t][0] = acc[rt][t][1] = 0.0;
+                for (int t = 0; t < MAXCT; ++t) acc[rt][t][0] = acc[rt][t][1] = 0.0;
             stage(0, 0);
             for (int q = 0; q < n_chunks; ++q) {
                 if (q + 1 < n_chunks) {
@@ -177,16 +205,16 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const 
                 for (int ks = 0; ks < kDrlChunk; ks += 4) {
                     const int kk = q * kDrlChunk + ks + (lane & 3);
                     const double* grow = g + (ks + (lane & 3)) * ldg + (lane >> 2);
-                    double a[4];
+                    double a[RT];
 #pragma unroll
-                    for (int rt = 0; rt < 4; ++rt) a[rt] = F[(8 * rt + (lane >> 2)) * ldf + kk];
+                    for (int rt = 0; rt < RT; ++rt) a[rt] = F[(8 * rt + (lane >> 2)) * ldf + kk];
 #pragma unroll
-                    for (int t = 0; t < kDrlMaxCt; ++t) {
+                    for (int t = 0; t < MAXCT; ++t) {
                         const int ct = warp + kDrlWarps * t;
                         if (ct < n_ct) {
                             const double b = grow[8 * ct];
 #pragma unroll
-                            for (int rt = 0; rt < 4; ++rt) mma_f64(acc[rt][t][0], acc[rt][t][1], a[rt], b);
+                            for (int rt = 0; rt < RT; ++rt) mma_f64(acc[rt][t][0], acc[rt][t][1], a[rt], b);
                         }
                     }
                 }
@@ -194,13 +222,15 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const 
                 __syncthreads();
             }
             // The damped update of the still-active voxels, and each one's total change.
-            double change[4] = {0.0, 0.0, 0.0, 0.0};
+            double change[RT];
 #pragma unroll
-            for (int t = 0; t < kDrlMaxCt; ++t) {
+            for (int rt = 0; rt < RT; ++rt) change[rt] = 0.0;
+#pragma unroll
+            for (int t = 0; t < MAXCT; ++t) {
                 const int ct = warp + kDrlWarps * t;
                 if (ct >= n_ct) continue;
 #pragma unroll
-                for (int rt = 0; rt < 4; ++rt) {
+                for (int rt = 0; rt < RT; ++rt) {
                     const int r = 8 * rt + (lane >> 2);
                     if (!active[r]) continue;
 #pragma unroll
@@ -218,51 +248,67 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1) drl_kernel(DrlDev P, const 
                 }
             }
 #pragma unroll
-            for (int rt = 0; rt < 4; ++rt) {
+            for (int rt = 0; rt < RT; ++rt) {
                 change[rt] += __shfl_xor_sync(0xffffffffu, change[rt], 1);
                 change[rt] += __shfl_xor_sync(0xffffffffu, change[rt], 2);
                 if ((lane & 3) == 0) part[warp][8 * rt + (lane >> 2)] = change[rt];
             }
             __syncthreads();
-            if (tid < kDrlRows && active[tid]) {
+            if (tid < kRows && active[tid]) {
                 double total = 0.0;
                 for (int w = 0; w < kDrlWarps; ++w) total += part[w][tid];
                 if (total <= threshold[tid]) active[tid] = 0;
             }
             __syncthreads();
         }
-        for (int e = tid; e < kDrlRows * ldf; e += blockDim.x) {
+        for (int e = tid; e < kRows * ldf; e += blockDim.x) {
             const int r = e / ldf, d = e - r * ldf;
-            const int64_t voxel = v0 + r;
-            if (voxel < v && d < c) fods[voxel * c + d] = F[e];
+            const int64_t voxel = vox[r];
+            if (voxel >= 0 && d < c) x[voxel * ldx + d] = F[e];
         }
         __syncthreads();
     }
+}
+
+template <int RT, int MAXCT>
+void launch_variant(const DrlDev& P, const DrlSignal& S, const int* list, int64_t count, const int* count_dev,
+                    double* x, int64_t ldx, cudaStream_t st, const char* name) {
+    auto kernel = drl_kernel<RT, MAXCT>;
+    const size_t smem = drl_smem_bytes(P.c);
+    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+               "cudaFuncSetAttribute");
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kDrlWarps * 32, smem),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    const int64_t tiles = (count + 8 * RT - 1) / (8 * RT);
+    const int64_t blocks =
+        std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sm_count()) * ctas_per_sm(per_sm, "drl.ctas_per_sm")));
+    LaunchScope scope(name, st);
+    kernel<<<unsigned(blocks), kDrlWarps * 32, smem, st>>>(P, S, list, count, count_dev, x, ldx);
+    cuda_check(cudaGetLastError(), "drl_kernel launch");
 }
 
 }  // namespace
 
 size_t drl_smem_bytes(int c) {
     const int cp = (c + 7) / 8 * 8;
-    return (2 * size_t(kDrlRows) * drl_ldf(cp) + 2 * size_t(kDrlChunk) * drl_ldg(cp)) * sizeof(double);
+    const size_t rows = c <= kNarrowMaxC ? 8 * kNarrowRt : 8 * kWideRt;
+    return (2 * rows * drl_ldf(cp) + 2 * size_t(kDrlChunk) * drl_ldg(cp)) * sizeof(double);
 }
 
-bool drl_fits(int c) { return c >= 1 && c <= 8 * kDrlWarps * kDrlMaxCt; }
+bool drl_fits(int c) { return c >= 1 && c <= kWideMaxC; }
+
+void launch_drl_listed(const DrlDev& P, const DrlSignal& S, const int* list, int64_t count, const int* count_dev,
+                       double* x, int64_t ldx, cudaStream_t st) {
+    if (count == 0) return;
+    if (P.c <= kNarrowMaxC)
+        launch_variant<kNarrowRt, kNarrowCt>(P, S, list, count, count_dev, x, ldx, st, "drl_kernel");
+    else
+        launch_variant<kWideRt, kWideCt>(P, S, list, count, count_dev, x, ldx, st, "drl_kernel_wide");
+}
 
 void launch_drl(const DrlDev& P, const double* signals, int64_t v, double* fods, cudaStream_t st) {
-    if (v == 0) return;
-    const size_t smem = drl_smem_bytes(P.c);
-    cuda_check(cudaFuncSetAttribute(drl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-               "cudaFuncSetAttribute");
-    int per_sm = 0;
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, drl_kernel, kDrlWarps * 32, smem),
-               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    const int64_t tiles = (v + kDrlRows - 1) / kDrlRows;
-    const int64_t blocks =
-        std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sm_count()) * ctas_per_sm(per_sm, "drl.ctas_per_sm")));
-    LaunchScope scope("drl_kernel", st);
-    drl_kernel<<<unsigned(blocks), kDrlWarps * 32, smem, st>>>(P, signals, v, fods);
-    cuda_check(cudaGetLastError(), "drl_kernel launch");
+    launch_drl_listed(P, DrlSignal{signals, nullptr, nullptr, nullptr, P.m, 0}, nullptr, v, nullptr, fods, P.c, st);
 }
 
 }  // namespace lar

@@ -17,7 +17,18 @@ struct DrlDev {
     double nu, init;
 };
 
-// Whether drl_kernel takes c directions (1 to 320).
+// The signal dRL deconvolves, entry i of voxel v: s(v, i) itself (a single-tissue fit), or the
+// anisotropic part max(s(v, i) w_i - sum_t W_iso(i, t) f_iso(v, t), 0) of a multi-tissue round
+// (cpp/src/sd/multi_tissue.cpp:68-72).
+struct DrlSignal {
+    const double* s;     // (v, m)
+    const double* w;     // (m,) shell weights, or null: the plain signal
+    const double* wiso;  // (m, ci): the weighted isotropic kernel
+    const double* fiso;  // (v, ci): the isotropic fractions of the round
+    int m, ci;
+};
+
+// Whether drl_kernel takes c directions (1 to 640).
 bool drl_fits(int c);
 
 // The shared memory drl_kernel takes for c directions.
@@ -25,5 +36,11 @@ size_t drl_smem_bytes(int c);
 
 // fods (v, c) of the signals (v, m), all device arrays: every voxel started at P.init.
 void launch_drl(const DrlDev& P, const double* signals, int64_t v, double* fods, cudaStream_t stream);
+
+// x(voxel, :) (row stride ldx) = the dRL FOD of each voxel list[p], p < count (the voxels
+// 0..count-1 when list is null; count capped by *count_dev when that is given), every voxel
+// started at P.init.
+void launch_drl_listed(const DrlDev& P, const DrlSignal& S, const int* list, int64_t count, const int* count_dev,
+                       double* x, int64_t ldx, cudaStream_t stream);
 
 }  // namespace lar

@@ -1123,8 +1123,6 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
                             bool device_rounds) {
     return guarded([&] {
         require(lr && hr && lr_solver && hr_solver, "kernels and solvers must not be NULL");
-        require(lr_solver->kind == 0 && hr_solver->kind == 0,
-                "the multi-tissue fit takes L2NNLS solvers: GRL (dRL solvers in the multi-tissue fit) is not built");
         require(weights != nullptr, "weights must not be NULL");
         const int64_t m = hr->m;
         require(lr->m == m && lr_solver->host.m == m && hr_solver->host.m == m,
@@ -1141,6 +1139,9 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
         const int max_rounds = int(std::min<int64_t>(max_outer, 1 << 20));
         const RidgeDev lrs = lr_solver->view(), hrs = hr_solver->view();
         const TissueDev lrt = lr->view(), hrt = hr->view();
+        // A dRL solver (GRL) replaces the correlations and the NNLS of its stage by drl_kernel on
+        // the stage's anisotropic signals; the fractions are the same.
+        const bool lr_drl = lr_solver->kind == 1, hr_drl = hr_solver->kind == 1;
         const NnlsLaunch lr_nnls = nnls_variant(c_lr), hr_nnls = nnls_variant(c_hr);
         const size_t lr_smem = nnls_smem_bytes(c_lr, lr_nnls.cap) * kMtWarps;
         const size_t hr_smem = nnls_smem_bytes(c_hr, hr_nnls.cap) * kMtWarps;
@@ -1150,15 +1151,15 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
         const size_t per_voxel = (size_t(std::max(c_lr, c_hr)) + size_t(c_lr) + 2 * size_t(ci) + 1) * sizeof(double) +
                                  3 * sizeof(int) + 1;
         const int64_t n_max = std::min<int64_t>(v, std::max<int64_t>(4096, int64_t((size_t(4) << 30) / per_voxel)));
-        const int64_t lr_slots = resident_slots(lr_nnls.kernel, lr_smem, n_max, "sd.nnls.ctas_per_sm");
+        const int64_t lr_slots = lr_drl ? 0 : resident_slots(lr_nnls.kernel, lr_smem, n_max, "sd.nnls.ctas_per_sm");
         // Low-resolution kernels of at most 48 directions with normal equations: two voxels per
         // warp (ridge_nnls_half_kernel), the voxels that need the QR fallback then refitted by
         // the one-warp kernel.
-        const bool half = lrs.normal_equations && c_lr <= 48;
+        const bool half = !lr_drl && lrs.normal_equations && c_lr <= 48;
         auto half_kernel = ridge_nnls_half_kernel<3>;
         const size_t half_smem = half_smem_bytes(c_lr) * 2 * kMtWarps;
         const int64_t half_warps = half ? resident_slots(half_kernel, half_smem, n_max, "sd.nnls.ctas_per_sm") : 0;
-        const int64_t hr_slots = resident_slots(hr_nnls.kernel, hr_smem, n_max, "sd.nnls.ctas_per_sm");
+        const int64_t hr_slots = hr_drl ? 0 : resident_slots(hr_nnls.kernel, hr_smem, n_max, "sd.nnls.ctas_per_sm");
         const int64_t lf_slots = resident_slots(lr_fractions_kernel, 0, n_max, "sd.fractions.ctas_per_sm");
         const int64_t hf_slots = resident_slots(hr_fractions_kernel, 0, n_max, "sd.fractions.ctas_per_sm");
         const size_t lr_slot = nnls_slot_doubles(mi, lr_nnls.cap), hr_slot = nnls_slot_doubles(mi, hr_nnls.cap);
@@ -1224,10 +1225,13 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
             for (int round = 0; round < max_rounds && count > 0; ++round) {
                 int* nxt = P.list[side];
                 int* nxt_count = P.counters + 2 + side;
-                launch_correlate(lr_sig, cur, count, cur_count, lrs, P.corr, c_lr, st);
+                if (!lr_drl) launch_correlate(lr_sig, cur, count, cur_count, lrs, P.corr, c_lr, st);
                 reset_queue();
                 cuda_check(cudaMemsetAsync(nxt_count, 0, sizeof(int), st), "cudaMemsetAsync");
-                if (half) {
+                if (lr_drl) {
+                    const DrlSignal lr_as{sig, dweights, lrt.wiso, P.fiso, mi, ci};
+                    launch_drl_listed(lr_solver->drl, lr_as, cur, count, cur_count, P.xlr, c_lr, st);
+                } else if (half) {
                     cuda_check(cudaMemsetAsync(P.counters + 4, 0, sizeof(int), st), "cudaMemsetAsync");
                     {
                         LaunchScope scope("ridge_nnls_half_kernel<3>", st);
@@ -1272,9 +1276,12 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
                 side ^= 1;
             }
             const SignalDev hr_sig{sig, dweights, hrt.wiso, P.fiso, mi, ci};
-            launch_correlate(hr_sig, nullptr, n, nullptr, hrs, P.corr, c_hr, st);
-            reset_queue();
-            {
+            if (hr_drl) {
+                const DrlSignal hr_as{sig, dweights, hrt.wiso, P.fiso, mi, ci};
+                launch_drl_listed(hr_solver->drl, hr_as, nullptr, n, nullptr, fods + v0 * c_hr, c_hr, st);
+            } else {
+                launch_correlate(hr_sig, nullptr, n, nullptr, hrs, P.corr, c_hr, st);
+                reset_queue();
                 LaunchScope scope(hr_nnls.name, st);
                 hr_nnls.kernel<<<blocks(hr_slots, n), kMtWarps * 32, hr_smem, st>>>(
                     hrs, hr_sig, nullptr, n, nullptr, P.corr, c_hr, fods + v0 * c_hr, c_hr, P.bad, P.counters, P.slots,
@@ -1315,7 +1322,7 @@ int lar_drl_create(const double* k_t, const double* k_t_k, int64_t c, int64_t m,
     return guarded([&] {
         require(out != nullptr, "out must not be NULL");
         require(k_t != nullptr && k_t_k != nullptr && c > 0 && m > 1, "k_t must be a non-empty (c, m) array, m > 1");
-        require(drl_fits(int(c)), "dRL takes at most 320 directions");
+        require(drl_fits(int(c)), "dRL takes at most 640 directions");
         require(n_iter >= 0, "n_iter must be at least 0");
         auto h = std::make_unique<lar_fod_solver_s>();
         h->kind = 1;

@@ -91,8 +91,7 @@ def to_sh(fods: np.ndarray, lmax: int, basis: str, *, exact_integral: bool = Fal
 class SDModel:
     """Spherical deconvolution with the mFOD method (L2NNLS FODs, one per anisotropic response,
     all shells weighted equally), on the GPU; the reference's SDModel (src/larmor/sd/model.py:84).
-    A single-tissue fit also takes the DRL solver (damped Richardson-Lucy); the GRL method's
-    multi-tissue rounds with dRL are not built yet."""
+    The GRL method takes the DRL solver (damped Richardson-Lucy), single- and multi-tissue."""
 
     def __init__(self, rfs, *, method="mFOD", solver=None, inner_shell_weight=None, lmax: int = 8,
                  basis: str = "tournier", progress: bool = False) -> None:
@@ -123,9 +122,6 @@ class SDModel:
         solver = self.solver if self.solver is not None else self.method.default_solver()
         if not isinstance(solver, (L2NNLS, DRL)):
             raise NotImplementedError("larmor_b200 runs the L2NNLS and DRL solvers only")
-        if isinstance(solver, DRL) and self.is_multi_tissue:
-            raise NotImplementedError("GRL (the multi-tissue rounds with dRL) is not part of larmor_b200 yet; DRL "
-                                      "runs single-tissue fits")
         threads = n_threads(n_jobs)
         check_dwi(volume, gtab)
         lmax = compute_max_lmax(gtab.bvals, self.lmax)

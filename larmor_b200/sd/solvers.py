@@ -71,8 +71,9 @@ class DRL:
     the FOD stays non-negative, and the updates of amplitudes below nu (nu_scale times the
     largest amplitude an undamped fit gives for an isotropic tissue of diffusivity target_adc) are
     damped. num_iter caps a single-tissue fit's iterations and hr_num_iter the final solve of a
-    multi-tissue one. Single-tissue fits run on the device; the multi-tissue (GRL) rounds with dRL
-    are not built.
+    multi-tissue one. Both run on the device: a multi-tissue (GRL) fit solves each round's
+    low-resolution FODs and the final high-resolution one by dRL, from MULTI_TISSUE_DRL_INIT,
+    with one iteration fewer than asked.
 
     Raises:
         ValueError: If an iteration count is below 1, or target_adc or nu_scale is not a
@@ -94,12 +95,15 @@ class DRL:
                 raise ValueError(f"{name} must be a positive number, got {value}")
 
     def _prepare(self, kernel: Kernel, bvals: np.ndarray, stage: Stage) -> _core.FodSolver:
-        if stage is not Stage.SINGLE:
-            raise NotImplementedError("GRL (the multi-tissue rounds with dRL) is not part of larmor_b200 yet; dRL "
-                                      "runs single-tissue fits")
         nu = calibrate_drl_nu(kernel, bvals, self.target_adc, self.nu_scale)
         k_t, k_t_k = _rl_products(kernel.w_k_aniso)
-        return _core.FodSolver.drl(k_t, k_t_k, nu=nu, n_iter=self.num_iter, init=1.0 / kernel.w_k_aniso.shape[1])
+        if stage is Stage.SINGLE:
+            return _core.FodSolver.drl(k_t, k_t_k, nu=nu, n_iter=self.num_iter,
+                                       init=1.0 / kernel.w_k_aniso.shape[1])
+        # A multi-tissue solve counts its near-zero start as the first iteration
+        # (src/larmor/sd/solvers.py:144-148).
+        n_iter = self.num_iter if stage is Stage.LOW_RES else self.hr_num_iter
+        return _core.FodSolver.drl(k_t, k_t_k, nu=nu, n_iter=n_iter - 1, init=MULTI_TISSUE_DRL_INIT)
 
 
 def _deconv_kernel(kernel: Kernel) -> _core.DeconvKernel:

@@ -26,6 +26,12 @@
 
 #include "dense.hpp"
 
+namespace oracle_rl {
+// Damped Richardson-Lucy of one voxel (drl.cpp): fod holds the start on entry.
+void solve(const double* k_t, const double* gram, int c, int m, double nu, int n_iter, const double* s,
+           double* fod);
+}  // namespace oracle_rl
+
 namespace oracle {
 
 namespace {
@@ -768,13 +774,31 @@ Vec anisotropic_signal(const double* ws, const Mat& w_iso, const Vec& f_iso) {
     return r;
 }
 
+// The FOD solve of one stage of the multi-tissue fit: the ridge NNLS (L2NNLS, plain NNLS in the
+// rounds) or, when k_t is set, damped Richardson-Lucy from init (GRL;
+// cpp/src/sd/solver.cpp:9-12).
+struct StageSolver {
+    const RidgeDesign* design = nullptr;
+    double tol = 0.0;
+    const double* k_t = nullptr;   // (c, m)
+    const double* gram = nullptr;  // (c, c)
+    Index c = 0, m = 0;
+    double nu = 0.0, init = 0.0;
+    Index n_iter = 0;
+    Vec operator()(const Vec& as) const {
+        if (k_t == nullptr) return solve_ridge_nnls(*design, as, 0.0, tol);
+        Vec fod(static_cast<size_t>(c), init);
+        oracle_rl::solve(k_t, gram, int(c), int(m), nu, int(n_iter), as.data(), fod.data());
+        return fod;
+    }
+};
+
 // One voxel of fit_multi_tissue_block (cpp/src/sd/multi_tissue.cpp:76-148); the loop's rounds
 // are independent per voxel, so a voxel alone gives the block's result
 // (cpp/tests/sd/test_multi_tissue.cpp:56).
 void fit_multi_tissue_voxel(const double* signal, const Vec& weights, const TissueKernel& lr,
-                            const RidgeDesign& lr_design, double lr_tol, const TissueKernel& hr,
-                            const RidgeDesign& hr_design, double hr_tol, Index max_rounds,
-                            double fraction_tol, double final_tol, double* out_fod,
+                            const StageSolver& lr_solve, const TissueKernel& hr, const StageSolver& hr_solve,
+                            Index max_rounds, double fraction_tol, double final_tol, double* out_fod,
                             double* out_fractions, int* out_rounds) {
     const Index m = lr.aniso.rows, ci = lr.iso.cols;
     Vec ws(static_cast<size_t>(m));
@@ -785,7 +809,7 @@ void fit_multi_tissue_voxel(const double* signal, const Vec& weights, const Tiss
     for (Index round = 0; round < max_rounds; ++round) {
         ++rounds;
         const Vec as = anisotropic_signal(ws.data(), lr.w_iso, f_iso);
-        const Vec fod = solve_ridge_nnls(lr_design, as, 0.0, lr_tol);
+        const Vec fod = lr_solve(as);
         const Vec fr = compute_fractions(fod, lr, signal, false, nullptr);
         for (Index j = 0; j < ci; ++j) f_iso[static_cast<size_t>(j)] = fr[static_cast<size_t>(1 + j)];
         bool converged = true;
@@ -795,7 +819,7 @@ void fit_multi_tissue_voxel(const double* signal, const Vec& weights, const Tiss
         prev = fr;
     }
     const Vec as = anisotropic_signal(ws.data(), hr.w_iso, f_iso);
-    const Vec fod = solve_ridge_nnls(hr_design, as, 0.0, hr_tol);
+    const Vec fod = hr_solve(as);
     std::copy(fod.begin(), fod.end(), out_fod);
     const Vec fr = compute_fractions(fod, hr, signal, true, &final_tol);
     double total = FRACTION_SUM_OFFSET;
@@ -911,8 +935,10 @@ int oracle_ridge_nnls(const double* k, Index m, Index c, double ridge, double to
     });
 }
 
-// fit_multi_tissue (cpp/src/python/sd.cpp:310) for L2NNLS solvers on both resolutions.
-// Kernels: k_aniso (m, ca), k_iso and w_k_iso (m, ci); blocks as (start, stop) pairs.
+// fit_multi_tissue (cpp/src/python/sd.cpp:310). Kernels: k_aniso (m, ca), k_iso and w_k_iso
+// (m, ci); blocks as (start, stop) pairs. Each stage solves by the ridge NNLS of its weighted
+// kernel w_aniso, or, when its k_t is not NULL, by damped Richardson-Lucy with K^T = k_t
+// (ca, m), K^T K = gram (ca, ca), nu, n_iter and init.
 int oracle_fit_multi_tissue(const double* signals, Index v, Index m, const double* weights,
                             const double* lr_aniso, Index lr_ca, const double* lr_iso,
                             const double* lr_w_iso, const double* lr_w_aniso, double lr_ridge,
@@ -921,7 +947,9 @@ int oracle_fit_multi_tissue(const double* signals, Index v, Index m, const doubl
                             const double* hr_w_aniso, double hr_ridge, double hr_tol, Index ci,
                             const Index* blocks, Index n_blocks, Index max_rounds,
                             double fraction_tol, double final_tol, int n_threads, double* fods,
-                            double* fractions, int* rounds) {
+                            double* fractions, int* rounds, const double* lr_k_t, const double* lr_gram,
+                            double lr_nu, Index lr_n_iter, double lr_init, const double* hr_k_t,
+                            const double* hr_gram, double hr_nu, Index hr_n_iter, double hr_init) {
     return guarded([&] {
         TissueKernel lr{Mat::from(lr_aniso, m, lr_ca), Mat::from(lr_iso, m, ci), Mat::from(lr_w_iso, m, ci), {}};
         TissueKernel hr{Mat::from(hr_aniso, m, hr_ca), Mat::from(hr_iso, m, ci), Mat::from(hr_w_iso, m, ci), {}};
@@ -929,13 +957,14 @@ int oracle_fit_multi_tissue(const double* signals, Index v, Index m, const doubl
         lr.blocks = {{0, lr_ca}};
         const RidgeDesign lr_d = make_ridge_design(Mat::from(lr_w_aniso, m, lr_ca), lr_ridge);
         const RidgeDesign hr_d = make_ridge_design(Mat::from(hr_w_aniso, m, hr_ca), hr_ridge);
+        const StageSolver lr_s{&lr_d, lr_tol, lr_k_t, lr_gram, lr_ca, m, lr_nu, lr_init, lr_n_iter};
+        const StageSolver hr_s{&hr_d, hr_tol, hr_k_t, hr_gram, hr_ca, m, hr_nu, hr_init, hr_n_iter};
         const Vec w(weights, weights + m);
         const Index nf = n_blocks + ci;
         parallel_blocks(v, 128, n_threads, [&](Index b, Index e) {
             for (Index i = b; i < e; ++i)
-                fit_multi_tissue_voxel(signals + i * m, w, lr, lr_d, lr_tol, hr, hr_d, hr_tol, max_rounds,
-                                       fraction_tol, final_tol, fods + i * hr_ca, fractions + i * nf,
-                                       rounds ? rounds + i : nullptr);
+                fit_multi_tissue_voxel(signals + i * m, w, lr, lr_s, hr, hr_s, max_rounds, fraction_tol, final_tol,
+                                       fods + i * hr_ca, fractions + i * nf, rounds ? rounds + i : nullptr);
         });
     });
 }

@@ -152,11 +152,13 @@ def ridge_nnls(k, ridge, tol_x, signals, n_threads=1):
 
 
 def fit_multi_tissue(signals, weights, lr, hr, lr_ridge=0.0, hr_ridge=0.1, tol_x=1e-6,
-                     max_rounds=50, fraction_tol=1e-7, final_tol=1e-2, n_threads=1, rounds=False):
+                     max_rounds=50, fraction_tol=1e-7, final_tol=1e-2, n_threads=1, rounds=False,
+                     lr_drl=None, hr_drl=None):
     """HR FODs (v, ca_hr) and fractions (v, n_blocks + ci) of the multi-tissue fit.
 
     lr and hr are dicts with k_aniso (m, ca), k_iso (m, ci), w_k_iso, w_k_aniso and, for hr,
-    blocks [(start, stop), ...].
+    blocks [(start, stop), ...]. lr_drl / hr_drl, dicts of nu, n_iter and init, make that
+    stage's FOD solve damped Richardson-Lucy on w_k_aniso (GRL) instead of the ridge NNLS.
     """
     signals, weights = _c64(signals), _c64(weights)
     v, m = signals.shape
@@ -169,12 +171,21 @@ def fit_multi_tissue(signals, weights, lr, hr, lr_ridge=0.0, hr_ridge=0.1, tol_x
     rd = np.zeros(v, np.int32)
     keep = [_c64(lr[key]) for key in ("k_iso", "w_k_iso", "w_k_aniso")] + \
            [_c64(hr[key]) for key in ("k_iso", "w_k_iso", "w_k_aniso")]
+
+    def drl_args(settings, w_aniso):
+        if settings is None:
+            return [None, None, _dbl(0.0), _i64(0), _dbl(0.0)]
+        k_t, gram = _c64(w_aniso.T), _c64(w_aniso.T @ w_aniso)
+        keep.extend([k_t, gram])
+        return [_p(k_t), _p(gram), _dbl(settings["nu"]), _i64(settings["n_iter"]), _dbl(settings["init"])]
+
+    extra = drl_args(lr_drl, keep[2]) + drl_args(hr_drl, keep[5])
     _check(lib().oracle_fit_multi_tissue(
         _p(signals), _i64(v), _i64(m), _p(weights),
         _p(la), _i64(la.shape[1]), _p(keep[0]), _p(keep[1]), _p(keep[2]), _dbl(lr_ridge), _dbl(tol_x),
         _p(ha), _i64(ha.shape[1]), _p(keep[3]), _p(keep[4]), _p(keep[5]), _dbl(hr_ridge), _dbl(tol_x),
         _i64(ci), _p(blocks), _i64(nb), _i64(max_rounds), _dbl(fraction_tol), _dbl(final_tol),
-        int(n_threads), _p(fods), _p(fr), _p(rd)))
+        int(n_threads), _p(fods), _p(fr), _p(rd), *extra))
     if rounds:
         return fods, fr, rd
     return fods, fr

@@ -36,6 +36,8 @@ What the fixtures hold, all from the reference's own code and data:
   shell of tests/sd/test_csd.py, and that test's synthetic voxels.
 - drl.npz: damped Richardson-Lucy (the reference's numpy drl_solver) on the voxels, kernel and
   calibrated nu of tests/sd/test_drl.py, for its three settings.
+- grl.npz: GRL (the multi-tissue fit with dRL) by the reference's numpy restatement on the MATLAB
+  and synthetic cases of tests/sd/test_grl.py, with both kernels' matrices.
 - dirs300.npy: the reference's 300 FOD directions (src/larmor/data/dir300.txt), a table the
   SD models must share exactly; also written to larmor_b200/data/dirs300.npy, where the
   package reads it.
@@ -249,6 +251,89 @@ def _drl_fixture(reference: Path) -> None:
         out[f"{name}_fods"] = np.array([drl_solver(init, sv, k_t, k_t_k, damping, 200) for sv in signals])
         out[f"{name}_start"], out[f"{name}_nu"] = start, damping
     np.savez_compressed(OUT / "drl.npz", **out)
+
+
+def _grl_fixture(reference: Path) -> None:
+    """grl.npz: GRL (the multi-tissue fit with damped Richardson-Lucy) on the two cases of
+    tests/sd/test_grl.py, by the reference's numpy restatement
+    (tests/sd/reference_solvers.py:fit_multi_tissue_voxel, 200 low- and 600 high-resolution
+    iterations asked for):
+    - "matlab": the 216 masked voxels of tests/data/grl_obj.mat, normalised by their b0s, with the
+      kernels of run_grl.m's responses (tests/conftest.py:_rfs, kernel_lr, kernel_hr) and MATLAB's
+      nu;
+    - "synthetic": test_grl.py's 150 seeded voxels of two anisotropic responses and two isotropic
+      ones, with nu calibrated as calibrate_drl_nu does (the numpy solver in place of the compiled
+      one).
+    Each case stores both kernels' matrices and blocks, the shell weights, the nu values, the
+    signals and the reference's high-resolution FODs and fractions."""
+    from scipy.io import loadmat
+
+    sys.path.insert(0, str(reference / "tests" / "sd"))
+    from reference_solvers import drl_solver, fit_multi_tissue_voxel
+
+    from larmor.sd import AnisotropicRF, IsotropicRF
+    from larmor.sd.kernel import Kernel
+    from larmor.sd.model import normalize_by_b0
+    from larmor.sd.sphere import DIRS_300, get_dirs
+    from larmor.types import GradientTable
+
+    grl = loadmat(reference / "tests" / "data" / "grl_obj.mat", simplify_cells=True)["grl_obj"]
+    bvals = grl["bvals"].astype(np.float64)
+    bvecs = grl["bvecs"].astype(np.float64)
+    weights = grl["shell_weight"]
+
+    def kernels(rfs):
+        lr = Kernel(rfs, bvals, bvecs, dirs=get_dirs(min(len(bvals), 45)), weights=weights)
+        hr = Kernel(rfs, bvals, bvecs, dirs=DIRS_300, weights=weights)
+        return lr, hr
+
+    def calibrate(kernel):
+        signal = np.full(len(bvals), np.exp(-max(bvals) * 0.7e-3))
+        k = kernel.k
+        fod = drl_solver(np.full(k.shape[1], 1.0 / k.shape[1]), signal, k.T, k.T @ k, 0.0, 200)
+        return float(0.2 * np.max(fod))
+
+    out = {"bvals": bvals, "bvecs": bvecs, "weights": np.asarray(weights, dtype=np.float64)}
+    # matlab
+    rfs = [AnisotropicRF(eigen_vals=[1.7e-3, 0.2e-3, 0.2e-3], mean_kurtosis=0.0), IsotropicRF(diffusivity=0.7e-3),
+           IsotropicRF(diffusivity=3e-3)]
+    lr, hr = kernels(rfs)
+    vox = np.argwhere(grl["mask"] == 1)
+    is_b0 = GradientTable(grl["bvals"], grl["bvecs"]).b0_mask
+    signals = normalize_by_b0(grl["img"][vox[:, 0], vox[:, 1], vox[:, 2]].astype(np.float64), is_b0)
+    cases = {"matlab": (signals, lr, hr, float(grl["NN_L"]), float(grl["NN_H"]))}
+    # synthetic
+    rfs2 = [AnisotropicRF(eigen_vals=[1.7e-3, 0.2e-3, 0.2e-3], mean_kurtosis=0.0),
+            AnisotropicRF(eigen_vals=[1.5e-3, 0.9e-3, 0.1e-3], mean_kurtosis=0.0),
+            IsotropicRF(diffusivity=0.7e-3), IsotropicRF(diffusivity=3e-3)]
+    lr2, hr2 = kernels(rfs2)
+    rng = np.random.default_rng(0)
+    n_dirs = len(DIRS_300)
+    syn = np.empty((150, len(bvals)))
+    for signal in syn:
+        fod = np.zeros(n_dirs)
+        cols = rng.choice(n_dirs, size=rng.integers(1, 4), replace=False)
+        fod[cols] = rng.dirichlet(np.ones(len(cols)))
+        f = rng.dirichlet(np.ones(4))
+        if rng.random() < 0.2:
+            f[rng.integers(4)] = 0.0
+            f /= f.sum()
+        signal[:] = (f[0] * hr2.k_aniso[:, :n_dirs] @ fod + f[1] * hr2.k_aniso[:, n_dirs:] @ fod
+                     + f[2] * np.exp(-bvals * 0.7e-3) + f[3] * np.exp(-bvals * 3e-3))
+        signal += rng.uniform(0.0, 0.03) * rng.standard_normal(len(bvals))
+    cases["synthetic"] = (syn, lr2, hr2, calibrate(lr2), calibrate(hr2))
+    for name, (sig, klr, khr, lr_nu, hr_nu) in cases.items():
+        fits = [fit_multi_tissue_voxel(sv, klr, khr, lr_nu, hr_nu) for sv in sig]
+        for tag, k in (("lr", klr), ("hr", khr)):
+            out[f"{name}_{tag}_k"] = k.k
+            out[f"{name}_{tag}_k_aniso"] = k.k_aniso
+            out[f"{name}_{tag}_k_iso"] = k.k_iso
+            out[f"{name}_{tag}_w_k_aniso"] = k.w_k_aniso
+            out[f"{name}_{tag}_w_k_iso"] = k.w_k_iso
+            out[f"{name}_{tag}_blocks"] = np.array([(b.start, b.stop) for b in k.aniso_blocks])
+        out.update({f"{name}_signals": np.ascontiguousarray(sig), f"{name}_lr_nu": lr_nu, f"{name}_hr_nu": hr_nu,
+                    f"{name}_fods": np.array([f[0] for f in fits]), f"{name}_fractions": np.array([f[1] for f in fits])})
+    np.savez_compressed(OUT / "grl.npz", **out)
 
 
 def _peaks_fixture(reference: Path) -> None:
@@ -478,6 +563,7 @@ def main(reference: Path) -> None:
     _staging_fixture()
     _csd_fixture()
     _drl_fixture(reference)
+    _grl_fixture(reference)
     np.save(OUT / "dirs300.npy", np.asarray(DIRS_300, dtype=np.float64))
     # The same table ships with the package: the SD models' FOD directions.
     np.save(OUT.parents[1] / "larmor_b200" / "data" / "dirs300.npy", np.asarray(DIRS_300, dtype=np.float64))

@@ -64,17 +64,6 @@ def test_drl_binding_refuses_bad_arguments(drl_fixture):
         _core.FodSolver.drl(k_t.astype(np.float32), k_t_k, nu=0.1, n_iter=10, init=0.1)
 
 
-def test_multi_tissue_grl_is_refused_clearly():
-    from larmor_b200.sd import DRL, IsotropicRF, SDModel
-    from larmor_b200.sd.rf import AnisotropicRF
-    from larmor_b200.sd.solvers import Stage
-
-    with pytest.raises(NotImplementedError, match="GRL"):
-        DRL()._prepare(None, None, Stage.LOW_RES)
-    model = SDModel([AnisotropicRF([1.7e-3, 0.2e-3, 0.2e-3], 0.0), IsotropicRF(3e-3)], method="GRL")
-    assert isinstance(model.method.default_solver(), DRL)
-
-
 # ---- GPU -----------------------------------------------------------------------------------
 
 
@@ -116,17 +105,19 @@ def test_gpu_drl_convergence_and_edge_cases(cuda, drl_fixture):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize(("n_meas", "n_dirs"), [(33, 300), (280, 300), (60, 45), (90, 130)])
-def test_gpu_drl_matches_the_oracle_on_more_voxels(cuda, oracle, n_meas, n_dirs):
-    """1,000 voxels (not a multiple of the 32-voxel tile) of random non-negative kernels, fibre and
-    isotropic-like signals, NaN in a few."""
+@pytest.mark.parametrize(("n_meas", "n_dirs", "n_vox"),
+                         [(33, 300, 1000), (280, 300, 1000), (60, 45, 1000), (90, 130, 1000), (33, 600, 203),
+                          (60, 450, 203)])
+def test_gpu_drl_matches_the_oracle_on_more_voxels(cuda, oracle, n_meas, n_dirs, n_vox):
+    """Voxel counts that are not a multiple of the tile (32 voxels; 8 past 320 directions) of random
+    non-negative kernels, fibre and isotropic-like signals, NaN in a few."""
     rng = np.random.default_rng(n_meas + n_dirs)
     k = np.abs(rng.normal(size=(n_meas, n_dirs))) * np.exp(-rng.uniform(0, 3, size=(n_meas, 1)))
-    fods = np.zeros((1000, n_dirs))
+    fods = np.zeros((n_vox, n_dirs))
     for f in fods:
         f[rng.choice(n_dirs, size=rng.integers(1, 4), replace=False)] = rng.dirichlet([1.0, 1.0, 1.0])[:1]
-    signals = fods @ k.T + rng.uniform(0, 0.05, size=(1000, 1)) * np.abs(rng.normal(size=(1000, n_meas)))
-    signals[:500:97, 3] = np.nan
+    signals = fods @ k.T + rng.uniform(0, 0.05, size=(n_vox, 1)) * np.abs(rng.normal(size=(n_vox, n_meas)))
+    signals[:n_vox // 2:97, 3] = np.nan
     k_t, k_t_k = _products(k)
     nu = 0.02
     got = _device_drl(signals, k, nu, 150, 1.0 / n_dirs)
