@@ -826,6 +826,89 @@ class DrlWorkload(_SdWorkloadBase):
         return done, time.perf_counter() - t0, f"first {n} voxels of the volume, repeated for ~{budget_s:.0f} s"
 
 
+class GrlWorkload(MfodWorkload):
+    """Three-tissue GRL (SDModel, method GRL: the DRL solver at both resolutions,
+    src/larmor/sd/method.py) of the config-3 volume: WM + GM + CSF, inner shells weighted 0.2,
+    up to 50 rounds of a low-resolution dRL FOD (44 directions, 199 iterations from 1e-6) and
+    the fractions until none moves by 1e-3, then the 300-direction FOD (599 iterations) and the
+    final fractions, on S0-normalised signals."""
+
+    name = "grl_3tissue_110x110x70"
+    kernels = ("drl_kernel", "lr_fractions_kernel", "hr_fractions_kernel")
+    fraction_tol = 1e-3
+
+    def __init__(self, seed: int) -> None:
+        from larmor_b200.synthetic import mfod_model_responses
+
+        from larmor_b200.sd.kernel import Kernel
+        from larmor_b200.sd.model import compute_shell_weights, low_resolution_dirs
+        from larmor_b200.sd.sphere import DIRS_300
+
+        self._volume(seed)
+        self.norm = np.ascontiguousarray(np.minimum(self.signals / self.s0[:, None], 1.0))
+        rfs = mfod_model_responses()
+        weights = compute_shell_weights(self.gtab.bvals, 0.2)
+        b, g = self.gtab.bvals, self.gtab.bvecs
+        self.hr = Kernel(rfs, b, g, dirs=DIRS_300, weights=weights)
+        self.lr = Kernel(rfs, b, g, dirs=low_resolution_dirs(rfs, len(b)), weights=weights)
+        self.config = {"workload": self.name, "grid": [110, 110, 70], "voxels": self.v, "measurements": 280,
+                       "tissues": "WM (300 directions) + GM + CSF", "solver": "DRL (200 / 600 iterations)",
+                       "max_rounds": 50, "fraction_tol": self.fraction_tol, "l2": "inputs (1.1 GB) larger than L2"}
+
+    def device_setup(self, torch, dev):
+        from larmor_b200.sd.solvers import DRL, Stage
+
+        super().device_setup(torch, dev)
+        self.hr_solver = DRL()._prepare(self.hr, self.gtab.bvals, Stage.HIGH_RES)
+        self.lr_solver = DRL()._prepare(self.lr, self.gtab.bvals, Stage.LOW_RES)
+
+    def step_device(self, precision=0):
+        from larmor_b200 import _core
+
+        _core.fit_multi_tissue_device(self.d_signals, self.lr.weights, self.k_lr, self.lr_solver, self.k_hr,
+                                      self.hr_solver, 50, self.fraction_tol, 1e-2, self.d_fods, self.d_fr)
+
+    def kernel_bytes(self) -> dict:
+        """Algorithmic DRAM bytes of one step, per kernel. A voxel-round of the low-resolution
+        loop reads the 280 signals and writes 44 amplitudes, whose fractions read those and the
+        signals and write 3 fractions; the high-resolution pass does the same with 300
+        directions once per voxel. dRL's iterations stay on the chip: K^T K comes from L2."""
+        from larmor_b200 import _core
+
+        rounds = self.torch.zeros((self.v,), dtype=self.torch.int32, device=self.d_signals.device)
+        _core.fit_multi_tissue_device(self.d_signals, self.lr.weights, self.k_lr, self.lr_solver, self.k_hr,
+                                      self.hr_solver, 50, self.fraction_tol, 1e-2, self.d_fods, self.d_fr,
+                                      rounds=rounds)
+        vr = int(rounds.sum().item())
+        m, c_lr, c_hr = 280, self.k_lr.ca, self.k_hr.ca
+        return {"drl_kernel": vr * 8 * (m + c_lr) + self.v * 8 * (m + c_hr),
+                "lr_fractions_kernel": vr * 8 * (c_lr + m + 3),
+                "hr_fractions_kernel": self.v * 8 * (c_hr + m + 3)}
+
+    def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
+        from larmor_b200.sd.solvers import _rl_products
+        from oracle import oracle as o
+
+        if not hasattr(self, "_nus"):
+            # nu of each kernel as calibrate_drl_nu sets it, by the oracle's dRL.
+            b = self.gtab.bvals
+            signal = np.full((1, len(b)), np.exp(-max(b) * 0.7e-3))
+            self._nus = tuple(0.2 * float(np.max(o.drl(signal, *_rl_products(k.k), 0.0, 200, 1.0 / k.k.shape[1])))
+                              for k in (self.lr, self.hr))
+        n = min(self.v, 4 * threads)
+        lr = dict(k_aniso=self.lr.k_aniso, k_iso=self.lr.k_iso, w_k_iso=self.lr.w_k_iso, w_k_aniso=self.lr.w_k_aniso)
+        hr = dict(k_aniso=self.hr.k_aniso, k_iso=self.hr.k_iso, w_k_iso=self.hr.w_k_iso, w_k_aniso=self.hr.w_k_aniso,
+                  blocks=[(b.start, b.stop) for b in self.hr.aniso_blocks])
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget_s:
+            o.fit_multi_tissue(self.norm[:n], self.lr.weights, lr, hr, max_rounds=50, fraction_tol=self.fraction_tol,
+                               final_tol=1e-2, n_threads=threads,
+                               lr_drl={"nu": self._nus[0], "n_iter": 199, "init": 1e-6},
+                               hr_drl={"nu": self._nus[1], "n_iter": 599, "init": 1e-6})
+            done += n
+        return done, time.perf_counter() - t0, f"first {n} voxels of the volume, repeated for ~{budget_s:.0f} s"
+
+
 class PeaksWorkload:
     """FOD peaks (find_peaks, src/larmor/sd/peaks.py) of lmax-8 FODs on the config-3 mask
     (110x110x70, 500,040 voxels): the amplitudes of each FOD on the 642-vertex icosphere, then
@@ -942,7 +1025,7 @@ class PeaksWorkload:
 
 WORKLOADS = {"dti": DtiWorkload, "dki": DkiWorkload, "mfod": MfodWorkload, "msmt": MsmtWorkload,
              "batch": BatchWorkload, "peaks": PeaksWorkload, "dti_model": DtiModelWorkload, "csd": CsdWorkload,
-             "drl": DrlWorkload}
+             "drl": DrlWorkload, "grl": GrlWorkload}
 
 
 
