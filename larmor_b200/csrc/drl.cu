@@ -19,6 +19,9 @@
 // change is reduced in a fixed order, so the stopping test does not depend on the schedule.
 // Converged voxels keep their FOD while the tile's others iterate.
 //
+// Up to 64 directions the whole K^T K (at most 36 KB) is loaded once per CTA instead, and an
+// iteration needs one barrier; the CTA then fits in half an SM.
+//
 // The multi-tissue rounds (GRL, cpp/src/sd/multi_tissue.cpp:40-95) run the same solve on a list
 // of voxels whose signal is the anisotropic part max(s w - W_iso f_iso, 0) of the round.
 
@@ -41,6 +44,9 @@ constexpr int kNarrowRt = 4, kNarrowCt = 5;   // 32 voxels, c <= 320
 constexpr int kWideRt = 1, kWideCt = 10;      // 8 voxels, c <= 640
 constexpr int kNarrowMaxC = 8 * kDrlWarps * kNarrowCt;
 constexpr int kWideMaxC = 8 * kDrlWarps * kWideCt;
+// Up to 64 directions (the low-resolution kernels of the multi-tissue rounds) all of K^T K stays
+// in shared memory for the CTA's life: 32 voxels, one column tile per warp, two CTAs per SM.
+constexpr int kResidentMaxC = 8 * kDrlWarps;
 
 // Row strides (doubles) of F and K^T s, and of the K^T K stage, for cp columns: the padding puts
 // the 8 rows of an A fragment, and the 4 rows of a B fragment, in different banks.
@@ -84,8 +90,8 @@ __device__ __forceinline__ double signal_at(const DrlSignal& S, int64_t voxel, i
 
 // x(list[p], :) = the dRL FOD of voxel list[p] for p < count (min(count, *count_dev) when
 // count_dev is given); no list: voxel p itself.
-template <int RT, int MAXCT>
-__global__ void __launch_bounds__(kDrlWarps * 32, 1)
+template <int RT, int MAXCT, bool RESIDENT>
+__global__ void __launch_bounds__(kDrlWarps * 32, RESIDENT ? 2 : 1)
     drl_kernel(DrlDev P, DrlSignal S, const int* __restrict__ list, int64_t count, const int* __restrict__ count_dev,
                double* __restrict__ x, int64_t ldx) {
     constexpr int kRows = 8 * RT;
@@ -99,12 +105,20 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1)
     const int c = P.c, m = P.m, cp = (c + 7) / 8 * 8, n_ct = cp / 8, ldf = drl_ldf(cp), ldg = drl_ldg(cp);
     double* F = reinterpret_cast<double*>(smem);  // (kRows, ldf)
     double* KS = F + kRows * ldf;                 // (kRows, ldf)
-    double* GS = KS + kRows * ldf;                // (2, kDrlChunk, ldg): the K^T K stage
+    double* GS = KS + kRows * ldf;                // (2, kDrlChunk, ldg): the K^T K stage; resident: (cp, ldg)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const double nu8 = power_8(P.nu);
-    // The stage's columns past c stay 0.
-    for (int e = threadIdx.x; e < 2 * kDrlChunk * ldg; e += blockDim.x)
-        if (e % ldg >= c) GS[e] = 0.0;
+    if constexpr (RESIDENT) {
+        // All of K^T K, zero past c (made visible by the barrier at the first tile's start).
+        for (int e = threadIdx.x; e < cp * ldg; e += blockDim.x) {
+            const int k = e / ldg, d = e - k * ldg;
+            GS[e] = (k < c && d < c) ? P.gram[size_t(k) * c + d] : 0.0;
+        }
+    } else {
+        // The stage's columns past c stay 0.
+        for (int e = threadIdx.x; e < 2 * kDrlChunk * ldg; e += blockDim.x)
+            if (e % ldg >= c) GS[e] = 0.0;
+    }
     const int n_chunks = cp / kDrlChunk;
     // Rows [8 q, 8 q + 8) of K^T K into stage buffer b, one row per 32 threads: cp.async of 16
     // bytes when the rows are 16-byte aligned (c even; the stage's row stride is a multiple of 16
@@ -191,35 +205,50 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1)
             for (int rt = 0; rt < RT; ++rt)
 #pragma unroll
                 for (int t = 0; t < MAXCT; ++t) acc[rt][t][0] = acc[rt][t][1] = 0.0;
-            stage(0, 0);
-            for (int q = 0; q < n_chunks; ++q) {
-                if (q + 1 < n_chunks) {
-                    stage(q + 1, (q + 1) & 1);
-                    cp_async_wait<1>();
-                } else {
-                    cp_async_wait<0>();
-                }
-                __syncthreads();
-                const double* g = GS + (q & 1) * kDrlChunk * ldg;
+            if constexpr (RESIDENT) {
+                const int ct = warp;
+                if (ct < n_ct) {
+                    for (int k0 = 0; k0 < cp; k0 += 4) {
+                        const int kk = k0 + (lane & 3);
+                        const double b = GS[kk * ldg + 8 * ct + (lane >> 2)];
 #pragma unroll
-                for (int ks = 0; ks < kDrlChunk; ks += 4) {
-                    const int kk = q * kDrlChunk + ks + (lane & 3);
-                    const double* grow = g + (ks + (lane & 3)) * ldg + (lane >> 2);
-                    double a[RT];
-#pragma unroll
-                    for (int rt = 0; rt < RT; ++rt) a[rt] = F[(8 * rt + (lane >> 2)) * ldf + kk];
-#pragma unroll
-                    for (int t = 0; t < MAXCT; ++t) {
-                        const int ct = warp + kDrlWarps * t;
-                        if (ct < n_ct) {
-                            const double b = grow[8 * ct];
-#pragma unroll
-                            for (int rt = 0; rt < RT; ++rt) mma_f64(acc[rt][t][0], acc[rt][t][1], a[rt], b);
-                        }
+                        for (int rt = 0; rt < RT; ++rt)
+                            mma_f64(acc[rt][0][0], acc[rt][0][1], F[(8 * rt + (lane >> 2)) * ldf + kk], b);
                     }
                 }
-                // The next stage overwrites this buffer: every warp is done with it first.
+                // The update overwrites F: every warp is done reading it first.
                 __syncthreads();
+            } else {
+                stage(0, 0);
+                for (int q = 0; q < n_chunks; ++q) {
+                    if (q + 1 < n_chunks) {
+                        stage(q + 1, (q + 1) & 1);
+                        cp_async_wait<1>();
+                    } else {
+                        cp_async_wait<0>();
+                    }
+                    __syncthreads();
+                    const double* g = GS + (q & 1) * kDrlChunk * ldg;
+#pragma unroll
+                    for (int ks = 0; ks < kDrlChunk; ks += 4) {
+                        const int kk = q * kDrlChunk + ks + (lane & 3);
+                        const double* grow = g + (ks + (lane & 3)) * ldg + (lane >> 2);
+                        double a[RT];
+#pragma unroll
+                        for (int rt = 0; rt < RT; ++rt) a[rt] = F[(8 * rt + (lane >> 2)) * ldf + kk];
+#pragma unroll
+                        for (int t = 0; t < MAXCT; ++t) {
+                            const int ct = warp + kDrlWarps * t;
+                            if (ct < n_ct) {
+                                const double b = grow[8 * ct];
+#pragma unroll
+                                for (int rt = 0; rt < RT; ++rt) mma_f64(acc[rt][t][0], acc[rt][t][1], a[rt], b);
+                            }
+                        }
+                    }
+                    // The next stage overwrites this buffer: every warp is done with it first.
+                    __syncthreads();
+                }
             }
             // The damped update of the still-active voxels, and each one's total change.
             double change[RT];
@@ -270,10 +299,10 @@ __global__ void __launch_bounds__(kDrlWarps * 32, 1)
     }
 }
 
-template <int RT, int MAXCT>
+template <int RT, int MAXCT, bool RESIDENT>
 void launch_variant(const DrlDev& P, const DrlSignal& S, const int* list, int64_t count, const int* count_dev,
                     double* x, int64_t ldx, cudaStream_t st, const char* name) {
-    auto kernel = drl_kernel<RT, MAXCT>;
+    auto kernel = drl_kernel<RT, MAXCT, RESIDENT>;
     const size_t smem = drl_smem_bytes(P.c);
     cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                "cudaFuncSetAttribute");
@@ -292,6 +321,7 @@ void launch_variant(const DrlDev& P, const DrlSignal& S, const int* list, int64_
 
 size_t drl_smem_bytes(int c) {
     const int cp = (c + 7) / 8 * 8;
+    if (c <= kResidentMaxC) return (2 * size_t(8 * kNarrowRt) * drl_ldf(cp) + size_t(cp) * drl_ldg(cp)) * sizeof(double);
     const size_t rows = c <= kNarrowMaxC ? 8 * kNarrowRt : 8 * kWideRt;
     return (2 * rows * drl_ldf(cp) + 2 * size_t(kDrlChunk) * drl_ldg(cp)) * sizeof(double);
 }
@@ -301,10 +331,12 @@ bool drl_fits(int c) { return c >= 1 && c <= kWideMaxC; }
 void launch_drl_listed(const DrlDev& P, const DrlSignal& S, const int* list, int64_t count, const int* count_dev,
                        double* x, int64_t ldx, cudaStream_t st) {
     if (count == 0) return;
-    if (P.c <= kNarrowMaxC)
-        launch_variant<kNarrowRt, kNarrowCt>(P, S, list, count, count_dev, x, ldx, st, "drl_kernel");
+    if (P.c <= kResidentMaxC)
+        launch_variant<kNarrowRt, 1, true>(P, S, list, count, count_dev, x, ldx, st, "drl_kernel_resident");
+    else if (P.c <= kNarrowMaxC)
+        launch_variant<kNarrowRt, kNarrowCt, false>(P, S, list, count, count_dev, x, ldx, st, "drl_kernel");
     else
-        launch_variant<kWideRt, kWideCt>(P, S, list, count, count_dev, x, ldx, st, "drl_kernel_wide");
+        launch_variant<kWideRt, kWideCt, false>(P, S, list, count, count_dev, x, ldx, st, "drl_kernel_wide");
 }
 
 void launch_drl(const DrlDev& P, const double* signals, int64_t v, double* fods, cudaStream_t st) {
