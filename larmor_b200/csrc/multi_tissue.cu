@@ -1125,11 +1125,17 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
         require(lr && hr && lr_solver && hr_solver, "kernels and solvers must not be NULL");
         require(weights != nullptr, "weights must not be NULL");
         const int64_t m = hr->m;
-        require(lr->m == m && lr_solver->host.m == m && hr_solver->host.m == m,
-                "signals, weights and the kernels' measurements do not match");
+        require(lr->m == m, "signals, weights and the kernels' measurements do not match");
         require(lr->ci == hr->ci, "the two kernels have different numbers of isotropic tissues");
-        require(lr_solver->host.c == lr->ca, "the low-resolution solver does not match its kernel");
-        require(hr_solver->host.c == hr->ca, "the high-resolution solver does not match its kernel");
+        // require_matching_solver (cpp/src/python/sd.cpp:294-307), with its message.
+        auto matching = [m](const char* name, const lar_deconv_kernel_s& k, const lar_fod_solver_s& sv) {
+            require(sv.host.c == k.ca && sv.host.m == m,
+                    std::string("the ") + name + " solver (" + std::to_string(sv.host.c) + " directions, " +
+                        std::to_string(sv.host.m) + " measurements) does not match its kernel (" +
+                        std::to_string(k.ca) + " directions, " + std::to_string(m) + " measurements)");
+        };
+        matching("low-resolution", *lr, *lr_solver);
+        matching("high-resolution", *hr, *hr_solver);
         require(max_outer >= 0, "max_outer must be at least 0");
         require(v >= 0, "v must be at least 0");
         if (v == 0) return;

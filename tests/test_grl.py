@@ -217,3 +217,40 @@ def test_gpu_grl_sd_model_matches_the_oracle(cuda, oracle):
     # The maps are float32, as the reference's.
     np.testing.assert_allclose(fit.fods[0].reshape(-1, ref_sh.shape[1]), ref_sh, rtol=1e-5, atol=1e-6)
     np.testing.assert_allclose(fit.tissue_fractions.reshape(-1, 3), rfr, rtol=0, atol=1e-6)
+
+
+@pytest.mark.gpu
+def test_gpu_grl_does_not_depend_on_thread_count(cuda, grl_fixture):
+    """tests/sd/test_grl.py:152-161: the fit is the same bit for bit for any n_threads."""
+    from larmor_b200 import _core
+
+    z = grl_fixture
+    lr, lr_solver, hr, hr_solver = _device_case(z, "matlab", float(z["matlab_lr_nu"]), float(z["matlab_hr_nu"]))
+    signals = np.ascontiguousarray(z["matlab_signals"])
+    one = _core.fit_multi_tissue(signals, z["weights"], lr, lr_solver, hr, hr_solver, 50, GRL_FRACTION_TOL, 1e-2, 1)
+    for n_threads in (2, 7):
+        got = _core.fit_multi_tissue(signals, z["weights"], lr, lr_solver, hr, hr_solver, 50, GRL_FRACTION_TOL, 1e-2,
+                                     n_threads)
+        np.testing.assert_array_equal(got[0], one[0])
+        np.testing.assert_array_equal(got[1], one[1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize(("mismatch", "resolution"),
+                         [("directions", "low-resolution"), ("measurements", "high-resolution")])
+def test_gpu_grl_refuses_a_solver_that_does_not_match_its_kernel(cuda, grl_fixture, mismatch, resolution):
+    """tests/sd/test_grl.py:316-335: a dRL solver with another kernel's directions, or one
+    measurement short, is refused with the reference's message."""
+    from larmor_b200 import _core
+
+    z = grl_fixture
+    lr, lr_solver, hr, hr_solver = _device_case(z, "matlab", float(z["matlab_lr_nu"]), float(z["matlab_hr_nu"]))
+    if mismatch == "directions":
+        lr_solver = hr_solver  # 300 directions against the low-resolution kernel's 33
+    else:
+        k = z["matlab_hr_w_k_aniso"][:-1]
+        hr_solver = _core.FodSolver.drl(np.ascontiguousarray(k.T), np.ascontiguousarray(k.T @ k), nu=0.01,
+                                        n_iter=10, init=0.1)
+    with pytest.raises(ValueError, match=f"the {resolution} solver .* does not match its kernel"):
+        _core.fit_multi_tissue(np.ascontiguousarray(z["matlab_signals"]), z["weights"], lr, lr_solver, hr,
+                               hr_solver, 50, GRL_FRACTION_TOL, 1e-2, 1)
