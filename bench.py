@@ -441,13 +441,18 @@ class MfodWorkload(_SdWorkloadBase):
                        "tissues": "WM (lmax 8 output, 300 directions) + GM + CSF", "max_rounds": 50,
                        "fraction_tol": 1e-7, "l2": "inputs (1.1 GB) larger than L2"}
 
+    def sd_solver(self):
+        from larmor_b200.sd.solvers import L2NNLS
+
+        return L2NNLS()
+
     def device_setup(self, torch, dev):
-        from larmor_b200.sd.solvers import L2NNLS, Stage, _deconv_kernel
+        from larmor_b200.sd.solvers import Stage, _deconv_kernel
 
         self.torch = torch
         self.k_lr, self.k_hr = _deconv_kernel(self.lr), _deconv_kernel(self.hr)
-        self.hr_solver = L2NNLS()._prepare(self.hr, self.gtab.bvals, Stage.HIGH_RES)
-        self.lr_solver = L2NNLS()._prepare(self.lr, self.gtab.bvals, Stage.LOW_RES)
+        self.hr_solver = self.sd_solver()._prepare(self.hr, self.gtab.bvals, Stage.HIGH_RES)
+        self.lr_solver = self.sd_solver()._prepare(self.lr, self.gtab.bvals, Stage.LOW_RES)
         self.d_signals = torch.from_numpy(self.norm).to(dev)
         self.d_fods = torch.empty((self.v, self.k_hr.ca), dtype=torch.float64, device=dev)
         self.d_fr = torch.empty((self.v, 3), dtype=torch.float64, device=dev)
@@ -855,12 +860,10 @@ class GrlWorkload(MfodWorkload):
                        "tissues": "WM (300 directions) + GM + CSF", "solver": "DRL (200 / 600 iterations)",
                        "max_rounds": 50, "fraction_tol": self.fraction_tol, "l2": "inputs (1.1 GB) larger than L2"}
 
-    def device_setup(self, torch, dev):
-        from larmor_b200.sd.solvers import DRL, Stage
+    def sd_solver(self):
+        from larmor_b200.sd.solvers import DRL
 
-        super().device_setup(torch, dev)
-        self.hr_solver = DRL()._prepare(self.hr, self.gtab.bvals, Stage.HIGH_RES)
-        self.lr_solver = DRL()._prepare(self.lr, self.gtab.bvals, Stage.LOW_RES)
+        return DRL()
 
     def step_device(self, precision=0):
         from larmor_b200 import _core
