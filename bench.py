@@ -45,6 +45,20 @@ def peaks() -> tuple[dict, str]:
     return {"hbm_gbs": FALLBACK_HBM_GBS, "bf16_tflops": 1590.0}, "fallback"
 
 
+# Nominal dense FP64 tensor-core rate of one B200 (NVIDIA's HGX B200 figure, TFLOP/s): the
+# denominator for the FP64 tensor-core kernels, which the measured peaks (an HBM copy and a bf16
+# GEMM) do not cover.
+NOMINAL_FP64_TENSOR_TFLOPS = 37.0
+
+
+def fp64_tensor_roofline(flops_per_launch: float, avg_launch_s: float) -> dict:
+    """The roofline fields of a kernel bound by the FP64 tensor cores."""
+    achieved = flops_per_launch / avg_launch_s / 1e12 if avg_launch_s > 0 else 0.0
+    return {"bound": "tensor", "achieved": achieved, "peak": NOMINAL_FP64_TENSOR_TFLOPS, "unit": "TFLOP/s",
+            "frac": achieved / NOMINAL_FP64_TENSOR_TFLOPS, "peak_source": "nominal FP64 tensor rate",
+            "algorithmic_flops_per_launch": flops_per_launch}
+
+
 def committed_traffic(kernel: str, workload: str, algorithmic_bytes: float) -> float | None:
     """Per-launch DRAM bytes of a kernel: the measured DRAM bytes per algorithmic byte of its
     committed ncu capture (profiles/traffic.json, a smaller case of the same workload) times
@@ -810,6 +824,12 @@ class DrlWorkload(_SdWorkloadBase):
         """Algorithmic DRAM bytes of one step: 280 signals in, 300 amplitudes out per voxel."""
         return {"drl_kernel": self.v * 8 * (280 + 300)}
 
+    flops_basis = "2 c^2 FLOP per voxel-iteration (the prediction F K^T K), 200 iterations per voxel (the cap)"
+
+    def kernel_flops(self) -> dict:
+        """FP64 FLOP of one step at the iteration cap: 2 x 300^2 per voxel-iteration."""
+        return {"drl_kernel": self.v * 200 * 2 * 300 ** 2}
+
     def step_e2e(self):
         self.d_signals.copy_(self.h_signals, non_blocking=True)
         self.step_device()
@@ -883,11 +903,19 @@ class GrlWorkload(MfodWorkload):
         _core.fit_multi_tissue_device(self.d_signals, self.lr.weights, self.k_lr, self.lr_solver, self.k_hr,
                                       self.hr_solver, 50, self.fraction_tol, 1e-2, self.d_fods, self.d_fr,
                                       rounds=rounds)
-        vr = int(rounds.sum().item())
+        vr = self._voxel_rounds = int(rounds.sum().item())
         m, c_lr, c_hr = 280, self.k_lr.ca, self.k_hr.ca
         return {"drl_kernel_resident": vr * 8 * (m + c_lr), "drl_kernel": self.v * 8 * (m + c_hr),
                 "lr_fractions_kernel": vr * 8 * (c_lr + m + 3),
                 "hr_fractions_kernel": self.v * 8 * (c_hr + m + 3)}
+
+    flops_basis = ("2 c^2 FLOP per voxel-iteration (the prediction F K^T K) at the iteration caps: 599 per "
+                   "voxel at 300 directions, 199 per voxel-round at 44")
+
+    def kernel_flops(self) -> dict:
+        """FP64 FLOP of one step at the iteration caps (the voxel-rounds from kernel_bytes)."""
+        return {"drl_kernel": self.v * 599 * 2 * self.k_hr.ca ** 2,
+                "drl_kernel_resident": self._voxel_rounds * 199 * 2 * self.k_lr.ca ** 2}
 
     def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
         from larmor_b200.sd.solvers import _rl_products
@@ -1337,6 +1365,13 @@ def main() -> int:
         "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
+    if hasattr(wl, "kernel_flops"):
+        # FP64 tensor-core kernels: FLOP over the nominal FP64 tensor rate; the HBM bytes stay
+        # beside it.
+        flops = wl.kernel_flops().get(top)
+        if flops is not None:
+            line["roofline"].update(fp64_tensor_roofline(flops * args.steps / max(top_launches, 1), avg_launch_s))
+            line["roofline"]["flops_basis"] = wl.flops_basis
     if hasattr(wl, "extra"):
         def timed_host(step):
             for _ in range(args.warmup):
