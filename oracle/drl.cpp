@@ -55,10 +55,13 @@ void solve(const double* k_t, const double* gram, int c, int m, double nu, int n
         ks[size_t(d)] = acc;
     }
     for (int it = 0; it < n_iter; ++it) {
-        for (int d = 0; d < c; ++d) {
-            double acc = 0.0;
-            for (int q = 0; q < c; ++q) acc += fod[q] * gram[size_t(q) * c + d];
-            pred[size_t(d)] = acc;
+        // pred = (K^T K) f, each entry summed over q in increasing order from 0; q outer, so that
+        // the inner loop runs over independent entries.
+        std::fill(pred.begin(), pred.end(), 0.0);
+        for (int q = 0; q < c; ++q) {
+            const double fq = fod[q];
+            const double* row = gram + size_t(q) * c;
+            for (int d = 0; d < c; ++d) pred[size_t(d)] += fq * row[d];
         }
         double change = 0.0;
         for (int d = 0; d < c; ++d) {
