@@ -32,14 +32,8 @@ from larmor_b200.sd.rf import IsotropicRF  # noqa: E402
 from larmor_b200 import _core  # noqa: E402
 from larmor_b200.sd.sh import BASES, build_basis_matrix, fit_sh  # noqa: E402
 from larmor_b200.sd.sphere import DIRS_300, get_dirs, get_theta_phi  # noqa: E402
-
-SHELL_TOLERANCE = 100.0
-# The relative peak threshold of SDModel's FODs (their truncation leaves side lobes).
-SD_MODEL_PEAK_RELATIVE_THRESHOLD = 0.2
-
-
-def shell_mask(bvals: np.ndarray, shell: float, *, tol: float = SHELL_TOLERANCE) -> np.ndarray:
-    return np.abs(bvals - shell) < tol
+from larmor_b200.dwi.shells import SHELL_TOLERANCE, shell_mask  # noqa: E402,F401
+from larmor_b200.sd.peaks import SD_MODEL_PEAK_RELATIVE_THRESHOLD  # noqa: E402
 
 
 def compute_max_lmax(bvals: np.ndarray, proposed_lmax: int) -> int:

@@ -13,10 +13,9 @@ from typing import ClassVar
 import numpy as np
 from scipy.special import eval_legendre
 
+# SHELL_TOLERANCE: a b-value belongs to a response's shell within this distance.
+from larmor_b200.dwi.shells import SHELL_TOLERANCE
 from larmor_b200.sd.sphere import get_theta_phi
-
-# A b-value belongs to a response's shell within this distance (src/larmor/dwi/shells.py:7).
-SHELL_TOLERANCE = 100.0
 
 
 @dataclass

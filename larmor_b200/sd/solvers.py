@@ -106,6 +106,11 @@ class DRL:
         return _core.FodSolver.drl(k_t, k_t_k, nu=nu, n_iter=n_iter - 1, init=MULTI_TISSUE_DRL_INIT)
 
 
+# The FOD solvers SDModel takes (src/larmor/sd/solvers.py:296, without the elastic net, which
+# this package does not include).
+type SDSolver = DRL | L2NNLS
+
+
 def _deconv_kernel(kernel: Kernel) -> _core.DeconvKernel:
     return _core.DeconvKernel(
         np.ascontiguousarray(kernel.k_aniso),
