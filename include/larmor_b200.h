@@ -230,6 +230,15 @@ int lar_fit_multi_tissue_async(const double* signals, int64_t v, const double* w
                                int64_t max_outer, double fraction_tol, double final_tol_x, double* fods,
                                double* fractions, int32_t* rounds, uint8_t* status, void* stream);
 
+/* Solves one non-negative least-squares problem, min ||c x - d|| over x >= 0, for c (m, n)
+ * row-major and d (m,), device doubles, by Lawson-Hanson with QR fits and at most 3 n inner
+ * steps (the fraction fits' solver). A column enters only when its gradient exceeds tol_x; with
+ * default_tol != 0, tol_x = 10 eps norm1(c) max(m, n) instead. Writes x (n,) (device double).
+ * m >= 1, 1 <= n <= 16. Replaces larmor._core.lsqnonneg (cpp/src/python/sd.cpp:208-228,
+ * cpp/src/sd/nnls.cpp:187-258). */
+int lar_lsqnonneg(const double* c, int64_t m, int64_t n, const double* d, int default_tol, double tol_x, double* x,
+                  void* stream);
+
 /* The FOD (v, c) of every row of signals (v, m) (device double) with one L2NNLS solver.
  * Replaces larmor._core.fit_single_tissue (cpp/src/python/sd.cpp, cpp/src/sd/solver.cpp:422). */
 int lar_fit_single_tissue(const double* signals, int64_t v, lar_fod_solver solver, double* fods,

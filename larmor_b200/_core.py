@@ -448,6 +448,39 @@ def fit_multi_tissue_device(signals, weights, lr, lr_solver, hr, hr_solver, max_
         _lib.ptr(fractions), _lib.ptr(rounds), _lib.ptr(status), _stream(torch)))
 
 
+def lsqnonneg(c, d, tol_x=None):
+    """Solves one non-negative least-squares problem, min ||c x - d|| with x >= 0, on the device
+    (cpp/src/python/sd.cpp:208-228): c is (m, n) and d (m,); a coefficient enters the solution
+    only when its gradient exceeds tol_x, None using 10 * eps * norm(c, 1) * max(m, n).
+
+    Raises:
+        TypeError: If c or d is not a float64 numpy array.
+        ValueError: If c is not C-contiguous, the shapes do not match, or c has more than 16
+            columns.
+    """
+    c = _array(c, "c", 2)
+    if not isinstance(d, np.ndarray) or d.dtype != np.float64:
+        raise TypeError(f"d must be a float64 numpy array, got {getattr(d, 'dtype', type(d).__name__)}")
+    if d.ndim != 1 or d.shape[0] != c.shape[0]:
+        raise ValueError(f"c must be (m, n) and d (m,): got ({c.shape[0]}, {c.shape[1]}) and "
+                         f"{d.shape[0] if d.ndim == 1 else d.shape}")
+    m, n = c.shape
+    if n > 16:
+        raise ValueError(f"lsqnonneg takes at most 16 columns, got {n}")
+    if n == 0:
+        return np.zeros(0)
+    if m == 0:
+        raise ValueError("c must have at least one row")
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    dc = torch.from_numpy(c).to(dev)
+    dd = torch.from_numpy(np.ascontiguousarray(d)).to(dev)
+    x = torch.empty(n, dtype=torch.float64, device=dev)
+    _lib.check(_lib.lib().lar_lsqnonneg(_lib.ptr(dc), m, n, _lib.ptr(dd), int(tol_x is None),
+                                        0.0 if tol_x is None else float(tol_x), _lib.ptr(x), _stream(torch)))
+    return x.cpu().numpy()
+
+
 def fit_single_tissue(signals, solver: FodSolver, n_threads):
     """The FOD (n, c) of every row of signals (n, m) with one solver."""
     signals = _array(signals, "signals", 2)

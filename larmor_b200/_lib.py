@@ -42,6 +42,7 @@ SIGNATURES: dict[str, tuple] = {
     "lar_deconv_kernel_destroy": (None, [_p]),
     "lar_fit_multi_tissue": (_i32, [_p, _i64, _p, _p, _p, _p, _p, _i64, _f64, _f64, _p, _p, _p, _p, _p]),
     "lar_fit_multi_tissue_async": (_i32, [_p, _i64, _p, _p, _p, _p, _p, _i64, _f64, _f64, _p, _p, _p, _p, _p]),
+    "lar_lsqnonneg": (_i32, [_p, _i64, _i64, _p, _i32, _f64, _p, _p]),
     "lar_fit_single_tissue": (_i32, [_p, _i64, _p, _p, _p, _p]),
     "lar_sh_projector_create": (_i32, [_p, _i64, _i64, _p]),
     "lar_sh_projector_destroy": (None, [_p]),

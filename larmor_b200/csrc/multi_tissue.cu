@@ -1050,6 +1050,30 @@ inline void launch_correlate(const SignalDev& S, const int* list, int64_t count,
     cuda_check(cudaGetLastError(), "correlate_kernel launch");
 }
 
+// lsqnonneg (cpp/src/python/sd.cpp:208-228): one warp solves min ||c x - d|| over x >= 0 for c
+// (m, n) row-major by the fraction fits' Lawson-Hanson with QR fits (cpp/src/sd/nnls.cpp:187-258),
+// at most 3 n inner steps. default_tol: tol = 10 eps norm1(c) max(m, n) (nnls.cpp:177-181).
+__global__ void __launch_bounds__(32) lsqnonneg_kernel(const double* __restrict__ c, int m, int n,
+                                                       const double* __restrict__ d, bool default_tol, double tol,
+                                                       double* __restrict__ x, double* __restrict__ workspace) {
+    __shared__ FracState st;
+    const int lane = threadIdx.x;
+    const FracSlot sl = carve_frac(workspace, m, 0, n);
+    if (default_tol) {
+        double colmax = 0.0;
+        for (int g = 0; g < n; ++g) {
+            double sum = 0.0;
+            for (int i = lane; i < m; i += 32) sum += fabs(c[size_t(i) * n + g]);
+            colmax = fmax(colmax, warp_sum(sum));
+        }
+        tol = 10.0 * kEps64 * colmax * double(max(m, n));
+    }
+    NnlsScratch ns{sl.fu, sl.fz, sl.fflag, st.fact, &st.fn_act, sl.res,
+                   QrScratch{sl.fsub, st.ftau, st.fnu, st.fnd, st.fperm, sl.frv}, kMaxGroups};
+    warp_nnls_explicit(c, m, n, d, tol, 3 * n, ns, lane);
+    for (int g = lane; g < n; g += 32) x[g] = sl.fu[g];
+}
+
 }  // namespace
 
 }  // namespace lar
@@ -1320,6 +1344,24 @@ int lar_fit_multi_tissue_async(const double* signals, int64_t v, const double* w
                                double* fractions, int32_t* rounds, uint8_t* status, void* stream) {
     return fit_multi_tissue(signals, v, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol, final_tol_x,
                             fods, fractions, rounds, status, stream, true);
+}
+
+int lar_lsqnonneg(const double* c, int64_t m, int64_t n, const double* d, int default_tol, double tol_x, double* x,
+                  void* stream) {
+    return guarded([&] {
+        require(m >= 1 && n >= 1 && n <= kMaxGroups, "lsqnonneg takes c of (m, n), m >= 1, 1 <= n <= 16");
+        require(c && d && x, "c, d and x must not be NULL");
+        auto st = static_cast<cudaStream_t>(stream);
+        double* ws = nullptr;
+        const size_t bytes = frac_slot_doubles(int(m), 0, int(n)) * sizeof(double);
+        cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&ws), bytes, st), "cudaMallocAsync");
+        {
+            LaunchScope scope("lsqnonneg_kernel", st);
+            lsqnonneg_kernel<<<1, 32, 0, st>>>(c, int(m), int(n), d, default_tol != 0, tol_x, x, ws);
+            cuda_check(cudaGetLastError(), "lsqnonneg_kernel launch");
+        }
+        cuda_check(cudaFreeAsync(ws, st), "cudaFreeAsync");
+    });
 }
 
 

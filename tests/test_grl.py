@@ -254,3 +254,83 @@ def test_gpu_grl_refuses_a_solver_that_does_not_match_its_kernel(cuda, grl_fixtu
     with pytest.raises(ValueError, match=f"the {resolution} solver .* does not match its kernel"):
         _core.fit_multi_tissue(np.ascontiguousarray(z["matlab_signals"]), z["weights"], lr, lr_solver, hr,
                                hr_solver, 50, GRL_FRACTION_TOL, 1e-2, 1)
+
+
+# ---- lsqnonneg (the fraction fits' NNLS, one problem) --------------------------------------
+
+
+def _fraction_problems():
+    """tests/sd/test_grl.py:165-177: 200 seeded problems of 2-6 decaying-exponential columns on
+    32 measurements (b = 0, 1000, 2000, 3000 x 8), a third of the true fractions 0, plus noise."""
+    rng = np.random.default_rng(1)
+    b = np.repeat([0.0, 1000.0, 2000.0, 3000.0], 8)
+    problems = []
+    for _ in range(200):
+        n = int(rng.integers(2, 7))
+        c = np.exp(-np.outer(b, np.sort(rng.uniform(0.1e-3, 3e-3, n))))
+        x = rng.dirichlet(np.ones(n))
+        x[rng.random(n) < 0.3] = 0.0
+        d = c @ x + rng.uniform(0.0, 0.02) * rng.standard_normal(len(b))
+        problems.append((np.ascontiguousarray(c), d))
+    return problems
+
+
+def test_oracle_nnls_matches_scipy_on_the_fraction_problems(oracle):
+    """The oracle's solve_nnls against scipy's nnls at the reference's bound (atol 1e-10)."""
+    from scipy.optimize import nnls
+
+    for c, d in _fraction_problems():
+        x, _ = oracle.nnls(c, d)
+        expected, _ = nnls(c, d)
+        np.testing.assert_array_equal(x == 0, expected == 0)
+        np.testing.assert_allclose(x, expected, rtol=0, atol=1e-10)
+
+
+def test_lsqnonneg_refuses_bad_arguments():
+    """tests/sd/test_grl.py:223-225, and the binding's type and width checks (before any
+    device work)."""
+    from larmor_b200 import _core
+
+    with pytest.raises(ValueError, match="c must be"):
+        _core.lsqnonneg(np.ones((32, 3)), np.ones(31))
+    with pytest.raises(TypeError):
+        _core.lsqnonneg(np.ones((32, 3), dtype=np.float32), np.ones(32))
+    with pytest.raises(ValueError, match="C-contiguous"):
+        _core.lsqnonneg(np.asfortranarray(np.ones((32, 3))), np.ones(32))
+    with pytest.raises(ValueError, match="at most 16 columns"):
+        _core.lsqnonneg(np.ones((32, 17)), np.ones(32))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize(("against", "tol_x", "atol"), [("scipy", None, 1e-10), ("oracle", None, 1e-10),
+                                                        ("oracle", 1e-2, 1e-13)])
+def test_gpu_lsqnonneg_matches_the_reference_nnls(cuda, oracle, against, tol_x, atol):
+    """tests/sd/test_grl.py:185-208: the same zero coefficients and values within atol, against
+    scipy (exact NNLS) and the oracle's solve_nnls (MATLAB's TolX rule)."""
+    from scipy.optimize import nnls
+
+    from larmor_b200 import _core
+
+    n_zeros = 0
+    for c, d in _fraction_problems():
+        x = _core.lsqnonneg(c, d, tol_x)
+        expected = nnls(c, d)[0] if against == "scipy" else oracle.nnls(c, d, tol_x)[0]
+        np.testing.assert_array_equal(x == 0, expected == 0)
+        np.testing.assert_allclose(x, expected, rtol=0, atol=atol)
+        n_zeros += int((x == 0).sum())
+    assert n_zeros > 0
+
+
+@pytest.mark.gpu
+def test_gpu_lsqnonneg_tol_x_zeroes_a_small_coefficient(cuda):
+    """tests/sd/test_grl.py:211-220: a 0.5% compartment is kept at the default TolX and dropped
+    at 1e-2."""
+    from larmor_b200 import _core
+
+    b = np.repeat([0.0, 1000.0, 2000.0, 3000.0], 8)
+    c = np.ascontiguousarray(np.exp(-np.outer(b, [0.7e-3, 3e-3])))
+    d = c @ np.array([0.995, 0.005])
+    assert (_core.lsqnonneg(c, d) > 0).all()
+    x = _core.lsqnonneg(c, d, 1e-2)
+    assert x[1] == 0
+    np.testing.assert_allclose(x[0], 1.0, atol=1e-2)
