@@ -59,6 +59,19 @@ def test_oracle_matches_the_reference_restatement(oracle, grl_fixture, name):
     _check(fods, fractions, z[f"{name}_fods"][rows], z[f"{name}_fractions"][rows])
 
 
+def test_oracle_grl_does_not_depend_on_thread_count(oracle, grl_fixture):
+    """The oracle's GRL of 48 MATLAB voxels, the same bit for bit on 1 and 5 threads."""
+    z = grl_fixture
+    kw = dict(max_rounds=50, fraction_tol=GRL_FRACTION_TOL, final_tol=1e-2,
+              lr_drl={"nu": float(z["matlab_lr_nu"]), "n_iter": LR_ITER - 1, "init": MULTI_TISSUE_INIT},
+              hr_drl={"nu": float(z["matlab_hr_nu"]), "n_iter": HR_ITER - 1, "init": MULTI_TISSUE_INIT})
+    args = (z["matlab_signals"][:48], z["weights"], _kernel(z, "matlab", "lr"), _kernel(z, "matlab", "hr"))
+    one = oracle.fit_multi_tissue(*args, n_threads=1, **kw)
+    five = oracle.fit_multi_tissue(*args, n_threads=5, **kw)
+    np.testing.assert_array_equal(one[0], five[0])
+    np.testing.assert_array_equal(one[1], five[1])
+
+
 def test_fixture_cases_cover_zero_fractions_and_two_fibre_blocks(grl_fixture):
     """tests/sd/test_grl.py:144-149: the synthetic voxels zero some tissues, and the final fit of
     the two-response kernel has one fraction per block."""
