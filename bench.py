@@ -70,6 +70,43 @@ def committed_traffic(kernel: str, workload: str, algorithmic_bytes: float) -> f
     return None if entry is None else float(entry["dram_per_algorithmic_byte"]) * algorithmic_bytes
 
 
+# The GPU arm prepares each synthetic volume's inputs with the product's device staging
+# (stage_dwi); the CPU reference arm, which runs no GPU code, with the oracle's numpy staging.
+# Both give the same float32 signals, and S0 and floors to 1e-13.
+REFERENCE_ARM = False
+
+
+def staged_inputs(w):
+    """The mask voxels' float32 signals (v, N), S0 (v) and floors (v) of a synthetic volume."""
+    if REFERENCE_ARM:
+        from oracle import staging
+
+        st = staging.stage(w.volume.data, w.volume.slope, w.volume.intercept, w.gtab.b0_mask, w.mask)
+        return st["signals"], st["s0"], st["floor"]
+    from larmor_b200.dwi.inputs import stage_dwi
+
+    st = stage_dwi(w.volume, w.gtab, w.mask)
+    return st.signals.cpu().numpy(), st.s0.cpu().numpy(), st.floor.cpu().numpy()
+
+
+def strided(v: int, n: int) -> np.ndarray:
+    """n voxel indices spread evenly over the whole volume (every voxel when v <= n)."""
+    return np.arange(v) if v <= n else np.linspace(0, v - 1, n).round().astype(np.int64)
+
+
+def tensor_fa_md(dt: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """FA and MD of tensors given as (v, 6) in the order xx, xy, xz, yy, yz, zz, by numpy's eigh
+    (the reference's compute_dti_metrics, src/larmor/dwi/dti.py:170-235)."""
+    xx, xy, xz, yy, yz, zz = dt.T
+    t = np.stack([np.stack([xx, xy, xz], -1), np.stack([xy, yy, yz], -1), np.stack([xz, yz, zz], -1)], -2)
+    ev = np.linalg.eigvalsh(t)
+    md = ev.mean(axis=1)
+    num = np.sqrt(((ev[:, 0] - ev[:, 1]) ** 2 + (ev[:, 1] - ev[:, 2]) ** 2 + (ev[:, 2] - ev[:, 0]) ** 2))
+    den = np.sqrt((ev ** 2).sum(axis=1))
+    fa = np.where(den > 1e-12, np.sqrt(0.5) * num / np.where(den > 1e-12, den, 1.0), 0.0)
+    return np.clip(fa, 0.0, 1.0), md
+
+
 # ---- clocks ------------------------------------------------------------------------------
 
 class ClockSampler:
@@ -128,7 +165,9 @@ class ClockSampler:
 # ---- workloads ---------------------------------------------------------------------------
 
 class DtiWorkload:
-    """Config 1: DTI WLLS on the 64x64x40 volume (79,912 voxels, 1 b0 + 30 directions)."""
+    """Config 1: DTI WLLS on the 64x64x40 volume (79,912 voxels, 1 b0 + 30 directions). value:
+    the fused fit and maps with the staged signals resident; e2e: the public model call
+    DTIModel(fit_method="wls").fit(volume, gtab, mask), raw host volume in, host maps out."""
 
     name = "dti_wlls_64x64x40"
     kernels = ("fit_dti_maps_kernel",)
@@ -139,21 +178,24 @@ class DtiWorkload:
 
     def __init__(self, seed: int) -> None:
         from larmor_b200.dwi.dti import dti_design
-        from larmor_b200.dwi.inputs import estimate_s0, masked_signals, sample_floors
         from larmor_b200.synthetic import dti_volume
 
-        w = dti_volume(seed=seed)
+        w = self.w = dti_volume(seed=seed)
+        self.mask = w.mask
         self.config = {"workload": self.name, "grid": [64, 64, 40], "voxels": w.n_voxels,
-                       "measurements": 31, "fit": "wls", "l2": "flushed (256 MiB write) before each step"}
+                       "measurements": 31, "fit": "wls", "l2": "flushed (256 MiB write) before each step",
+                       "e2e_api": "DTIModel(fit_method='wls').fit(volume, gtab, mask)"}
         self.design = dti_design(w.gtab)
-        s0 = estimate_s0(w.volume, w.gtab, w.mask)[w.mask]
-        self.signals = masked_signals(w.volume, np.nonzero(w.mask))
-        self.floor = sample_floors(s0, None, len(self.signals))
+        self.signals, _, self.floor = staged_inputs(w)
         self.v = len(self.signals)
 
     def subset(self, n: int) -> None:
         self.signals, self.floor = self.signals[:n], self.floor[:n]
         self.v = len(self.signals)
+        flat = np.flatnonzero(self.mask)
+        keep = np.zeros(self.mask.size, dtype=bool)
+        keep[flat[:n]] = True
+        self.mask = keep.reshape(self.mask.shape)
         self.config["voxels"] = self.v
 
     def device_setup(self, torch, dev):
@@ -164,11 +206,8 @@ class DtiWorkload:
         self.d_floor = torch.from_numpy(self.floor).to(dev)
         self.d_maps = torch.empty((16, self.v), dtype=torch.float32, device=dev)
         self.d_npd = torch.empty((self.v,), dtype=torch.uint8, device=dev)
-        self.h_signals = torch.from_numpy(self.signals).pin_memory()
-        self.h_floor = torch.from_numpy(self.floor).pin_memory()
-        self.h_maps = torch.empty((16, self.v), dtype=torch.float32).pin_memory()
-        self.h_npd = torch.empty((self.v,), dtype=torch.uint8).pin_memory()
-        self.h2d_bytes = self.signals.nbytes + self.floor.nbytes
+        # The model call copies the raw volume and the mask voxels' indices in, the masked maps out.
+        self.h2d_bytes = self.w.volume.data.nbytes + 8 * self.v
         self.d2h_bytes = 16 * 4 * self.v + self.v
 
     def step_device(self, precision=0):
@@ -182,13 +221,9 @@ class DtiWorkload:
         return {"fit_dti_maps_kernel": self.bytes_per_voxel * self.v}
 
     def step_e2e(self):
-        from larmor_b200 import _core
+        from larmor_b200.dwi import DTIModel
 
-        self.d_signals.copy_(self.h_signals, non_blocking=True)
-        self.d_floor.copy_(self.h_floor, non_blocking=True)
-        _core.fit_dti_maps_device(self.handle, self.d_signals, self.d_floor, True, self.d_maps, self.d_npd)
-        self.h_maps.copy_(self.d_maps, non_blocking=True)
-        self.h_npd.copy_(self.d_npd, non_blocking=True)
+        self.e2e_fit = DTIModel(fit_method="wls").fit(self.w.volume, self.w.gtab, self.mask)
 
     def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
         from oracle import oracle as o
@@ -198,9 +233,34 @@ class DtiWorkload:
         o.fit_log_signal(self.design, None, log_s[:256], True, n_threads=threads)  # warm-up
         done, t0 = 0, time.perf_counter()
         while time.perf_counter() - t0 < budget_s:
-            o.fit_log_signal(self.design, None, log_s, True, n_threads=threads)
+            params, _ = o.fit_log_signal(self.design, None, log_s, True, n_threads=threads)
             done += len(log_s)
+        self.reference_params = params
         return done, time.perf_counter() - t0, f"whole volume ({self.v} voxels) repeated for ~{budget_s:.0f} s"
+
+    def parity(self) -> dict:
+        """FA and MD of every voxel, from the device's fused fit and maps (float32 maps) and from
+        the FP64 oracle's parameters of the cpu_baseline run (numpy eigh), and the tensors."""
+        self.step_device()
+        maps = self.d_maps.cpu().numpy().astype(np.float64)
+        fa, md = tensor_fa_md(self.reference_params[:, 1:7])
+        fa_err = float(np.abs(maps[6] - fa).max())
+        md_err = float(np.abs(maps[7] - md).max())
+        dt_rel = float((np.abs(maps[0:6].T - self.reference_params[:, 1:7]).max(axis=1)
+                        / np.abs(self.reference_params[:, 1:7]).max(axis=1)).max())
+        return {"against": "FP64 oracle (C++ restatement of cpp/src/dwi/log_fit.cpp), numpy eigh for FA/MD",
+                "voxels": self.v, "fa_abs_max": fa_err, "md_abs_max": md_err, "dt_rel_max": dt_rel,
+                "tolerance": {"fa_abs": 1e-4, "md_abs": 1e-4},
+                "within_tolerance": bool(fa_err <= 1e-4 and md_err <= 1e-4)}
+
+    def fp32_parity(self) -> dict:
+        """The plain FP32 kernel's FA, MD and tensors against the same FP64 oracle fit."""
+        self.step_device(precision=1)
+        maps = self.d_maps.cpu().numpy().astype(np.float64)
+        fa, md = tensor_fa_md(self.reference_params[:, 1:7])
+        ref = self.reference_params[:, 1:7]
+        return {"fa_abs_max": float(np.abs(maps[6] - fa).max()), "md_abs_max": float(np.abs(maps[7] - md).max()),
+                "dt_rel_max": float((np.abs(maps[0:6].T - ref).max(axis=1) / np.abs(ref).max(axis=1)).max())}
 
 
 class DtiModelWorkload:
@@ -208,8 +268,7 @@ class DtiModelWorkload:
     64x64x40 volume (79,912 mask voxels), from the raw float32 volume to the maps. The device
     stages the inputs: the mask voxels' samples, S0 with its neighbourhood repair, the
     per-voxel floors (lar_stage_dwi); then the fused fit and maps. value: staging + fit with the
-    raw volume resident; e2e: the whole model call, host volume in, host maps out; host_staging:
-    the same call with the inputs prepared on the host (numpy) instead."""
+    raw volume resident; e2e: the whole model call, host volume in, host maps out."""
 
     name = "dti_model_wlls_64x64x40"
     kernels = ("stage_gather_kernel", "stage_index_kernel", "stage_repair_kernel", "stage_floor_kernel",
@@ -270,25 +329,6 @@ class DtiModelWorkload:
 
         DTIModel(fit_method="wls").fit(self.w.volume, self.w.gtab, self.mask)
 
-    def extra(self, timed) -> dict:
-        """The model call with the host (numpy) preparation of the inputs, timed the same way."""
-        from larmor_b200.dwi.dti import dti_design, fit_dti_signals
-        from larmor_b200.dwi.inputs import estimate_s0, largest_finite_signal, masked_signals, sample_floors
-        from larmor_b200.dwi.mask import unmask
-
-        design = dti_design(self.w.gtab)
-
-        def host_staged():
-            s0 = estimate_s0(self.w.volume, self.w.gtab, self.mask)[self.mask]
-            signals = masked_signals(self.w.volume, np.nonzero(self.mask))
-            largest = None if (np.isfinite(s0) & (s0 > 0)).all() else largest_finite_signal(signals)
-            maps, npd = fit_dti_signals(design, signals, sample_floors(s0, largest, len(signals)), True)
-            unmask(maps[6], self.mask)
-
-        ms = timed(host_staged)
-        return {"host_staging": {"value": self.v / (ms / 1e3), "unit": "voxel fits/s", "ms_per_step": ms,
-                                 "what": "the same DTIModel call with S0, the gather and the floors on the host"}}
-
     def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
         from larmor_b200.dwi.dti import dti_design
         from oracle import oracle as o
@@ -318,16 +358,12 @@ class DkiWorkload:
 
     def __init__(self, seed: int) -> None:
         from larmor_b200.dwi.dki import dki_constraints, dki_design
-        from larmor_b200.dwi.inputs import estimate_s0, masked_signals, sample_floors
         from larmor_b200.synthetic import dki_volume
 
         w = dki_volume(seed=2 + 10 * (seed - 1))
         self.design = dki_design(w.gtab)
         self.g = dki_constraints(w.gtab)
-        s0 = estimate_s0(w.volume, w.gtab, w.mask)[w.mask]
-        self.s0 = s0
-        self.signals = masked_signals(w.volume, np.nonzero(w.mask))
-        self.floor = sample_floors(s0, None, len(self.signals))
+        self.signals, self.s0, self.floor = staged_inputs(w)
         self.is_b0 = w.gtab.b0_mask.astype(np.uint8)
         self.v = len(self.signals)
         self.config = {"workload": self.name, "grid": [96, 96, 60], "voxels": self.v, "measurements": 134,
@@ -409,13 +445,12 @@ class _SdWorkloadBase:
     """The config-3 volume (110x110x70, 500,040 voxels, 10 b0 + 3 x 90) for the SD fits."""
 
     def _volume(self, seed: int):
-        from larmor_b200.dwi.inputs import estimate_s0, masked_signals
         from larmor_b200.synthetic import mfod_volume
 
         w = mfod_volume(seed=3 + 10 * (seed - 1))
         self.gtab = w.gtab
-        self.signals = masked_signals(w.volume, np.nonzero(w.mask)).astype(np.float64)
-        self.s0 = estimate_s0(w.volume, w.gtab, w.mask)[w.mask]
+        signals, self.s0, _ = staged_inputs(w)
+        self.signals = signals.astype(np.float64)
         self.v = len(self.signals)
 
     def subset(self, n: int) -> None:
@@ -428,7 +463,9 @@ class _SdWorkloadBase:
 
 class MfodWorkload(_SdWorkloadBase):
     """Config 3: three-tissue mFOD (SDModel, method mFOD): WM L2NNLS FOD on 300 directions
-    (44 in the loop) + GM + CSF, up to 50 rounds, on S0-normalised signals."""
+    (44 in the loop) + GM + CSF, up to 50 rounds, on S0-normalised signals. value: the fit with
+    the signals resident; e2e: the drop-in call _core.fit_multi_tissue with host numpy arrays
+    (float64 signals in, new FOD and fraction arrays out)."""
 
     name = "mfod_3tissue_110x110x70"
     kernels = ("correlate_kernel", "ridge_nnls_half_kernel<3>", "ridge_nnls_kernel<1,2>", "lr_fractions_kernel",
@@ -453,7 +490,8 @@ class MfodWorkload(_SdWorkloadBase):
         self.lr = Kernel(rfs, b, g, dirs=low_resolution_dirs(rfs, len(b)), weights=weights)
         self.config = {"workload": self.name, "grid": [110, 110, 70], "voxels": self.v, "measurements": 280,
                        "tissues": "WM (lmax 8 output, 300 directions) + GM + CSF", "max_rounds": 50,
-                       "fraction_tol": 1e-7, "l2": "inputs (1.1 GB) larger than L2"}
+                       "fraction_tol": 1e-7, "l2": "inputs (1.1 GB) larger than L2",
+                       "e2e_api": "_core.fit_multi_tissue(numpy float64 signals) -> numpy FODs, fractions"}
 
     def sd_solver(self):
         from larmor_b200.sd.solvers import L2NNLS
@@ -470,11 +508,8 @@ class MfodWorkload(_SdWorkloadBase):
         self.d_signals = torch.from_numpy(self.norm).to(dev)
         self.d_fods = torch.empty((self.v, self.k_hr.ca), dtype=torch.float64, device=dev)
         self.d_fr = torch.empty((self.v, 3), dtype=torch.float64, device=dev)
-        self.h_signals = torch.from_numpy(self.norm).pin_memory()
-        self.h_fods = torch.empty((self.v, self.k_hr.ca), dtype=torch.float64).pin_memory()
-        self.h_fr = torch.empty((self.v, 3), dtype=torch.float64).pin_memory()
         self.h2d_bytes = self.norm.nbytes
-        self.d2h_bytes = self.h_fods.numel() * 8 + self.h_fr.numel() * 8
+        self.d2h_bytes = self.v * (self.k_hr.ca + 3) * 8
 
     def step_device(self, precision=0):
         from larmor_b200 import _core
@@ -493,6 +528,7 @@ class MfodWorkload(_SdWorkloadBase):
         rounds = torch.zeros((self.v,), dtype=torch.int32, device=self.d_signals.device)
         _core.fit_multi_tissue_device(self.d_signals, self.lr.weights, self.k_lr, self.lr_solver, self.k_hr,
                                       self.hr_solver, 50, 1e-7, 1e-2, self.d_fods, self.d_fr, rounds=rounds)
+        self.d_rounds = rounds
         vr = int(rounds.sum().item())
         m, c_lr, c_hr = 280, self.k_lr.ca, self.k_hr.ca
         # The low-resolution NNLS runs two voxels per warp; the one-warp kernel refits only the
@@ -505,23 +541,51 @@ class MfodWorkload(_SdWorkloadBase):
                 "hr_fractions_kernel": self.v * 8 * (c_hr + m + 3)}
 
     def step_e2e(self):
-        self.d_signals.copy_(self.h_signals, non_blocking=True)
-        self.step_device()
-        self.h_fods.copy_(self.d_fods, non_blocking=True)
-        self.h_fr.copy_(self.d_fr, non_blocking=True)
+        from larmor_b200 import _core
+
+        self.e2e_out = _core.fit_multi_tissue(self.norm, self.lr.weights, self.k_lr, self.lr_solver, self.k_hr,
+                                              self.hr_solver, 50, 1e-7, 1e-2, n_threads=1)
 
     def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
         from oracle import oracle as o
 
-        n = min(self.v, 2048)
+        self.sample = idx = strided(self.v, 2048)
+        signals = np.ascontiguousarray(self.norm[idx])
         lr = dict(k_aniso=self.lr.k_aniso, k_iso=self.lr.k_iso, w_k_iso=self.lr.w_k_iso, w_k_aniso=self.lr.w_k_aniso)
         hr = dict(k_aniso=self.hr.k_aniso, k_iso=self.hr.k_iso, w_k_iso=self.hr.w_k_iso, w_k_aniso=self.hr.w_k_aniso,
                   blocks=[(b.start, b.stop) for b in self.hr.aniso_blocks])
         done, t0 = 0, time.perf_counter()
         while time.perf_counter() - t0 < budget_s:
-            o.fit_multi_tissue(self.norm[:n], self.lr.weights, lr, hr, n_threads=threads)
-            done += n
-        return done, time.perf_counter() - t0, f"first {n} voxels of the volume, repeated for ~{budget_s:.0f} s"
+            out = o.fit_multi_tissue(signals, self.lr.weights, lr, hr, n_threads=threads, rounds=True)
+            done += len(idx)
+        self.reference_out = out
+        return done, time.perf_counter() - t0, (f"{len(idx)} voxels spread evenly over the volume, repeated for "
+                                                f"~{budget_s:.0f} s")
+
+    def parity(self) -> dict:
+        """The device fit of the whole volume against the FP64 oracle on the cpu_baseline sample:
+        the FOD amplitudes' largest error relative to the voxel's largest amplitude, the
+        fractions' largest absolute error, and how many voxels have the oracle's final active
+        set (the zero pattern of the 300 amplitudes) and round count."""
+        fods, fr, rounds = self.reference_out
+        idx = self.torch.from_numpy(self.sample).to(self.d_fods.device)
+        got = self.d_fods[idx].cpu().numpy()
+        got_fr = self.d_fr[idx].cpu().numpy()
+        got_rounds = self.d_rounds[idx].cpu().numpy()
+        scale = np.maximum(np.abs(fods).max(axis=1), 1e-300)
+        rel = float((np.abs(got - fods).max(axis=1) / scale).max())
+        fr_err = float(np.abs(got_fr - fr).max())
+        same_set = float(((got > 0) == (fods > 0)).all(axis=1).mean())
+        same_rounds = float((got_rounds == rounds).mean())
+        e2e_fods, e2e_fr = self.e2e_out
+        e2e_same = bool(np.array_equal(e2e_fods[self.sample], got) and np.array_equal(e2e_fr[self.sample], got_fr))
+        return {"against": "FP64 oracle (C++ restatement of cpp/src/sd/{nnls,fractions,multi_tissue}.cpp)",
+                "voxels": int(len(self.sample)), "sample": "spread evenly over the volume",
+                "fod_rel_max": rel, "fractions_abs_max": fr_err,
+                "identical_active_sets": same_set, "identical_round_counts": same_rounds,
+                "e2e_equals_device_fit": e2e_same,
+                "tolerance": {"fod_rel": 1e-4, "fractions_abs": 1e-4, "identical_active_sets": 1.0},
+                "within_tolerance": bool(rel <= 1e-4 and fr_err <= 1e-4 and same_set == 1.0)}
 
 
 class MsmtWorkload(_SdWorkloadBase):
@@ -1063,13 +1127,13 @@ WORKLOADS = {"dti": DtiWorkload, "dki": DkiWorkload, "mfod": MfodWorkload, "msmt
 
 # ---- runs --------------------------------------------------------------------------------
 
-def _serve_jobs(seed: int, count: int):
+def _serve_jobs(seed: int, count: int, wl=None):
     """Fit requests drawn from the config-3 distribution: contiguous runs of voxels of the
     110x110x70 three-tissue volume (S0-normalised), their lengths log-uniform in [4096, 65536]."""
     from larmor_b200.batch import MfodJob
     from larmor_b200.synthetic import mfod_model_responses
 
-    wl = MfodWorkload(seed=1)
+    wl = MfodWorkload(seed=1) if wl is None else wl
     rng = np.random.default_rng(seed)
     jobs = []
     for _ in range(count):
@@ -1079,7 +1143,7 @@ def _serve_jobs(seed: int, count: int):
     return jobs
 
 
-def run_serving(args) -> dict:
+def run_serving(args, source=None) -> dict:
     """Config 5: Poisson arrivals of mFOD fit requests at rates swept up to saturation through
     the continuous-batching server, against the plain per-request fit (one request at a time).
     Latency is arrival to result on the host (wall clock), the quantity a client sees."""
@@ -1088,7 +1152,7 @@ def run_serving(args) -> dict:
     from larmor_b200 import _core
     from larmor_b200.serve import FitServer
 
-    jobs = _serve_jobs(5, args.serve_requests)
+    jobs = _serve_jobs(5, args.serve_requests, source)
     voxels = sum(j.voxels for j in jobs)
     # Warm-up: the largest request on every slot at once, so that each slot's handles and
     # scratch are built and sized before the timed arrivals (growing scratch later would free
@@ -1175,85 +1239,16 @@ def run_reference(args, wl) -> dict:
     }
 
 
-def main() -> int:
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="mfod", choices=sorted(WORKLOADS) + ["serve"])
-    ap.add_argument("--impl", default="larmor_b200", choices=["larmor_b200", "reference"])
-    ap.add_argument("--reference-budget", type=float, default=3.0,
-                    help="seconds of CPU work per reference step")
-    ap.add_argument("--cpu-budget", type=float, default=10.0,
-                    help="seconds of CPU baseline work on rank 0")
-    ap.add_argument("--voxels", type=int, default=0,
-                    help="fit only the first N voxels of the volume (small cases for ncu)")
-    ap.add_argument("--serve-requests", type=int, default=24, help="requests per arrival rate (serve)")
-    ap.add_argument("--serve-slots", type=int, default=6, help="requests on the GPU at once (serve)")
-    ap.add_argument("--serve-load", type=float, nargs="+", default=[0.5, 1.0, 2.0, 4.0],
-                    help="arrival rates as multiples of the plain per-request rate (serve)")
-    ap.add_argument("--profile", action="store_true",
-                    help="warm-up and K device-resident steps only, timed per step on stdout (for ncu); "
-                         "prints no bench line")
-    args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-
-    if args.workload == "serve":
-        if rank != 0:
-            return 0
-        if args.impl == "reference":
-            wl = MfodWorkload(seed=1)
-            line = run_reference(args, wl)
-            line["config"] = {"workload": "serve_mfod_poisson", "reference": "the mFOD fit of config-3 voxels"}
-            print(json.dumps(line))
-            return 0
-        print(json.dumps(run_serving(args)))
-        return 0
-
-    if args.impl == "reference":
-        if rank != 0:
-            return 0
-        wl = WORKLOADS[args.workload](seed=1)
-        print(json.dumps(run_reference(args, wl)))
-        return 0
-
+def measure(wl, args, world: int, rank: int, dist, dev) -> dict:
+    """The bench line of one workload: K device-resident steps (value), the plain FP32 variant
+    where the workload has one, K end-to-end steps through the public call (e2e), the dominant
+    kernel's roofline, and on rank 0 the FP64 oracle on a bounded sample of the same workload
+    (cpu_baseline) with the device results' error against it (parity). Every rank takes the
+    same collective steps."""
     import torch
 
-    dist = None
-    if world > 1:
-        import datetime
+    from larmor_b200 import _core
 
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    dev = torch.device("cuda", local if world > 1 else torch.cuda.current_device())
-    torch.cuda.set_device(dev)
-
-    wl = WORKLOADS[args.workload](seed=1 + rank)
-    if args.voxels:
-        wl.subset(args.voxels)
-    wl.device_setup(torch, dev)
-    if args.profile:
-        from larmor_b200 import _core
-
-        for i in range(args.warmup + args.steps):
-            last = i == args.warmup + args.steps - 1
-            _core.kernel_timing(last)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            wl.step_device()
-            torch.cuda.synchronize()
-            print(f"{wl.name} voxels {wl.v} step {i} {1e3 * (time.perf_counter() - t0):.3f} ms")
-        times = {k: _core.kernel_time(k) for k in wl.kernels}
-        _core.kernel_timing(False)
-        print("kernels (ms, launches) of the last step:",
-              ", ".join(f"{k} {t:.2f} ({n})" for k, (t, n) in times.items() if n))
-        return 0
     flush = torch.empty(256 * 2**20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
 
@@ -1289,7 +1284,6 @@ def main() -> int:
     gpu_index = dev.index if dev.index is not None else 0
     visible = os.environ.get("CUDA_VISIBLE_DEVICES")
     smi_index = int(visible.split(",")[gpu_index]) if visible and visible.split(",")[gpu_index].isdigit() else gpu_index
-    from larmor_b200 import _core
 
     _core.kernel_timing(True)
     launches0 = _core.launch_count()
@@ -1320,10 +1314,11 @@ def main() -> int:
         fp32_ms = max_over_ranks(timed(lambda: wl.step_device(precision=1), args.steps))
 
     # End to end through host buffers.
-    for _ in range(args.warmup):
+    e2e_steps = max(1, min(args.steps, getattr(wl, "e2e_steps", args.steps)))
+    for _ in range(min(args.warmup, 3)):
         wl.step_e2e()
     barrier()
-    e2e_ms = max_over_ranks(timed(wl.step_e2e, args.steps))
+    e2e_ms = max_over_ranks(timed(wl.step_e2e, e2e_steps))
 
     voxels_all = wl.v * world
     value = voxels_all * args.steps / (dev_ms / 1e3)
@@ -1338,12 +1333,16 @@ def main() -> int:
     traffic = committed_traffic(top, wl.name, bytes_per_launch)
     total_kernel_ms = max(sum(t for t, _ in kernel_ms.values()), 1e-30)
 
-    cpu = None
+    cpu, parity, fp32_parity = None, None, None
     if rank == 0:
         threads = os.cpu_count() or 1
         done, secs, sample = wl.cpu_sample(threads, args.cpu_budget)
         cpu = {"value": done / secs, "unit": getattr(wl, "unit", "voxel fits/s"), "cores": threads, "kind": "port",
                "sample": sample}
+        if hasattr(wl, "parity"):
+            parity = wl.parity()
+        if fp32_ms is not None and hasattr(wl, "fp32_parity"):
+            fp32_parity = wl.fp32_parity()
 
     line = {
         "metric": METRIC, "value": value, "unit": getattr(wl, "unit", "voxel fits/s"), "n_gpus": world,
@@ -1357,11 +1356,12 @@ def main() -> int:
                      "avg_launch_ms": avg_launch_s * 1e3, "launches": top_launches,
                      "kernel_share": {k: round(t / total_kernel_ms, 4) for k, (t, _) in kernel_ms.items()}},
         "cpu_baseline": cpu,
-        "e2e": {"value": voxels_all * args.steps / (e2e_ms / 1e3), "unit": getattr(wl, "unit", "voxel fits/s"),
-                "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes},
+        "e2e": {"value": voxels_all * e2e_steps / (e2e_ms / 1e3), "unit": getattr(wl, "unit", "voxel fits/s"),
+                "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes, "steps": e2e_steps},
         "plain_fp32": None if fp32_ms is None else {
             "value": voxels_all * args.steps / (fp32_ms / 1e3), "unit": "voxel fits/s",
-            "ms_per_step": fp32_ms / args.steps},
+            "ms_per_step": fp32_ms / args.steps, "parity": fp32_parity},
+        "parity": parity,
         "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
@@ -1372,6 +1372,8 @@ def main() -> int:
         if flops is not None:
             line["roofline"].update(fp64_tensor_roofline(flops * args.steps / max(top_launches, 1), avg_launch_s))
             line["roofline"]["flops_basis"] = wl.flops_basis
+    if hasattr(wl, "issue_roofline"):
+        line["issue_roofline"] = wl.issue_roofline(kernel_ms, args.steps)
     if hasattr(wl, "extra"):
         def timed_host(step):
             for _ in range(args.warmup):
@@ -1380,6 +1382,115 @@ def main() -> int:
             return max_over_ranks(timed(step, args.steps)) / args.steps
 
         line.update(wl.extra(timed_host))
+    del flush
+    return line
+
+
+def main() -> int:
+    global REFERENCE_ARM
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default="mfod", choices=sorted(WORKLOADS) + ["serve"])
+    ap.add_argument("--impl", default="larmor_b200", choices=["larmor_b200", "reference"])
+    ap.add_argument("--reference-budget", type=float, default=3.0,
+                    help="seconds of CPU work per reference step")
+    ap.add_argument("--cpu-budget", type=float, default=10.0,
+                    help="seconds of CPU baseline work on rank 0")
+    ap.add_argument("--voxels", type=int, default=0,
+                    help="fit only the first N voxels of the volume (small cases for ncu)")
+    ap.add_argument("--serve-requests", type=int, default=24, help="requests per arrival rate (serve)")
+    ap.add_argument("--serve-slots", type=int, default=6, help="requests on the GPU at once (serve)")
+    ap.add_argument("--serve-load", type=float, nargs="+", default=[0.5, 1.0, 2.0, 4.0],
+                    help="arrival rates as multiples of the plain per-request rate (serve)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="the mfod line without its DTI and serving sub-objects")
+    ap.add_argument("--profile", action="store_true",
+                    help="warm-up and K device-resident steps only, timed per step on stdout (for ncu); "
+                         "prints no bench line")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        REFERENCE_ARM = True
+        if rank != 0:
+            return 0
+        if args.workload == "serve":
+            wl = MfodWorkload(seed=1)
+            line = run_reference(args, wl)
+            line["config"] = {"workload": "serve_mfod_poisson", "reference": "the mFOD fit of config-3 voxels"}
+        else:
+            wl = WORKLOADS[args.workload](seed=1)
+            line = run_reference(args, wl)
+        print(json.dumps(line))
+        return 0
+
+    if args.workload == "serve":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_serving(args)))
+        return 0
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local if world > 1 else torch.cuda.current_device())
+    torch.cuda.set_device(dev)
+
+    wl = WORKLOADS[args.workload](seed=1 + rank)
+    if args.voxels:
+        wl.subset(args.voxels)
+    wl.device_setup(torch, dev)
+    if args.profile:
+        from larmor_b200 import _core
+
+        for i in range(args.warmup + args.steps):
+            last = i == args.warmup + args.steps - 1
+            _core.kernel_timing(last)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            wl.step_device()
+            torch.cuda.synchronize()
+            print(f"{wl.name} voxels {wl.v} step {i} {1e3 * (time.perf_counter() - t0):.3f} ms")
+        times = {k: _core.kernel_time(k) for k in wl.kernels}
+        _core.kernel_timing(False)
+        print("kernels (ms, launches) of the last step:",
+              ", ".join(f"{k} {t:.2f} ({n})" for k, (t, n) in times.items() if n))
+        return 0
+
+    line = measure(wl, args, world, rank, dist, dev)
+    if args.workload == "mfod" and not args.no_extras and not args.voxels:
+        # The metric names DTI and serving beside mFOD: config 1 measured the same way, and a
+        # short serving sweep (rank 0 only; it has no collective) of requests cut from the same
+        # volume.
+        source = argparse.Namespace(v=wl.v, gtab=wl.gtab, norm=wl.norm)
+        del wl
+        dti = DtiWorkload(seed=1 + rank)
+        dti.device_setup(torch, dev)
+        sub = argparse.Namespace(**vars(args))
+        sub.cpu_budget = min(args.cpu_budget, 5.0)
+        line["dti"] = measure(dti, sub, world, rank, dist, dev)
+        for key in ("metric", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "data"):
+            line["dti"].pop(key, None)
+        del dti
+        if rank == 0:
+            srv = argparse.Namespace(**vars(args))
+            srv.serve_requests, srv.serve_load = 16, [1.0, 2.0]
+            serve = run_serving(srv, source)
+            line["serve"] = {k: serve[k] for k in ("value", "unit", "config", "serving", "plain_per_request",
+                                                   "saturation", "dominant_kernel", "gpu_launches", "clocks")}
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:

@@ -54,11 +54,122 @@ def _array(a, name: str, ndim: int, dtype=np.float64) -> np.ndarray:
     return a
 
 
+class _Transfers:
+    """Copies between the caller's (pageable) numpy arrays and the device through two reusable
+    page-locked buffers of CHUNK bytes: while the DMA engine moves one chunk, host threads copy
+    the next one into (or the previous one out of) the other buffer, so a large array crosses
+    at close to the link's rate instead of through the driver's pageable staging. The buffers
+    are allocated once per process and kept; the copies run on the current stream."""
+
+    CHUNK = 32 << 20
+    THREADS = 8
+
+    def __init__(self) -> None:
+        import threading
+
+        self.buffers = None
+        self.events = [None, None]
+        self.pool = None
+        self.lock = threading.Lock()
+
+    def _setup(self, torch):
+        if self.buffers is None:
+            from concurrent.futures import ThreadPoolExecutor
+
+            self.buffers = [torch.empty(self.CHUNK, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+            self.views = [b.numpy() for b in self.buffers]
+            self.pool = ThreadPoolExecutor(self.THREADS, thread_name_prefix="larmor-copy")
+
+    def _host_copy(self, dst: np.ndarray, src: np.ndarray) -> None:
+        """dst[:] = src for flat uint8 views, split over the host threads (numpy releases the GIL
+        while it copies)."""
+        n = len(src)
+        if n < (4 << 20):
+            dst[:] = src
+            return
+        step = -(-n // self.THREADS)
+        parts = [(i, min(i + step, n)) for i in range(0, n, step)]
+        for f in [self.pool.submit(np.copyto, dst[a:b], src[a:b]) for a, b in parts]:
+            f.result()
+
+    def _wait(self, k: int) -> None:
+        if self.events[k] is not None:
+            self.events[k].synchronize()
+            self.events[k] = None
+
+    def upload(self, torch, a: np.ndarray, dev):
+        """A new C-contiguous device tensor with the contents of the host array a."""
+        out = torch.empty(a.shape, dtype=getattr(torch, a.dtype.name), device=dev)
+        if a.nbytes < (1 << 20):
+            out.copy_(torch.from_numpy(a))
+            return out
+        with self.lock:
+            return self._upload(torch, a, out)
+
+    def _upload(self, torch, a, out):
+        self._setup(torch)
+        src = np.ascontiguousarray(a).reshape(-1).view(np.uint8)
+        dst = out.view(-1).view(torch.uint8)
+        stream = torch.cuda.current_stream()
+        for i, start in enumerate(range(0, len(src), self.CHUNK)):
+            k = i & 1
+            stop = min(start + self.CHUNK, len(src))
+            self._wait(k)  # the buffer's previous DMA has finished
+            self._host_copy(self.views[k][:stop - start], src[start:stop])
+            dst[start:stop].copy_(self.buffers[k][:stop - start], non_blocking=True)
+            self.events[k] = torch.cuda.Event()
+            self.events[k].record(stream)
+        return out
+
+    def download(self, torch, t) -> np.ndarray:
+        """A new numpy array with the contents of the device tensor t (waits for t's stream)."""
+        t = t.contiguous()
+        out = np.empty(tuple(t.shape), dtype=np.dtype(str(t.dtype).replace("torch.", "")))
+        nbytes = out.nbytes
+        if nbytes < (1 << 20):
+            out[...] = t.cpu().numpy()
+            return out
+        with self.lock:
+            return self._download(torch, t, out)
+
+    def _download(self, torch, t, out):
+        nbytes = out.nbytes
+        self._setup(torch)
+        src = t.view(-1).view(torch.uint8)
+        dst = out.reshape(-1).view(np.uint8)
+        stream = torch.cuda.current_stream()
+        pending = None
+        for i, start in enumerate(range(0, nbytes, self.CHUNK)):
+            k = i & 1
+            stop = min(start + self.CHUNK, nbytes)
+            self._wait(k)
+            self.buffers[k][:stop - start].copy_(src[start:stop], non_blocking=True)
+            self.events[k] = torch.cuda.Event()
+            self.events[k].record(stream)
+            if pending is not None:  # the previous chunk, while this one moves
+                pk, pa, pb = pending
+                self._wait(pk)
+                self._host_copy(dst[pa:pb], self.views[pk][:pb - pa])
+            pending = (k, start, stop)
+        pk, pa, pb = pending
+        self._wait(pk)
+        self._host_copy(dst[pa:pb], self.views[pk][:pb - pa])
+        return out
+
+
+_transfers = _Transfers()
+
+
 def _on_device(torch, a, dev):
     """A C-contiguous device tensor of a host array, or the device tensor itself."""
     if isinstance(a, np.ndarray):
-        return torch.from_numpy(a).to(dev)
+        return _transfers.upload(torch, a, dev)
     return a.contiguous()
+
+
+def _to_host(t) -> np.ndarray:
+    """A new numpy array of a device tensor, copied through the page-locked buffers."""
+    return _transfers.download(_torch(), t)
 
 
 def _require_threads(n_threads: int) -> None:
@@ -173,9 +284,9 @@ def fit_log_signal(x, g, log_s, weighted, max_iter, tol, n_threads):
     params = torch.empty((v, p), dtype=torch.float64, device=dev)
     broke = torch.empty((v,), dtype=torch.uint8, device=dev)
     if v:
-        ls = torch.from_numpy(log_s).to(dev)
+        ls = _on_device(torch, log_s, dev)
         fit_log_signal_device(design, ls, bool(weighted), int(max_iter), float(tol), params, broke)
-    return params.cpu().numpy(), broke.cpu().numpy().astype(bool)
+    return _to_host(params), _to_host(broke).astype(bool)
 
 
 def fit_log_signal_device(design: LogDesign, log_s, weighted: bool, max_iter: int, tol: float,
@@ -264,9 +375,9 @@ def fit_lsi(signals, design: LsiDesign, n_threads):
     x = torch.empty((v, design.n), dtype=torch.float64, device=dev)
     conv = torch.empty((v,), dtype=torch.uint8, device=dev)
     if v:
-        s = torch.from_numpy(signals).to(dev)
+        s = _on_device(torch, signals, dev)
         fit_lsi_device(design, s, x, conv)
-    return x.cpu().numpy(), conv.cpu().numpy().astype(bool)
+    return _to_host(x), _to_host(conv).astype(bool)
 
 
 def fit_lsi_device(design: LsiDesign, signals, x, converged, status=None, outer=None, active=None,
@@ -415,7 +526,7 @@ def fit_multi_tissue(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, 
         raise ValueError("max_outer must be at least 0")
     fods, fractions = _fit_multi_tissue_on_device(signals, weights, lr, lr_solver, hr, hr_solver, max_outer,
                                                   fraction_tol, final_tol_x)
-    return fods.cpu().numpy(), fractions.cpu().numpy()
+    return _to_host(fods), _to_host(fractions)
 
 
 def _fit_multi_tissue_on_device(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol,
@@ -487,7 +598,7 @@ def fit_single_tissue(signals, solver: FodSolver, n_threads):
     if signals.shape[1] != solver.n_meas:
         raise ValueError(f"signals {signals.shape} do not have the solver's {solver.n_meas} measurements")
     _require_threads(n_threads)
-    return _fit_single_tissue_on_device(signals, solver).cpu().numpy()
+    return _to_host(_fit_single_tissue_on_device(signals, solver))
 
 
 def _fit_single_tissue_on_device(signals, solver: FodSolver):
@@ -616,9 +727,9 @@ def fit_csd(signals, initial, forward, constraint, norm_weight, threshold, max_i
     torch = _torch()
     problem = CsdProblem.cached(initial, forward, constraint, norm_weight, threshold, max_iter)
     dev = torch.device("cuda", torch.cuda.current_device())
-    s = torch.from_numpy(signals).to(dev)
+    s = _on_device(torch, signals, dev)
     fods, conv = fit_csd_device(problem, s)
-    return fods.cpu().numpy(), conv.cpu().numpy().astype(bool)
+    return _to_host(fods), _to_host(conv).astype(bool)
 
 
 # ---- FOD peaks (cpp/src/python/sh.cpp) ---------------------------------------------------

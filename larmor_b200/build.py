@@ -43,14 +43,34 @@ def stale() -> bool:
 
 
 def build(verbose: bool = False, force: bool = False) -> Path:
-    """Compiles every CUDA source into liblarmor_b200.so; returns its path."""
+    """Compiles every CUDA source into liblarmor_b200.so (one nvcc per source, in parallel, then
+    one link); returns its path."""
     if not force and not stale():
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, *(str(CSRC / s) for s in SOURCES), "-o", str(LIB)]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+    import os
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
+
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    with tempfile.TemporaryDirectory(prefix="larmor_b200_build_") as tmp:
+        objects = [str(Path(tmp) / (Path(src).stem + ".o")) for src in SOURCES]
+
+        def compile_one(job):
+            src, obj = job
+            cmd = [nvcc(), *compile_flags, "-c", str(CSRC / src), "-o", obj]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+            return subprocess.run(cmd, capture_output=True, text=True)
+
+        with ThreadPoolExecutor(max(1, min(len(SOURCES), os.cpu_count() or 1))) as pool:
+            results = list(pool.map(compile_one, zip(SOURCES, objects)))
+        for src, r in zip(SOURCES, results):
+            if verbose or r.returncode:
+                sys.stderr.write(r.stdout + r.stderr)
+            if r.returncode:
+                raise subprocess.CalledProcessError(r.returncode, f"nvcc -c {src}")
+        link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objects, "-o", str(LIB)]
+        subprocess.run(link, check=True)
     return LIB
 
 

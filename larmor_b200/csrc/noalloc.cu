@@ -93,8 +93,16 @@ extern "C" int lar_fit_log_signal_noalloc(const double* x, int64_t n, int64_t p,
         if (need > kNoAllocScratchBytes || (m > 0 && slots < 4)) {
             const size_t fixed = (m > 0 ? 4 * slot_bytes : 0) + up256(design_doubles * sizeof(double)) + 1024;
             const size_t per_voxel = m > 0 ? sizeof(int64_t) + size_t(p) * sizeof(double) : 0;
-            const long long max_v =
-                per_voxel == 0 ? 0 : fixed >= kNoAllocScratchBytes ? 0 : (long long)((kNoAllocScratchBytes - fixed) / per_voxel);
+            if (per_voxel == 0 || fixed >= kNoAllocScratchBytes)
+                // No voxel count fits: the design (and the re-fit's smallest workspace) alone
+                // outgrow the array.
+                throw Error(LAR_ERR_INVALID,
+                            "lar_fit_log_signal_noalloc: a design of (n, p, m) = (" + std::to_string(n) + ", " +
+                                std::to_string(p) + ", " + std::to_string(m) + ") needs " + std::to_string(fixed) +
+                                " bytes of scratch before any voxel, more than the " +
+                                std::to_string(kNoAllocScratchBytes) +
+                                "-byte (32 MiB) static array; the design itself is too large for this entry point");
+            const long long max_v = (long long)((kNoAllocScratchBytes - fixed) / per_voxel);
             throw Error(LAR_ERR_INVALID,
                         "lar_fit_log_signal_noalloc: a design of (n, p, m) = (" + std::to_string(n) + ", " +
                             std::to_string(p) + ", " + std::to_string(m) + ") with " + std::to_string(v) +

@@ -1,8 +1,8 @@
 """Input checks and signal preparation of the DWI fits (src/larmor/dwi/inputs.py).
 
-These host steps run once per volume, before the device fit: the mask check, the S0 estimate
-with its neighbourhood repair, the per-voxel floor of samples that are not finite and positive,
-and the gather of the masked voxels' float32 signals.
+The host checks the volume, table and mask; the preparation of the fit's inputs -- the gather of
+the mask voxels' float32 signals, the S0 estimate with its neighbourhood repair and the per-voxel
+floor of samples that are not finite and positive -- runs on the device (lar_stage_dwi).
 """
 
 from __future__ import annotations
@@ -10,14 +10,8 @@ from __future__ import annotations
 from dataclasses import dataclass
 
 import numpy as np
-from scipy.ndimage import uniform_filter
 
 from larmor_b200.types import GradientTable, Volume
-
-# Neighbourhood widths searched, in order, for the S0 of a voxel whose b0s are implausible.
-S0_NEIGHBOURHOODS = (3, 5)
-# Fraction of S0 that replaces a measurement that is not finite and positive.
-SIGNAL_FLOOR = 1e-3
 
 
 def check_dwi(volume: Volume, gtab: GradientTable) -> None:
@@ -41,62 +35,24 @@ def as_mask(volume: Volume, mask) -> np.ndarray:
 
 
 def estimate_s0(volume: Volume, gtab: GradientTable, mask: np.ndarray) -> np.ndarray:
-    """S0 of every voxel: the mean b0, repaired from plausible neighbours where the voxel's own
-    b0s are at or below its mean diffusion-weighted signal (src/larmor/dwi/inputs.py:78-134)."""
+    """S0 on the volume's grid (float64): each voxel's mean b0; inside the mask, a voxel whose
+    mean b0 is not above its mean diffusion-weighted sample takes the mean S0 of the plausible
+    mask voxels in its 3x3x3, else 5x5x5, neighbourhood, NaN when there is none
+    (src/larmor/dwi/inputs.py:78-134). The mask voxels' S0 and its repair come from the device
+    staging (lar_stage_dwi); outside the mask S0 is the plain b0 mean.
+
+    Raises:
+        ValueError: If the volume and table do not match or the table has no b0.
+    """
     check_dwi(volume, gtab)
     is_b0 = gtab.b0_mask
     if not np.any(is_b0):
         raise ValueError(f"No b0 volume: no b-value is at or below {gtab.b0_threshold} s/mm^2.")
-    data = volume.as_float()
-    b0_sum = data[..., is_b0].sum(axis=-1, dtype=np.float64)
-    s0 = b0_sum / is_b0.sum()
-    n_dw = int((~is_b0).sum())
-    if n_dw == 0:
-        return s0
-    mean_dw = (data.sum(axis=-1, dtype=np.float64) - b0_sum) / n_dw
-    finite = np.isfinite(s0) & np.isfinite(mean_dw)
-    plausible = mask & finite & (s0 > mean_dw)
-    to_repair = mask & finite & ~plausible
-    repaired = np.full(s0.shape, np.nan)
-    for width in S0_NEIGHBOURHOODS:
-        open_voxels = to_repair & np.isnan(repaired)
-        if not open_voxels.any():
-            break
-        size = width**3
-        count = np.rint(uniform_filter(plausible.astype(np.float64), width, mode="constant") * size)
-        total = uniform_filter(np.where(plausible, s0, 0.0), width, mode="constant")
-        found = open_voxels & (count > 0)
-        repaired[found] = total[found] * size / count[found]
-    s0[to_repair] = repaired[to_repair]
+    mask = as_mask(volume, mask)
+    s0 = volume.as_float()[..., is_b0].sum(axis=-1, dtype=np.float64) / int(is_b0.sum())
+    if mask.any():
+        s0[mask] = stage_dwi(volume, gtab, mask).s0.cpu().numpy()
     return s0
-
-
-def masked_signals(volume: Volume, voxels: tuple[np.ndarray, ...]) -> np.ndarray:
-    """The scaled float32 signals (v, N) of the given voxels, scaled as Volume.as_float does."""
-    signal = volume.data[voxels]
-    scaled = signal.astype(np.float32)
-    if volume.slope != 1.0 or volume.intercept != 0.0:
-        scaled *= np.float32(volume.slope)
-        scaled += np.float32(volume.intercept)
-    return np.ascontiguousarray(scaled)
-
-
-def largest_finite_signal(signals: np.ndarray) -> float:
-    """The largest finite value of the signals, or 1 when none is positive."""
-    finite = signals[np.isfinite(signals)]
-    largest = float(finite.max()) if finite.size else -np.inf
-    return largest if largest > 0 else 1.0
-
-
-def sample_floors(s0: np.ndarray | None, largest: float | None, v: int) -> np.ndarray:
-    """The value (v,) that replaces each voxel's samples that are not finite and positive:
-    1e-3 S0 where S0 is finite and positive, else 1e-3 times the largest finite signal
-    (src/larmor/dwi/inputs.py:227-252)."""
-    floor = np.full(v, SIGNAL_FLOOR * (1.0 if largest is None else largest))
-    if s0 is not None:
-        usable = np.isfinite(s0) & (s0 > 0)
-        floor[usable] = SIGNAL_FLOOR * s0[usable]
-    return floor
 
 
 @dataclass

@@ -1,9 +1,8 @@
 """Generates the golden fixtures of tests/golden from the reference (larmor-dmri 2.2.0).
 
-Run in a container that has the reference checkout (default /root/reference, or the path given
-as the first argument):
+Run in a container that has the reference checkout, whose path is the one required argument:
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
 
 The reference's compiled core cannot be built without Eigen and nanobind, and its Python layer
 needs Python >= 3.14. Its numpy/scipy code does run on 3.12 from a temporary copy of its source
@@ -572,4 +571,6 @@ def main(reference: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py /path/to/reference")
+    main(Path(sys.argv[1]))

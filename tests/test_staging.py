@@ -101,6 +101,22 @@ def test_device_staging_matches_the_oracle(cuda, staging_fixture, name):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_estimate_s0_matches_the_reference_on_the_grid(cuda, staging_fixture, name):
+    """dwi.estimate_s0 (the mask's S0 and repair staged on the device, the plain b0 mean outside
+    the mask) against the reference's estimate_s0 over the whole grid."""
+    from larmor_b200.dwi import estimate_s0
+
+    z = staging_fixture
+    vol, gtab = _volume(z, name)
+    got = estimate_s0(vol, gtab, z["mask"])
+    ref = z[f"{name}_s0"]
+    assert got.shape == ref.shape
+    np.testing.assert_array_equal(np.isnan(got), np.isnan(ref))
+    np.testing.assert_allclose(got, ref, rtol=1e-13, atol=0)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("dtype", ["uint16", "int32", "uint8", "float64"])
 def test_device_staging_of_a_larger_volume(cuda, dtype):
     """A 48x40x30 volume of 6 b0s + 40 dw samples with dark-b0 patches of several sizes, in

@@ -58,6 +58,47 @@ def test_no_alloc_fit_matches_the_design_handle_fit_on_two_calls_in_a_row(cuda, 
         np.testing.assert_allclose(got * scale, want * scale, rtol=0, atol=1e-10)
 
 
+@pytest.mark.gpu
+def test_no_alloc_fit_without_constraints_matches_the_design_handle_fit(cuda, dki_block):
+    """The DTI design with no constraint rows (m = 0): the route with no violator list and no
+    counters to clear, twice in a row (weighted, then ordinary on the voxels reversed)."""
+    import torch
+
+    from larmor_b200 import _core, _lib
+
+    design = np.ascontiguousarray(dki_block["dti_design"])
+    g = np.zeros((0, design.shape[1]))
+    s = dki_block["signals_f32"].astype(np.float64)[dki_block["positive"]]
+    scale = np.linalg.norm(design, axis=0)
+    dev = torch.device("cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for log_s, weighted in [(np.log(s), True), (np.log(s[::-1]), False)]:
+        log_s = np.ascontiguousarray(log_s)
+        v = len(log_s)
+        d_log = torch.from_numpy(log_s).to(dev)
+        d_params = torch.full((v, design.shape[1]), np.nan, dtype=torch.float64, device=dev)
+        d_broke = torch.full((v,), 7, dtype=torch.uint8, device=dev)
+        _noalloc(_lib, design, g, d_log, d_params, d_broke, weighted, stream)
+        torch.cuda.synchronize()
+        want, want_broke = _core.fit_log_signal(design, g, log_s, weighted, 20, 1e-6, 1)
+        got_broke = d_broke.cpu().numpy().astype(bool)
+        np.testing.assert_array_equal(got_broke, want_broke)
+        assert not got_broke.any()
+        np.testing.assert_allclose(d_params.cpu().numpy() * scale, want * scale, rtol=0, atol=1e-10)
+
+
+def test_no_alloc_fit_refuses_a_design_larger_than_its_array():
+    from larmor_b200 import _lib
+
+    x = np.ascontiguousarray(np.random.default_rng(0).normal(size=(80_000, 32)))
+    status = _lib.lib().lar_fit_log_signal_noalloc(
+        _lib.ptr(x), 80_000, 32, ctypes.c_void_p(None), 0, ctypes.c_void_p(None), 10, 1, 20, 1e-6,
+        ctypes.c_void_p(None), ctypes.c_void_p(None), ctypes.c_void_p(None))
+    assert status == _lib.LAR_ERR_INVALID
+    message = _lib.lib().lar_last_error().decode()
+    assert "design itself is too large" in message
+
+
 def test_no_alloc_fit_refuses_more_voxels_than_its_array_holds():
     from larmor_b200 import _lib
 
