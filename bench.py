@@ -470,7 +470,11 @@ class MfodWorkload(_SdWorkloadBase):
     name = "mfod_3tissue_110x110x70"
     kernels = ("correlate_kernel", "ridge_nnls_half_kernel<3>", "ridge_nnls_kernel<1,2>", "lr_fractions_kernel",
                "ridge_nnls_kernel<8,10>", "hr_fractions_kernel")
-    has_fp32 = False
+    has_fp32 = True
+    # The plain FP32 fit takes seconds per step: a few timed steps bound the run.
+    fp32_steps = 2
+    fp32_what = ("lar_fit_multi_tissue_plain_fp32: one warp per voxel runs all its rounds in FP32 with the "
+                 "textbook Lawson-Hanson steps (the direct GPU port of the reference's per-voxel loop)")
     # 280 double samples in, 300 double amplitudes + 3 fractions out.
     bytes_per_voxel = 8 * 280 + 8 * 303
 
@@ -510,10 +514,22 @@ class MfodWorkload(_SdWorkloadBase):
         self.d_fr = torch.empty((self.v, 3), dtype=torch.float64, device=dev)
         self.h2d_bytes = self.norm.nbytes
         self.d2h_bytes = self.v * (self.k_hr.ca + 3) * 8
+        if type(self) is MfodWorkload:
+            # The plain single-precision fit's inputs and outputs.
+            self.d_signals32 = self.d_signals.float()
+            self.d_fods32 = torch.empty((self.v, self.k_hr.ca), dtype=torch.float32, device=dev)
+            self.d_fr32 = torch.empty((self.v, 3), dtype=torch.float32, device=dev)
+            self.d_rounds32 = torch.empty((self.v,), dtype=torch.int32, device=dev)
+            self.d_status32 = torch.empty((self.v,), dtype=torch.uint8, device=dev)
 
     def step_device(self, precision=0):
         from larmor_b200 import _core
 
+        if precision == 1:
+            _core.fit_multi_tissue_plain_fp32_device(self.d_signals32, self.lr.weights, self.k_lr, self.lr_solver,
+                                                     self.k_hr, self.hr_solver, 50, 1e-7, 1e-2, self.d_fods32,
+                                                     self.d_fr32, self.d_rounds32, self.d_status32)
+            return
         _core.fit_multi_tissue_device(self.d_signals, self.lr.weights, self.k_lr, self.lr_solver, self.k_hr,
                                       self.hr_solver, 50, 1e-7, 1e-2, self.d_fods, self.d_fr)
 
@@ -562,6 +578,24 @@ class MfodWorkload(_SdWorkloadBase):
         return done, time.perf_counter() - t0, (f"{len(idx)} voxels spread evenly over the volume, repeated for "
                                                 f"~{budget_s:.0f} s")
 
+    def fp32_parity(self) -> dict:
+        """The plain FP32 fit against the same FP64 oracle fit of the cpu_baseline sample."""
+        fods, fr, rounds = self.reference_out
+        self.step_device(precision=1)
+        idx = self.torch.from_numpy(self.sample).to(self.d_fods32.device)
+        got = self.d_fods32[idx].double().cpu().numpy()
+        got_fr = self.d_fr32[idx].double().cpu().numpy()
+        got_rounds = self.d_rounds32[idx].cpu().numpy()
+        status = self.d_status32[idx].cpu().numpy()
+        scale = np.maximum(np.abs(fods).max(axis=1), 1e-300)
+        rel = np.abs(got - fods).max(axis=1) / scale
+        return {"voxels": int(len(self.sample)), "fod_rel_max": float(rel.max()),
+                "fod_rel_median": float(np.median(rel)), "fod_rel_p99": float(np.percentile(rel, 99)),
+                "fractions_abs_max": float(np.abs(got_fr - fr).max()),
+                "identical_active_sets": float(((got > 0) == (fods > 0)).all(axis=1).mean()),
+                "identical_round_counts": float((got_rounds == rounds).mean()),
+                "status_nonzero": float((status != 0).mean())}
+
     def parity(self) -> dict:
         """The device fit of the whole volume against the FP64 oracle on the cpu_baseline sample:
         the FOD amplitudes' largest error relative to the voxel's largest amplitude, the
@@ -581,6 +615,7 @@ class MfodWorkload(_SdWorkloadBase):
         e2e_same = bool(np.array_equal(e2e_fods[self.sample], got) and np.array_equal(e2e_fr[self.sample], got_fr))
         return {"against": "FP64 oracle (C++ restatement of cpp/src/sd/{nnls,fractions,multi_tissue}.cpp)",
                 "voxels": int(len(self.sample)), "sample": "spread evenly over the volume",
+                "fods": "the 300 high-resolution amplitudes",
                 "fod_rel_max": rel, "fractions_abs_max": fr_err,
                 "identical_active_sets": same_set, "identical_round_counts": same_rounds,
                 "e2e_equals_device_fit": e2e_same,
@@ -925,6 +960,7 @@ class GrlWorkload(MfodWorkload):
     name = "grl_3tissue_110x110x70"
     kernels = ("drl_kernel_resident", "drl_kernel", "lr_fractions_kernel", "hr_fractions_kernel")
     fraction_tol = 1e-3
+    has_fp32 = False
 
     def __init__(self, seed: int) -> None:
         from larmor_b200.synthetic import mfod_model_responses
@@ -1307,11 +1343,12 @@ def measure(wl, args, world: int, rank: int, dist, dev) -> dict:
 
     # The plain FP32 kernel, for comparison.
     fp32_ms = None
+    fp32_steps = max(1, min(args.steps, getattr(wl, "fp32_steps", args.steps)))
     if wl.has_fp32:
-        for _ in range(args.warmup):
+        for _ in range(min(args.warmup, fp32_steps)):
             wl.step_device(precision=1)
         barrier()
-        fp32_ms = max_over_ranks(timed(lambda: wl.step_device(precision=1), args.steps))
+        fp32_ms = max_over_ranks(timed(lambda: wl.step_device(precision=1), fp32_steps))
 
     # End to end through host buffers.
     e2e_steps = max(1, min(args.steps, getattr(wl, "e2e_steps", args.steps)))
@@ -1359,8 +1396,9 @@ def measure(wl, args, world: int, rank: int, dist, dev) -> dict:
         "e2e": {"value": voxels_all * e2e_steps / (e2e_ms / 1e3), "unit": getattr(wl, "unit", "voxel fits/s"),
                 "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes, "steps": e2e_steps},
         "plain_fp32": None if fp32_ms is None else {
-            "value": voxels_all * args.steps / (fp32_ms / 1e3), "unit": "voxel fits/s",
-            "ms_per_step": fp32_ms / args.steps, "parity": fp32_parity},
+            "value": voxels_all * fp32_steps / (fp32_ms / 1e3), "unit": "voxel fits/s",
+            "ms_per_step": fp32_ms / fp32_steps, "steps": fp32_steps, "parity": fp32_parity,
+            "what": getattr(wl, "fp32_what", "the same kernels in FP32 (precision=LAR_FP32)")},
         "parity": parity,
         "gpu_launches": launches,
         "clocks": clocks.summary(),

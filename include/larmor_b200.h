@@ -45,6 +45,7 @@ extern "C" {
  * single-precision variant of the same kernels, kept as the comparison baseline. */
 #define LAR_FP64 0
 #define LAR_FP32 1
+#define LAR_TF32X3 2 /* dRL only: products on the tensor cores as three TF32 products, FP32 state */
 
 /* Sample types of a raw volume for lar_stage_dwi. */
 #define LAR_DTYPE_F32 0
@@ -192,6 +193,19 @@ int lar_drl_create(const double* k_t, const double* k_t_k, int64_t c, int64_t m,
                    double init, lar_fod_solver* out);
 
 int lar_l2nnls_create(const double* k, int64_t m, int64_t c, double reg, double tol_x, lar_fod_solver* out);
+
+/* The arithmetic of a dRL solver's fits (no reference counterpart: the reference computes in
+ * double). LAR_FP64 (the default): the FP64 kernels, the reference's arithmetic. LAR_TF32X3:
+ * for 65 to 320 directions, each iteration's product K^T K f on the tcgen05 tensor cores as
+ * three TF32 products with FP32 accumulation (the operands split into TF32 heads and FP32
+ * remainders), the amplitudes and their update in FP32: FODs within 1e-4 of the voxel's
+ * largest amplitude of the FP64 fit. Fails with LAR_ERR_INVALID for another solver, precision
+ * or size. */
+int lar_drl_set_precision(lar_fod_solver solver, int precision);
+
+/* 1 in *out when a tensor-core dRL fit of this solver stopped at a bounded wait (its FODs are
+ * then not valid), else 0. Waits for the device. */
+int lar_drl_errors(lar_fod_solver solver, int* out);
 void lar_fod_solver_destroy(lar_fod_solver solver);
 
 /* One resolution of a multi-tissue kernel (host arrays): k_aniso (m, ca), k_iso and w_k_iso
@@ -229,6 +243,19 @@ int lar_fit_multi_tissue_async(const double* signals, int64_t v, const double* w
                                lar_fod_solver lr_solver, lar_deconv_kernel hr, lar_fod_solver hr_solver,
                                int64_t max_outer, double fraction_tol, double final_tol_x, double* fods,
                                double* fractions, int32_t* rounds, uint8_t* status, void* stream);
+
+/* The plain single-precision multi-tissue fit, the comparison baseline of lar_fit_multi_tissue
+ * (no reference counterpart: the reference computes in double only). The same model and
+ * arguments in FP32: signals (v, m), FODs (v, ca_hr) and fractions (v, nb + ci) are device
+ * floats, weights (m,) a host double array. One warp per voxel runs all its rounds in one kernel
+ * with the textbook Lawson-Hanson steps (a Cholesky factor formed anew for every fit, at most 64
+ * active columns, no QR fallback). Takes L2NNLS solvers, at most 512 measurements, 320
+ * directions and 4 fraction columns. status (v,) gets 0, 1 (the factor failed) or 2 (a step
+ * limit); rounds and status may be NULL. */
+int lar_fit_multi_tissue_plain_fp32(const float* signals, int64_t v, const double* weights, lar_deconv_kernel lr,
+                                    lar_fod_solver lr_solver, lar_deconv_kernel hr, lar_fod_solver hr_solver,
+                                    int64_t max_outer, double fraction_tol, double final_tol_x, float* fods,
+                                    float* fractions, int32_t* rounds, uint8_t* status, void* stream);
 
 /* Solves one non-negative least-squares problem, min ||c x - d|| over x >= 0, for c (m, n)
  * row-major and d (m,), device doubles, by Lawson-Hanson with QR fits and at most 3 n inner

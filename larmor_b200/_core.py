@@ -470,6 +470,30 @@ class FodSolver(_Handle):
                                              float(init), ctypes.byref(solver._handle)))
         return solver
 
+    def set_precision(self, precision: str) -> "FodSolver":
+        """The arithmetic of a dRL solver's fits: "fp64" (the default, the reference's) or
+        "tf32x3" (65 to 320 directions: each iteration's product on the tcgen05 tensor cores as
+        three TF32 products, FP32 amplitudes; FODs within 1e-4 of the voxel's largest amplitude
+        of the FP64 fit); lar_drl_set_precision.
+
+        Raises:
+            ValueError: If the solver is not a dRL solver, or tf32x3 does not take its size.
+        """
+        codes = {"fp64": _lib.LAR_FP64, "tf32x3": _lib.LAR_TF32X3}
+        if precision not in codes:
+            raise ValueError(f"precision must be one of {', '.join(codes)}, got {precision!r}")
+        _lib.check(_lib.lib().lar_drl_set_precision(self._handle, codes[precision]))
+        self.precision = precision
+        return self
+
+    def check_errors(self) -> None:
+        """Raises RuntimeError when a tensor-core fit of this solver stopped at a bounded wait
+        (lar_drl_errors)."""
+        flag = ctypes.c_int(0)
+        _lib.check(_lib.lib().lar_drl_errors(self._handle, ctypes.byref(flag)))
+        if flag.value:
+            raise RuntimeError("a tensor-core dRL fit stopped at a bounded wait; its FODs are not valid")
+
     @staticmethod
     def lasso(*_args, **_kwargs):
         raise NotImplementedError("the elastic-net solver is not part of larmor_b200")
@@ -554,6 +578,19 @@ def fit_multi_tissue_device(signals, weights, lr, lr_solver, hr, hr_solver, max_
     weights = np.ascontiguousarray(weights, dtype=np.float64)
     entry = _lib.lib().lar_fit_multi_tissue_async if asynchronous else _lib.lib().lar_fit_multi_tissue
     _lib.check(entry(
+        _lib.ptr(signals), signals.shape[0], _lib.ptr(weights), lr.handle, lr_solver.handle, hr.handle,
+        hr_solver.handle, int(max_outer), float(fraction_tol), float(final_tol_x), _lib.ptr(fods),
+        _lib.ptr(fractions), _lib.ptr(rounds), _lib.ptr(status), _stream(torch)))
+
+
+def fit_multi_tissue_plain_fp32_device(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol,
+                                       final_tol_x, fods, fractions, rounds=None, status=None) -> None:
+    """The plain single-precision fit of fit_multi_tissue_device, the comparison baseline: float32
+    signals (v, m) in, float32 FODs (v, ca_hr) and fractions (v, nb + ci) out (torch CUDA
+    tensors; weights a host array); lar_fit_multi_tissue_plain_fp32."""
+    torch = _torch()
+    weights = np.ascontiguousarray(weights, dtype=np.float64)
+    _lib.check(_lib.lib().lar_fit_multi_tissue_plain_fp32(
         _lib.ptr(signals), signals.shape[0], _lib.ptr(weights), lr.handle, lr_solver.handle, hr.handle,
         hr_solver.handle, int(max_outer), float(fraction_tol), float(final_tol_x), _lib.ptr(fods),
         _lib.ptr(fractions), _lib.ptr(rounds), _lib.ptr(status), _stream(torch)))

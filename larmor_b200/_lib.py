@@ -42,12 +42,15 @@ SIGNATURES: dict[str, tuple] = {
     "lar_deconv_kernel_destroy": (None, [_p]),
     "lar_fit_multi_tissue": (_i32, [_p, _i64, _p, _p, _p, _p, _p, _i64, _f64, _f64, _p, _p, _p, _p, _p]),
     "lar_fit_multi_tissue_async": (_i32, [_p, _i64, _p, _p, _p, _p, _p, _i64, _f64, _f64, _p, _p, _p, _p, _p]),
+    "lar_fit_multi_tissue_plain_fp32": (_i32, [_p, _i64, _p, _p, _p, _p, _p, _i64, _f64, _f64, _p, _p, _p, _p, _p]),
     "lar_lsqnonneg": (_i32, [_p, _i64, _i64, _p, _i32, _f64, _p, _p]),
     "lar_fit_single_tissue": (_i32, [_p, _i64, _p, _p, _p, _p]),
     "lar_sh_projector_create": (_i32, [_p, _i64, _i64, _p]),
     "lar_sh_projector_destroy": (None, [_p]),
     "lar_project_sh": (_i32, [_p, _p, _i64, _i64, _i32, _p, _i64, _p]),
     "lar_drl_create": (_i32, [_p, _p, _i64, _i64, _f64, _i64, _f64, _p]),
+    "lar_drl_set_precision": (_i32, [_p, _i32]),
+    "lar_drl_errors": (_i32, [_p, _p]),
     "lar_csd_create": (_i32, [_p, _i64, _i64, _p, _i64, _p, _i64, _f64, _f64, _i64, _p]),
     "lar_csd_destroy": (None, [_p]),
     "lar_fit_csd": (_i32, [_p, _p, _i64, _p, _p, _p]),
@@ -62,7 +65,7 @@ SIGNATURES: dict[str, tuple] = {
 }
 
 LAR_OK, LAR_ERR_INVALID, LAR_ERR_CUDA, LAR_ERR_MEMORY = 0, 1, 2, 3
-LAR_FP64, LAR_FP32 = 0, 1
+LAR_FP64, LAR_FP32, LAR_TF32X3 = 0, 1, 2
 # Sample types of lar_stage_dwi, by numpy dtype.
 LAR_DTYPES = {"float32": 0, "float64": 1, "int16": 2, "uint16": 3, "int8": 4, "uint8": 5, "int32": 6, "uint32": 7}
 

@@ -11,13 +11,19 @@
 // constraints up to rounding. Where any step fails the voxel keeps its unconstrained fit, as
 // in the reference.
 //
+// The NNLS matrix C = [R^-T G^T; -(G p_free)^T] ((p+1) x m) is never formed whole. Its
+// gradient C^T r is G t with t = R^-1 r[:p] - r[p] p_free (G, shared by every voxel, stays in
+// L2), and only the columns that join the active set are formed, each once per voxel, into a
+// column cache. So a voxel moves its design's QR and the few columns it uses, not the 768-column
+// system (which made the kernel move ~300x its algorithmic bytes).
+//
 // Work distribution: the violators were compacted into a list by the unconstrained fit; a
 // fixed number of warps take them from a device work counter (no host round trip, so the pair
 // of launches can be captured in a CUDA graph). Each warp owns a slot of global scratch
-// memory: the QR of the weighted design (n x p), the NNLS matrix ((p+1) x m), the active
-// columns' QR ((p+1) x 64), and the NNLS vectors. Lanes split the rows of the design for the
-// reflections, the m constraint columns for gradients and steps, and the active columns for
-// the small QR.
+// memory: the QR of the weighted design (n x p), the column cache (m x (p+1), touched only for
+// the columns used), the active columns' QR ((p+1) x 64), and the NNLS vectors. Lanes split
+// the rows of the design for the reflections, the m constraint columns for gradients and
+// steps, and the active columns for the small QR.
 
 #include <algorithm>
 #include <cfloat>
@@ -41,33 +47,188 @@ constexpr double kConstraintTolerance = 1e-9;
 __device__ __forceinline__ double wsum(double v) { return warp_sum(v); }
 __device__ __forceinline__ double wmax(double v) { return warp_max(v); }
 
-// Per-warp shared state.
+// Per-warp shared state (p + 1 <= 32).
 struct WarpShared {
-    double vec[4][64];  // p-sized vectors: unconstrained and free solutions, scratch
-    double tau[64];     // reflectors of the weighted design
-    double qtau[kMaxActive], qnu[kMaxActive], qnd[kMaxActive], rv[64], res[64];
+    double vec[4][32];  // p- or (p+1)-sized vectors: unconstrained and free solutions, scratch
+    double tau[32];     // reflectors of the weighted design
+    double qtau[kMaxActive], qnu[kMaxActive], qnd[kMaxActive], rv[32], res[32];
+    double t[32];       // R^-1 r[:p] - r[p] p_free of the gradient
+    double ysub[31 * 32];  // one forward substitution per lane, entry i at [i * 32 + lane]
     int qperm[kMaxActive];
     int act[kMaxActive];
     int n_act;
 };
 
+// The NNLS system C = [R^-T G^T; -(G p_free)^T] of one voxel, formed column by column on demand.
+struct ImplicitSystem {
+    const double* g;      // (m, p) constraints
+    const double* qr;     // (n, p): R in its upper triangle
+    const double* pfree;  // (p,)
+    double* cache;        // (m, p + 1)
+    uint8_t* ready;       // (m,)
+    int p, m;
+    // Column c into the cache (lane 0), unless it is there: forward substitution R^T y = g_c,
+    // then y_p = -g_c p_free.
+    __device__ void form(int c, int lane) const {
+        if (lane == 0 && !ready[c]) {
+            const double* gc = g + size_t(c) * p;
+            double* col = cache + size_t(c) * (p + 1);
+            double gf = 0.0;
+            for (int i = 0; i < p; ++i) {
+                double si = gc[i];
+                for (int k = 0; k < i; ++k) si -= qr[size_t(k) * p + i] * col[k];
+                col[i] = si / qr[size_t(i) * p + i];
+                gf += gc[i] * pfree[i];
+            }
+            col[p] = -gf;
+            ready[c] = 1;
+        }
+        __syncwarp();
+    }
+};
+
+struct CachedColumns {
+    const double* cache;
+    int rows;
+    __device__ __forceinline__ double operator()(int r, int col, int /*q*/) const {
+        return cache[size_t(col) * rows + r];
+    }
+};
+
+// Lawson-Hanson with QR fits on C (rows = p + 1, m columns) and d, as warp_nnls_explicit, with
+// C's gradient C^T (d - C u) = G t and the active columns from the cache. Returns 1 when the
+// method ended by its rule, 0 when the inner-step limit ran out, -1 past acap active columns.
+__device__ int implicit_nnls(const ImplicitSystem& sys, const double* d, double tol, int max_inner, NnlsScratch s,
+                             double* t, int lane) {
+    const int m = sys.m, p = sys.p, rows = p + 1;
+    const CachedColumns cols{sys.cache, rows};
+    for (int j = lane; j < m; j += 32) {
+        s.u[j] = 0.0;
+        s.z[j] = 0.0;
+        s.flag[j] = 0;
+    }
+    if (lane == 0) *s.n_act = 0;
+    __syncwarp();
+    int inner = 0;
+    for (;;) {
+        const int na = *s.n_act;
+        for (int r = lane; r < rows; r += 32) {
+            double acc = d[r];
+            for (int q = 0; q < na; ++q) acc -= sys.cache[size_t(s.act[q]) * rows + r] * s.u[s.act[q]];
+            s.res[r] = acc;
+        }
+        __syncwarp();
+        // t = R^-1 res[:p] - res[p] p_free (back substitution on lane 0).
+        if (lane == 0) {
+            for (int i = p - 1; i >= 0; --i) {
+                double acc = s.res[i];
+                for (int j = i + 1; j < p; ++j) acc -= sys.qr[size_t(i) * p + j] * t[j];
+                t[i] = acc / sys.qr[size_t(i) * p + i];
+            }
+            const double rp = s.res[p];
+            for (int i = 0; i < p; ++i) t[i] -= rp * sys.pfree[i];
+        }
+        __syncwarp();
+        // The gradient of every inactive column, g_c . t, lanes over the columns (each lane in
+        // increasing order: the first on a tie).
+        double bv = 0.0;
+        int bi = -1;
+        for (int c = lane; c < m; c += 32) {
+            if (s.flag[c]) continue;
+            const double* gc = sys.g + size_t(c) * p;
+            double w = 0.0;
+            for (int a = 0; a < p; ++a) w += gc[a] * t[a];
+            if (bi < 0 || w > bv) {
+                bv = w;
+                bi = c;
+            }
+        }
+        const int e = warp_argmax_first(bv, bi);
+        const double ge = e >= 0 ? __shfl_sync(0xffffffffu, bv, e & 31) : 0.0;
+        if (e < 0 || ge <= tol) return 1;
+        if (na >= s.acap) return -1;
+        sys.form(e, lane);
+        if (lane == 0) {
+            int q = na;
+            while (q > 0 && s.act[q - 1] > e) {
+                s.act[q] = s.act[q - 1];
+                --q;
+            }
+            s.act[q] = e;
+            *s.n_act = na + 1;
+            s.flag[e] = 1;
+        }
+        __syncwarp();
+        warp_qr_least_squares_cols(cols, rows, s.act, *s.n_act, d, s.qr, s.z, lane);
+        for (;;) {
+            const int n2 = *s.n_act;
+            bool any = false;
+            for (int q = lane; q < n2; q += 32) any |= s.z[s.act[q]] <= 0.0;
+            if (!__any_sync(0xffffffffu, any)) break;
+            if (++inner > max_inner) {
+                for (int j = lane; j < m; j += 32) s.u[j] = s.flag[j] ? s.z[j] : 0.0;
+                __syncwarp();
+                return 0;
+            }
+            double sv = 0.0;
+            int si = -1;
+            for (int q = lane; q < n2; q += 32) {
+                const int col = s.act[q];
+                if (s.z[col] > 0.0) continue;
+                const double dist = s.u[col] - s.z[col];
+                const double st = dist > 0.0 ? s.u[col] / dist : 0.0;
+                if (si < 0 || st < sv || (st == sv && col < si)) {
+                    sv = st;
+                    si = col;
+                }
+            }
+            double step;
+            const int bcol = warp_argmin_first(sv, si, &step);
+            for (int j = lane; j < m; j += 32) {
+                const double zj = s.flag[j] ? s.z[j] : 0.0;
+                s.u[j] += step * (zj - s.u[j]);
+            }
+            __syncwarp();
+            if (lane == 0) {
+                s.u[bcol] = 0.0;
+                int w = 0;
+                for (int q = 0; q < n2; ++q) {
+                    const int col = s.act[q];
+                    if (col == bcol || !(fabs(s.u[col]) >= tol)) {
+                        s.flag[col] = 0;
+                        continue;
+                    }
+                    s.act[w++] = col;
+                }
+                *s.n_act = w;
+            }
+            __syncwarp();
+            warp_qr_least_squares_cols(cols, rows, s.act, *s.n_act, d, s.qr, s.z, lane);
+        }
+        for (int j = lane; j < m; j += 32) s.u[j] = s.flag[j] ? s.z[j] : 0.0;
+        __syncwarp();
+    }
+}
+
 template <class Src>
 __global__ void __launch_bounds__(kCWarps * 32, 4) constrained_fit_kernel(
     LogDesignDevice<double> d, Src src, int weighted, ViolatorList<double> list, int* queue,
     double* __restrict__ workspace, size_t slot_doubles, double* __restrict__ params) {
-    __shared__ WarpShared shared[kCWarps];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WarpShared* shared = reinterpret_cast<WarpShared*>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     WarpShared& sh = shared[warp];
     const int n = d.n, p = d.p, m = d.m, rows = p + 1;
     double* slot = workspace + (size_t(blockIdx.x) * kCWarps + warp) * slot_doubles;
     double* qr = slot;                          // (n, p) row-major
-    double* cm = qr + size_t(n) * p;            // (rows, m) row-major
-    double* sub = cm + size_t(rows) * m;        // (kMaxActive, rows) QR of the active columns
+    double* cache = qr + size_t(n) * p;         // (m, rows): column c of C at cache[c * rows]
+    double* sub = cache + size_t(rows) * m;     // (kMaxActive, rows) QR of the active columns
     double* u = sub + size_t(rows) * kMaxActive;  // (m,)
     double* z = u + m;                          // (m,)
     double* ys = z + m;                         // (n,) log signals, then weighted
     double* rw = ys + n;                        // (n,) root weights
     uint8_t* flag = reinterpret_cast<uint8_t*>(rw + n);  // (m,) active flags
+    uint8_t* ready = flag + m;                           // (m,) whether cache holds column c
     const int total = min(*list.count, list.capacity);
     for (;;) {
         int idx = 0;
@@ -183,70 +344,51 @@ __global__ void __launch_bounds__(kCWarps * 32, 4) constrained_fit_kernel(
             }
         }
         __syncwarp();
-        // NNLS matrix: rows 0..p-1 = R^-T G^T, row p = -(G p_free)^T; lanes over constraints, four
-        // columns at a time so that their substitution chains overlap.
+        // The NNLS tolerance 10 eps norm1(C) max(p + 1, m) needs every column's absolute sum:
+        // sum_i |(R^-T g_c)_i| + |g_c p_free|. Lanes over constraints, each substitution's
+        // entries in the warp's shared column of ysub; the columns themselves are not kept.
         double colsum_max = 0.0;
-        for (int c0 = lane; c0 < m; c0 += 4 * 32) {
-            int cc[4];
-            bool in[4];
-            double acc_abs[4], gf[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                cc[q] = c0 + 32 * q;
-                in[q] = cc[q] < m;
-                acc_abs[q] = 0.0;
-                gf[q] = 0.0;
-            }
+        double* ysub = sh.ysub;
+        for (int c = lane; c < m; c += 32) {
+            const double* gc = d.g + size_t(c) * p;
+            double acc_abs = 0.0, gf = 0.0;
             for (int i = 0; i < p; ++i) {
-                double sv[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) sv[q] = in[q] ? d.g[size_t(cc[q]) * p + i] : 0.0;
-                for (int k = 0; k < i; ++k) {
-                    const double rki = qr[size_t(k) * p + i];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        if (in[q]) sv[q] -= rki * cm[size_t(k) * m + cc[q]];
+                double s0 = gc[i], s1 = 0.0;
+                int k = 0;
+                for (; k + 1 < i; k += 2) {
+                    s0 -= qr[size_t(k) * p + i] * ysub[k * 32 + lane];
+                    s1 -= qr[size_t(k + 1) * p + i] * ysub[(k + 1) * 32 + lane];
                 }
-                const double rii = qr[size_t(i) * p + i];
-                const double pf = pfree[i];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (!in[q]) continue;
-                    const double si = sv[q] / rii;
-                    cm[size_t(i) * m + cc[q]] = si;
-                    acc_abs[q] += fabs(si);
-                    gf[q] += d.g[size_t(cc[q]) * p + i] * pf;
-                }
+                if (k < i) s0 -= qr[size_t(k) * p + i] * ysub[k * 32 + lane];
+                const double si = (s0 + s1) / qr[size_t(i) * p + i];
+                ysub[i * 32 + lane] = si;
+                acc_abs += fabs(si);
+                gf += gc[i] * pfree[i];
             }
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (!in[q]) continue;
-                cm[size_t(p) * m + cc[q]] = -gf[q];
-                acc_abs[q] += fabs(gf[q]);
-                colsum_max = fmax(colsum_max, acc_abs[q]);
-                u[cc[q]] = 0.0;
-            }
+            acc_abs += fabs(gf);
+            colsum_max = fmax(colsum_max, acc_abs);
         }
         colsum_max = wmax(colsum_max);
         const double tol = 10.0 * kEps * colsum_max * double(max(rows, m));
+        for (int c = lane; c < m; c += 32) ready[c] = 0;
+        __syncwarp();
         // Lawson-Hanson (cpp/src/sd/nnls.cpp:187-221) on C u ~ e_p.
-        double* unit = sh.rv;  // e_p, then the residual rows below
+        double* unit = sh.vec[2];
         for (int r = lane; r < rows; r += 32) unit[r] = (r == p) ? 1.0 : 0.0;
         __syncwarp();
-        double* unit_copy = sh.vec[2];
-        for (int r = lane; r < rows; r += 32) unit_copy[r] = unit[r];
-        __syncwarp();
+        const ImplicitSystem sys{d.g, qr, pfree, cache, ready, p, m};
         NnlsScratch ns{u, z, flag, sh.act, &sh.n_act, sh.res,
                        QrScratch{sub, sh.qtau, sh.qnu, sh.qnd, sh.qperm, sh.rv}, kMaxActive};
-        const int outcome = warp_nnls_explicit(cm, rows, m, unit_copy, tol, kInnerStepsPerConstraint * m, ns, lane);
+        const int outcome = implicit_nnls(sys, unit, tol, kInnerStepsPerConstraint * m, ns, sh.t, lane);
         if (outcome != 1) continue;
         double* res = sh.vec[2];
-        // Residual C u - e_p over all columns with non-zero u.
+        // Residual C u - e_p over the active columns (u is zero elsewhere).
         if (lane < rows) {
             double s = (lane == p) ? -1.0 : 0.0;
-            for (int c = 0; c < m; ++c) {
+            for (int q = 0; q < sh.n_act; ++q) {
+                const int c = sh.act[q];
                 const double uc = u[c];
-                if (uc != 0.0) s += cm[size_t(lane) * m + c] * uc;
+                if (uc != 0.0) s += cache[size_t(c) * rows + lane] * uc;
             }
             res[lane] = s;
         }
@@ -289,10 +431,21 @@ __global__ void __launch_bounds__(kCWarps * 32, 4) constrained_fit_kernel(
 
 }  // namespace
 
+constexpr size_t kCSmem = kCWarps * sizeof(WarpShared);
+
+template <class Src>
+void allow_smem() {
+    static_assert(kCSmem <= 200 * 1024, "the re-fit's shared state outgrows an SM");
+    cuda_check(cudaFuncSetAttribute(constrained_fit_kernel<Src>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(kCSmem)),
+               "cudaFuncSetAttribute");
+}
+
 int constrained_resident_warps() {
     int per_sm = 0;
+    allow_smem<CappedSource>();
     cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, constrained_fit_kernel<CappedSource>,
-                                                             kCWarps * 32, 0),
+                                                             kCWarps * 32, kCSmem),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     return sm_count() * ctas_per_sm(per_sm, "dki.refit.ctas_per_sm") * kCWarps;
 }
@@ -303,8 +456,9 @@ void launch_constrained(const LogDesignDevice<double>& d, const Src& src, int we
                         double* workspace, int slots, double* params, cudaStream_t stream) {
     require(d.p + 1 <= 32, "the constrained fit takes at most 31 parameters");
     const int blocks = std::max(1, slots / kCWarps);
+    allow_smem<Src>();
     LaunchScope scope("constrained_fit_kernel", stream);
-    constrained_fit_kernel<Src><<<blocks, kCWarps * 32, 0, stream>>>(
+    constrained_fit_kernel<Src><<<blocks, kCWarps * 32, kCSmem, stream>>>(
         d, src, weighted, list, queue, workspace, constrained_slot_doubles(d.n, d.p, d.m), params);
     cuda_check(cudaGetLastError(), "constrained_fit_kernel launch");
 }

@@ -331,6 +331,10 @@ bool drl_fits(int c) { return c >= 1 && c <= kWideMaxC; }
 void launch_drl_listed(const DrlDev& P, const DrlSignal& S, const int* list, int64_t count, const int* count_dev,
                        double* x, int64_t ldx, cudaStream_t st) {
     if (count == 0) return;
+    if (P.gtc != nullptr && drl_tc_fits(P.c) && drl_tc_fits_measurements(P.c, P.m)) {
+        launch_drl_tc(P, P.gtc, S, list, count, count_dev, x, ldx, P.err, st);
+        return;
+    }
     if (P.c <= kResidentMaxC)
         launch_variant<kNarrowRt, 1, true>(P, S, list, count, count_dev, x, ldx, st, "drl_kernel_resident");
     else if (P.c <= kNarrowMaxC)

@@ -2,6 +2,8 @@
 // FOD solver handle uses.
 #pragma once
 
+#include <vector>
+
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -15,6 +17,10 @@ struct DrlDev {
     const double* gram;  // (c, c): K^T K
     int c, m, n_iter;
     double nu, init;
+    // The tensor-core mode (LAR_TF32X3): K^T K split and laid out for drl_tc.cu, and a device
+    // int where that kernel records a wait that ran out; null for the FP64 kernels.
+    const float* gtc = nullptr;
+    int* err = nullptr;
 };
 
 // The signal dRL deconvolves, entry i of voxel v: s(v, i) itself (a single-tissue fit), or the
@@ -30,6 +36,16 @@ struct DrlSignal {
 
 // Whether drl_kernel takes c directions (1 to 640).
 bool drl_fits(int c);
+
+// The tensor-core dRL (drl_tc.cu): whether it takes c directions (65 to 320), its shared
+// memory, the layout of K^T K it reads (TF32 heads and remainders in 8-direction chunks), and
+// its launch over a voxel list as launch_drl_listed.
+bool drl_tc_fits(int c);
+bool drl_tc_fits_measurements(int c, int m);
+size_t drl_tc_smem_bytes(int c);
+std::vector<float> drl_tc_layout(const double* gram, int c);
+void launch_drl_tc(const DrlDev& P, const float* gtc, const DrlSignal& S, const int* list, int64_t count,
+                   const int* count_dev, double* x, int64_t ldx, int* err, cudaStream_t st);
 
 // The shared memory drl_kernel takes for c directions.
 size_t drl_smem_bytes(int c);

@@ -1,0 +1,507 @@
+// Damped Richardson-Lucy with its product F K^T K on the 5th-generation tensor cores
+// (tcgen05.mma, kind::tf32, accumulators in tensor memory): the precision mode LAR_TF32X3 of
+// FodSolver.drl.
+//
+// The iteration is that of drl.cu (cpp/src/sd/drl.cpp:39-100): p = K^T K f, then
+// f <- max(f (1 + u (K^T s - p) / (p + 1e-16)), 1e-6) with the damping u of f and nu, until a
+// voxel's total change is at most 1e-4 of its largest signal. Here the product runs as three
+// TF32 products with FP32 accumulation, P = G_hi F_hi + G_hi F_lo + G_lo F_hi, where each
+// operand is split into its TF32 head (the low 13 mantissa bits cleared) and the FP32
+// remainder: the split recovers the bits TF32 drops (the "3xTF32" scheme), so P carries FP32
+// accuracy (~1e-6 relative) instead of TF32's ~5e-4. The state F and the update are FP32; K^T s
+// is summed in FP64 and kept in FP32. The results match the FP64 path to ~1e-5 of a voxel's
+// largest amplitude (the tests bound them at the FOD tolerance 1e-4).
+//
+// Mapping: one CTA of 4 warps per SM (it takes all 512 columns of tensor memory) fits 48 voxels
+// at a time. The MMA computes P^T = G F^T: M = 128 directions per tile (ceil(c / 128) tiles),
+// N = 48 voxels, K = 8 directions per instruction. F^T's two parts (48 x c, K-major, the
+// canonical no-swizzle layout of 8 x 16-byte core matrices) stay in shared memory; G's two
+// parts are read from a copy prepared once per solver in the same layout, chunk by chunk
+// (8 directions of every tile and part, 24 KB), by bulk copies (cp.async.bulk, the TMA engine)
+// into a 4-stage ring. Thread 0 issues the copies and the MMAs, completion is tracked with
+// mbarriers (the copies' transaction bytes, tcgen05.commit for the MMAs). P and K^T s live in
+// tensor memory (lane = direction, column = voxel); after each product every warp reads its
+// 32-lane quadrant (tcgen05.ld), applies the update, writes F's parts back to shared memory
+// and sums each voxel's change in a fixed order.
+//
+// Every wait on an mbarrier is bounded (about a second); past the bound the kernel records an
+// error in *err, stops issuing work, frees its tensor memory and returns.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include <math_constants.h>
+
+#include "common.cuh"
+#include "drl.cuh"
+
+namespace lar {
+namespace {
+
+constexpr int kTcThreads = 128;
+constexpr int kTcN = 48;          // voxels per tile (the MMA's N)
+constexpr int kTcM = 128;         // directions per MMA tile (the MMA's M)
+constexpr int kTcK = 8;           // directions per MMA step (K of kind::tf32)
+constexpr int kTcStages = 4;
+constexpr int kTcMaxTiles = 3;    // up to 384 padded directions
+constexpr int kTcTmemCols = 512;
+constexpr int kTcKsCol = 256;     // K^T s at tensor-memory columns [256, 256 + tiles * N)
+constexpr long long kTcWaitCycles = 2000000000LL;  // about a second at 1.9 GHz
+
+// Bytes of one prepared chunk of G: every tile's two parts, 128 rows x 8 directions each.
+constexpr int kTcBlockBytes = kTcM * kTcK * 4;
+
+__host__ __device__ inline int tc_kpad(int c) { return (c + kTcK - 1) / kTcK * kTcK; }
+__host__ __device__ inline int tc_tiles(int c) { return (c + kTcM - 1) / kTcM; }
+__host__ __device__ inline size_t tc_chunk_bytes(int c) { return size_t(tc_tiles(c)) * 2 * kTcBlockBytes; }
+// Bytes of one part of F^T in shared memory.
+__host__ __device__ inline size_t tc_f_bytes(int c) { return size_t(kTcN) * tc_kpad(c) * 4; }
+
+// Offset (floats) of entry (row r, direction k) in a K-major block of 8 x 4 core matrices whose
+// 8-row groups are `group` floats apart.
+__host__ __device__ inline size_t kmajor_offset(int r, int k, size_t group) {
+    return size_t(r >> 3) * group + size_t(k >> 2) * 32 + size_t(r & 7) * 4 + size_t(k & 3);
+}
+
+struct TcShared {
+    unsigned long long full[kTcStages];   // a stage's bulk copy has landed
+    unsigned long long empty[kTcStages];  // the MMAs that read a stage have finished
+    unsigned long long done;              // every MMA of an iteration has finished
+    unsigned tmem_base;
+    int n_active;
+    int abort;
+    float strength[kTcN], threshold[kTcN];
+    int active[kTcN];
+    long long vox[kTcN];
+    float part[4][kTcN];
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for the phase of the given parity; false when the wait outlasts the bound.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    const long long start = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - start > kTcWaitCycles) return false;
+    return true;
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// The shared-memory matrix descriptor of a K-major operand without swizzling: 8-row groups
+// `sbo` bytes apart, the two 16-byte direction chunks of an MMA step 128 bytes apart.
+__device__ __forceinline__ unsigned long long umma_desc(const void* p, unsigned sbo) {
+    const unsigned long long addr = smem_u32(p);
+    return ((addr >> 4) & 0x3FFFull) | ((128ull >> 4) << 16) | ((unsigned long long)((sbo >> 4) & 0x3FFF) << 32) |
+           (1ull << 46);
+}
+
+// kind::tf32, FP32 accumulators, both operands K-major, M = 128, N = kTcN.
+constexpr unsigned kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (unsigned(kTcN >> 3) << 17) |
+                              (unsigned(kTcM >> 4) << 24);
+
+__device__ __forceinline__ void umma_tf32(unsigned d_tmem, unsigned long long a, unsigned long long b,
+                                          unsigned accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(kTcIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(unsigned long long* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
+    unsigned r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_st16(unsigned taddr, const float (&v)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+        "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+        "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+        "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+        "r"(__float_as_uint(v[15])));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// The TF32 head of x (its low 13 mantissa bits cleared) and the FP32 remainder.
+__device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
+    hi = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
+    lo = x - hi;
+}
+
+__device__ __forceinline__ float pow8f(float x) {
+    const float x2 = x * x, x4 = x2 * x2;
+    return x4 * x4;
+}
+
+// Entry i of the signal dRL deconvolves for `voxel` (as drl.cu's signal_at).
+__device__ __forceinline__ double tc_signal(const DrlSignal& S, int64_t voxel, int i) {
+    const double si = S.s[voxel * S.m + i];
+    if (S.w == nullptr) return si;
+    const double ws = __dmul_rn(si, S.w[i]);
+    double r = 0.0;
+    for (int t = 0; t < S.ci; ++t) r = fma(S.wiso[size_t(i) * S.ci + t], S.fiso[voxel * S.ci + t], r);
+    return fmax(ws - r, 0.0);
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    drl_tc_kernel(DrlDev P, const float* __restrict__ gtc, DrlSignal S, const int* __restrict__ list, int64_t count,
+                  const int* __restrict__ count_dev, double* __restrict__ x, int64_t ldx, int* err) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ TcShared sh;
+    if (count_dev) count = min(count, int64_t(*count_dev));
+    const int c = P.c, m = P.m, kpad = tc_kpad(c), tiles = tc_tiles(c), nq = kpad / kTcK;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const size_t fbytes = tc_f_bytes(c);
+    float* FH = reinterpret_cast<float*>(smem);
+    float* FL = reinterpret_cast<float*>(smem + fbytes);
+    unsigned char* stage_base = smem + 2 * fbytes;
+    const size_t chunk = tc_chunk_bytes(c);
+    const size_t fgroup = size_t(kpad / 4) * 32;  // floats between 8-voxel groups of F^T
+    const float nu = float(P.nu);
+
+    if (tid == 0) {
+        for (int s = 0; s < kTcStages; ++s) {
+            mbar_init(&sh.full[s], 1);
+            mbar_init(&sh.empty[s], 1);
+        }
+        mbar_init(&sh.done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        sh.abort = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh.tmem_base)),
+                     "r"(kTcTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = sh.tmem_base;
+    const unsigned lane_base = unsigned(32 * warp) << 16;
+    // Phase parities of the barriers (thread 0 tracks the stages; everyone tracks `done`).
+    unsigned full_phase = 0, empty_phase = 0, done_phase = 0;
+
+    for (int64_t p0 = int64_t(blockIdx.x) * kTcN; p0 < count && !sh.abort; p0 += int64_t(gridDim.x) * kTcN) {
+        if (tid < kTcN) sh.vox[tid] = p0 + tid < count ? (list ? int64_t(list[p0 + tid]) : p0 + tid) : -1;
+        __syncthreads();
+        // Each voxel's damping strength and stopping threshold (drl.cu), a warp per voxel.
+        for (int j = warp; j < kTcN; j += 4) {
+            const int64_t voxel = sh.vox[j];
+            if (voxel < 0) {
+                if (lane == 0) {
+                    sh.active[j] = 0;
+                    sh.strength[j] = sh.threshold[j] = 0.f;
+                }
+                continue;
+            }
+            double sum = 0.0, mx = -CUDART_INF;
+            bool any = false;
+            for (int i = lane; i < m; i += 32) {
+                const double si = tc_signal(S, voxel, i);
+                sum += si;
+                if (!isnan(si)) {
+                    mx = any ? fmax(mx, si) : si;
+                    any = true;
+                }
+            }
+            const double mean = warp_sum(sum) / m;
+            double ss = 0.0;
+            for (int i = lane; i < m; i += 32) {
+                const double si = tc_signal(S, voxel, i);
+                ss += (si - mean) * (si - mean);
+            }
+            ss = warp_sum(ss);
+            const bool all_nan = !__any_sync(0xffffffffu, any);
+            mx = warp_max(any ? mx : -CUDART_INF);
+            if (lane == 0) {
+                sh.strength[j] = float(fmax(1.0 - 4.0 * sqrt(ss / double(m - 1)), 0.0));
+                sh.threshold[j] = float(1e-4 * (all_nan ? CUDART_NAN : mx));
+                sh.active[j] = 1;
+            }
+        }
+        // The tile's signals (FP64) in the F area, then K^T s per direction (a thread per
+        // direction lane of each tile) into tensor memory, then the start value in F.
+        double* sig = reinterpret_cast<double*>(smem);
+        for (int e = tid; e < kTcN * m; e += kTcThreads) {
+            const int j = e / m, i = e - j * m;
+            const int64_t voxel = sh.vox[j];
+            sig[e] = voxel >= 0 ? tc_signal(S, voxel, i) : 0.0;
+        }
+        __syncthreads();
+        for (int t = 0; t < tiles; ++t) {
+            const int d = kTcM * t + 32 * warp + lane;
+            for (int j0 = 0; j0 < kTcN; j0 += 16) {
+                float ks[16];
+#pragma unroll
+                for (int jj = 0; jj < 16; ++jj) {
+                    double acc = 0.0;
+                    if (d < c) {
+                        const double* kt = P.k_t + size_t(d) * m;
+                        const double* sj = sig + size_t(j0 + jj) * m;
+                        for (int i = 0; i < m; ++i) acc = fma(kt[i], sj[i], acc);
+                    }
+                    ks[jj] = float(acc);
+                }
+                tmem_st16(tmem + lane_base + unsigned(kTcKsCol + t * kTcN + j0), ks);
+            }
+        }
+        tmem_wait_st();
+        __syncthreads();
+        {
+            float hi, lo;
+            split_tf32(float(P.init), hi, lo);
+            for (int e = tid; e < kTcN * kpad; e += kTcThreads) {
+                const int j = e / kpad, k = e - j * kpad;
+                const bool real = sh.vox[j] >= 0 && k < c;
+                const size_t off = kmajor_offset(j, k, fgroup);
+                FH[off] = real ? hi : 0.f;
+                FL[off] = real ? lo : 0.f;
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+
+        for (int it = 0; it < P.n_iter; ++it) {
+            if (tid == 0) {
+                int a = 0;
+                for (int j = 0; j < kTcN; ++j) a += sh.active[j];
+                sh.n_active = a;
+            }
+            __syncthreads();
+            if (sh.n_active == 0 || sh.abort) break;
+            // The product: thread 0 streams G's chunks and issues the MMAs. Chunk q + 3 is
+            // loaded into the stage chunk q - 1 used, once the MMAs of chunk q - 1 are done
+            // (those of chunk q are queued behind them meanwhile).
+            if (tid == 0) {
+                tc_fence_after();
+                bool ok = true;
+                const int preload = min(kTcStages, nq);
+                for (int q = 0; q < preload; ++q) {
+                    mbar_expect_tx(&sh.full[q], unsigned(chunk));
+                    bulk_load(stage_base + size_t(q) * chunk, reinterpret_cast<const unsigned char*>(gtc) + size_t(q) * chunk,
+                              unsigned(chunk), &sh.full[q]);
+                }
+                for (int q = 0; q < nq && ok; ++q) {
+                    const int s = q % kTcStages;
+                    ok = mbar_wait(&sh.full[s], (full_phase >> s) & 1u);
+                    full_phase ^= 1u << s;
+                    if (!ok) break;
+                    tc_fence_after();
+                    const unsigned char* st = stage_base + size_t(s) * chunk;
+                    const unsigned long long bh = umma_desc(reinterpret_cast<const unsigned char*>(FH) + size_t(q) * 256,
+                                                            unsigned(fgroup * 4));
+                    const unsigned long long bl = umma_desc(reinterpret_cast<const unsigned char*>(FL) + size_t(q) * 256,
+                                                            unsigned(fgroup * 4));
+                    for (int t = 0; t < tiles; ++t) {
+                        const unsigned long long ah = umma_desc(st + size_t(2 * t) * kTcBlockBytes, 256);
+                        const unsigned long long al = umma_desc(st + size_t(2 * t + 1) * kTcBlockBytes, 256);
+                        const unsigned d_tmem = tmem + unsigned(t * kTcN);
+                        umma_tf32(d_tmem, ah, bh, q > 0 ? 1u : 0u);
+                        umma_tf32(d_tmem, ah, bl, 1u);
+                        umma_tf32(d_tmem, al, bh, 1u);
+                    }
+                    umma_commit(&sh.empty[s]);
+                    const int r = q + kTcStages - 1;  // the chunk to load next
+                    if (q >= 1 && r < nq) {
+                        const int sp = (q - 1) % kTcStages;
+                        ok = mbar_wait(&sh.empty[sp], (empty_phase >> sp) & 1u);
+                        empty_phase ^= 1u << sp;
+                        if (!ok) break;
+                        mbar_expect_tx(&sh.full[sp], unsigned(chunk));
+                        bulk_load(stage_base + size_t(sp) * chunk,
+                                  reinterpret_cast<const unsigned char*>(gtc) + size_t(r) * chunk, unsigned(chunk),
+                                  &sh.full[sp]);
+                    }
+                }
+                // The commits no reload waited for complete with the iteration: account for
+                // their phases.
+                for (int q = 0; q < nq; ++q) {
+                    const bool waited = q + kTcStages < nq;  // chunk q's stage was reloaded
+                    if (!waited) empty_phase ^= 1u << (q % kTcStages);
+                }
+                umma_commit(&sh.done);
+                if (!ok) {
+                    sh.abort = 1;
+                    atomicExch(err, 1);
+                }
+            }
+            __syncthreads();
+            if (sh.abort) break;
+            // Everyone waits for the product.
+            if (!mbar_wait(&sh.done, done_phase & 1u)) {
+                atomicExch(err, 1);
+                sh.abort = 1;
+            }
+            done_phase ^= 1u;
+            tc_fence_after();
+            __syncthreads();
+            if (sh.abort) break;
+            // The damped update of the still-active voxels; each thread holds direction lanes.
+            float change[kTcN];
+#pragma unroll
+            for (int j = 0; j < kTcN; ++j) change[j] = 0.f;
+            for (int t = 0; t < tiles; ++t) {
+                const int d = kTcM * t + 32 * warp + lane;
+#pragma unroll
+                for (int j0 = 0; j0 < kTcN; j0 += 16) {
+                    float pv[16], kv[16];
+                    tmem_ld16(tmem + lane_base + unsigned(t * kTcN + j0), pv);
+                    tmem_ld16(tmem + lane_base + unsigned(kTcKsCol + t * kTcN + j0), kv);
+                    tmem_wait_ld();
+                    if (d >= c) continue;
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) {
+                        const int j = j0 + jj;
+                        if (!sh.active[j]) continue;
+                        const size_t off = kmajor_offset(j, d, fgroup);
+                        const float f = FH[off] + FL[off];
+                        // f^8 / (f^8 + nu^8) as 1 / (1 + (nu / f)^8): no underflow of f^8.
+                        const float q8 = pow8f(nu / f);
+                        const float damping = 1.f - sh.strength[j] * (1.f - 1.f / (1.f + q8));
+                        const float ratio = (kv[jj] - pv[jj]) / (pv[jj] + 1e-16f);
+                        const float updated = fmaxf(f * (1.f + damping * ratio), 1e-6f);
+                        float hi, lo;
+                        split_tf32(updated, hi, lo);
+                        FH[off] = hi;
+                        FL[off] = lo;
+                        change[j] += fabsf(updated - f);
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kTcN; ++j) {
+                const float v = warp_sum(change[j]);
+                if (lane == 0) sh.part[warp][j] = v;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tc_fence_before();
+            __syncthreads();
+            if (tid < kTcN && sh.active[tid]) {
+                const float total = sh.part[0][tid] + sh.part[1][tid] + sh.part[2][tid] + sh.part[3][tid];
+                if (total <= sh.threshold[tid]) sh.active[tid] = 0;
+            }
+            __syncthreads();
+        }
+        if (sh.abort) break;
+        for (int e = tid; e < kTcN * c; e += kTcThreads) {
+            const int j = e / c, k = e - j * c;
+            const int64_t voxel = sh.vox[j];
+            if (voxel >= 0) {
+                const size_t off = kmajor_offset(j, k, fgroup);
+                x[voxel * ldx + k] = double(FH[off] + FL[off]);
+            }
+        }
+        __syncthreads();
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols));
+}
+
+}  // namespace
+
+bool drl_tc_fits(int c) { return c > 64 && c <= kTcMaxTiles * kTcM && c <= 320; }
+
+// The tile's FP64 signals are staged in the kernel's shared memory before its first product.
+bool drl_tc_fits_measurements(int c, int m) { return size_t(kTcN) * m * 8 <= drl_tc_smem_bytes(c); }
+
+size_t drl_tc_smem_bytes(int c) { return 2 * tc_f_bytes(c) + size_t(kTcStages) * tc_chunk_bytes(c); }
+
+// G = K^T K in the layout the kernel's bulk copies read: chunk q (directions 8q..8q+7) holds,
+// for every tile t of 128 directions, the TF32 head then the remainder of rows 128t..128t+127,
+// each a K-major block of 8 x 4 core matrices; rows and directions past c are zero.
+std::vector<float> drl_tc_layout(const double* gram, int c) {
+    const int kpad = tc_kpad(c), tiles = tc_tiles(c), nq = kpad / kTcK;
+    const size_t block = size_t(kTcM) * kTcK;
+    std::vector<float> out(size_t(nq) * tiles * 2 * block, 0.f);
+    for (int q = 0; q < nq; ++q)
+        for (int t = 0; t < tiles; ++t)
+            for (int r = 0; r < kTcM; ++r)
+                for (int kk = 0; kk < kTcK; ++kk) {
+                    const int row = kTcM * t + r, k = kTcK * q + kk;
+                    const float v = (row < c && k < c) ? float(gram[size_t(row) * c + k]) : 0.f;
+                    uint32_t bits;
+                    std::memcpy(&bits, &v, 4);
+                    bits &= 0xFFFFE000u;
+                    float hi;
+                    std::memcpy(&hi, &bits, 4);
+                    const float lo = v - hi;
+                    const size_t base = (size_t(q) * tiles + t) * 2 * block;
+                    const size_t off = kmajor_offset(r, kk, 64);
+                    out[base + off] = hi;
+                    out[base + block + off] = lo;
+                }
+    return out;
+}
+
+void launch_drl_tc(const DrlDev& P, const float* gtc, const DrlSignal& S, const int* list, int64_t count,
+                   const int* count_dev, double* x, int64_t ldx, int* err, cudaStream_t st) {
+    if (count == 0) return;
+    require(drl_tc_fits(P.c), "the tensor-core dRL takes 65 to 320 directions");
+    const size_t smem = drl_tc_smem_bytes(P.c);
+    require(smem <= 227 * 1024, "the tensor-core dRL's shared memory outgrows an SM");
+    cuda_check(cudaFuncSetAttribute(drl_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+               "cudaFuncSetAttribute");
+    const int64_t tiles = (count + kTcN - 1) / kTcN;
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>(tiles, sm_count()));
+    LaunchScope scope("drl_tc_kernel", st);
+    drl_tc_kernel<<<unsigned(blocks), kTcThreads, smem, st>>>(P, gtc, S, list, count, count_dev, x, ldx, err);
+    cuda_check(cudaGetLastError(), "drl_tc_kernel launch");
+}
+
+}  // namespace lar

@@ -34,7 +34,7 @@ constexpr int kMaxActive = 64;
 // Doubles of global workspace one warp of the constrained re-fit uses.
 inline size_t constrained_slot_doubles(int n, int p, int m) {
     return size_t(n) * p + size_t(p + 1) * m + size_t(p + 1) * kMaxActive + 2 * size_t(m) + 2 * size_t(n) +
-           (size_t(m) + 7) / 8 + 64;
+           (2 * size_t(m) + 7) / 8 + 64;
 }
 
 // Re-fits the violators of `list` subject to g p >= 0 (cpp/src/dwi/log_fit.cpp:170-216), in

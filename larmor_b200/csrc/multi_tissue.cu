@@ -35,6 +35,7 @@
 #include "host_la.hpp"
 #include "drl.cuh"
 #include "group_nnls.cuh"
+#include "plain_fp32.cuh"
 #include "warp_chol.cuh"
 #include "warp_nnls.cuh"
 
@@ -1078,15 +1079,26 @@ __global__ void __launch_bounds__(32) lsqnonneg_kernel(const double* __restrict_
 
 }  // namespace lar
 
+namespace lar {
+// A device FP32 copy of an FP64 host array (rounded to nearest).
+inline void upload_fp32(DeviceArray<float>& dst, const std::vector<double>& src) {
+    std::vector<float> f(src.begin(), src.end());
+    dst.upload(f.data(), f.size());
+}
+}  // namespace lar
+
 // FodSolver.l2nnls (cpp/src/python/sd.cpp:89-102, cpp/src/sd/solver.cpp:464-467).
 struct lar_fod_solver_s {
     // 0: the ridge NNLS (L2NNLS) with its design below; 1: damped Richardson-Lucy (dRL).
     int kind = 0;
     lar::DeviceArray<double> drl_kt, drl_gram;
+    lar::DeviceArray<float> drl_gtc;  // K^T K for the tensor-core dRL (precision LAR_TF32X3)
+    lar::DeviceArray<int> drl_err;    // where the tensor-core dRL records a wait that ran out
     lar::DrlDev drl{};
     lar::host::RidgeDesignHost host;
     double tol = 0.0;
     lar::DeviceArray<double> k, gram;
+    lar::DeviceArray<float> k32, gram32;  // FP32 copies for the plain single-precision fit
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
     int* pinned = nullptr;  // one host int the round loop reads the next round's count into
@@ -1130,6 +1142,7 @@ struct lar_fod_solver_s {
 struct lar_deconv_kernel_s {
     int64_t m = 0, ca = 0, ci = 0, nb = 0;
     lar::DeviceArray<double> kt, iso, wiso;
+    lar::DeviceArray<float> kt32, iso32, wiso32;  // FP32 copies for the plain single-precision fit
     lar::DeviceArray<int> blocks;
     lar::TissueDev view() const {
         return lar::TissueDev{int(m), int(ca), int(ci), int(nb), kt.ptr, iso.ptr, wiso.ptr, blocks.ptr};
@@ -1346,6 +1359,45 @@ int lar_fit_multi_tissue_async(const double* signals, int64_t v, const double* w
                             fods, fractions, rounds, status, stream, true);
 }
 
+int lar_fit_multi_tissue_plain_fp32(const float* signals, int64_t v, const double* weights, lar_deconv_kernel lr,
+                                    lar_fod_solver lr_solver, lar_deconv_kernel hr, lar_fod_solver hr_solver,
+                                    int64_t max_outer, double fraction_tol, double final_tol_x, float* fods,
+                                    float* fractions, int32_t* rounds, uint8_t* status, void* stream) {
+    return guarded([&] {
+        require(lr && hr && lr_solver && hr_solver, "kernels and solvers must not be NULL");
+        require(weights != nullptr, "weights must not be NULL");
+        require(lr_solver->kind == 0 && hr_solver->kind == 0, "the plain FP32 fit takes L2NNLS solvers");
+        const int64_t m = hr->m;
+        require(lr->m == m && lr_solver->host.m == m && hr_solver->host.m == m,
+                "signals, weights and the kernels' measurements do not match");
+        require(lr_solver->host.c == lr->ca && hr_solver->host.c == hr->ca, "a solver does not match its kernel");
+        require(lr->ci == hr->ci && lr->nb == 1, "the low-resolution kernel must have one anisotropic block and the "
+                                                 "isotropic tissues of the high-resolution one");
+        require(m <= kPlainMaxMeasurements && std::max(lr->ca, hr->ca) <= kPlainMaxColumns &&
+                    hr->nb + hr->ci <= kPlainMaxGroups && 1 + lr->ci <= kPlainMaxGroups,
+                "the plain FP32 fit takes at most 512 measurements, 320 directions and 4 fraction columns");
+        require(max_outer >= 0 && v >= 0, "max_outer and v must be at least 0");
+        if (v == 0) return;
+        require(signals && fods && fractions, "signals, fods and fractions must not be NULL");
+        auto st = static_cast<cudaStream_t>(stream);
+        auto stage = [](const lar_deconv_kernel_s& k, const lar_fod_solver_s& sv) {
+            return PlainStage{int(k.m), int(k.ca), int(k.ci), int(k.nb), float(sv.tol), sv.k32.ptr, sv.gram32.ptr,
+                              k.kt32.ptr, k.iso32.ptr, k.wiso32.ptr, k.blocks.ptr};
+        };
+        std::vector<float> w32(weights, weights + m);
+        float* dw = nullptr;
+        cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&dw), size_t(m) * sizeof(float), st), "cudaMallocAsync");
+        cuda_check(cudaMemcpyAsync(dw, w32.data(), size_t(m) * sizeof(float), cudaMemcpyHostToDevice, st),
+                   "cudaMemcpyAsync");
+        launch_plain_fp32(stage(*lr, *lr_solver), stage(*hr, *hr_solver), signals, v, dw,
+                          int(std::min<int64_t>(max_outer, 1 << 20)), float(fraction_tol), float(final_tol_x), fods,
+                          fractions, rounds, status, st);
+        // The weights' host copy must outlive the copy above.
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        cuda_check(cudaFreeAsync(dw, st), "cudaFreeAsync");
+    });
+}
+
 int lar_lsqnonneg(const double* c, int64_t m, int64_t n, const double* d, int default_tol, double tol_x, double* x,
                   void* stream) {
     return guarded([&] {
@@ -1395,7 +1447,43 @@ int lar_l2nnls_create(const double* k, int64_t m, int64_t c, double reg, double 
         h->tol = tol_x;
         h->k.upload(h->host.kernel.data(), h->host.kernel.size());
         h->gram.upload(h->host.gram.data(), h->host.gram.size());
+        upload_fp32(h->k32, h->host.kernel);
+        upload_fp32(h->gram32, h->host.gram);
         *out = h.release();
+    });
+}
+
+int lar_drl_set_precision(lar_fod_solver solver, int precision) {
+    return guarded([&] {
+        require(solver != nullptr && solver->kind == 1, "solver must be a dRL solver");
+        require(precision == LAR_FP64 || precision == LAR_TF32X3, "precision must be LAR_FP64 or LAR_TF32X3");
+        if (precision == LAR_FP64) {
+            solver->drl.gtc = nullptr;
+            solver->drl.err = nullptr;
+            return;
+        }
+        const int c = int(solver->host.c);
+        require(drl_tc_fits(c) && drl_tc_fits_measurements(c, int(solver->host.m)),
+                "the tensor-core dRL takes 65 to 320 directions and at most " +
+                    std::to_string(drl_tc_smem_bytes(c) / (48 * 8)) + " measurements");
+        std::vector<double> gram(size_t(c) * c);
+        cuda_check(cudaMemcpy(gram.data(), solver->drl_gram.ptr, gram.size() * sizeof(double), cudaMemcpyDeviceToHost),
+                   "cudaMemcpy");
+        const std::vector<float> layout = drl_tc_layout(gram.data(), c);
+        solver->drl_gtc.upload(layout.data(), layout.size());
+        const int zero = 0;
+        solver->drl_err.upload(&zero, 1);
+        solver->drl.gtc = solver->drl_gtc.ptr;
+        solver->drl.err = solver->drl_err.ptr;
+    });
+}
+
+int lar_drl_errors(lar_fod_solver solver, int* out) {
+    return guarded([&] {
+        require(solver != nullptr && out != nullptr, "solver and out must not be NULL");
+        *out = 0;
+        if (solver->drl.err == nullptr) return;
+        cuda_check(cudaMemcpy(out, solver->drl.err, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy");
     });
 }
 
@@ -1422,6 +1510,7 @@ int lar_deconv_kernel_create(const double* k_aniso, int64_t m, int64_t ca, const
         for (int64_t i = 0; i < m; ++i)
             for (int64_t j = 0; j < ca; ++j) kt[size_t(j * m + i)] = k_aniso[i * ca + j];
         h->kt.upload(kt.data(), kt.size());
+        upload_fp32(h->kt32, kt);
         std::vector<double> iso(size_t(std::max<int64_t>(1, m * ci)), 0.0), wiso(iso.size(), 0.0);
         if (ci > 0) {
             std::copy(k_iso, k_iso + m * ci, iso.begin());
@@ -1429,6 +1518,8 @@ int lar_deconv_kernel_create(const double* k_aniso, int64_t m, int64_t ca, const
         }
         h->iso.upload(iso.data(), iso.size());
         h->wiso.upload(wiso.data(), wiso.size());
+        upload_fp32(h->iso32, iso);
+        upload_fp32(h->wiso32, wiso);
         std::vector<int> bl(size_t(2 * nb));
         for (int64_t b = 0; b < 2 * nb; ++b) bl[size_t(b)] = int(blocks[b]);
         h->blocks.upload(bl.data(), bl.size());

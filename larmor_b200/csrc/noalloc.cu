@@ -35,7 +35,6 @@ namespace lar {
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
-constexpr int kNoAllocMaxSlots = 128;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -87,7 +86,7 @@ extern "C" int lar_fit_log_signal_noalloc(const double* x, int64_t n, int64_t p,
         int slots = 0;
         if (m > 0) {
             const size_t room = slots_off < kNoAllocScratchBytes ? kNoAllocScratchBytes - slots_off : 0;
-            slots = int(std::min<size_t>(kNoAllocMaxSlots, room / slot_bytes)) / 4 * 4;
+            slots = int(std::min<size_t>(room / slot_bytes, 1 << 20)) / 4 * 4;
         }
         const size_t need = m > 0 ? slots_off + 4 * slot_bytes : params_off;
         if (need > kNoAllocScratchBytes || (m > 0 && slots < 4)) {
@@ -112,6 +111,8 @@ extern "C" int lar_fit_log_signal_noalloc(const double* x, int64_t n, int64_t p,
         }
 
         require(log_s && params && broke, "log_s, params and broke must not be NULL");
+        // As many warp slots as the re-fit keeps resident, as far as the array has room.
+        if (m > 0) slots = std::max(4, std::min(slots, constrained_resident_warps()) / 4 * 4);
         unsigned char* base = noalloc_scratch_address();
         auto st = static_cast<cudaStream_t>(stream);
 

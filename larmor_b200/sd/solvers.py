@@ -73,17 +73,19 @@ class DRL:
     damped. num_iter caps a single-tissue fit's iterations and hr_num_iter the final solve of a
     multi-tissue one. Both run on the device: a multi-tissue (GRL) fit solves each round's
     low-resolution FODs and the final high-resolution one by dRL, from MULTI_TISSUE_DRL_INIT,
-    with one iteration fewer than asked.
+    with one iteration fewer than asked. precision "fp64" keeps the reference's arithmetic;
+    "tf32x3" runs the solves of 65 to 320 directions on the tensor cores (FodSolver.set_precision).
 
     Raises:
-        ValueError: If an iteration count is below 1, or target_adc or nu_scale is not a
-            positive number.
+        ValueError: If an iteration count is below 1, target_adc or nu_scale is not a positive
+            number, or precision is unknown.
     """
 
     num_iter: int = 200
     hr_num_iter: int = 600
     target_adc: float = 0.7e-3
     nu_scale: float = 0.2
+    precision: str = "fp64"
 
     def __post_init__(self) -> None:
         if self.num_iter < 1 or self.hr_num_iter < 1:
@@ -93,17 +95,24 @@ class DRL:
             value = getattr(self, name)
             if not (np.isfinite(value) and value > 0):
                 raise ValueError(f"{name} must be a positive number, got {value}")
+        if self.precision not in ("fp64", "tf32x3"):
+            raise ValueError(f"precision must be 'fp64' or 'tf32x3', got {self.precision!r}")
+
+    def _solver(self, k_t, k_t_k, nu, n_iter, init) -> _core.FodSolver:
+        solver = _core.FodSolver.drl(k_t, k_t_k, nu=nu, n_iter=n_iter, init=init)
+        if self.precision != "fp64" and 64 < k_t.shape[0] <= 320:
+            solver.set_precision(self.precision)
+        return solver
 
     def _prepare(self, kernel: Kernel, bvals: np.ndarray, stage: Stage) -> _core.FodSolver:
         nu = calibrate_drl_nu(kernel, bvals, self.target_adc, self.nu_scale)
         k_t, k_t_k = _rl_products(kernel.w_k_aniso)
         if stage is Stage.SINGLE:
-            return _core.FodSolver.drl(k_t, k_t_k, nu=nu, n_iter=self.num_iter,
-                                       init=1.0 / kernel.w_k_aniso.shape[1])
+            return self._solver(k_t, k_t_k, nu, self.num_iter, 1.0 / kernel.w_k_aniso.shape[1])
         # A multi-tissue solve counts its near-zero start as the first iteration
         # (src/larmor/sd/solvers.py:144-148).
         n_iter = self.num_iter if stage is Stage.LOW_RES else self.hr_num_iter
-        return _core.FodSolver.drl(k_t, k_t_k, nu=nu, n_iter=n_iter - 1, init=MULTI_TISSUE_DRL_INIT)
+        return self._solver(k_t, k_t_k, nu, n_iter - 1, MULTI_TISSUE_DRL_INIT)
 
 
 # The FOD solvers SDModel takes (src/larmor/sd/solvers.py:296, without the elastic net, which

@@ -162,3 +162,72 @@ def test_gpu_calibration_and_single_tissue_model(cuda, oracle, drl_fixture):
     ref = to_sh(amps, fit.lmax, "tournier", exact_integral=True)
     got = fit.fods[0].reshape(-1, ref.shape[1])
     assert (np.abs(got - ref).max(axis=1) / np.abs(ref).max(axis=1)).max() < 1e-5
+
+
+# ---- the tensor-core mode (precision tf32x3) -------------------------------------------------
+
+# The tensor-core mode computes each product as three TF32 products (FP32 accuracy) and keeps
+# the amplitudes in FP32: its FODs are held to the project's FOD tolerance, 1e-4 of the voxel's
+# largest amplitude, against the FP64 fit, not to the FP64 path's 1e-10.
+TC_FOD_REL = 1e-4
+
+
+def _tc_fit(signals, k, nu, n_iter, start, precision):
+    from larmor_b200 import _core
+
+    k_t, k_t_k = _products(k)
+    solver = _core.FodSolver.drl(k_t, k_t_k, nu=nu, n_iter=n_iter, init=start)
+    if precision != "fp64":
+        solver.set_precision(precision)
+    got = _core.fit_single_tissue(np.ascontiguousarray(signals), solver, 1)
+    solver.check_errors()
+    return got
+
+
+def _rel(got, ref):
+    return np.abs(got - ref).max(axis=1) / np.abs(ref).max(axis=1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", SETTINGS)
+def test_tensor_core_drl_matches_the_reference_solver(cuda, drl_fixture, name):
+    z = drl_fixture
+    got = _tc_fit(z["signals"], z["k"], float(z[f"{name}_nu"]), 200, float(z[f"{name}_start"]), "tf32x3")
+    rel = _rel(got, z[f"{name}_fods"])
+    print(f"tensor-core dRL, {name}: FOD rel max {rel.max():.3e}, median {np.median(rel):.3e}")
+    assert rel.max() <= TC_FOD_REL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize(("n_meas", "n_dirs", "n_vox"), [(280, 300, 1000), (90, 130, 203), (60, 72, 97)])
+def test_tensor_core_drl_matches_the_oracle_on_more_voxels(cuda, oracle, n_meas, n_dirs, n_vox):
+    """Tiles of 48 voxels with a ragged last one, one to three 128-direction tiles, NaN signals."""
+    rng = np.random.default_rng(7 * n_meas + n_dirs)
+    k = np.abs(rng.normal(size=(n_meas, n_dirs))) * np.exp(-rng.uniform(0, 3, size=(n_meas, 1)))
+    fods = np.zeros((n_vox, n_dirs))
+    for f in fods:
+        f[rng.choice(n_dirs, size=rng.integers(1, 4), replace=False)] = rng.dirichlet([1.0, 1.0, 1.0])[:1]
+    signals = fods @ k.T + rng.uniform(0, 0.05, size=(n_vox, 1)) * np.abs(rng.normal(size=(n_vox, n_meas)))
+    signals[:n_vox // 2:37, 3] = np.nan
+    k_t, k_t_k = _products(k)
+    got = _tc_fit(signals, k, 0.02, 150, 1.0 / n_dirs, "tf32x3")
+    ref = oracle.drl(signals, k_t, k_t_k, 0.02, 150, 1.0 / n_dirs, n_threads=8)
+    np.testing.assert_array_equal(np.isnan(got), np.isnan(ref))
+    ok = ~np.isnan(ref).any(axis=1)
+    rel = _rel(got[ok], ref[ok])
+    print(f"tensor-core dRL {n_meas}x{n_dirs}, {n_vox} voxels: FOD rel max {rel.max():.3e}, "
+          f"median {np.median(rel):.3e}")
+    assert rel.max() <= TC_FOD_REL
+
+
+@pytest.mark.gpu
+def test_tensor_core_drl_refuses_sizes_it_does_not_take(cuda, drl_fixture):
+    from larmor_b200 import _core
+
+    k = drl_fixture["k"][:, :40]
+    k_t, k_t_k = _products(k)
+    solver = _core.FodSolver.drl(k_t, k_t_k, nu=0.1, n_iter=10, init=0.1)
+    with pytest.raises(ValueError, match="65 to 320 directions"):
+        solver.set_precision("tf32x3")
+    with pytest.raises(ValueError, match="precision must be"):
+        solver.set_precision("fp16")

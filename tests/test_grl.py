@@ -347,3 +347,25 @@ def test_gpu_lsqnonneg_tol_x_zeroes_a_small_coefficient(cuda):
     x = _core.lsqnonneg(c, d, 1e-2)
     assert x[1] == 0
     np.testing.assert_allclose(x[0], 1.0, atol=1e-2)
+
+
+@pytest.mark.gpu
+def test_gpu_grl_on_the_tensor_cores_stays_within_the_fod_tolerance(cuda, grl_fixture):
+    """The MATLAB case (one 300-direction response) with the final high-resolution solve in the
+    tensor-core mode (tf32x3): FODs within 1e-4 of the voxel's largest amplitude and fractions
+    within 1e-4 of the reference's (the low-resolution rounds, 44 directions, stay FP64)."""
+    from larmor_b200 import _core
+
+    z = grl_fixture
+    name = "matlab"
+    lr, lr_solver, hr, hr_solver = _device_case(z, name, float(z[f"{name}_lr_nu"]), float(z[f"{name}_hr_nu"]))
+    hr_solver.set_precision("tf32x3")
+    fods, fractions = _core.fit_multi_tissue(np.ascontiguousarray(z[f"{name}_signals"]), z["weights"], lr, lr_solver,
+                                             hr, hr_solver, 50, GRL_FRACTION_TOL, 1e-2, 1)
+    hr_solver.check_errors()
+    ref, ref_fr = z[f"{name}_fods"], z[f"{name}_fractions"]
+    rel = np.abs(fods - ref).max(axis=1) / np.abs(ref).max(axis=1)
+    print(f"GRL tensor-core final solve: FOD rel max {rel.max():.3e}, fractions abs max "
+          f"{np.abs(fractions - ref_fr).max():.3e}")
+    assert rel.max() <= 1e-4
+    assert np.abs(fractions - ref_fr).max() <= 1e-4

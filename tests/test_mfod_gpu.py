@@ -158,3 +158,37 @@ def test_async_multi_tissue_equals_the_waiting_call(cuda, mfod_fixture):
     np.testing.assert_array_equal(out["fr"].cpu().numpy(), fr)
     np.testing.assert_array_equal(out["rd"].cpu().numpy(), rd)
     np.testing.assert_array_equal(out["st"].cpu().numpy(), st)
+
+
+def test_plain_fp32_fit_stays_near_the_fp64_oracle(cuda, oracle, mfod_fixture):
+    """The plain single-precision fit (the comparison baseline) on the MRIToolkit block: its
+    FODs and fractions near the FP64 oracle's, at the accuracy FP32 arithmetic allows."""
+    import torch
+
+    from larmor_b200 import _core
+
+    z = mfod_fixture
+    signals, lr, hr = mfod_inputs(z)
+    lrk = _core.DeconvKernel(np.ascontiguousarray(z["lr_k_aniso"]), np.ascontiguousarray(z["lr_k_iso"]),
+                             np.ascontiguousarray(z["lr_w_k_iso"]), [(0, z["lr_k_aniso"].shape[1])])
+    hrk = _core.DeconvKernel(np.ascontiguousarray(z["hr_k_aniso"]), np.ascontiguousarray(z["hr_k_iso"]),
+                             np.ascontiguousarray(z["hr_w_k_iso"]), [tuple(b) for b in z["hr_blocks"]])
+    lr_solver = _core.FodSolver.l2nnls(np.ascontiguousarray(z["lr_w_k_aniso"]), 0.0, 1e-6)
+    hr_solver = _core.FodSolver.l2nnls(np.ascontiguousarray(z["hr_w_k_aniso"]), 0.1, 1e-6)
+    dev = torch.device("cuda")
+    v = len(signals)
+    s = torch.from_numpy(np.ascontiguousarray(signals)).to(dev).float()
+    fods = torch.empty((v, hrk.ca), dtype=torch.float32, device=dev)
+    fr = torch.empty((v, hrk.nb + hrk.ci), dtype=torch.float32, device=dev)
+    rd = torch.empty((v,), dtype=torch.int32, device=dev)
+    st = torch.empty((v,), dtype=torch.uint8, device=dev)
+    _core.fit_multi_tissue_plain_fp32_device(s, z["weights"], lrk, lr_solver, hrk, hr_solver, 50, 1e-7, 1e-2, fods,
+                                             fr, rd, st)
+    got, got_fr = fods.double().cpu().numpy(), fr.double().cpu().numpy()
+    rfods, rfr = oracle.fit_multi_tissue(signals, z["weights"], lr, hr, n_threads=4)
+    rel = np.abs(got - rfods).max(axis=1) / np.abs(rfods).max(axis=1)
+    print(f"plain FP32, {v} voxels: FOD rel max {rel.max():.3e}, median {np.median(rel):.3e}; fractions abs max "
+          f"{np.abs(got_fr - rfr).max():.3e}; status nonzero {(st.cpu().numpy() != 0).mean():.4f}")
+    assert np.isfinite(got).all() and np.isfinite(got_fr).all()
+    assert np.median(rel) <= 1e-2
+    assert np.abs(got_fr - rfr).max() <= 1e-2
