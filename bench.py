@@ -74,6 +74,9 @@ def committed_traffic(kernel: str, workload: str, algorithmic_bytes: float) -> f
 # (stage_dwi); the CPU reference arm, which runs no GPU code, with the oracle's numpy staging.
 # Both give the same float32 signals, and S0 and floors to 1e-13.
 REFERENCE_ARM = False
+# dRL's arithmetic in the drl and grl workloads: "fp64" (the reference's) or "tf32x3" (the
+# 300-direction solves on the tcgen05 tensor cores).
+DRL_PRECISION = "fp64"
 
 
 def staged_inputs(w):
@@ -471,6 +474,7 @@ class MfodWorkload(_SdWorkloadBase):
     kernels = ("correlate_kernel", "ridge_nnls_half_kernel<3>", "ridge_nnls_kernel<1,2>", "lr_fractions_kernel",
                "ridge_nnls_kernel<8,10>", "hr_fractions_kernel")
     has_fp32 = True
+    fraction_tol = 1e-7
     # The plain FP32 fit takes seconds per step: a few timed steps bound the run.
     fp32_steps = 2
     fp32_what = ("lar_fit_multi_tissue_plain_fp32: one warp per voxel runs all its rounds in FP32 with the "
@@ -560,7 +564,7 @@ class MfodWorkload(_SdWorkloadBase):
         from larmor_b200 import _core
 
         self.e2e_out = _core.fit_multi_tissue(self.norm, self.lr.weights, self.k_lr, self.lr_solver, self.k_hr,
-                                              self.hr_solver, 50, 1e-7, 1e-2, n_threads=1)
+                                              self.hr_solver, 50, self.fraction_tol, 1e-2, n_threads=1)
 
     def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
         from oracle import oracle as o
@@ -888,7 +892,7 @@ class DrlWorkload(_SdWorkloadBase):
     up to 200 iterations per voxel."""
 
     name = "drl_single_tissue_110x110x70"
-    kernels = ("drl_kernel",)
+    kernels = ("drl_kernel", "drl_tc_kernel")
     has_fp32 = False
 
     def __init__(self, seed: int) -> None:
@@ -901,13 +905,14 @@ class DrlWorkload(_SdWorkloadBase):
         self.kernel = Kernel([AnisotropicRF([1.7e-3, 0.2e-3, 0.2e-3], 0.0)], self.gtab.bvals, self.gtab.bvecs,
                              dirs=DIRS_300)
         self.config = {"workload": self.name, "grid": [110, 110, 70], "voxels": self.v, "measurements": 280,
-                       "directions": 300, "max_iter": 200, "l2": "inputs (1.1 GB) larger than L2"}
+                       "directions": 300, "max_iter": 200, "l2": "inputs (1.1 GB) larger than L2",
+                       "precision": DRL_PRECISION}
 
     def device_setup(self, torch, dev):
         from larmor_b200.sd.solvers import DRL, Stage
 
         self.torch = torch
-        self.solver = DRL()._prepare(self.kernel, self.gtab.bvals, Stage.SINGLE)
+        self.solver = DRL(precision=DRL_PRECISION)._prepare(self.kernel, self.gtab.bvals, Stage.SINGLE)
         self.d_signals = torch.from_numpy(self.norm).to(dev)
         self.h_signals = torch.from_numpy(self.norm).pin_memory()
         self.h_fods = torch.empty((self.v, 300), dtype=torch.float64).pin_memory()
@@ -921,13 +926,13 @@ class DrlWorkload(_SdWorkloadBase):
 
     def kernel_bytes(self) -> dict:
         """Algorithmic DRAM bytes of one step: 280 signals in, 300 amplitudes out per voxel."""
-        return {"drl_kernel": self.v * 8 * (280 + 300)}
+        return {"drl_kernel": self.v * 8 * (280 + 300), "drl_tc_kernel": self.v * 8 * (280 + 300)}
 
     flops_basis = "2 c^2 FLOP per voxel-iteration (the prediction F K^T K), 200 iterations per voxel (the cap)"
 
     def kernel_flops(self) -> dict:
-        """FP64 FLOP of one step at the iteration cap: 2 x 300^2 per voxel-iteration."""
-        return {"drl_kernel": self.v * 200 * 2 * 300 ** 2}
+        """FLOP of the product of one step at the iteration cap: 2 x 300^2 per voxel-iteration."""
+        return {"drl_kernel": self.v * 200 * 2 * 300 ** 2, "drl_tc_kernel": self.v * 200 * 2 * 300 ** 2}
 
     def step_e2e(self):
         self.d_signals.copy_(self.h_signals, non_blocking=True)
@@ -945,9 +950,23 @@ class DrlWorkload(_SdWorkloadBase):
         n = min(self.v, 512)
         done, t0 = 0, time.perf_counter()
         while time.perf_counter() - t0 < budget_s:
-            o.drl(self.norm[:n], k_t, k_t_k, nu, 200, 1.0 / 300, n_threads=threads)
+            self.reference_out = o.drl(self.norm[:n], k_t, k_t_k, nu, 200, 1.0 / 300, n_threads=threads)
             done += n
         return done, time.perf_counter() - t0, f"first {n} voxels of the volume, repeated for ~{budget_s:.0f} s"
+
+    def parity(self) -> dict:
+        """The device FODs of the cpu_baseline sample against the FP64 oracle's."""
+        if not hasattr(self, "solver"):
+            return None
+        self.step_device()
+        ref = self.reference_out
+        got = self.d_fods[:len(ref)].cpu().numpy()
+        ok = ~np.isnan(ref).any(axis=1)
+        rel = np.abs(got[ok] - ref[ok]).max(axis=1) / np.abs(ref[ok]).max(axis=1)
+        tol = 1e-4 if DRL_PRECISION != "fp64" else 1e-9
+        return {"against": "FP64 oracle (restatement of cpp/src/sd/drl.cpp)", "voxels": int(ok.sum()),
+                "precision": DRL_PRECISION, "fod_rel_max": float(rel.max()), "fod_rel_median": float(np.median(rel)),
+                "tolerance": {"fod_rel": tol}, "within_tolerance": bool(rel.max() <= tol)}
 
 
 class GrlWorkload(MfodWorkload):
@@ -958,7 +977,7 @@ class GrlWorkload(MfodWorkload):
     final fractions, on S0-normalised signals."""
 
     name = "grl_3tissue_110x110x70"
-    kernels = ("drl_kernel_resident", "drl_kernel", "lr_fractions_kernel", "hr_fractions_kernel")
+    kernels = ("drl_kernel_resident", "drl_kernel", "drl_tc_kernel", "lr_fractions_kernel", "hr_fractions_kernel")
     fraction_tol = 1e-3
     has_fp32 = False
 
@@ -978,12 +997,14 @@ class GrlWorkload(MfodWorkload):
         self.lr = Kernel(rfs, b, g, dirs=low_resolution_dirs(rfs, len(b)), weights=weights)
         self.config = {"workload": self.name, "grid": [110, 110, 70], "voxels": self.v, "measurements": 280,
                        "tissues": "WM (300 directions) + GM + CSF", "solver": "DRL (200 / 600 iterations)",
-                       "max_rounds": 50, "fraction_tol": self.fraction_tol, "l2": "inputs (1.1 GB) larger than L2"}
+                       "max_rounds": 50, "fraction_tol": self.fraction_tol, "l2": "inputs (1.1 GB) larger than L2",
+                       "precision": DRL_PRECISION + (" (the 300-direction final solve; the 44-direction rounds FP64)"
+                                                     if DRL_PRECISION != "fp64" else "")}
 
     def sd_solver(self):
         from larmor_b200.sd.solvers import DRL
 
-        return DRL()
+        return DRL(precision=DRL_PRECISION)
 
     def step_device(self, precision=0):
         from larmor_b200 import _core
@@ -1006,6 +1027,7 @@ class GrlWorkload(MfodWorkload):
         vr = self._voxel_rounds = int(rounds.sum().item())
         m, c_lr, c_hr = 280, self.k_lr.ca, self.k_hr.ca
         return {"drl_kernel_resident": vr * 8 * (m + c_lr), "drl_kernel": self.v * 8 * (m + c_hr),
+                "drl_tc_kernel": self.v * 8 * (m + c_hr),
                 "lr_fractions_kernel": vr * 8 * (c_lr + m + 3),
                 "hr_fractions_kernel": self.v * 8 * (c_hr + m + 3)}
 
@@ -1014,8 +1036,22 @@ class GrlWorkload(MfodWorkload):
 
     def kernel_flops(self) -> dict:
         """FP64 FLOP of one step at the iteration caps (the voxel-rounds from kernel_bytes)."""
-        return {"drl_kernel": self.v * 599 * 2 * self.k_hr.ca ** 2,
+        return {"drl_kernel": self.v * 599 * 2 * self.k_hr.ca ** 2, "drl_tc_kernel": self.v * 599 * 2 * self.k_hr.ca ** 2,
                 "drl_kernel_resident": self._voxel_rounds * 199 * 2 * self.k_lr.ca ** 2}
+
+    def parity(self) -> dict:
+        """The device fit of the cpu_baseline sample's voxels against the FP64 oracle's GRL."""
+        ref, ref_fr = self.reference_out
+        n = len(ref)
+        got = self.d_fods[:n].cpu().numpy()
+        got_fr = self.d_fr[:n].cpu().numpy()
+        rel = np.abs(got - ref).max(axis=1) / np.abs(ref).max(axis=1)
+        tol = 1e-4 if DRL_PRECISION != "fp64" else 1e-9
+        fr_err = float(np.abs(got_fr - ref_fr).max())
+        return {"against": "FP64 oracle (restatement of cpp/src/sd/{drl,multi_tissue,fractions}.cpp)", "voxels": n,
+                "precision": DRL_PRECISION, "fod_rel_max": float(rel.max()), "fractions_abs_max": fr_err,
+                "tolerance": {"fod_rel": tol, "fractions_abs": 1e-4},
+                "within_tolerance": bool(rel.max() <= tol and fr_err <= 1e-4)}
 
     def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
         from larmor_b200.sd.solvers import _rl_products
@@ -1033,10 +1069,10 @@ class GrlWorkload(MfodWorkload):
                   blocks=[(b.start, b.stop) for b in self.hr.aniso_blocks])
         done, t0 = 0, time.perf_counter()
         while time.perf_counter() - t0 < budget_s:
-            o.fit_multi_tissue(self.norm[:n], self.lr.weights, lr, hr, max_rounds=50, fraction_tol=self.fraction_tol,
-                               final_tol=1e-2, n_threads=threads,
-                               lr_drl={"nu": self._nus[0], "n_iter": 199, "init": 1e-6},
-                               hr_drl={"nu": self._nus[1], "n_iter": 599, "init": 1e-6})
+            self.reference_out = o.fit_multi_tissue(
+                self.norm[:n], self.lr.weights, lr, hr, max_rounds=50, fraction_tol=self.fraction_tol, final_tol=1e-2,
+                n_threads=threads, lr_drl={"nu": self._nus[0], "n_iter": 199, "init": 1e-6},
+                hr_drl={"nu": self._nus[1], "n_iter": 599, "init": 1e-6})
             done += n
         return done, time.perf_counter() - t0, f"first {n} voxels of the volume, repeated for ~{budget_s:.0f} s"
 
@@ -1425,7 +1461,7 @@ def measure(wl, args, world: int, rank: int, dist, dev) -> dict:
 
 
 def main() -> int:
-    global REFERENCE_ARM
+    global REFERENCE_ARM, DRL_PRECISION
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -1442,6 +1478,8 @@ def main() -> int:
     ap.add_argument("--serve-slots", type=int, default=6, help="requests on the GPU at once (serve)")
     ap.add_argument("--serve-load", type=float, nargs="+", default=[0.5, 1.0, 2.0, 4.0],
                     help="arrival rates as multiples of the plain per-request rate (serve)")
+    ap.add_argument("--drl-precision", default="fp64", choices=["fp64", "tf32x3"],
+                    help="dRL arithmetic of the drl and grl workloads")
     ap.add_argument("--no-extras", action="store_true",
                     help="the mfod line without its DTI and serving sub-objects")
     ap.add_argument("--profile", action="store_true",
@@ -1449,6 +1487,7 @@ def main() -> int:
                          "prints no bench line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    DRL_PRECISION = args.drl_precision
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -333,6 +333,13 @@ int lar_stage_dwi(const void* volume, int dtype, int64_t nx, int64_t ny, int64_t
 
 /* The SD models' S0-normalised signals (src/larmor/sd/model.py:184-200): normalised (v, n) =
  * min(signals / s0, 1) in FP64, finite (v) = 1 where every quotient is finite. Device arrays. */
+/* Puts map-major values (rows, v) (device floats) of the mask voxels back on the grid:
+ * out(voxels[i], r) = values(r, i) with out (grid, rows) voxel-major, device floats; out's other
+ * entries are left as they are (the caller fills them). Replaces the host unmask of the model
+ * results (src/larmor/dwi/mask.py:139), so one copy of the grid maps leaves the device. */
+int lar_unmask_rows(const float* values, int64_t rows, int64_t v, const int64_t* voxels, int64_t grid, float* out,
+                    void* stream);
+
 int lar_normalise_signals(const float* signals, const double* s0, int64_t v, int64_t n, double* normalised,
                           uint8_t* finite, void* stream);
 

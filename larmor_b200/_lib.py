@@ -56,6 +56,7 @@ SIGNATURES: dict[str, tuple] = {
     "lar_fit_csd": (_i32, [_p, _p, _i64, _p, _p, _p]),
     "lar_stage_dwi": (_i32, [_p, _i32, _i64, _i64, _i64, _i64, _f64, _f64, _p, _i64, _p, _p, _p, _p, _p, _p, _p]),
     "lar_normalise_signals": (_i32, [_p, _p, _i64, _i64, _p, _p, _p]),
+    "lar_unmask_rows": (_i32, [_p, _i64, _i64, _p, _i64, _p, _p]),
     "lar_peak_sphere_create": (_i32, [_p, _p, _i64, _p]),
     "lar_peak_sphere_destroy": (None, [_p]),
     "lar_sh_derivatives": (_i32, [_p, _i64, _i64, _i32, _i32, _p, _p, _p, _p]),

@@ -188,6 +188,17 @@ void launch_gather(const void* volume, int64_t n, float slope, float intercept, 
                                                    v, is_b0, n_b0, signals, s0_raw, state, row_max, finite);
 }
 
+// out(voxels[i], r) = values(r, i): the rows of a map-major (rows, v) array put back on the grid,
+// voxel-major (grid, rows), as unmask does on the host (src/larmor/dwi/mask.py:139). Consecutive
+// threads take consecutive voxels of one row: coalesced reads, writes strided by `rows`.
+__global__ void __launch_bounds__(256) unmask_rows_kernel(const float* __restrict__ values, int64_t rows, int64_t v,
+                                                          const int64_t* __restrict__ voxels, float* __restrict__ out) {
+    const int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= rows * v) return;
+    const int64_t r = e / v, i = e - r * v;
+    out[voxels[i] * rows + r] = values[e];
+}
+
 }  // namespace
 }  // namespace lar
 
@@ -258,6 +269,20 @@ int lar_stage_dwi(const void* volume, int dtype, int64_t nx, int64_t ny, int64_t
             cuda_check(cudaGetLastError(), "stage_floor_kernel launch");
         }
         cuda_check(cudaFreeAsync(ws, st), "cudaFreeAsync");
+    });
+}
+
+int lar_unmask_rows(const float* values, int64_t rows, int64_t v, const int64_t* voxels, int64_t grid, float* out,
+                    void* stream) {
+    return guarded([&] {
+        require(rows >= 1 && v >= 0 && grid >= v, "rows must be at least 1 and v between 0 and the grid's size");
+        if (v == 0) return;
+        require(values && voxels && out, "values, voxels and out must not be NULL");
+        auto st = static_cast<cudaStream_t>(stream);
+        LaunchScope scope("unmask_rows_kernel", st);
+        const int64_t total = rows * v;
+        unmask_rows_kernel<<<unsigned((total + 255) / 256), 256, 0, st>>>(values, rows, v, voxels, out);
+        cuda_check(cudaGetLastError(), "unmask_rows_kernel launch");
     });
 }
 

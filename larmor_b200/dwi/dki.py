@@ -22,7 +22,7 @@ from larmor_b200.dwi.inputs import (
     check_dwi,
     stage_dwi,
 )
-from larmor_b200.dwi.mask import unmask
+from larmor_b200.dwi.mask import unmask_maps
 from larmor_b200.types import GradientTable, Volume
 
 FIT_METHODS = ("ols", "wls")
@@ -162,24 +162,33 @@ class DKIModel:
                 signals, s0, floor = signals[keep], s0[keep], floor[keep]
             fitted[mask] = usable
         g = dki_constraints(gtab) if self.constrained else np.zeros((0, design.shape[1]))
-        maps, npd, broke = fit_dki_signals(design, g, signals, s0, floor, is_b0,
-                                           self.fit_method == "wls", PRECISIONS[self.precision])
+        maps, npd, broke = fit_dki_device(design, g, signals, s0, floor, is_b0,
+                                          self.fit_method == "wls", PRECISIONS[self.precision])
         if self.constrained:
-            LarmorLogger.info("%d of %d voxels break a constraint.", int(broke.sum()), len(broke))
-        return DKIFit(
-            dt=unmask(maps[0:6].T, fitted), kt=unmask(maps[16:31].T, fitted),
-            s0=unmask(maps[31], fitted), fa=unmask(maps[6], fitted), md=unmask(maps[7], fitted),
-            ad=unmask(maps[8], fitted), rd=unmask(maps[9], fitted), pe=unmask(maps[10:13].T, fitted),
-            eigen_vals=unmask(maps[13:16].T, fitted),
-            npd=unmask(npd, fitted, fill_value=False, dtype=bool),
-            mk=unmask(maps[32], fitted), ak=unmask(maps[33], fitted), rk=unmask(maps[34], fitted),
-            ka=unmask(maps[35], fitted),
-        )
+            LarmorLogger.info("%d of %d voxels break a constraint.", int(broke.sum().item()), len(broke))
+        # The maps go back on the grid on the device; one copy of the grid leaves it.
+        torch = _core._torch()
+        flat = staged.flat if fitted is mask or np.array_equal(fitted, mask) else \
+            torch.from_numpy(np.flatnonzero(fitted).astype(np.int64)).to(maps.device)
+        grid = unmask_maps(maps, DKI_MAP_ROWS, flat, fitted.shape, flags=npd)
+        return DKIFit(npd=grid["flags"], **{name: grid[name] for name, _, _ in DKI_MAP_ROWS})
+
+
+# The rows of the fused fit's (36, v) maps that make up each DKIFit map.
+DKI_MAP_ROWS = [("dt", 0, 6), ("fa", 6, 1), ("md", 7, 1), ("ad", 8, 1), ("rd", 9, 1), ("pe", 10, 3),
+                ("eigen_vals", 13, 3), ("kt", 16, 15), ("s0", 31, 1), ("mk", 32, 1), ("ak", 33, 1),
+                ("rk", 34, 1), ("ka", 35, 1)]
 
 
 def fit_dki_signals(design, g, signals, s0, floor, is_b0, weighted, precision=_lib.LAR_FP64):
     """Fits float32 signals (v, N) on the device (host arrays, or device tensors for signals, s0
-    and floor); returns maps (36, v), npd (v,), broke (v,)."""
+    and floor); returns maps (36, v), npd (v,), broke (v,) on the host."""
+    maps, npd, broke = fit_dki_device(design, g, signals, s0, floor, is_b0, weighted, precision)
+    return _core._to_host(maps), _core._to_host(npd).astype(bool), _core._to_host(broke).astype(bool)
+
+
+def fit_dki_device(design, g, signals, s0, floor, is_b0, weighted, precision=_lib.LAR_FP64):
+    """fit_dki_signals with the maps (36, v) float32, npd and broke (v,) uint8 on the device."""
     torch = _core._torch()
     dev = torch.device("cuda", torch.cuda.current_device())
     handle = _core.LogDesign.cached(design, g)
@@ -202,7 +211,7 @@ def fit_dki_signals(design, g, signals, s0, floor, is_b0, weighted, precision=_l
             handle.handle, _lib.ptr(s), _lib.ptr(s0d), _lib.ptr(f), _lib.ptr(b0), v, int(weighted),
             MAX_REWEIGHTINGS, LOG_SIGNAL_TOL, int(precision), _lib.ptr(maps), _lib.ptr(npd),
             _lib.ptr(broke), _lib.ptr(params), _core._stream(torch)))
-    return maps.cpu().numpy(), npd.cpu().numpy().astype(bool), broke.cpu().numpy().astype(bool)
+    return maps, npd, broke
 
 
 def dki_maps_device(params, maps, npd) -> None:

@@ -18,7 +18,7 @@ from larmor_b200 import _core, _lib
 from larmor_b200._log import LarmorLogger
 from larmor_b200._threads import n_threads
 from larmor_b200.dwi.inputs import as_mask, check_dwi, stage_dwi
-from larmor_b200.dwi.mask import unmask
+from larmor_b200.dwi.mask import unmask_maps
 from larmor_b200.types import GradientTable, Volume
 
 FIT_METHODS = ("ols", "wls")
@@ -85,28 +85,32 @@ class DTIModel:
         mask = as_mask(volume, mask)
         design = dti_design(gtab)
         staged = stage_dwi(volume, gtab, mask)
-        maps, npd = fit_dti_signals(design, staged.signals, staged.floor, self.fit_method == "wls",
-                                    PRECISIONS[self.precision])
-        if npd.any():
+        maps, npd = fit_dti_device(design, staged.signals, staged.floor, self.fit_method == "wls",
+                                   PRECISIONS[self.precision])
+        # The maps go back on the grid on the device; one copy of the grid leaves it.
+        grid = unmask_maps(maps, DTI_MAP_ROWS, staged.flat, mask.shape, flags=npd)
+        n_npd = int(grid["flags"].sum())
+        if n_npd:
             LarmorLogger.warning(
-                "%d of %d fitted voxels have a tensor that is not positive definite.",
-                int(npd.sum()), len(npd))
-        return DTIFit(
-            dt=unmask(maps[0:6].T, mask),
-            fa=unmask(maps[6], mask),
-            md=unmask(maps[7], mask),
-            ad=unmask(maps[8], mask),
-            rd=unmask(maps[9], mask),
-            pe=unmask(maps[10:13].T, mask),
-            eigen_vals=unmask(maps[13:16].T, mask),
-            npd=unmask(npd, mask, fill_value=False, dtype=bool),
-        )
+                "%d of %d fitted voxels have a tensor that is not positive definite.", n_npd, int(mask.sum()))
+        return DTIFit(npd=grid["flags"], **{name: grid[name] for name, _, _ in DTI_MAP_ROWS})
+
+
+# The rows of the fused fit's (16, v) maps that make up each DTIFit map.
+DTI_MAP_ROWS = [("dt", 0, 6), ("fa", 6, 1), ("md", 7, 1), ("ad", 8, 1), ("rd", 9, 1), ("pe", 10, 3),
+                ("eigen_vals", 13, 3)]
 
 
 def fit_dti_signals(design: np.ndarray, signals: np.ndarray, floor: np.ndarray, weighted: bool,
                     precision: int = _lib.LAR_FP64) -> tuple[np.ndarray, np.ndarray]:
     """Fits float32 signals (v, N) (a host array or a device tensor) with per-voxel floors (v,)
-    on the device; returns maps (16, v) and npd (v,)."""
+    on the device; returns maps (16, v) and npd (v,) on the host."""
+    maps, npd = fit_dti_device(design, signals, floor, weighted, precision)
+    return _core._to_host(maps), _core._to_host(npd).astype(bool)
+
+
+def fit_dti_device(design: np.ndarray, signals, floor, weighted: bool, precision: int = _lib.LAR_FP64):
+    """fit_dti_signals with the maps (16, v) float32 and npd (v,) uint8 left on the device."""
     torch = _core._torch()
     dev = torch.device("cuda", torch.cuda.current_device())
     handle = _core.LogDesign.cached(design, np.zeros((0, design.shape[1])))
@@ -120,4 +124,4 @@ def fit_dti_signals(design: np.ndarray, signals: np.ndarray, floor: np.ndarray, 
             if isinstance(floor, np.ndarray) else floor.contiguous()
         _core.fit_dti_maps_device(handle, s, f, weighted, maps, npd, max_iter=MAX_REWEIGHTINGS,
                                   tol=LOG_SIGNAL_TOL, precision=precision)
-    return maps.cpu().numpy(), npd.cpu().numpy().astype(bool)
+    return maps, npd

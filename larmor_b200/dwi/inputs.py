@@ -69,6 +69,7 @@ class StagedDwi:
     finite: object
     floor: object
     largest: object
+    flat: object = None  # the mask voxels' flat grid indices, an int64 device tensor
 
     @property
     def voxels(self) -> tuple[np.ndarray, ...]:
@@ -91,8 +92,7 @@ def upload_volume(volume: Volume):
                          f"{', '.join(_lib.LAR_DTYPES)}.")
     torch = _core._torch()
     dev = torch.device("cuda", torch.cuda.current_device())
-    raw = torch.empty(data.nbytes, dtype=torch.uint8, device=dev)
-    raw.copy_(torch.from_numpy(data.reshape(-1).view(np.uint8)))
+    raw = _core._on_device(torch, data.reshape(-1).view(np.uint8), dev)
     return raw, code
 
 
@@ -129,7 +129,7 @@ def stage_dwi(volume: Volume, gtab: GradientTable, mask: np.ndarray, *, raw=None
         _lib.ptr(data), code, nx, ny, nz, n, float(volume.slope), float(volume.intercept), _lib.ptr(d_voxels), v,
         is_b0.ctypes.data, _lib.ptr(signals), _lib.ptr(s0), _lib.ptr(finite), _lib.ptr(floor), _lib.ptr(largest),
         _core._stream(torch)))
-    return StagedDwi(mask, signals, s0, finite, floor, largest)
+    return StagedDwi(mask, signals, s0, finite, floor, largest, d_voxels)
 
 
 def normalise_signals(signals, s0):

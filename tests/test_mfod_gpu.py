@@ -160,35 +160,48 @@ def test_async_multi_tissue_equals_the_waiting_call(cuda, mfod_fixture):
     np.testing.assert_array_equal(out["st"].cpu().numpy(), st)
 
 
-def test_plain_fp32_fit_stays_near_the_fp64_oracle(cuda, oracle, mfod_fixture):
-    """The plain single-precision fit (the comparison baseline) on the MRIToolkit block: its
-    FODs and fractions near the FP64 oracle's, at the accuracy FP32 arithmetic allows."""
+def test_plain_fp32_fit_stays_near_the_fp64_oracle(cuda, oracle):
+    """The plain single-precision fit (the comparison baseline) of 256 voxels of the three-tissue
+    generator (WM on the 300 directions, GM, CSF): finite FODs and fractions near the FP64
+    oracle's, at the accuracy FP32 arithmetic allows (a median FOD error below 1e-2 of the
+    voxel's largest amplitude, fractions within 5e-2)."""
     import torch
 
     from larmor_b200 import _core
+    from larmor_b200.sd.kernel import Kernel
+    from larmor_b200.sd.model import compute_shell_weights, low_resolution_dirs
+    from larmor_b200.sd.solvers import L2NNLS, Stage, _deconv_kernel
+    from larmor_b200.sd.sphere import DIRS_300
+    from larmor_b200.synthetic import mfod_model_responses, mfod_signals, mfod_table
 
-    z = mfod_fixture
-    signals, lr, hr = mfod_inputs(z)
-    lrk = _core.DeconvKernel(np.ascontiguousarray(z["lr_k_aniso"]), np.ascontiguousarray(z["lr_k_iso"]),
-                             np.ascontiguousarray(z["lr_w_k_iso"]), [(0, z["lr_k_aniso"].shape[1])])
-    hrk = _core.DeconvKernel(np.ascontiguousarray(z["hr_k_aniso"]), np.ascontiguousarray(z["hr_k_iso"]),
-                             np.ascontiguousarray(z["hr_w_k_iso"]), [tuple(b) for b in z["hr_blocks"]])
-    lr_solver = _core.FodSolver.l2nnls(np.ascontiguousarray(z["lr_w_k_aniso"]), 0.0, 1e-6)
-    hr_solver = _core.FodSolver.l2nnls(np.ascontiguousarray(z["hr_w_k_aniso"]), 0.1, 1e-6)
+    rng = np.random.default_rng(11)
+    gtab = mfod_table(rng)
+    sig = mfod_signals(rng, gtab, 256).astype(np.float64)
+    norm = np.ascontiguousarray(np.minimum(sig / sig[:, gtab.b0_mask].mean(axis=1)[:, None], 1.0))
+    rfs = mfod_model_responses()
+    w = compute_shell_weights(gtab.bvals, 1.0)
+    hr = Kernel(rfs, gtab.bvals, gtab.bvecs, dirs=DIRS_300, weights=w)
+    lr = Kernel(rfs, gtab.bvals, gtab.bvecs, dirs=low_resolution_dirs(rfs, len(gtab.bvals)), weights=w)
+    k_lr, k_hr = _deconv_kernel(lr), _deconv_kernel(hr)
+    lr_solver = L2NNLS()._prepare(lr, gtab.bvals, Stage.LOW_RES)
+    hr_solver = L2NNLS()._prepare(hr, gtab.bvals, Stage.HIGH_RES)
     dev = torch.device("cuda")
-    v = len(signals)
-    s = torch.from_numpy(np.ascontiguousarray(signals)).to(dev).float()
-    fods = torch.empty((v, hrk.ca), dtype=torch.float32, device=dev)
-    fr = torch.empty((v, hrk.nb + hrk.ci), dtype=torch.float32, device=dev)
+    v = len(norm)
+    s = torch.from_numpy(norm).to(dev).float()
+    fods = torch.empty((v, k_hr.ca), dtype=torch.float32, device=dev)
+    fr = torch.empty((v, 3), dtype=torch.float32, device=dev)
     rd = torch.empty((v,), dtype=torch.int32, device=dev)
     st = torch.empty((v,), dtype=torch.uint8, device=dev)
-    _core.fit_multi_tissue_plain_fp32_device(s, z["weights"], lrk, lr_solver, hrk, hr_solver, 50, 1e-7, 1e-2, fods,
+    _core.fit_multi_tissue_plain_fp32_device(s, lr.weights, k_lr, lr_solver, k_hr, hr_solver, 50, 1e-7, 1e-2, fods,
                                              fr, rd, st)
     got, got_fr = fods.double().cpu().numpy(), fr.double().cpu().numpy()
-    rfods, rfr = oracle.fit_multi_tissue(signals, z["weights"], lr, hr, n_threads=4)
+    lrd = dict(k_aniso=lr.k_aniso, k_iso=lr.k_iso, w_k_iso=lr.w_k_iso, w_k_aniso=lr.w_k_aniso)
+    hrd = dict(k_aniso=hr.k_aniso, k_iso=hr.k_iso, w_k_iso=hr.w_k_iso, w_k_aniso=hr.w_k_aniso,
+               blocks=[(b.start, b.stop) for b in hr.aniso_blocks])
+    rfods, rfr = oracle.fit_multi_tissue(norm, lr.weights, lrd, hrd, n_threads=4)
     rel = np.abs(got - rfods).max(axis=1) / np.abs(rfods).max(axis=1)
     print(f"plain FP32, {v} voxels: FOD rel max {rel.max():.3e}, median {np.median(rel):.3e}; fractions abs max "
           f"{np.abs(got_fr - rfr).max():.3e}; status nonzero {(st.cpu().numpy() != 0).mean():.4f}")
     assert np.isfinite(got).all() and np.isfinite(got_fr).all()
     assert np.median(rel) <= 1e-2
-    assert np.abs(got_fr - rfr).max() <= 1e-2
+    assert np.abs(got_fr - rfr).max() <= 5e-2
