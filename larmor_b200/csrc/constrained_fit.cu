@@ -62,24 +62,29 @@ struct WarpShared {
 // The NNLS system C = [R^-T G^T; -(G p_free)^T] of one voxel, formed column by column on demand.
 struct ImplicitSystem {
     const double* g;      // (m, p) constraints
+    const double* gt;     // (p, m) the same, transposed
     const double* qr;     // (n, p): R in its upper triangle
     const double* pfree;  // (p,)
     double* cache;        // (m, p + 1)
     uint8_t* ready;       // (m,)
     int p, m;
-    // Column c into the cache (lane 0), unless it is there: forward substitution R^T y = g_c,
-    // then y_p = -g_c p_free.
+    // Column c into the cache, unless it is there: the forward substitution R^T y = g_c with
+    // lane i holding entry i (column-oriented: entry k is final once the rows above it are
+    // subtracted), then y_p = -g_c p_free.
     __device__ void form(int c, int lane) const {
-        if (lane == 0 && !ready[c]) {
-            const double* gc = g + size_t(c) * p;
-            double* col = cache + size_t(c) * (p + 1);
-            double gf = 0.0;
-            for (int i = 0; i < p; ++i) {
-                double si = gc[i];
-                for (int k = 0; k < i; ++k) si -= qr[size_t(k) * p + i] * col[k];
-                col[i] = si / qr[size_t(i) * p + i];
-                gf += gc[i] * pfree[i];
-            }
+        if (ready[c]) return;
+        const double* gc = g + size_t(c) * p;
+        double* col = cache + size_t(c) * (p + 1);
+        const double gi = lane < p ? gc[lane] : 0.0;
+        double si = gi;
+        for (int k = 0; k < p; ++k) {
+            const double yk = __shfl_sync(0xffffffffu, si, k) / qr[size_t(k) * p + k];
+            if (lane > k && lane < p) si -= qr[size_t(k) * p + lane] * yk;
+            if (lane == k) si = yk;
+        }
+        const double gf = warp_sum(lane < p ? gi * pfree[lane] : 0.0);
+        if (lane < p) col[lane] = si;
+        if (lane == 0) {
             col[p] = -gf;
             ready[c] = 1;
         }
@@ -118,15 +123,16 @@ __device__ int implicit_nnls(const ImplicitSystem& sys, const double* d, double 
             s.res[r] = acc;
         }
         __syncwarp();
-        // t = R^-1 res[:p] - res[p] p_free (back substitution on lane 0).
-        if (lane == 0) {
-            for (int i = p - 1; i >= 0; --i) {
-                double acc = s.res[i];
-                for (int j = i + 1; j < p; ++j) acc -= sys.qr[size_t(i) * p + j] * t[j];
-                t[i] = acc / sys.qr[size_t(i) * p + i];
+        // t = R^-1 res[:p] - res[p] p_free: column-oriented back substitution, lane i holding
+        // entry i (entry k is final once the columns right of it are subtracted).
+        {
+            double yi = lane < p ? s.res[lane] : 0.0;
+            for (int k = p - 1; k >= 0; --k) {
+                const double tk = __shfl_sync(0xffffffffu, yi, k) / sys.qr[size_t(k) * p + k];
+                if (lane < k) yi -= sys.qr[size_t(lane) * p + k] * tk;
+                if (lane == k) yi = tk;
             }
-            const double rp = s.res[p];
-            for (int i = 0; i < p; ++i) t[i] -= rp * sys.pfree[i];
+            if (lane < p) t[lane] = yi - s.res[p] * sys.pfree[lane];
         }
         __syncwarp();
         // The gradient of every inactive column, g_c . t, lanes over the columns (each lane in
@@ -135,9 +141,8 @@ __device__ int implicit_nnls(const ImplicitSystem& sys, const double* d, double 
         int bi = -1;
         for (int c = lane; c < m; c += 32) {
             if (s.flag[c]) continue;
-            const double* gc = sys.g + size_t(c) * p;
             double w = 0.0;
-            for (int a = 0; a < p; ++a) w += gc[a] * t[a];
+            for (int a = 0; a < p; ++a) w += sys.gt[size_t(a) * m + c] * t[a];
             if (bi < 0 || w > bv) {
                 bv = w;
                 bi = c;
@@ -376,7 +381,7 @@ __global__ void __launch_bounds__(kCWarps * 32, 4) constrained_fit_kernel(
         double* unit = sh.vec[2];
         for (int r = lane; r < rows; r += 32) unit[r] = (r == p) ? 1.0 : 0.0;
         __syncwarp();
-        const ImplicitSystem sys{d.g, qr, pfree, cache, ready, p, m};
+        const ImplicitSystem sys{d.g, d.gt, qr, pfree, cache, ready, p, m};
         NnlsScratch ns{u, z, flag, sh.act, &sh.n_act, sh.res,
                        QrScratch{sub, sh.qtau, sh.qnu, sh.qnd, sh.qperm, sh.rv}, kMaxActive};
         const int outcome = implicit_nnls(sys, unit, tol, kInnerStepsPerConstraint * m, ns, sh.t, lane);

@@ -119,6 +119,17 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
                  : "memory");
 }
 
+// Chunk `chunk_index` of G into a stage: one bulk copy per 4 KB block (tile and part), so that
+// the copy engines fetch the blocks in parallel; the mbarrier expects the whole chunk.
+__device__ __forceinline__ void load_chunk(unsigned char* stage, const float* gtc, int chunk_index, int tiles,
+                                           unsigned long long* bar) {
+    const unsigned bytes = unsigned(tiles) * 2 * kTcBlockBytes;
+    mbar_expect_tx(bar, bytes);
+    const unsigned char* src = reinterpret_cast<const unsigned char*>(gtc) + size_t(chunk_index) * bytes;
+    for (int b = 0; b < 2 * tiles; ++b)
+        bulk_load(stage + size_t(b) * kTcBlockBytes, src + size_t(b) * kTcBlockBytes, kTcBlockBytes, bar);
+}
+
 // The shared-memory matrix descriptor of a K-major operand without swizzling: 8-row groups
 // `sbo` bytes apart, the two 16-byte direction chunks of an MMA step 128 bytes apart.
 __device__ __forceinline__ unsigned long long umma_desc(const void* p, unsigned sbo) {
@@ -231,8 +242,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_fence_after();
     const unsigned tmem = sh.tmem_base;
     const unsigned lane_base = unsigned(32 * warp) << 16;
-    // Phase parities of the barriers (thread 0 tracks the stages; everyone tracks `done`).
-    unsigned full_phase = 0, empty_phase = 0, done_phase = 0;
+    // G streams through the stage ring continuously, across iterations and tiles (it does not
+    // change): chunk R of the stream is data chunk R % nq in stage R % kTcStages, the (R /
+    // kTcStages)-th use of that stage, so its barriers' phase parity is (R / kTcStages) & 1.
+    // Thread 0 counts the chunks consumed (`used`) and loaded (`loaded`); everyone tracks `done`.
+    long long used = 0, loaded = 0;
+    unsigned done_phase = 0;
+    if (tid == 0) {
+        for (; loaded < kTcStages; ++loaded)
+            load_chunk(stage_base + size_t(loaded) * chunk, gtc, int(loaded % nq), tiles, &sh.full[loaded]);
+    }
 
     for (int64_t p0 = int64_t(blockIdx.x) * kTcN; p0 < count && !sh.abort; p0 += int64_t(gridDim.x) * kTcN) {
         if (tid < kTcN) sh.vox[tid] = p0 + tid < count ? (list ? int64_t(list[p0 + tid]) : p0 + tid) : -1;
@@ -272,34 +291,38 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 sh.active[j] = 1;
             }
         }
-        // The tile's signals (FP64) in the F area, then K^T s per direction (a thread per
-        // direction lane of each tile) into tensor memory, then the start value in F.
+        // K^T s of the tile into tensor memory (FP64 sums, kept in FP32), 16 voxels at a time:
+        // their signals (FP64) staged in the F area, then a thread per direction lane of each
+        // tile reads its row of K^T once for the 16.
         double* sig = reinterpret_cast<double*>(smem);
-        for (int e = tid; e < kTcN * m; e += kTcThreads) {
-            const int j = e / m, i = e - j * m;
-            const int64_t voxel = sh.vox[j];
-            sig[e] = voxel >= 0 ? tc_signal(S, voxel, i) : 0.0;
-        }
-        __syncthreads();
-        for (int t = 0; t < tiles; ++t) {
-            const int d = kTcM * t + 32 * warp + lane;
-            for (int j0 = 0; j0 < kTcN; j0 += 16) {
+        for (int j0 = 0; j0 < kTcN; j0 += 16) {
+            for (int e = tid; e < 16 * m; e += kTcThreads) {
+                const int jj = e / m, i = e - jj * m;
+                const int64_t voxel = sh.vox[j0 + jj];
+                sig[e] = voxel >= 0 ? tc_signal(S, voxel, i) : 0.0;
+            }
+            __syncthreads();
+            for (int t = 0; t < tiles; ++t) {
+                const int d = kTcM * t + 32 * warp + lane;
+                double acc[16];
+#pragma unroll
+                for (int jj = 0; jj < 16; ++jj) acc[jj] = 0.0;
+                if (d < c) {
+                    const double* kt = P.k_t + size_t(d) * m;
+                    for (int i = 0; i < m; ++i) {
+                        const double k = kt[i];
+#pragma unroll
+                        for (int jj = 0; jj < 16; ++jj) acc[jj] = fma(k, sig[jj * m + i], acc[jj]);
+                    }
+                }
                 float ks[16];
 #pragma unroll
-                for (int jj = 0; jj < 16; ++jj) {
-                    double acc = 0.0;
-                    if (d < c) {
-                        const double* kt = P.k_t + size_t(d) * m;
-                        const double* sj = sig + size_t(j0 + jj) * m;
-                        for (int i = 0; i < m; ++i) acc = fma(kt[i], sj[i], acc);
-                    }
-                    ks[jj] = float(acc);
-                }
+                for (int jj = 0; jj < 16; ++jj) ks[jj] = float(acc[jj]);
                 tmem_st16(tmem + lane_base + unsigned(kTcKsCol + t * kTcN + j0), ks);
             }
+            tmem_wait_st();
+            __syncthreads();
         }
-        tmem_wait_st();
-        __syncthreads();
         {
             float hi, lo;
             split_tf32(float(P.init), hi, lo);
@@ -323,22 +346,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
             __syncthreads();
             if (sh.n_active == 0 || sh.abort) break;
-            // The product: thread 0 streams G's chunks and issues the MMAs. Chunk q + 3 is
-            // loaded into the stage chunk q - 1 used, once the MMAs of chunk q - 1 are done
-            // (those of chunk q are queued behind them meanwhile).
+            // The product: thread 0 issues the MMAs of the iteration's nq chunks as they land.
+            // Once the MMAs of chunk R - 1 are done its stage takes chunk R + 3 of the stream
+            // (those of chunk R are queued behind them meanwhile).
             if (tid == 0) {
                 tc_fence_after();
                 bool ok = true;
-                const int preload = min(kTcStages, nq);
-                for (int q = 0; q < preload; ++q) {
-                    mbar_expect_tx(&sh.full[q], unsigned(chunk));
-                    bulk_load(stage_base + size_t(q) * chunk, reinterpret_cast<const unsigned char*>(gtc) + size_t(q) * chunk,
-                              unsigned(chunk), &sh.full[q]);
-                }
                 for (int q = 0; q < nq && ok; ++q) {
-                    const int s = q % kTcStages;
-                    ok = mbar_wait(&sh.full[s], (full_phase >> s) & 1u);
-                    full_phase ^= 1u << s;
+                    const long long R = used;
+                    const int s = int(R % kTcStages);
+                    ok = mbar_wait(&sh.full[s], unsigned(R / kTcStages) & 1u);
                     if (!ok) break;
                     tc_fence_after();
                     const unsigned char* st = stage_base + size_t(s) * chunk;
@@ -355,23 +372,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         umma_tf32(d_tmem, al, bh, 1u);
                     }
                     umma_commit(&sh.empty[s]);
-                    const int r = q + kTcStages - 1;  // the chunk to load next
-                    if (q >= 1 && r < nq) {
-                        const int sp = (q - 1) % kTcStages;
-                        ok = mbar_wait(&sh.empty[sp], (empty_phase >> sp) & 1u);
-                        empty_phase ^= 1u << sp;
+                    ++used;
+                    if (R >= 1) {
+                        const long long Rp = R - 1;
+                        const int sp = int(Rp % kTcStages);
+                        ok = mbar_wait(&sh.empty[sp], unsigned(Rp / kTcStages) & 1u);
                         if (!ok) break;
-                        mbar_expect_tx(&sh.full[sp], unsigned(chunk));
-                        bulk_load(stage_base + size_t(sp) * chunk,
-                                  reinterpret_cast<const unsigned char*>(gtc) + size_t(r) * chunk, unsigned(chunk),
-                                  &sh.full[sp]);
+                        load_chunk(stage_base + size_t(sp) * chunk, gtc, int(loaded % nq), tiles, &sh.full[sp]);
+                        ++loaded;
                     }
-                }
-                // The commits no reload waited for complete with the iteration: account for
-                // their phases.
-                for (int q = 0; q < nq; ++q) {
-                    const bool waited = q + kTcStages < nq;  // chunk q's stage was reloaded
-                    if (!waited) empty_phase ^= 1u << (q % kTcStages);
                 }
                 umma_commit(&sh.done);
                 if (!ok) {
@@ -447,6 +456,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         __syncthreads();
     }
+    // The stream's copies still in flight land before the CTA exits (bounded waits).
+    if (tid == 0)
+        for (long long R = used; R < loaded; ++R)
+            if (!mbar_wait(&sh.full[R % kTcStages], unsigned(R / kTcStages) & 1u)) {
+                atomicExch(err, 1);
+                break;
+            }
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
@@ -457,8 +473,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
 bool drl_tc_fits(int c) { return c > 64 && c <= kTcMaxTiles * kTcM && c <= 320; }
 
-// The tile's FP64 signals are staged in the kernel's shared memory before its first product.
-bool drl_tc_fits_measurements(int c, int m) { return size_t(kTcN) * m * 8 <= drl_tc_smem_bytes(c); }
+// 16 voxels' FP64 signals are staged in the F area of the kernel's shared memory for K^T s.
+bool drl_tc_fits_measurements(int c, int m) { return size_t(16) * m * 8 <= 2 * tc_f_bytes(c); }
 
 size_t drl_tc_smem_bytes(int c) { return 2 * tc_f_bytes(c) + size_t(kTcStages) * tc_chunk_bytes(c); }
 

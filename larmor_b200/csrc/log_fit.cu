@@ -402,7 +402,7 @@ void upload_design(lar_log_design_s* h, DeviceArray<T>& x, DeviceArray<T>& pinvt
     const auto& hd = h->host;
     const int64_t n = hd.n, p = hd.p, m = hd.m, pp = p * (p + 1) / 2;
     std::vector<T> xv(static_cast<size_t>(n * p)), pt(static_cast<size_t>(n * p)), zv(static_cast<size_t>(n * pp)),
-        gv(static_cast<size_t>(m * p)), sv(static_cast<size_t>(p));
+        gv(static_cast<size_t>(2 * m * p)), sv(static_cast<size_t>(p));
     for (int64_t i = 0; i < n; ++i)
         for (int64_t a = 0; a < p; ++a) {
             xv[size_t(i * p + a)] = T(hd.x[size_t(i * p + a)]);
@@ -413,7 +413,12 @@ void upload_design(lar_log_design_s* h, DeviceArray<T>& x, DeviceArray<T>& pinvt
         for (int64_t a = 0; a < p; ++a)
             for (int64_t b = a; b < p; ++b) zv[size_t(i * pp + k++)] = T(hd.x[size_t(i * p + a)] * hd.x[size_t(i * p + b)]);
     }
-    for (size_t i = 0; i < gv.size(); ++i) gv[i] = T(hd.g[i]);
+    // g (m, p) row-major, then its transpose (p, m).
+    for (int64_t c = 0; c < m; ++c)
+        for (int64_t a = 0; a < p; ++a) {
+            gv[size_t(c * p + a)] = T(hd.g[size_t(c * p + a)]);
+            gv[size_t(m * p + a * m + c)] = T(hd.g[size_t(c * p + a)]);
+        }
     for (int64_t a = 0; a < p; ++a) sv[size_t(a)] = T(hd.scales[size_t(a)]);
     x.upload(xv.data(), xv.size());
     pinvt.upload(pt.data(), pt.size());
@@ -427,6 +432,7 @@ void upload_design(lar_log_design_s* h, DeviceArray<T>& x, DeviceArray<T>& pinvt
     view.pinvt = pinvt.ptr;
     view.z = z.ptr;
     view.g = g.ptr;
+    view.gt = m > 0 ? g.ptr + m * p : nullptr;
     view.scales = scales.ptr;
 }
 

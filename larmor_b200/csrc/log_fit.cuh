@@ -14,6 +14,7 @@ struct LogDesignDevice {
     const T* pinvt = nullptr;      // (n, p) transposed pseudo-inverse
     const T* z = nullptr;          // (n, p(p+1)/2) products x_na x_nb, a <= b
     const T* g = nullptr;          // (m, p) constraints, column-scaled
+    const T* gt = nullptr;         // (p, m) the same, transposed (lanes over constraints read it coalesced)
     const T* scales = nullptr;     // (p,) column norms
     const double* scales64 = nullptr;  // (p,) column norms in double, for the outputs
 };

@@ -77,7 +77,7 @@ extern "C" int lar_fit_log_signal_noalloc(const double* x, int64_t n, int64_t p,
 
         // Scratch layout: [count, queue] ints | design (x, pinv^T, g, scales) | violator ids |
         // violator parameters | warp slots of the constrained re-fit.
-        const size_t design_doubles = size_t(2 * n * p + m * p + p);
+        const size_t design_doubles = size_t(2 * n * p + 2 * m * p + p);
         const size_t design_off = 256;
         const size_t ids_off = up256(design_off + design_doubles * sizeof(double));
         const size_t params_off = up256(ids_off + (m > 0 ? size_t(v) * sizeof(int64_t) : 0));
@@ -122,11 +122,14 @@ extern "C" int lar_fit_log_signal_noalloc(const double* x, int64_t n, int64_t p,
         double* px_ = packed.data();
         double* ppinvt = px_ + n * p;
         double* pg = ppinvt + n * p;
-        double* pscales = pg + m * p;
+        double* pgt = pg + m * p;
+        double* pscales = pgt + m * p;
         std::memcpy(px_, h.x.data(), sizeof(double) * size_t(n * p));
         for (int64_t i = 0; i < n; ++i)
             for (int64_t a = 0; a < p; ++a) ppinvt[i * p + a] = h.pinv[size_t(a * n + i)];
         if (m > 0) std::memcpy(pg, h.g.data(), sizeof(double) * size_t(m * p));
+        for (int64_t c = 0; c < m; ++c)
+            for (int64_t a = 0; a < p; ++a) pgt[a * m + c] = h.g[size_t(c * p + a)];
         std::memcpy(pscales, h.scales.data(), sizeof(double) * size_t(p));
         cuda_check(cudaMemcpyAsync(base + design_off, packed.data(), packed.size() * sizeof(double),
                                    cudaMemcpyHostToDevice, st),
@@ -143,7 +146,8 @@ extern "C" int lar_fit_log_signal_noalloc(const double* x, int64_t n, int64_t p,
         d.pinvt = dx + n * p;
         d.z = nullptr;
         d.g = dx + 2 * n * p;
-        d.scales = dx + 2 * n * p + m * p;
+        d.gt = m > 0 ? dx + 2 * n * p + m * p : nullptr;
+        d.scales = dx + 2 * n * p + 2 * m * p;
         d.scales64 = d.scales;
 
         ViolatorList<double> list;
