@@ -110,6 +110,21 @@ def tensor_fa_md(dt: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
     return np.clip(fa, 0.0, 1.0), md
 
 
+def committed_issue(kernel: str, workload: str, algorithmic_bytes: float) -> dict | None:
+    """Warp instructions per launch of a kernel: the measured warp instructions per algorithmic
+    byte of its committed ncu capture (profiles/issue.json) times this launch's algorithmic
+    bytes, with the capture's issue-active fraction and active lanes per instruction."""
+    path = ROOT / "profiles" / "issue.json"
+    if not path.exists():
+        return None
+    entry = json.loads(path.read_text()).get("kernels", {}).get(f"{workload}:{kernel}")
+    if entry is None:
+        return None
+    return {"warp_instructions": float(entry["warp_instructions_per_algorithmic_byte"]) * algorithmic_bytes,
+            "issue_active_pct_ncu": entry["issue_active_pct"], "threads_per_instruction": entry["threads_per_instruction"],
+            "warp_instructions_per_voxel_round": entry.get("warp_instructions_per_voxel_round")}
+
+
 # ---- clocks ------------------------------------------------------------------------------
 
 class ClockSampler:
@@ -1446,8 +1461,21 @@ def measure(wl, args, world: int, rank: int, dist, dev) -> dict:
         if flops is not None:
             line["roofline"].update(fp64_tensor_roofline(flops * args.steps / max(top_launches, 1), avg_launch_s))
             line["roofline"]["flops_basis"] = wl.flops_basis
-    if hasattr(wl, "issue_roofline"):
-        line["issue_roofline"] = wl.issue_roofline(kernel_ms, args.steps)
+    issue = committed_issue(top, wl.name, bytes_per_launch)
+    if issue is not None and avg_launch_s > 0:
+        # The issue roofline of an instruction-bound kernel: warp instructions per second
+        # against the SMs' issue slots (4 schedulers x 1 warp instruction per cycle each).
+        sm_mhz = line["clocks"].get("sm_mhz") or line["clocks"].get("sm_max_mhz") or 1965.0
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        peak = sms * 4 * sm_mhz * 1e6
+        achieved = issue["warp_instructions"] / avg_launch_s
+        line["issue_roofline"] = {
+            "kernel": top, "unit": "warp instructions/s", "achieved": achieved, "peak": peak, "frac": achieved / peak,
+            "peak_basis": f"{sms} SMs x 4 schedulers x 1 warp instruction per cycle at the median SM clock {sm_mhz} MHz",
+            "warp_instructions_per_launch": issue["warp_instructions"],
+            "warp_instructions_per_voxel_round": issue["warp_instructions_per_voxel_round"],
+            "threads_per_instruction": issue["threads_per_instruction"],
+            "source": "profiles/issue.json (ncu smsp__inst_executed.sum per algorithmic byte, scaled to this launch)"}
     if hasattr(wl, "extra"):
         def timed_host(step):
             for _ in range(args.warmup):

@@ -58,12 +58,17 @@ __host__ __device__ inline int tc_kpad(int c) { return (c + kTcK - 1) / kTcK * k
 __host__ __device__ inline int tc_tiles(int c) { return (c + kTcM - 1) / kTcM; }
 __host__ __device__ inline size_t tc_chunk_bytes(int c) { return size_t(tc_tiles(c)) * 2 * kTcBlockBytes; }
 // Bytes of one part of F^T in shared memory.
-__host__ __device__ inline size_t tc_f_bytes(int c) { return size_t(kTcN) * tc_kpad(c) * 4; }
+// F^T's direction groups of 4 are 36 floats (144 bytes, the MMA's leading byte offset) apart
+// instead of 32: the epilogue's 32 lanes (32 consecutive directions of one voxel) then hit 32
+// different banks.
+constexpr int kTcFGroupFloats = 36;
+__host__ __device__ inline size_t tc_f_bytes(int c) { return size_t(kTcN / 8) * (tc_kpad(c) / 4) * kTcFGroupFloats * 4; }
 
-// Offset (floats) of entry (row r, direction k) in a K-major block of 8 x 4 core matrices whose
-// 8-row groups are `group` floats apart.
-__host__ __device__ inline size_t kmajor_offset(int r, int k, size_t group) {
-    return size_t(r >> 3) * group + size_t(k >> 2) * 32 + size_t(r & 7) * 4 + size_t(k & 3);
+// Offset (floats) of entry (row r, direction k) in a K-major layout of 8 x 4 core matrices
+// (8 rows x 16 bytes, 32 floats each): 8-row groups `group` floats apart, direction groups of 4
+// `kstride` floats apart.
+__host__ __device__ inline size_t kmajor_offset(int r, int k, size_t group, int kstride = 32) {
+    return size_t(r >> 3) * group + size_t(k >> 2) * kstride + size_t(r & 7) * 4 + size_t(k & 3);
 }
 
 struct TcShared {
@@ -131,11 +136,11 @@ __device__ __forceinline__ void load_chunk(unsigned char* stage, const float* gt
 }
 
 // The shared-memory matrix descriptor of a K-major operand without swizzling: 8-row groups
-// `sbo` bytes apart, the two 16-byte direction chunks of an MMA step 128 bytes apart.
-__device__ __forceinline__ unsigned long long umma_desc(const void* p, unsigned sbo) {
+// `sbo` bytes apart, the two 16-byte direction chunks of an MMA step `lbo` bytes apart.
+__device__ __forceinline__ unsigned long long umma_desc(const void* p, unsigned sbo, unsigned lbo = 128) {
     const unsigned long long addr = smem_u32(p);
-    return ((addr >> 4) & 0x3FFFull) | ((128ull >> 4) << 16) | ((unsigned long long)((sbo >> 4) & 0x3FFF) << 32) |
-           (1ull << 46);
+    return ((addr >> 4) & 0x3FFFull) | ((unsigned long long)((lbo >> 4) & 0x3FFF) << 16) |
+           ((unsigned long long)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
 
 // kind::tf32, FP32 accumulators, both operands K-major, M = 128, N = kTcN.
@@ -220,7 +225,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     float* FL = reinterpret_cast<float*>(smem + fbytes);
     unsigned char* stage_base = smem + 2 * fbytes;
     const size_t chunk = tc_chunk_bytes(c);
-    const size_t fgroup = size_t(kpad / 4) * 32;  // floats between 8-voxel groups of F^T
+    const size_t fgroup = size_t(kpad / 4) * kTcFGroupFloats;  // floats between 8-voxel groups of F^T
+    constexpr unsigned kFLbo = kTcFGroupFloats * 4;          // bytes between its direction groups
     const float nu = float(P.nu);
 
     if (tid == 0) {
@@ -329,7 +335,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             for (int e = tid; e < kTcN * kpad; e += kTcThreads) {
                 const int j = e / kpad, k = e - j * kpad;
                 const bool real = sh.vox[j] >= 0 && k < c;
-                const size_t off = kmajor_offset(j, k, fgroup);
+                const size_t off = kmajor_offset(j, k, fgroup, kTcFGroupFloats);
                 FH[off] = real ? hi : 0.f;
                 FL[off] = real ? lo : 0.f;
             }
@@ -359,10 +365,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     if (!ok) break;
                     tc_fence_after();
                     const unsigned char* st = stage_base + size_t(s) * chunk;
-                    const unsigned long long bh = umma_desc(reinterpret_cast<const unsigned char*>(FH) + size_t(q) * 256,
-                                                            unsigned(fgroup * 4));
-                    const unsigned long long bl = umma_desc(reinterpret_cast<const unsigned char*>(FL) + size_t(q) * 256,
-                                                            unsigned(fgroup * 4));
+                    const unsigned long long bh = umma_desc(
+                        reinterpret_cast<const unsigned char*>(FH) + size_t(q) * 2 * kFLbo, unsigned(fgroup * 4), kFLbo);
+                    const unsigned long long bl = umma_desc(
+                        reinterpret_cast<const unsigned char*>(FL) + size_t(q) * 2 * kFLbo, unsigned(fgroup * 4), kFLbo);
                     for (int t = 0; t < tiles; ++t) {
                         const unsigned long long ah = umma_desc(st + size_t(2 * t) * kTcBlockBytes, 256);
                         const unsigned long long al = umma_desc(st + size_t(2 * t + 1) * kTcBlockBytes, 256);
@@ -416,12 +422,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     for (int jj = 0; jj < 16; ++jj) {
                         const int j = j0 + jj;
                         if (!sh.active[j]) continue;
-                        const size_t off = kmajor_offset(j, d, fgroup);
+                        const size_t off = kmajor_offset(j, d, fgroup, kTcFGroupFloats);
                         const float f = FH[off] + FL[off];
                         // f^8 / (f^8 + nu^8) as 1 / (1 + (nu / f)^8): no underflow of f^8.
-                        const float q8 = pow8f(nu / f);
-                        const float damping = 1.f - sh.strength[j] * (1.f - 1.f / (1.f + q8));
-                        const float ratio = (kv[jj] - pv[jj]) / (pv[jj] + 1e-16f);
+                        // Fast divisions (about 2 ulp): the product carries ~1e-6 already.
+                        const float q8 = pow8f(__fdividef(nu, f));
+                        const float damping = 1.f - sh.strength[j] * (1.f - __fdividef(1.f, 1.f + q8));
+                        const float ratio = __fdividef(kv[jj] - pv[jj], pv[jj] + 1e-16f);
                         const float updated = fmaxf(f * (1.f + damping * ratio), 1e-6f);
                         float hi, lo;
                         split_tf32(updated, hi, lo);
@@ -450,7 +457,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const int j = e / c, k = e - j * c;
             const int64_t voxel = sh.vox[j];
             if (voxel >= 0) {
-                const size_t off = kmajor_offset(j, k, fgroup);
+                const size_t off = kmajor_offset(j, k, fgroup, kTcFGroupFloats);
                 x[voxel * ldx + k] = double(FH[off] + FL[off]);
             }
         }
