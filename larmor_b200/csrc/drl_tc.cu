@@ -41,7 +41,8 @@
 namespace lar {
 namespace {
 
-constexpr int kTcThreads = 128;
+constexpr int kTcThreads = 256;   // 8 warps: warp w reads tensor-memory lanes 32 (w % 4).., voxels 24 (w / 4)..
+constexpr int kTcHalf = 24;       // voxels of a tile each of a quadrant's two warps updates
 constexpr int kTcN = 48;          // voxels per tile (the MMA's N)
 constexpr int kTcM = 128;         // directions per MMA tile (the MMA's M)
 constexpr int kTcK = 8;           // directions per MMA step (K of kind::tf32)
@@ -81,7 +82,7 @@ struct TcShared {
     float strength[kTcN], threshold[kTcN];
     int active[kTcN];
     long long vox[kTcN];
-    float part[4][kTcN];
+    float part[4][kTcN];  // each lane quadrant's share of a voxel's change
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -164,28 +165,20 @@ __device__ __forceinline__ void umma_commit(unsigned long long* bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
-    unsigned r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
+__device__ __forceinline__ void tmem_ld8(unsigned taddr, float (&v)[8]) {
+    unsigned r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void tmem_st16(unsigned taddr, const float (&v)[16]) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16};" ::"r"(taddr),
-        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
-        "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
-        "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
-        "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
-        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
-        "r"(__float_as_uint(v[15])));
+__device__ __forceinline__ void tmem_st8(unsigned taddr, const float (&v)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+                 "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+                 "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])));
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -247,14 +240,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncthreads();
     tc_fence_after();
     const unsigned tmem = sh.tmem_base;
-    const unsigned lane_base = unsigned(32 * warp) << 16;
+    const int quad = warp & 3, half = warp >> 2;
+    const unsigned lane_base = unsigned(32 * quad) << 16;
     // G streams through the stage ring continuously, across iterations and tiles (it does not
     // change): chunk R of the stream is data chunk R % nq in stage R % kTcStages, the (R /
     // kTcStages)-th use of that stage, so its barriers' phase parity is (R / kTcStages) & 1.
-    // Thread 0 counts the chunks consumed (`used`) and loaded (`loaded`); everyone tracks `done`.
+    // Thread 0 issues the MMAs and counts the chunks consumed (`used`); thread 32 (the producer)
+    // issues the copies and counts the chunks loaded (`loaded`), kTcStages ahead; everyone
+    // tracks `done`.
+    constexpr int kProducer = 32;
     long long used = 0, loaded = 0;
     unsigned done_phase = 0;
-    if (tid == 0) {
+    if (tid == kProducer) {
         for (; loaded < kTcStages; ++loaded)
             load_chunk(stage_base + size_t(loaded) * chunk, gtc, int(loaded % nq), tiles, &sh.full[loaded]);
     }
@@ -263,7 +260,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (tid < kTcN) sh.vox[tid] = p0 + tid < count ? (list ? int64_t(list[p0 + tid]) : p0 + tid) : -1;
         __syncthreads();
         // Each voxel's damping strength and stopping threshold (drl.cu), a warp per voxel.
-        for (int j = warp; j < kTcN; j += 4) {
+        for (int j = warp; j < kTcN; j += kTcThreads / 32) {
             const int64_t voxel = sh.vox[j];
             if (voxel < 0) {
                 if (lane == 0) {
@@ -309,22 +306,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
             __syncthreads();
             for (int t = 0; t < tiles; ++t) {
-                const int d = kTcM * t + 32 * warp + lane;
-                double acc[16];
+                const int d = kTcM * t + 32 * quad + lane;
+                double acc[8];
 #pragma unroll
-                for (int jj = 0; jj < 16; ++jj) acc[jj] = 0.0;
+                for (int jj = 0; jj < 8; ++jj) acc[jj] = 0.0;
                 if (d < c) {
                     const double* kt = P.k_t + size_t(d) * m;
+                    const double* sh8 = sig + size_t(8 * half) * m;
                     for (int i = 0; i < m; ++i) {
                         const double k = kt[i];
 #pragma unroll
-                        for (int jj = 0; jj < 16; ++jj) acc[jj] = fma(k, sig[jj * m + i], acc[jj]);
+                        for (int jj = 0; jj < 8; ++jj) acc[jj] = fma(k, sh8[jj * m + i], acc[jj]);
                     }
                 }
-                float ks[16];
+                float ks[8];
 #pragma unroll
-                for (int jj = 0; jj < 16; ++jj) ks[jj] = float(acc[jj]);
-                tmem_st16(tmem + lane_base + unsigned(kTcKsCol + t * kTcN + j0), ks);
+                for (int jj = 0; jj < 8; ++jj) ks[jj] = float(acc[jj]);
+                tmem_st8(tmem + lane_base + unsigned(kTcKsCol + t * kTcN + j0 + 8 * half), ks);
             }
             tmem_wait_st();
             __syncthreads();
@@ -352,9 +350,24 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
             __syncthreads();
             if (sh.n_active == 0 || sh.abort) break;
-            // The product: thread 0 issues the MMAs of the iteration's nq chunks as they land.
-            // Once the MMAs of chunk R - 1 are done its stage takes chunk R + 3 of the stream
-            // (those of chunk R are queued behind them meanwhile).
+            // The product: thread 0 issues the MMAs of the iteration's nq chunks as they land,
+            // while the producer refills each stage with chunk R + kTcStages of the stream as
+            // soon as the MMAs of chunk R are done with it.
+            if (tid == kProducer) {
+                bool ok = true;
+                for (int i = 0; i < nq && ok; ++i) {
+                    const long long R = loaded, Rw = R - kTcStages;
+                    const int s = int(R % kTcStages);
+                    ok = mbar_wait(&sh.empty[s], unsigned(Rw / kTcStages) & 1u);
+                    if (!ok) break;
+                    load_chunk(stage_base + size_t(s) * chunk, gtc, int(R % nq), tiles, &sh.full[s]);
+                    ++loaded;
+                }
+                if (!ok) {
+                    sh.abort = 1;
+                    atomicExch(err, 1);
+                }
+            }
             if (tid == 0) {
                 tc_fence_after();
                 bool ok = true;
@@ -379,14 +392,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     }
                     umma_commit(&sh.empty[s]);
                     ++used;
-                    if (R >= 1) {
-                        const long long Rp = R - 1;
-                        const int sp = int(Rp % kTcStages);
-                        ok = mbar_wait(&sh.empty[sp], unsigned(Rp / kTcStages) & 1u);
-                        if (!ok) break;
-                        load_chunk(stage_base + size_t(sp) * chunk, gtc, int(loaded % nq), tiles, &sh.full[sp]);
-                        ++loaded;
-                    }
                 }
                 umma_commit(&sh.done);
                 if (!ok) {
@@ -405,21 +410,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             tc_fence_after();
             __syncthreads();
             if (sh.abort) break;
-            // The damped update of the still-active voxels; each thread holds direction lanes.
-            float change[kTcN];
+            // The damped update of the still-active voxels: a thread holds one direction lane of
+            // each tile and the 24 voxels of its warp's half.
+            float change[kTcHalf];
 #pragma unroll
-            for (int j = 0; j < kTcN; ++j) change[j] = 0.f;
+            for (int j = 0; j < kTcHalf; ++j) change[j] = 0.f;
             for (int t = 0; t < tiles; ++t) {
-                const int d = kTcM * t + 32 * warp + lane;
+                const int d = kTcM * t + 32 * quad + lane;
 #pragma unroll
-                for (int j0 = 0; j0 < kTcN; j0 += 16) {
-                    float pv[16], kv[16];
-                    tmem_ld16(tmem + lane_base + unsigned(t * kTcN + j0), pv);
-                    tmem_ld16(tmem + lane_base + unsigned(kTcKsCol + t * kTcN + j0), kv);
+                for (int g = 0; g < kTcHalf; g += 8) {
+                    const int j0 = kTcHalf * half + g;
+                    float pv[8], kv[8];
+                    tmem_ld8(tmem + lane_base + unsigned(t * kTcN + j0), pv);
+                    tmem_ld8(tmem + lane_base + unsigned(kTcKsCol + t * kTcN + j0), kv);
                     tmem_wait_ld();
                     if (d >= c) continue;
 #pragma unroll
-                    for (int jj = 0; jj < 16; ++jj) {
+                    for (int jj = 0; jj < 8; ++jj) {
                         const int j = j0 + jj;
                         if (!sh.active[j]) continue;
                         const size_t off = kmajor_offset(j, d, fgroup, kTcFGroupFloats);
@@ -434,14 +441,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         split_tf32(updated, hi, lo);
                         FH[off] = hi;
                         FL[off] = lo;
-                        change[j] += fabsf(updated - f);
+                        change[g + jj] += fabsf(updated - f);
                     }
                 }
             }
 #pragma unroll
-            for (int j = 0; j < kTcN; ++j) {
+            for (int j = 0; j < kTcHalf; ++j) {
                 const float v = warp_sum(change[j]);
-                if (lane == 0) sh.part[warp][j] = v;
+                if (lane == 0) sh.part[quad][kTcHalf * half + j] = v;
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             tc_fence_before();
@@ -463,9 +470,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         __syncthreads();
     }
-    // The stream's copies still in flight land before the CTA exits (bounded waits).
-    if (tid == 0)
-        for (long long R = used; R < loaded; ++R)
+    // The stream's copies still in flight (the kTcStages loaded past the last chunk consumed)
+    // land before the CTA exits (bounded waits).
+    if (tid == kProducer)
+        for (long long R = loaded - kTcStages; R < loaded; ++R)
             if (!mbar_wait(&sh.full[R % kTcStages], unsigned(R / kTcStages) & 1u)) {
                 atomicExch(err, 1);
                 break;
