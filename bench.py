@@ -59,6 +59,19 @@ def fp64_tensor_roofline(flops_per_launch: float, avg_launch_s: float) -> dict:
             "algorithmic_flops_per_launch": flops_per_launch}
 
 
+def tf32_tensor_roofline(hw_flops_per_launch: float, useful_flops_per_launch: float, avg_launch_s: float,
+                         pk: dict) -> dict:
+    """The roofline fields of a kernel bound by the TF32 tensor cores: the tensor FLOP it issues
+    (three TF32 products over the padded tiles) against half the measured bf16 GEMM rate, TF32's
+    dense rate being half of bf16's on this part (1.1 vs 2.25 PFLOP/s nominal)."""
+    peak = pk["bf16_tflops"] / 2.0
+    achieved = hw_flops_per_launch / avg_launch_s / 1e12 if avg_launch_s > 0 else 0.0
+    return {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_source": "half the measured bf16 GEMM rate (TF32 dense rate)",
+            "tensor_flops_per_launch": hw_flops_per_launch, "algorithmic_flops_per_launch": useful_flops_per_launch,
+            "useful_tflops": useful_flops_per_launch / avg_launch_s / 1e12 if avg_launch_s > 0 else 0.0}
+
+
 def committed_traffic(kernel: str, workload: str, algorithmic_bytes: float) -> float | None:
     """Per-launch DRAM bytes of a kernel: the measured DRAM bytes per algorithmic byte of its
     committed ncu capture (profiles/traffic.json, a smaller case of the same workload) times
@@ -949,6 +962,11 @@ class DrlWorkload(_SdWorkloadBase):
         """FLOP of the product of one step at the iteration cap: 2 x 300^2 per voxel-iteration."""
         return {"drl_kernel": self.v * 200 * 2 * 300 ** 2, "drl_tc_kernel": self.v * 200 * 2 * 300 ** 2}
 
+    def kernel_tensor_flops(self) -> dict:
+        """The tensor FLOP the tensor-core mode issues at the iteration cap: three TF32 products
+        over three 128-direction tiles (384) and 304 padded directions per voxel-iteration."""
+        return {"drl_tc_kernel": self.v * 200 * 3 * 2 * 384 * 304}
+
     def step_e2e(self):
         self.d_signals.copy_(self.h_signals, non_blocking=True)
         self.step_device()
@@ -1053,6 +1071,11 @@ class GrlWorkload(MfodWorkload):
         """FP64 FLOP of one step at the iteration caps (the voxel-rounds from kernel_bytes)."""
         return {"drl_kernel": self.v * 599 * 2 * self.k_hr.ca ** 2, "drl_tc_kernel": self.v * 599 * 2 * self.k_hr.ca ** 2,
                 "drl_kernel_resident": self._voxel_rounds * 199 * 2 * self.k_lr.ca ** 2}
+
+    def kernel_tensor_flops(self) -> dict:
+        """The tensor FLOP of the tensor-core final solve at its iteration cap (599): three TF32
+        products over the padded 384 x 304 tiles per voxel-iteration."""
+        return {"drl_tc_kernel": self.v * 599 * 3 * 2 * 384 * 304}
 
     def parity(self) -> dict:
         """The device fit of the cpu_baseline sample's voxels against the FP64 oracle's GRL."""
@@ -1455,10 +1478,14 @@ def measure(wl, args, world: int, rank: int, dist, dev) -> dict:
         "clocks": clocks.summary(),
     }
     if hasattr(wl, "kernel_flops"):
-        # FP64 tensor-core kernels: FLOP over the nominal FP64 tensor rate; the HBM bytes stay
-        # beside it.
+        # Tensor-core kernels: FP64 ones against the nominal FP64 tensor rate, the TF32 one
+        # against the TF32 rate; the HBM bytes stay beside it.
         flops = wl.kernel_flops().get(top)
-        if flops is not None:
+        if flops is not None and top == "drl_tc_kernel":
+            hw = wl.kernel_tensor_flops()[top] * args.steps / max(top_launches, 1)
+            line["roofline"].update(tf32_tensor_roofline(hw, flops * args.steps / max(top_launches, 1), avg_launch_s, pk))
+            line["roofline"]["flops_basis"] = wl.flops_basis + "; tensor FLOP: 3 x 2 x 384 x 304 per voxel-iteration"
+        elif flops is not None:
             line["roofline"].update(fp64_tensor_roofline(flops * args.steps / max(top_launches, 1), avg_launch_s))
             line["roofline"]["flops_basis"] = wl.flops_basis
     issue = committed_issue(top, wl.name, bytes_per_launch)

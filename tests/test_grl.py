@@ -372,3 +372,36 @@ def test_gpu_grl_on_the_tensor_cores_stays_within_the_fod_tolerance(cuda, grl_fi
           f"{np.abs(fractions - ref_fr).max():.3e}")
     assert rel.max() <= 5e-4 and np.median(rel) <= 1e-4
     assert np.abs(fractions - ref_fr).max() <= 1e-4
+
+
+def _wide_and_rank_deficient_problems():
+    """Seeded problems the fraction fits never build: fewer rows than columns (the QR's wide
+    case, rank at most the row count) and duplicated columns (rank-deficient), where the
+    column-pivoted QR's rank threshold decides which columns get zero."""
+    rng = np.random.default_rng(12)
+    problems = []
+    for _ in range(40):
+        m, n = int(rng.integers(2, 6)), int(rng.integers(6, 12))
+        c = np.abs(rng.standard_normal((m, n)))
+        problems.append((np.ascontiguousarray(c), c @ np.abs(rng.standard_normal(n)) + 0.1 * rng.standard_normal(m)))
+    for _ in range(40):
+        m, n = 24, int(rng.integers(3, 8))
+        base = np.exp(-np.outer(np.linspace(0, 3e3, m), rng.uniform(0.1e-3, 3e-3, n)))
+        dup = int(rng.integers(0, n))
+        c = np.ascontiguousarray(np.concatenate([base, base[:, dup:dup + 1]], axis=1))
+        problems.append((c, c @ rng.dirichlet(np.ones(n + 1)) + 0.01 * rng.standard_normal(m)))
+    return problems
+
+
+@pytest.mark.gpu
+def test_gpu_lsqnonneg_matches_the_oracle_on_wide_and_rank_deficient_problems(cuda, oracle):
+    """The device NNLS against the oracle's (the reference's ColPivHouseholderQR rank rule) on
+    wide problems (m < n) and problems with a duplicated column: the same zero coefficients and
+    values within 1e-10 of the largest."""
+    from larmor_b200 import _core
+
+    for c, d in _wide_and_rank_deficient_problems():
+        x = _core.lsqnonneg(c, d)
+        expected = oracle.nnls(c, d)[0]
+        np.testing.assert_array_equal(x == 0, expected == 0)
+        np.testing.assert_allclose(x, expected, rtol=0, atol=1e-10 * max(1.0, np.abs(expected).max()))
