@@ -500,7 +500,7 @@ class MfodWorkload(_SdWorkloadBase):
 
     name = "mfod_3tissue_110x110x70"
     kernels = ("correlate_kernel", "ridge_nnls_half_kernel<3>", "ridge_nnls_kernel<1,2>", "lr_fractions_kernel",
-               "ridge_nnls_kernel<8,10>", "hr_fractions_kernel")
+               "ridge_nnls_first_kernel<1,10>", "ridge_nnls_kernel<8,10>", "hr_fractions_kernel")
     has_fp32 = True
     fraction_tol = 1e-7
     # The plain FP32 fit takes seconds per step: a few timed steps bound the run.
@@ -579,13 +579,15 @@ class MfodWorkload(_SdWorkloadBase):
         self.d_rounds = rounds
         vr = int(rounds.sum().item())
         m, c_lr, c_hr = 280, self.k_lr.ca, self.k_hr.ca
-        # The low-resolution NNLS runs two voxels per warp; the one-warp kernel refits only the
-        # few voxels that need its QR fallback (counted with the two-voxel kernel's).
+        # The low-resolution NNLS runs two voxels per warp and the high-resolution one a first
+        # pass with a 32-column factor; the full-factor kernels refit only the few voxels handed
+        # back (counted with the first kernels').
         return {"correlate_kernel": vr * 8 * (m + c_lr) + self.v * 8 * (m + c_hr),
                 "ridge_nnls_half_kernel<3>": vr * 8 * 2 * c_lr,
                 "ridge_nnls_kernel<1,2>": 0,
                 "lr_fractions_kernel": vr * 8 * (c_lr + m + 3),
-                "ridge_nnls_kernel<8,10>": self.v * 8 * 2 * c_hr,
+                "ridge_nnls_first_kernel<1,10>": self.v * 8 * 2 * c_hr,
+                "ridge_nnls_kernel<8,10>": 0,
                 "hr_fractions_kernel": self.v * 8 * (c_hr + m + 3)}
 
     def step_e2e(self):
@@ -734,7 +736,8 @@ def _job_kernel_bytes(job) -> dict:
             "ridge_nnls_half_kernel<3>": vr * 8 * 2 * c_lr,
             "ridge_nnls_kernel<1,2>": 0,
             "lr_fractions_kernel": vr * 8 * (c_lr + n + 3),
-            "ridge_nnls_kernel<8,10>": v * 8 * 2 * c_hr,
+            "ridge_nnls_first_kernel<1,10>": v * 8 * 2 * c_hr,
+            "ridge_nnls_kernel<8,10>": 0,
             "hr_fractions_kernel": v * 8 * (c_hr + n + 3)}
 
 
@@ -746,7 +749,7 @@ class BatchWorkload:
     name = "batch_uneven_64_volumes"
     kernels = ("fit_dti_maps_kernel", "fit_log_warp_kernel", "constrained_fit_kernel", "dki_maps_kernel",
                "correlate_kernel", "ridge_nnls_half_kernel<3>", "ridge_nnls_kernel<1,2>", "lr_fractions_kernel",
-               "ridge_nnls_kernel<8,10>", "hr_fractions_kernel")
+               "ridge_nnls_first_kernel<1,10>", "ridge_nnls_kernel<8,10>", "hr_fractions_kernel")
     has_fp32 = False
 
     def __init__(self, seed: int) -> None:

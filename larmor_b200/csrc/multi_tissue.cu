@@ -247,10 +247,14 @@ __device__ __noinline__ bool ridge_qr_fit(const RidgeDev R, const double* sig, c
 // the flags, the workspace pointers) stays in registers; the outer (entering column) and inner
 // (blocking step) iterations of Lawson-Hanson share one loop with one fit, so the factor code
 // is emitted once.
-template <int VPL, int CPL, class State>
+//
+// With REDO, a fit the factor cannot take (more than VPL * 32 active columns, or a pivot below the
+// relative tolerance) stops at once with *redo set, instead of continuing by QR: the caller refits
+// that voxel from the start with a larger factor, which takes the same steps up to that point.
+template <int VPL, int CPL, bool REDO = false, class State>
 __device__ __forceinline__ bool ridge_nnls(const RidgeDev R, const SignalDev S, int64_t voxel,
                                            const double* __restrict__ corr, const NnlsSlot sl, State& st,
-                                           int lane) {
+                                           int lane, bool* redo = nullptr) {
     const int c = R.c;
     const InvFactor fac{sl.L, sl.M, sl.h, sl.w, sl.y, st.cols, VPL * 32};
     for (int j = lane; j < c; j += 32) {
@@ -363,6 +367,10 @@ __device__ __forceinline__ bool ridge_nnls(const RidgeDev R, const SignalDev S, 
                         ? inv_append<1>(fac, na, gee, corr[entering], entering, kMinPivot, lane)
                         : inv_append<VPL>(fac, na, gee, corr[entering], entering, kMinPivot, lane);
                 if (!appended) {
+                    if constexpr (REDO) {
+                        *redo = true;
+                        return true;
+                    }
                     failed = true;
                 } else {
                     if (lane == 0) sl.inf[entering] = 1;
@@ -417,6 +425,39 @@ __global__ void __launch_bounds__(kMtWarps * 32, (CPL <= 2 ? 6 : 4)) ridge_nnls_
         const bool ok = ridge_nnls<VPL, CPL>(R, S, voxel, corr + voxel * ldc, sl, st, lane);
         for (int j = lane; j < R.c; j += 32) x_out[voxel * ldx + j] = sl.x[j];
         if (lane == 0 && !ok && bad) bad[voxel] = 1;
+        __syncwarp();
+    }
+}
+
+// The first pass of the high-resolution NNLS: one warp per voxel with a factor of VPL * 32 columns
+// (the active sets of the 300-direction FODs stay below 32; a larger factor takes more shared
+// memory and registers and fewer warps per SM); a voxel whose fit outgrows it, or needs the QR
+// fallback, goes on `redo` for ridge_nnls_kernel with the full factor, which fits it from the
+// start. Below the capacity the two take the same steps with the same factor code, so every
+// voxel gets the result the full-factor kernel gives.
+template <int VPL, int CPL>
+__global__ void __launch_bounds__(kMtWarps * 32, 5) ridge_nnls_first_kernel(
+    RidgeDev R, SignalDev S, int64_t count, const double* __restrict__ corr, int ldc, double* __restrict__ x_out,
+    int ldx, int* __restrict__ redo, int* redo_count, int* queue, double* __restrict__ workspace, size_t slot_size) {
+    using State = NnlsState<VPL * 32, CPL * 32>;
+    __shared__ State states[kMtWarps];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    State& st = states[warp];
+    NnlsSlot sl = carve_nnls(workspace + (size_t(blockIdx.x) * kMtWarps + warp) * slot_size,
+                             smem_raw + warp * nnls_smem_bytes(R.c, VPL * 32), R.m, R.c, VPL * 32);
+    for (;;) {
+        int64_t voxel = 0;
+        if (lane == 0) voxel = atomicAdd(queue, 1);
+        voxel = __shfl_sync(0xffffffffu, voxel, 0);
+        if (voxel >= count) break;
+        bool again = false;
+        ridge_nnls<VPL, CPL, true>(R, S, voxel, corr + voxel * ldc, sl, st, lane, &again);
+        if (again) {
+            if (lane == 0) redo[atomicAdd(redo_count, 1)] = int(voxel);
+        } else {
+            for (int j = lane; j < R.c; j += 32) x_out[voxel * ldx + j] = sl.x[j];
+        }
         __syncwarp();
     }
 }
@@ -1203,14 +1244,22 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
         const size_t half_smem = half_smem_bytes(c_lr) * 2 * kMtWarps;
         const int64_t half_warps = half ? resident_slots(half_kernel, half_smem, n_max, "sd.nnls.ctas_per_sm") : 0;
         const int64_t hr_slots = hr_drl ? 0 : resident_slots(hr_nnls.kernel, hr_smem, n_max, "sd.nnls.ctas_per_sm");
+        // High-resolution kernels of 65 to 320 directions with normal equations: a first pass with
+        // a 32-column factor, the voxels that outgrow it refitted by the full-factor kernel.
+        const bool hr_first = !hr_drl && hrs.normal_equations && c_hr > 64 && c_hr <= 320;
+        auto first_kernel = ridge_nnls_first_kernel<1, 10>;
+        const size_t first_smem = nnls_smem_bytes(c_hr, 32) * kMtWarps;
+        const int64_t first_slots = hr_first ? resident_slots(first_kernel, first_smem, n_max, "sd.nnls.ctas_per_sm") : 0;
+        const size_t first_slot = nnls_slot_doubles(mi, 32);
         const int64_t lf_slots = resident_slots(lr_fractions_kernel, 0, n_max, "sd.fractions.ctas_per_sm");
         const int64_t hf_slots = resident_slots(hr_fractions_kernel, 0, n_max, "sd.fractions.ctas_per_sm");
         const size_t lr_slot = nnls_slot_doubles(mi, lr_nnls.cap), hr_slot = nnls_slot_doubles(mi, hr_nnls.cap);
         const size_t lf_slot = frac_slot_doubles(mi, c_lr, 1 + ci), hf_slot = frac_slot_doubles(mi, c_hr, nf);
         const size_t slot_doubles =
-            std::max(std::max(std::max(size_t(lr_slots) * lr_slot, size_t(hr_slots) * hr_slot),
-                              std::max(size_t(lf_slots) * lf_slot, size_t(hf_slots) * hf_slot)),
-                     size_t(2 * half_warps) * half_slot_doubles());
+            std::max(std::max(std::max(std::max(size_t(lr_slots) * lr_slot, size_t(hr_slots) * hr_slot),
+                                       std::max(size_t(lf_slots) * lf_slot, size_t(hf_slots) * hf_slot)),
+                              size_t(2 * half_warps) * half_slot_doubles()),
+                     size_t(first_slots) * first_slot);
         struct Pieces {
             int* counters;  // [0] the persistent kernels' work counter, [2], [3] the two lists' counts,
                             // [4] the voxels to refit by the one-warp NNLS
@@ -1325,11 +1374,30 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
             } else {
                 launch_correlate(hr_sig, nullptr, n, nullptr, hrs, P.corr, c_hr, st);
                 reset_queue();
-                LaunchScope scope(hr_nnls.name, st);
-                hr_nnls.kernel<<<blocks(hr_slots, n), kMtWarps * 32, hr_smem, st>>>(
-                    hrs, hr_sig, nullptr, n, nullptr, P.corr, c_hr, fods + v0 * c_hr, c_hr, P.bad, P.counters, P.slots,
-                    hr_slot);
-                cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
+                if (hr_first) {
+                    cuda_check(cudaMemsetAsync(P.counters + 4, 0, sizeof(int), st), "cudaMemsetAsync");
+                    {
+                        LaunchScope scope("ridge_nnls_first_kernel<1,10>", st);
+                        first_kernel<<<blocks(first_slots, n), kMtWarps * 32, first_smem, st>>>(
+                            hrs, hr_sig, n, P.corr, c_hr, fods + v0 * c_hr, c_hr, P.redo, P.counters + 4, P.counters,
+                            P.slots, first_slot);
+                        cuda_check(cudaGetLastError(), "ridge_nnls_first_kernel launch");
+                    }
+                    reset_queue();
+                    // The voxels the first pass handed back (rare): a grid of one CTA per SM.
+                    LaunchScope scope(hr_nnls.name, st);
+                    const unsigned redo_blocks = std::min<unsigned>(blocks(hr_slots, n), unsigned(sm_count()));
+                    hr_nnls.kernel<<<redo_blocks, kMtWarps * 32, hr_smem, st>>>(
+                        hrs, hr_sig, P.redo, n, P.counters + 4, P.corr, c_hr, fods + v0 * c_hr, c_hr, P.bad,
+                        P.counters, P.slots, hr_slot);
+                    cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
+                } else {
+                    LaunchScope scope(hr_nnls.name, st);
+                    hr_nnls.kernel<<<blocks(hr_slots, n), kMtWarps * 32, hr_smem, st>>>(
+                        hrs, hr_sig, nullptr, n, nullptr, P.corr, c_hr, fods + v0 * c_hr, c_hr, P.bad, P.counters,
+                        P.slots, hr_slot);
+                    cuda_check(cudaGetLastError(), "ridge_nnls_kernel launch");
+                }
             }
             reset_queue();
             LaunchScope scope("hr_fractions_kernel", st);
