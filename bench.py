@@ -726,7 +726,7 @@ def _job_kernel_bytes(job) -> dict:
     if job.kind == "dti":
         return {"fit_dti_maps_kernel": v * (4 * n + 8 + 16 * 4 + 1)}
     if job.kind == "dki":
-        viol = job.handles["design"].violators()
+        viol = int(job.out["broke"].sum().item())  # the voxels whose fit broke a constraint
         return {"fit_log_warp_kernel": v * (4 * n + 16 + 22 * 8 + 1),
                 "constrained_fit_kernel": viol * (4 * n + 16 + 2 * 22 * 8),
                 "dki_maps_kernel": v * (22 * 8 + 36 * 4 + 1)}
@@ -741,15 +741,26 @@ def _job_kernel_bytes(job) -> dict:
             "hr_fractions_kernel": v * 8 * (c_hr + n + 3)}
 
 
+# The kernels of the per-family work queues and the single-volume kernels whose per-voxel work
+# they do (the same algorithmic bytes).
+QUEUE_KERNELS = {"batch_dti_kernel": "fit_dti_maps_kernel", "batch_log_warp_kernel": "fit_log_warp_kernel",
+                 "batch_refit_kernel": "constrained_fit_kernel", "batch_dki_maps_kernel": "dki_maps_kernel",
+                 "batch_plan_kernel": None, "batch_correlate_kernel": "correlate_kernel",
+                 "batch_half_kernel<3>": "ridge_nnls_half_kernel<3>", "batch_redo_kernel<1,2>": "ridge_nnls_kernel<1,2>",
+                 "batch_lr_fractions_kernel": "lr_fractions_kernel",
+                 "batch_first_kernel<1,10>": "ridge_nnls_first_kernel<1,10>",
+                 "batch_redo_kernel<8,10>": "ridge_nnls_kernel<8,10>",
+                 "batch_hr_fractions_kernel": "hr_fractions_kernel"}
+
+
 class BatchWorkload:
     """Config 4: 64 seeded volumes of uneven size (10k-400k voxels), gradient table (1-3 shells
     of 30-90 directions) and model (DTI/DKI/mFOD 40/20/40), all fitted by one replay of one
-    CUDA graph whose parallel branches run the volumes side by side."""
+    CUDA graph: each model family's stages are single launches over all of its volumes, taking
+    (volume, voxel-block) tickets from one device queue; the three families run side by side."""
 
     name = "batch_uneven_64_volumes"
-    kernels = ("fit_dti_maps_kernel", "fit_log_warp_kernel", "constrained_fit_kernel", "dki_maps_kernel",
-               "correlate_kernel", "ridge_nnls_half_kernel<3>", "ridge_nnls_kernel<1,2>", "lr_fractions_kernel",
-               "ridge_nnls_first_kernel<1,10>", "ridge_nnls_kernel<8,10>", "hr_fractions_kernel")
+    kernels = tuple(QUEUE_KERNELS)
     has_fp32 = False
 
     def __init__(self, seed: int) -> None:
@@ -760,7 +771,8 @@ class BatchWorkload:
         kinds = {k: sum(1 for j in self.jobs if j.kind == k) for k in ("dti", "dki", "mfod")}
         self.config = {"workload": self.name, "volumes": len(self.jobs), "voxels": self.v, "jobs": kinds,
                        "voxels_per_volume": [min(j.voxels for j in self.jobs), max(j.voxels for j in self.jobs)],
-                       "launch": "one CUDA graph replay per step (4 parallel branches)",
+                       "launch": "one CUDA graph replay per step: one work queue per model family "
+                                 "(3 parallel branches)",
                        "l2": "inputs (4.8 GB) larger than L2"}
 
     def subset(self, n: int) -> None:
@@ -772,7 +784,7 @@ class BatchWorkload:
         from larmor_b200.batch import Batch
 
         self.torch = torch
-        self.batch = Batch(self.jobs, branches=4, tune=True)
+        self.batch = Batch(self.jobs, tune=True)
         self.config["launch_settings"] = self.batch.launch_settings
         self.batch.capture()
         self.h_in = [tuple(torch.from_numpy(np.ascontiguousarray(t.cpu().numpy())).pin_memory() for t in j.d_in)
@@ -803,11 +815,11 @@ class BatchWorkload:
 
     def kernel_bytes(self) -> dict:
         self.torch.cuda.synchronize()
-        total: dict = {}
+        single: dict = {}
         for j in self.jobs:
             for k, b in _job_kernel_bytes(j).items():
-                total[k] = total.get(k, 0) + b
-        return total
+                single[k] = single.get(k, 0) + b
+        return {k: single.get(v, 0) if v else 0 for k, v in QUEUE_KERNELS.items()}
 
     def cpu_sample(self, threads: int, budget_s: float) -> tuple[int, float, str]:
         from larmor_b200.dwi.dki import dki_constraints, dki_design

@@ -384,6 +384,54 @@ int lar_find_peaks(lar_peak_sphere sphere, const double* coeffs, int64_t n, int6
                    const double* on_sphere, int64_t lds, int n_peaks, double relative_threshold, double threshold,
                    double* directions, double* amplitudes, void* stream);
 
+/* ---- Batches: many volumes, one work queue per model family ---------------------------- */
+
+/* A batch of volumes ("jobs") of the DTI, DKI and multi-tissue (mFOD) models, of different
+ * sizes and gradient tables. Each family's stages run as single launches over all of the
+ * family's volumes, whose CTAs or warps take (volume, voxel-block) tickets from one device
+ * counter, as the reference's block queue does within a volume
+ * (cpp/src/common/parallel.hpp:26-84); a volume's results equal those of its own fit
+ * (lar_fit_dti_maps, lar_fit_dki_maps with LAR_FP64, lar_fit_multi_tissue). No reference
+ * function takes several volumes at once: the batched-uneven workload is a driver loop over
+ * volumes there. */
+typedef struct lar_batch_s* lar_batch;
+
+#define LAR_BATCH_DTI 1
+#define LAR_BATCH_DKI 2
+#define LAR_BATCH_MFOD 4
+
+int lar_batch_create(lar_batch* out);
+void lar_batch_destroy(lar_batch batch);
+
+/* Adds a DTI volume: the arguments of lar_fit_dti_maps (device pointers, FP64, no params).
+ * Every DTI job of a batch takes the same weighted, max_iter and tol. */
+int lar_batch_add_dti(lar_batch batch, lar_log_design design, const float* signals, const double* floor, int64_t v,
+                      int weighted, int64_t max_iter, double tol, float* maps, uint8_t* npd);
+
+/* Adds a DKI volume: the arguments of lar_fit_dki_maps (device pointers, FP64). Every DKI job
+ * of a batch takes the same weighted, max_iter and tol. */
+int lar_batch_add_dki(lar_batch batch, lar_log_design design, const float* signals, const double* s0,
+                      const double* floor, const uint8_t* is_b0, int64_t v, int weighted, int64_t max_iter, double tol,
+                      float* maps, uint8_t* npd, uint8_t* broke, double* params);
+
+/* Adds a multi-tissue volume: the arguments of lar_fit_multi_tissue (signals and outputs on the
+ * device, weights (m,) on the host). The solvers must be ridge NNLS (L2NNLS) solvers with normal
+ * equations, the low-resolution kernel of at most 48 directions and the high-resolution one of
+ * 65 to 320; every mFOD job of a batch takes the same max_outer, fraction_tol and final_tol_x. */
+int lar_batch_add_mfod(lar_batch batch, const double* signals, int64_t v, const double* weights, lar_deconv_kernel lr,
+                       lar_fod_solver lr_solver, lar_deconv_kernel hr, lar_fod_solver hr_solver, int64_t max_outer,
+                       double fraction_tol, double final_tol_x, double* fods, double* fractions, int32_t* rounds,
+                       uint8_t* status);
+
+/* Uploads the job tables and allocates the batch's scratch; no job can be added afterwards.
+ * The jobs' designs, kernels, solvers, inputs and outputs must outlive the batch. */
+int lar_batch_finalize(lar_batch batch);
+
+/* Enqueues the stages of the families in `families` (LAR_BATCH_* bits) on `stream`. A
+ * family's runs must not overlap one another on the GPU; different families may run on
+ * different streams at once. Allocates nothing and does not wait on the host. */
+int lar_batch_run(lar_batch batch, int families, void* stream);
+
 /* ---- A fit that allocates no device memory ------------------------------------------- */
 
 /* No counterpart in the reference: an entry point for callers that cannot allocate device

@@ -44,6 +44,13 @@ SIGNATURES: dict[str, tuple] = {
     "lar_fit_multi_tissue_async": (_i32, [_p, _i64, _p, _p, _p, _p, _p, _i64, _f64, _f64, _p, _p, _p, _p, _p]),
     "lar_fit_multi_tissue_plain_fp32": (_i32, [_p, _i64, _p, _p, _p, _p, _p, _i64, _f64, _f64, _p, _p, _p, _p, _p]),
     "lar_lsqnonneg": (_i32, [_p, _i64, _i64, _p, _i32, _f64, _p, _p]),
+    "lar_batch_create": (_i32, [_p]),
+    "lar_batch_destroy": (None, [_p]),
+    "lar_batch_add_dti": (_i32, [_p, _p, _p, _p, _i64, _i32, _i64, _f64, _p, _p]),
+    "lar_batch_add_dki": (_i32, [_p, _p, _p, _p, _p, _p, _i64, _i32, _i64, _f64, _p, _p, _p, _p]),
+    "lar_batch_add_mfod": (_i32, [_p, _p, _i64, _p, _p, _p, _p, _p, _i64, _f64, _f64, _p, _p, _p, _p]),
+    "lar_batch_finalize": (_i32, [_p]),
+    "lar_batch_run": (_i32, [_p, _i32, _p]),
     "lar_fit_single_tissue": (_i32, [_p, _i64, _p, _p, _p, _p]),
     "lar_sh_projector_create": (_i32, [_p, _i64, _i64, _p]),
     "lar_sh_projector_destroy": (None, [_p]),
@@ -67,6 +74,7 @@ SIGNATURES: dict[str, tuple] = {
 
 LAR_OK, LAR_ERR_INVALID, LAR_ERR_CUDA, LAR_ERR_MEMORY = 0, 1, 2, 3
 LAR_FP64, LAR_FP32, LAR_TF32X3 = 0, 1, 2
+LAR_BATCH_DTI, LAR_BATCH_DKI, LAR_BATCH_MFOD = 1, 2, 4
 # Sample types of lar_stage_dwi, by numpy dtype.
 LAR_DTYPES = {"float32": 0, "float64": 1, "int16": 2, "uint16": 3, "int8": 4, "uint8": 5, "int32": 6, "uint32": 7}
 

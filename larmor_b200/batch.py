@@ -1,17 +1,22 @@
 """Batched fits of many volumes in one CUDA graph.
 
 A batch holds jobs of different models (DTI, DKI, mFOD), gradient tables and voxel counts. Each
-job gets its own device inputs, outputs and design handles (a handle owns scratch memory, so
-two jobs never share one). `Batch.capture()` runs every job once eagerly, which sizes each
-handle's scratch and uploads its shell weights, then records all of them into one CUDA graph:
-the jobs are spread over parallel branches of the graph (longest first onto the least-loaded
-branch), so that a volume too small to fill the GPU runs beside others. `Batch.run()` replays
-the graph: one launch for the whole batch. With `tune=True` the launch shapes of each model's
-kernels are first chosen by measurement (larmor_b200.autotune). The results stay on the device in each job's output
-tensors.
+job gets its own device inputs, outputs and design handles. By default (`queue=True`) the jobs
+of each model family are fitted through one device work queue (lar_batch_*): every stage of the
+family is one launch over all of the family's volumes, whose CTAs or warps take (volume,
+voxel-block) tickets from one counter, so uneven volumes and uneven per-voxel NNLS costs are
+absorbed across the whole batch; the three families run on parallel branches. With
+`queue=False` each job runs its own chain of kernels, the jobs spread over parallel branches
+(longest first onto the least-loaded branch).
 
-The per-model work is the same kernels as the single fits (larmor_b200._core), so a job's
-result in the batch equals its result alone.
+`Batch.capture()` runs the batch once eagerly (which sizes the per-job scratch of the chained
+mode and uploads shell weights), then records it into one CUDA graph; `Batch.run()` replays
+it: one launch for the whole batch. With `tune=True` the launch shapes of each model's kernels
+are first chosen by measurement (larmor_b200.autotune). The results stay on the device in each
+job's output tensors.
+
+The per-voxel work is the same device code as the single fits (larmor_b200._core), so a job's
+result in the batch equals its result alone, bit for bit.
 """
 
 from __future__ import annotations
@@ -203,12 +208,70 @@ def job_device_bytes(job) -> int:
     return v * (8 * n + 8 * 303 + 5) + v * (8 * (300 + 44 + 2 + 3) + 12)
 
 
+class FamilyQueues:
+    """The jobs of a batch fitted through one device work queue per model family: a lar_batch
+    holding every job's inputs, outputs and handles (which must outlive it). run(family)
+    enqueues the family's stages on the current stream."""
+
+    FAMILIES = {"dti": _lib.LAR_BATCH_DTI, "dki": _lib.LAR_BATCH_DKI, "mfod": _lib.LAR_BATCH_MFOD}
+
+    def __init__(self, jobs) -> None:
+        import ctypes
+
+        from larmor_b200.sd.solvers import FINAL_FRACTION_TOL_X, MAX_ROUNDS
+
+        lib = _lib.lib()
+        handle = ctypes.c_void_p()
+        _lib.check(lib.lar_batch_create(ctypes.byref(handle)))
+        self.handle = handle
+        self.kinds = []
+        try:
+            for job in jobs:
+                h, d_in, out = job.handles, job.d_in, job.out
+                if job.kind == "dti":
+                    s, floor = d_in
+                    _lib.check(lib.lar_batch_add_dti(
+                        handle, h["design"].handle, _lib.ptr(s), _lib.ptr(floor), job.voxels, 1, 20, 1e-6,
+                        _lib.ptr(out["maps"]), _lib.ptr(out["npd"])))
+                elif job.kind == "dki":
+                    s, s0, floor, b0 = d_in
+                    _lib.check(lib.lar_batch_add_dki(
+                        handle, h["design"].handle, _lib.ptr(s), _lib.ptr(s0), _lib.ptr(floor), _lib.ptr(b0),
+                        job.voxels, 1, 20, 1e-6, _lib.ptr(out["maps"]), _lib.ptr(out["npd"]),
+                        _lib.ptr(out["broke"]), _lib.ptr(out["params"])))
+                else:
+                    _lib.check(lib.lar_batch_add_mfod(
+                        handle, _lib.ptr(d_in[0]), job.voxels, _lib.ptr(h["weights"]), h["k_lr"].handle,
+                        h["lr_solver"].handle, h["k_hr"].handle, h["hr_solver"].handle, MAX_ROUNDS, 1e-7,
+                        FINAL_FRACTION_TOL_X, _lib.ptr(out["fods"]), _lib.ptr(out["fractions"]),
+                        _lib.ptr(out["rounds"]), _lib.ptr(out["status"])))
+                if job.kind not in self.kinds:
+                    self.kinds.append(job.kind)
+            _lib.check(lib.lar_batch_finalize(handle))
+        except Exception:
+            lib.lar_batch_destroy(handle)
+            raise
+
+    def run(self, kind: str) -> None:
+        """Enqueues the stages of one family ("dti", "dki" or "mfod") on the current stream."""
+        import torch
+
+        _lib.check(_lib.lib().lar_batch_run(self.handle, self.FAMILIES[kind], _core._stream(torch)))
+
+    def __del__(self) -> None:
+        handle = getattr(self, "handle", None)
+        if handle is not None and handle.value:
+            _lib.lib().lar_batch_destroy(handle)
+            self.handle = None
+
+
 class Batch:
     """Jobs fitted together, replayed as one CUDA graph (see the module docstring)."""
 
-    def __init__(self, jobs, branches: int = 4, tune: bool = False, tuner=None) -> None:
+    def __init__(self, jobs, branches: int = 4, tune: bool = False, tuner=None, queue: bool = True) -> None:
         """tune: first pick each model's launch settings on a sample of its largest volume
-        (larmor_b200.autotune; the choice is cached per GPU and workload signature)."""
+        (larmor_b200.autotune; the choice is cached per GPU and workload signature). queue: one
+        work queue per model family (else a chain of kernels per job on `branches` branches)."""
         import torch
 
         self.torch = torch
@@ -219,17 +282,26 @@ class Batch:
 
             self.launch_settings = tune_jobs(self.jobs, tuner)
         self.dev = torch.device("cuda", torch.cuda.current_device())
-        self.streams = [torch.cuda.Stream(self.dev) for _ in range(max(1, branches))]
-        self.assignment = assign_branches([j.cost() for j in self.jobs], len(self.streams))
         self.graph = None
         for job in self.jobs:
             job.handles = job_handles(job)
             job.d_in = tuple(torch.from_numpy(a).to(self.dev) for a in job_inputs_host(job))
             job.out = job_outputs(job, job.handles, self.dev)
+        self.queues = FamilyQueues(self.jobs) if queue else None
+        n_streams = len(self.queues.kinds) if queue else branches
+        self.streams = [torch.cuda.Stream(self.dev) for _ in range(max(1, n_streams))]
+        self.assignment = assign_branches([j.cost() for j in self.jobs], len(self.streams))
 
     def _enqueue(self) -> None:
         torch = self.torch
         root = torch.cuda.current_stream(self.dev)
+        if self.queues is not None:
+            for stream, kind in zip(self.streams, self.queues.kinds):
+                stream.wait_stream(root)
+                with torch.cuda.stream(stream):
+                    self.queues.run(kind)
+                root.wait_stream(stream)
+            return
         for stream, idx in zip(self.streams, self.assignment):
             stream.wait_stream(root)
             with torch.cuda.stream(stream):

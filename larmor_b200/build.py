@@ -17,7 +17,7 @@ PACKAGE = Path(__file__).resolve().parent
 ROOT = PACKAGE.parent
 CSRC = PACKAGE / "csrc"
 LIB = PACKAGE / "liblarmor_b200.so"
-SOURCES = ["capi.cu", "log_fit.cu", "log_fit_warp.cu", "constrained_fit.cu", "dki_metrics.cu", "noalloc.cu", "lsi.cu", "multi_tissue.cu", "sh_project.cu", "peaks.cu", "staging.cu", "csd.cu", "drl.cu", "plain_fp32.cu", "drl_tc.cu"]
+SOURCES = ["capi.cu", "log_fit.cu", "log_fit_warp.cu", "constrained_fit.cu", "dki_metrics.cu", "noalloc.cu", "lsi.cu", "multi_tissue.cu", "sh_project.cu", "peaks.cu", "staging.cu", "csd.cu", "drl.cu", "plain_fp32.cu", "drl_tc.cu", "batch.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",

@@ -29,6 +29,7 @@
 #include <cfloat>
 #include <cstdint>
 
+#include "batch.cuh"
 #include "common.cuh"
 #include "log_fit.cuh"
 #include "log_fit_warp.cuh"
@@ -215,16 +216,13 @@ __device__ int implicit_nnls(const ImplicitSystem& sys, const double* d, double 
     }
 }
 
+// The constrained re-fit of one violator on a warp (its unconstrained scaled parameters in
+// pin): where every step succeeds, out (p) gets the constrained parameters.
 template <class Src>
-__global__ void __launch_bounds__(kCWarps * 32, 4) constrained_fit_kernel(
-    LogDesignDevice<double> d, Src src, int weighted, ViolatorList<double> list, int* queue,
-    double* __restrict__ workspace, size_t slot_doubles, double* __restrict__ params) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    WarpShared* shared = reinterpret_cast<WarpShared*>(smem_raw);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    WarpShared& sh = shared[warp];
+__device__ __forceinline__ void refit_violator(const LogDesignDevice<double>& d, const Src& src, int weighted,
+                                               int64_t voxel, const double* pin, double* slot, WarpShared& sh,
+                                               double* out, int lane) {
     const int n = d.n, p = d.p, m = d.m, rows = p + 1;
-    double* slot = workspace + (size_t(blockIdx.x) * kCWarps + warp) * slot_doubles;
     double* qr = slot;                          // (n, p) row-major
     double* cache = qr + size_t(n) * p;         // (m, rows): column c of C at cache[c * rows]
     double* sub = cache + size_t(rows) * m;     // (kMaxActive, rows) QR of the active columns
@@ -234,6 +232,208 @@ __global__ void __launch_bounds__(kCWarps * 32, 4) constrained_fit_kernel(
     double* rw = ys + n;                        // (n,) root weights
     uint8_t* flag = reinterpret_cast<uint8_t*>(rw + n);  // (m,) active flags
     uint8_t* ready = flag + m;                           // (m,) whether cache holds column c
+    double* pu = sh.vec[0];
+    if (lane < p) pu[lane] = pin[lane];
+    src.template warp_stage<double>(voxel, ys, lane);
+    __syncwarp();
+    // Root weights exp(pred - max pred) of the unconstrained solution (:259-263).
+    double mx = -INFINITY;
+    for (int j = lane; j < n; j += 32) {
+        double pred = 0.0;
+        for (int a = 0; a < p; ++a) pred += d.x[size_t(j) * p + a] * pu[a];
+        rw[j] = pred;
+        mx = fmax(mx, pred);
+    }
+    mx = wmax(mx);
+    __syncwarp();
+    for (int j = lane; j < n; j += 32) rw[j] = weighted ? exp(rw[j] - mx) : 1.0;
+    __syncwarp();
+    // W^(1/2) X and W^(1/2) y.
+    for (int i = lane; i < n * p; i += 32) qr[i] = rw[i / p] * d.x[i];
+    for (int j = lane; j < n; j += 32) ys[j] = rw[j] * ys[j];
+    __syncwarp();
+    // Householder QR (unpivoted), rotating ys along.
+    double* tau = sh.tau;
+    for (int k = 0; k < p; ++k) {
+        const double c0 = qr[size_t(k) * p + k];
+        double tail = 0.0;
+        for (int r = k + 1 + lane; r < n; r += 32) tail += qr[size_t(r) * p + k] * qr[size_t(r) * p + k];
+        tail = wsum(tail);
+        double tk, beta;
+        if (tail <= DBL_MIN) {
+            tk = 0.0;
+            beta = c0;
+            for (int r = k + 1 + lane; r < n; r += 32) qr[size_t(r) * p + k] = 0.0;
+        } else {
+            beta = sqrt(c0 * c0 + tail);
+            if (c0 >= 0.0) beta = -beta;
+            const double den = c0 - beta;
+            for (int r = k + 1 + lane; r < n; r += 32) qr[size_t(r) * p + k] /= den;
+            tk = (beta - c0) / beta;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            qr[size_t(k) * p + k] = beta;
+            tau[k] = tk;
+        }
+        __syncwarp();
+        if (tk != 0.0) {
+            // Columns j > k and the data (column p), eight at a time: the dot products of a
+            // group in one pass over the rows and independent warp reductions, then the
+            // updates. Each dot keeps its rows' order and its reduction's.
+            for (int j0 = k + 1; j0 <= p; j0 += 8) {
+                double dv[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) dv[q] = 0.0;
+                for (int r = k + 1 + lane; r < n; r += 32) {
+                    const double vr = qr[size_t(r) * p + k];
+                    const double* row = qr + size_t(r) * p;
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int j = j0 + q;
+                        if (j < p) dv[q] += vr * row[j];
+                        else if (j == p) dv[q] += vr * ys[r];
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int j = j0 + q;
+                    if (j <= p) dv[q] = wsum(dv[q]) + (j < p ? qr[size_t(k) * p + j] : ys[k]);
+                }
+                __syncwarp();
+                if (lane == 0) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int j = j0 + q;
+                        if (j < p) qr[size_t(k) * p + j] -= tk * dv[q];
+                        else if (j == p) ys[k] -= tk * dv[q];
+                    }
+                }
+                for (int r = k + 1 + lane; r < n; r += 32) {
+                    double* row = qr + size_t(r) * p;
+                    const double vr = row[k];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int j = j0 + q;
+                        if (j < p) row[j] -= tk * vr * dv[q];
+                        else if (j == p) ys[r] -= tk * vr * dv[q];
+                    }
+                }
+                __syncwarp();
+            }
+        }
+    }
+    // Rank check on the diagonal of R (:183-188).
+    double dmax = 0.0, dmin = INFINITY;
+    for (int k = 0; k < p; ++k) {
+        dmax = fmax(dmax, fabs(qr[size_t(k) * p + k]));
+        dmin = fmin(dmin, fabs(qr[size_t(k) * p + k]));
+    }
+    if (!(dmin > double(n) * kEps * dmax)) return;
+    // p_free = R^-1 (Q^T W^(1/2) y)[:p].
+    double* pfree = sh.vec[1];
+    if (lane == 0) {
+        for (int i = p - 1; i >= 0; --i) {
+            double s = ys[i];
+            for (int j = i + 1; j < p; ++j) s -= qr[size_t(i) * p + j] * pfree[j];
+            pfree[i] = s / qr[size_t(i) * p + i];
+        }
+    }
+    __syncwarp();
+    // The NNLS tolerance 10 eps norm1(C) max(p + 1, m) needs every column's absolute sum:
+    // sum_i |(R^-T g_c)_i| + |g_c p_free|. Lanes over constraints, each substitution's
+    // entries in the warp's shared column of ysub; the columns themselves are not kept.
+    double colsum_max = 0.0;
+    double* ysub = sh.ysub;
+    for (int c = lane; c < m; c += 32) {
+        const double* gc = d.g + size_t(c) * p;
+        double acc_abs = 0.0, gf = 0.0;
+        for (int i = 0; i < p; ++i) {
+            double s0 = gc[i], s1 = 0.0;
+            int k = 0;
+            for (; k + 1 < i; k += 2) {
+                s0 -= qr[size_t(k) * p + i] * ysub[k * 32 + lane];
+                s1 -= qr[size_t(k + 1) * p + i] * ysub[(k + 1) * 32 + lane];
+            }
+            if (k < i) s0 -= qr[size_t(k) * p + i] * ysub[k * 32 + lane];
+            const double si = (s0 + s1) / qr[size_t(i) * p + i];
+            ysub[i * 32 + lane] = si;
+            acc_abs += fabs(si);
+            gf += gc[i] * pfree[i];
+        }
+        acc_abs += fabs(gf);
+        colsum_max = fmax(colsum_max, acc_abs);
+    }
+    colsum_max = wmax(colsum_max);
+    const double tol = 10.0 * kEps * colsum_max * double(max(rows, m));
+    for (int c = lane; c < m; c += 32) ready[c] = 0;
+    __syncwarp();
+    // Lawson-Hanson (cpp/src/sd/nnls.cpp:187-221) on C u ~ e_p.
+    double* unit = sh.vec[2];
+    for (int r = lane; r < rows; r += 32) unit[r] = (r == p) ? 1.0 : 0.0;
+    __syncwarp();
+    const ImplicitSystem sys{d.g, d.gt, qr, pfree, cache, ready, p, m};
+    NnlsScratch ns{u, z, flag, sh.act, &sh.n_act, sh.res,
+                   QrScratch{sub, sh.qtau, sh.qnu, sh.qnd, sh.qperm, sh.rv}, kMaxActive};
+    const int outcome = implicit_nnls(sys, unit, tol, kInnerStepsPerConstraint * m, ns, sh.t, lane);
+    if (outcome != 1) return;
+    double* res = sh.vec[2];
+    // Residual C u - e_p over the active columns (u is zero elsewhere).
+    if (lane < rows) {
+        double s = (lane == p) ? -1.0 : 0.0;
+        for (int q = 0; q < sh.n_act; ++q) {
+            const int c = sh.act[q];
+            const double uc = u[c];
+            if (uc != 0.0) s += cache[size_t(c) * rows + lane] * uc;
+        }
+        res[lane] = s;
+    }
+    __syncwarp();
+    const double last = res[p];
+    if (last >= -kFeasibilityMargin) return;
+    // p = p_free + R^-1 (-res[:p] / res[p]).
+    double* pc = sh.vec[3];
+    if (lane == 0) {
+        for (int i = p - 1; i >= 0; --i) {
+            double s = -res[i] / last;
+            for (int j = i + 1; j < p; ++j) s -= qr[size_t(i) * p + j] * pc[j];
+            pc[i] = s / qr[size_t(i) * p + i];
+        }
+        for (int i = 0; i < p; ++i) pc[i] = pfree[i] + pc[i];
+    }
+    __syncwarp();
+    bool finite = true;
+    for (int a = 0; a < p; ++a) finite &= bool(isfinite(pc[a]));
+    if (!finite) return;
+    // meets_the_constraints (:156-163).
+    double vmin = INFINITY, size = 0.0;
+    for (int c = lane; c < m; c += 32) {
+        const double* gr = d.g + size_t(c) * p;
+        double val = 0.0, sz = 0.0;
+        for (int a = 0; a < p; ++a) {
+            val += gr[a] * pc[a];
+            sz += fabs(gr[a]) * (fabs(pc[a]) + fabs(pfree[a]));
+        }
+        vmin = fmin(vmin, val);
+        size = fmax(size, sz);
+    }
+    vmin = -wmax(-vmin);
+    size = wmax(size);
+    if (!(vmin >= -kConstraintTolerance * size)) return;
+    if (lane < p) out[lane] = pc[lane] / d.scales64[lane];
+    __syncwarp();
+}
+
+template <class Src>
+__global__ void __launch_bounds__(kCWarps * 32, 4) constrained_fit_kernel(
+    LogDesignDevice<double> d, Src src, int weighted, ViolatorList<double> list, int* queue,
+    double* __restrict__ workspace, size_t slot_doubles, double* __restrict__ params) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WarpShared* shared = reinterpret_cast<WarpShared*>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpShared& sh = shared[warp];
+    const int p = d.p;
+    double* slot = workspace + (size_t(blockIdx.x) * kCWarps + warp) * slot_doubles;
     const int total = min(*list.count, list.capacity);
     for (;;) {
         int idx = 0;
@@ -241,196 +441,33 @@ __global__ void __launch_bounds__(kCWarps * 32, 4) constrained_fit_kernel(
         idx = __shfl_sync(0xffffffffu, idx, 0);
         if (idx >= total) break;
         const int64_t voxel = list.voxel[idx];
-        double* pu = sh.vec[0];
-        if (lane < p) pu[lane] = list.params[size_t(idx) * p + lane];
-        src.template warp_stage<double>(voxel, ys, lane);
-        __syncwarp();
-        // Root weights exp(pred - max pred) of the unconstrained solution (:259-263).
-        double mx = -INFINITY;
-        for (int j = lane; j < n; j += 32) {
-            double pred = 0.0;
-            for (int a = 0; a < p; ++a) pred += d.x[size_t(j) * p + a] * pu[a];
-            rw[j] = pred;
-            mx = fmax(mx, pred);
-        }
-        mx = wmax(mx);
-        __syncwarp();
-        for (int j = lane; j < n; j += 32) rw[j] = weighted ? exp(rw[j] - mx) : 1.0;
-        __syncwarp();
-        // W^(1/2) X and W^(1/2) y.
-        for (int i = lane; i < n * p; i += 32) qr[i] = rw[i / p] * d.x[i];
-        for (int j = lane; j < n; j += 32) ys[j] = rw[j] * ys[j];
-        __syncwarp();
-        // Householder QR (unpivoted), rotating ys along.
-        double* tau = sh.tau;
-        for (int k = 0; k < p; ++k) {
-            const double c0 = qr[size_t(k) * p + k];
-            double tail = 0.0;
-            for (int r = k + 1 + lane; r < n; r += 32) tail += qr[size_t(r) * p + k] * qr[size_t(r) * p + k];
-            tail = wsum(tail);
-            double tk, beta;
-            if (tail <= DBL_MIN) {
-                tk = 0.0;
-                beta = c0;
-                for (int r = k + 1 + lane; r < n; r += 32) qr[size_t(r) * p + k] = 0.0;
-            } else {
-                beta = sqrt(c0 * c0 + tail);
-                if (c0 >= 0.0) beta = -beta;
-                const double den = c0 - beta;
-                for (int r = k + 1 + lane; r < n; r += 32) qr[size_t(r) * p + k] /= den;
-                tk = (beta - c0) / beta;
-            }
-            __syncwarp();
-            if (lane == 0) {
-                qr[size_t(k) * p + k] = beta;
-                tau[k] = tk;
-            }
-            __syncwarp();
-            if (tk != 0.0) {
-                // Columns j > k and the data (column p), eight at a time: the dot products of a
-                // group in one pass over the rows and independent warp reductions, then the
-                // updates. Each dot keeps its rows' order and its reduction's.
-                for (int j0 = k + 1; j0 <= p; j0 += 8) {
-                    double dv[8];
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) dv[q] = 0.0;
-                    for (int r = k + 1 + lane; r < n; r += 32) {
-                        const double vr = qr[size_t(r) * p + k];
-                        const double* row = qr + size_t(r) * p;
-#pragma unroll
-                        for (int q = 0; q < 8; ++q) {
-                            const int j = j0 + q;
-                            if (j < p) dv[q] += vr * row[j];
-                            else if (j == p) dv[q] += vr * ys[r];
-                        }
-                    }
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        const int j = j0 + q;
-                        if (j <= p) dv[q] = wsum(dv[q]) + (j < p ? qr[size_t(k) * p + j] : ys[k]);
-                    }
-                    __syncwarp();
-                    if (lane == 0) {
-#pragma unroll
-                        for (int q = 0; q < 8; ++q) {
-                            const int j = j0 + q;
-                            if (j < p) qr[size_t(k) * p + j] -= tk * dv[q];
-                            else if (j == p) ys[k] -= tk * dv[q];
-                        }
-                    }
-                    for (int r = k + 1 + lane; r < n; r += 32) {
-                        double* row = qr + size_t(r) * p;
-                        const double vr = row[k];
-#pragma unroll
-                        for (int q = 0; q < 8; ++q) {
-                            const int j = j0 + q;
-                            if (j < p) row[j] -= tk * vr * dv[q];
-                            else if (j == p) ys[r] -= tk * vr * dv[q];
-                        }
-                    }
-                    __syncwarp();
-                }
-            }
-        }
-        // Rank check on the diagonal of R (:183-188).
-        double dmax = 0.0, dmin = INFINITY;
-        for (int k = 0; k < p; ++k) {
-            dmax = fmax(dmax, fabs(qr[size_t(k) * p + k]));
-            dmin = fmin(dmin, fabs(qr[size_t(k) * p + k]));
-        }
-        if (!(dmin > double(n) * kEps * dmax)) continue;
-        // p_free = R^-1 (Q^T W^(1/2) y)[:p].
-        double* pfree = sh.vec[1];
-        if (lane == 0) {
-            for (int i = p - 1; i >= 0; --i) {
-                double s = ys[i];
-                for (int j = i + 1; j < p; ++j) s -= qr[size_t(i) * p + j] * pfree[j];
-                pfree[i] = s / qr[size_t(i) * p + i];
-            }
-        }
-        __syncwarp();
-        // The NNLS tolerance 10 eps norm1(C) max(p + 1, m) needs every column's absolute sum:
-        // sum_i |(R^-T g_c)_i| + |g_c p_free|. Lanes over constraints, each substitution's
-        // entries in the warp's shared column of ysub; the columns themselves are not kept.
-        double colsum_max = 0.0;
-        double* ysub = sh.ysub;
-        for (int c = lane; c < m; c += 32) {
-            const double* gc = d.g + size_t(c) * p;
-            double acc_abs = 0.0, gf = 0.0;
-            for (int i = 0; i < p; ++i) {
-                double s0 = gc[i], s1 = 0.0;
-                int k = 0;
-                for (; k + 1 < i; k += 2) {
-                    s0 -= qr[size_t(k) * p + i] * ysub[k * 32 + lane];
-                    s1 -= qr[size_t(k + 1) * p + i] * ysub[(k + 1) * 32 + lane];
-                }
-                if (k < i) s0 -= qr[size_t(k) * p + i] * ysub[k * 32 + lane];
-                const double si = (s0 + s1) / qr[size_t(i) * p + i];
-                ysub[i * 32 + lane] = si;
-                acc_abs += fabs(si);
-                gf += gc[i] * pfree[i];
-            }
-            acc_abs += fabs(gf);
-            colsum_max = fmax(colsum_max, acc_abs);
-        }
-        colsum_max = wmax(colsum_max);
-        const double tol = 10.0 * kEps * colsum_max * double(max(rows, m));
-        for (int c = lane; c < m; c += 32) ready[c] = 0;
-        __syncwarp();
-        // Lawson-Hanson (cpp/src/sd/nnls.cpp:187-221) on C u ~ e_p.
-        double* unit = sh.vec[2];
-        for (int r = lane; r < rows; r += 32) unit[r] = (r == p) ? 1.0 : 0.0;
-        __syncwarp();
-        const ImplicitSystem sys{d.g, d.gt, qr, pfree, cache, ready, p, m};
-        NnlsScratch ns{u, z, flag, sh.act, &sh.n_act, sh.res,
-                       QrScratch{sub, sh.qtau, sh.qnu, sh.qnd, sh.qperm, sh.rv}, kMaxActive};
-        const int outcome = implicit_nnls(sys, unit, tol, kInnerStepsPerConstraint * m, ns, sh.t, lane);
-        if (outcome != 1) continue;
-        double* res = sh.vec[2];
-        // Residual C u - e_p over the active columns (u is zero elsewhere).
-        if (lane < rows) {
-            double s = (lane == p) ? -1.0 : 0.0;
-            for (int q = 0; q < sh.n_act; ++q) {
-                const int c = sh.act[q];
-                const double uc = u[c];
-                if (uc != 0.0) s += cache[size_t(c) * rows + lane] * uc;
-            }
-            res[lane] = s;
-        }
-        __syncwarp();
-        const double last = res[p];
-        if (last >= -kFeasibilityMargin) continue;
-        // p = p_free + R^-1 (-res[:p] / res[p]).
-        double* pc = sh.vec[3];
-        if (lane == 0) {
-            for (int i = p - 1; i >= 0; --i) {
-                double s = -res[i] / last;
-                for (int j = i + 1; j < p; ++j) s -= qr[size_t(i) * p + j] * pc[j];
-                pc[i] = s / qr[size_t(i) * p + i];
-            }
-            for (int i = 0; i < p; ++i) pc[i] = pfree[i] + pc[i];
-        }
-        __syncwarp();
-        bool finite = true;
-        for (int a = 0; a < p; ++a) finite &= bool(isfinite(pc[a]));
-        if (!finite) continue;
-        // meets_the_constraints (:156-163).
-        double vmin = INFINITY, size = 0.0;
-        for (int c = lane; c < m; c += 32) {
-            const double* gr = d.g + size_t(c) * p;
-            double val = 0.0, sz = 0.0;
-            for (int a = 0; a < p; ++a) {
-                val += gr[a] * pc[a];
-                sz += fabs(gr[a]) * (fabs(pc[a]) + fabs(pfree[a]));
-            }
-            vmin = fmin(vmin, val);
-            size = fmax(size, sz);
-        }
-        vmin = -wmax(-vmin);
-        size = wmax(size);
-        if (!(vmin >= -kConstraintTolerance * size)) continue;
-        if (lane < p) params[voxel * p + lane] = pc[lane] / d.scales64[lane];
-        __syncwarp();
+        refit_violator<Src>(d, src, weighted, voxel, list.params + size_t(idx) * p, slot, sh, params + voxel * p,
+                            lane);
+    }
+}
+
+// The DKI family of a batch (batch.cuh): warps take the violators of every DKI volume from one
+// list, each with its volume's design, signals and outputs.
+__global__ void __launch_bounds__(kCWarps * 32, 4) batch_refit_kernel(
+    const DkiBatchJob* __restrict__ jobs, BatchViolators list, int weighted, int* queue,
+    double* __restrict__ workspace, size_t slot_doubles) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WarpShared* shared = reinterpret_cast<WarpShared*>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpShared& sh = shared[warp];
+    double* slot = workspace + (size_t(blockIdx.x) * kCWarps + warp) * slot_doubles;
+    const int total = min(*list.count, list.capacity);
+    for (;;) {
+        int idx = 0;
+        if (lane == 0) idx = atomicAdd(queue, 1);
+        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (idx >= total) break;
+        const DkiBatchJob& job = jobs[list.job[idx]];
+        const LogDesignDevice<double> d = job.d;
+        const CappedSource src{job.s, job.s0, job.floor, job.is_b0, d.n};
+        const int64_t voxel = list.voxel[idx];
+        refit_violator<CappedSource>(d, src, weighted, voxel, list.params + size_t(idx) * d.p, slot, sh,
+                                     job.params + voxel * d.p, lane);
     }
 }
 
@@ -453,6 +490,22 @@ int constrained_resident_warps() {
                                                              kCWarps * 32, kCSmem),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     return sm_count() * ctas_per_sm(per_sm, "dki.refit.ctas_per_sm") * kCWarps;
+}
+
+size_t batch_refit_slot_doubles(int n_max, int p, int m_max) { return constrained_slot_doubles(n_max, p, m_max); }
+
+int batch_refit_slots() { return constrained_resident_warps(); }
+
+void launch_batch_refit(const DkiBatchJob* jobs, const BatchViolators& violators, int weighted, int* queue,
+                        double* workspace, int slots, size_t slot_doubles, cudaStream_t stream) {
+    const int blocks = std::max(1, slots / kCWarps);
+    cuda_check(cudaFuncSetAttribute(batch_refit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kCSmem)),
+               "cudaFuncSetAttribute");
+    cuda_check(cudaMemsetAsync(queue, 0, sizeof(int), stream), "cudaMemsetAsync");
+    LaunchScope scope("batch_refit_kernel", stream);
+    batch_refit_kernel<<<blocks, kCWarps * 32, kCSmem, stream>>>(jobs, violators, weighted, queue, workspace,
+                                                                 slot_doubles);
+    cuda_check(cudaGetLastError(), "batch_refit_kernel launch");
 }
 
 template <class Src>

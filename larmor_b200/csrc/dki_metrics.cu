@@ -18,6 +18,7 @@
 #include <mutex>
 #include <vector>
 
+#include "batch.cuh"
 #include "common.cuh"
 #include "dki_metrics.cuh"
 #include "tensor_maps.cuh"
@@ -70,11 +71,10 @@ struct KaQuadrature {
     const double* weight;  // (nodes,)
 };
 
-__global__ void __launch_bounds__(128) dki_maps_kernel(const double* __restrict__ params, int64_t v,
-                                                       KaQuadrature quad, float* __restrict__ maps,
-                                                       uint8_t* __restrict__ npd) {
-    const int64_t voxel = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (voxel >= v) return;
+// The 36 DKI maps of one voxel from its 22 parameters.
+__device__ __forceinline__ void dki_maps_voxel(const double* __restrict__ params, int64_t voxel, int64_t v,
+                                               const KaQuadrature& quad, float* __restrict__ maps,
+                                               uint8_t* __restrict__ npd) {
     const double* p = params + voxel * 22;
     double d[6];
 #pragma unroll
@@ -151,6 +151,26 @@ __global__ void __launch_bounds__(128) dki_maps_kernel(const double* __restrict_
     maps[33 * v + voxel] = float(ak);
     maps[34 * v + voxel] = float(rk);
     maps[35 * v + voxel] = float(ka);
+}
+
+__global__ void __launch_bounds__(128) dki_maps_kernel(const double* __restrict__ params, int64_t v,
+                                                       KaQuadrature quad, float* __restrict__ maps,
+                                                       uint8_t* __restrict__ npd) {
+    const int64_t voxel = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (voxel < v) dki_maps_voxel(params, voxel, v, quad, maps, npd);
+}
+
+// The DKI family of a batch (batch.cuh): one launch over every DKI volume, a CTA per ticket of
+// kMapsBatchVoxels voxels of one volume.
+__global__ void __launch_bounds__(kMapsBatchVoxels) batch_dki_maps_kernel(const DkiBatchJob* __restrict__ jobs,
+                                                                          const int64_t* __restrict__ first,
+                                                                          int n_jobs, KaQuadrature quad) {
+    const int64_t t = blockIdx.x;
+    if (t >= first[n_jobs]) return;
+    const int j = ticket_job(first, n_jobs, t);
+    const DkiBatchJob& job = jobs[j];
+    const int64_t voxel = (t - first[j]) * kMapsBatchVoxels + threadIdx.x;
+    if (voxel < job.v) dki_maps_voxel(job.params, voxel, job.v, quad, job.maps, job.npd);
 }
 
 // Gauss-Legendre nodes and weights on [-1, 1] by Newton's method on P_n with the three-term
@@ -232,6 +252,15 @@ KaQuadrature ka_quadrature() {
 }
 
 }  // namespace
+
+void launch_batch_dki_maps(const DkiBatchJob* jobs, const int64_t* first, int n_jobs, int64_t tickets,
+                           cudaStream_t stream) {
+    if (n_jobs == 0 || tickets == 0) return;
+    const KaQuadrature quad = ka_quadrature();
+    LaunchScope scope("batch_dki_maps_kernel", stream);
+    batch_dki_maps_kernel<<<unsigned(tickets), kMapsBatchVoxels, 0, stream>>>(jobs, first, n_jobs, quad);
+    cuda_check(cudaGetLastError(), "batch_dki_maps_kernel launch");
+}
 
 void launch_dki_maps(const double* params, int64_t v, float* maps, uint8_t* npd, cudaStream_t stream) {
     if (v == 0) return;

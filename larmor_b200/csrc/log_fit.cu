@@ -22,6 +22,7 @@
 #include "common.cuh"
 #include "host_la.hpp"
 #include "log_fit.cuh"
+#include "batch.cuh"
 #include "log_fit_warp.cuh"
 #include "tensor_maps.cuh"
 
@@ -267,6 +268,57 @@ __global__ void __launch_bounds__(BLOCK) fit_dti_maps_kernel(LogDesignDevice<T> 
     dti_maps<T>(dt, voxel, v, maps, npd);
 }
 
+// The DTI family of a batch (batch.cuh): a persistent grid whose CTAs take tickets of
+// kDtiBatchBlock voxels of one volume from a device counter across every DTI volume; a CTA
+// restages the design when its ticket moves to another volume. Per voxel the same fit and maps
+// as fit_dti_maps_kernel (FP64).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) batch_dti_kernel(const DtiBatchJob* __restrict__ jobs,
+                                                          const int64_t* __restrict__ first, int n_jobs,
+                                                          int weighted, int max_rw, double tol,
+                                                          int* __restrict__ queue) {
+    using T = double;
+    constexpr int P = 7;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ long long ticket;
+    T* sm = reinterpret_cast<T*>(smem_raw);
+    const int64_t total = first[n_jobs];
+    int cur = -1;
+    for (;;) {
+        if (threadIdx.x == 0) ticket = atomicAdd(reinterpret_cast<unsigned long long*>(queue), 1ull);
+        __syncthreads();
+        const int64_t t = ticket;
+        if (t >= total) break;
+        const int j = ticket_job(first, n_jobs, t);
+        const DtiBatchJob& job = jobs[j];
+        const LogDesignDevice<T> d = job.d;
+        const int n = d.n;
+        T* ys = sm + n * (2 * P + P * (P + 1) / 2);
+        if (j != cur) {
+            stage_design<T, P>(d, sm);
+            cur = j;
+        }
+        unsigned char* raw = reinterpret_cast<unsigned char*>(ys + n * BLOCK);
+        const int64_t v = job.v;
+        const int64_t block_first = (t - first[j]) * BLOCK;
+        const int count = int(v - block_first < int64_t(BLOCK) ? v - block_first : int64_t(BLOCK));
+        const FlooredSource src{job.s, job.floor, n};
+        src.template stage<T, BLOCK>(block_first, count, raw, ys);
+        __syncthreads();
+        if (threadIdx.x < count) {
+            const int64_t voxel = block_first + threadIdx.x;
+            T p[P];
+            fit_voxel_small<T, P>(sm, sm + n * P, sm + n * (P + P * (P + 1) / 2), n, ys + threadIdx.x, BLOCK,
+                                  weighted != 0, max_rw, T(tol), p);
+            T dt[6];
+#pragma unroll
+            for (int a = 0; a < 6; ++a) dt[a] = p[a + 1] / d.scales[a + 1];
+            dti_maps<T>(dt, voxel, v, job.maps, job.npd);
+        }
+        __syncthreads();
+    }
+}
+
 template <class T>
 const LogDesignDevice<T>& device_view(const lar_log_design_s* h);
 template <>
@@ -396,6 +448,28 @@ void launch_dti_maps(const lar_log_design_s* h, const float* s, const double* fl
     else run(fit_dti_maps_kernel<T, 16>, 16);
 }
 
+}  // namespace
+
+size_t batch_dti_smem(int n_max) { return SmallFit<double, 7>::bytes(n_max, kDtiBatchBlock, FlooredSource::raw_bytes); }
+
+void launch_batch_dti(const DtiBatchJob* jobs, const int64_t* first, int n_jobs, int n_max, int64_t tickets,
+                      int weighted, int max_rw, double tol, int* queue, cudaStream_t stream) {
+    if (n_jobs == 0 || tickets == 0) return;
+    auto kernel = batch_dti_kernel<kDtiBatchBlock>;
+    const size_t sm = batch_dti_smem(n_max);
+    set_smem(kernel, sm);
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kDtiBatchBlock, sm),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    const int64_t grid = std::min<int64_t>(tickets, int64_t(sm_count()) * std::max(per_sm, 1));
+    cuda_check(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), stream), "cudaMemsetAsync");
+    LaunchScope scope("batch_dti_kernel", stream);
+    kernel<<<unsigned(grid), kDtiBatchBlock, sm, stream>>>(jobs, first, n_jobs, weighted, max_rw, tol, queue);
+    cuda_check(cudaGetLastError(), "batch_dti_kernel launch");
+}
+
+namespace {
+
 template <class T>
 void upload_design(lar_log_design_s* h, DeviceArray<T>& x, DeviceArray<T>& pinvt, DeviceArray<T>& z,
                    DeviceArray<T>& g, DeviceArray<T>& scales, LogDesignDevice<T>& view) {
@@ -443,6 +517,10 @@ void launch_dki_maps(const double* params, int64_t v, float* maps, uint8_t* npd,
 }  // namespace lar
 
 using namespace lar;
+
+namespace lar {
+LogDesignDevice<double> log_design_view(const lar_log_design_s* h) { return h->d64; }
+}  // namespace lar
 
 extern "C" {
 

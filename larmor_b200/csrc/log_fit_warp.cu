@@ -14,6 +14,7 @@
 
 #include "common.cuh"
 #include "log_fit.cuh"
+#include "batch.cuh"
 #include "log_fit_warp.cuh"
 
 namespace lar {
@@ -75,147 +76,195 @@ __device__ bool warp_ldlt_solve(T* a, int p, int px, T* b, T* col, int lane) {
     return true;
 }
 
+// A CTA's shared memory for the warp fits: the design (X with its rows padded to px, pinv^T,
+// the (a, b) of each normal-matrix entry), then each warp's slice (y, w, normal matrix, four
+// 32-vectors).
+template <class T>
+struct WarpSmem {
+    T *xs, *pinvt, *ys, *ws, *gm, *pv, *rv, *ov, *cv;
+    uint8_t *ea, *eb;
+};
+
+template <class T>
+__device__ __forceinline__ WarpSmem<T> carve_warp(unsigned char* smem_raw, const WarpLayout<T>& lay, int warp) {
+    WarpSmem<T> w;
+    T* base = reinterpret_cast<T*>(smem_raw);
+    w.xs = base;
+    w.pinvt = base + size_t(lay.n) * lay.px;
+    w.ea = reinterpret_cast<uint8_t*>(base + lay.design_elems() + kWarps * lay.warp_elems());
+    w.eb = w.ea + lay.pp;
+    w.ys = base + lay.design_elems() + warp * lay.warp_elems();
+    w.ws = w.ys + lay.n;
+    w.gm = w.ws + lay.n;
+    w.pv = w.gm + size_t(lay.p) * lay.px;  // current parameters
+    w.rv = w.pv + 32;                      // right-hand side / next parameters
+    w.ov = w.rv + 32;                      // ordinary fit
+    w.cv = w.ov + 32;                      // column scratch of the solve
+    return w;
+}
+
+// The CTA stages the design (the caller synchronises before and after).
+template <class T>
+__device__ __forceinline__ void stage_warp_design(const LogDesignDevice<T>& d, const WarpLayout<T>& lay,
+                                                  const WarpSmem<T>& w) {
+    const int n = lay.n, p = lay.p, px = lay.px, pp = lay.pp;
+    for (int i = threadIdx.x; i < n * p; i += blockDim.x) {
+        const int r = i / p, c = i % p;
+        w.xs[r * px + c] = d.x[i];
+        w.pinvt[i] = d.pinvt[i];
+    }
+    for (int e = threadIdx.x; e < pp; e += blockDim.x) {
+        // Entry e of the packed upper triangle, row by row.
+        int a = 0, rem = e;
+        while (rem >= p - a) { rem -= p - a; ++a; }
+        w.ea[e] = uint8_t(a);
+        w.eb[e] = uint8_t(a + rem);
+    }
+}
+
+// One voxel's fit on a warp: its scaled parameters end in w.pv. Returns the number of weighted
+// fits and sets *violated_out when the (finite) solution breaks a constraint.
+template <class T, class Src>
+__device__ __forceinline__ int log_warp_voxel(const LogDesignDevice<T>& d, const WarpLayout<T>& lay,
+                                              const WarpSmem<T>& w, const Src& src, int64_t voxel,
+                                              int weighted, int max_rw, T tol, bool* violated_out,
+                                              int lane) {
+    const int n = lay.n, p = lay.p, px = lay.px, pp = lay.pp;
+    T* const xs = w.xs;
+    T* const pinvt = w.pinvt;
+    const uint8_t* const ea = w.ea;
+    const uint8_t* const eb = w.eb;
+    T* const ys = w.ys;
+    T* const ws = w.ws;
+    T* const gm = w.gm;
+    T* const pv = w.pv;
+    T* const rv = w.rv;
+    T* const ov = w.ov;
+    T* const cv = w.cv;
+        src.template warp_stage<T>(voxel, ys, lane);
+    __syncwarp();
+    // Ordinary fit.
+    if (lane < p) {
+        T acc = T(0);
+        for (int j = 0; j < n; ++j) acc = fma(pinvt[j * p + lane], ys[j], acc);
+        ov[lane] = acc;
+        pv[lane] = acc;
+    }
+    __syncwarp();
+    bool finite = true;
+    for (int a = 0; a < p; ++a) finite &= bool(isfinite(pv[a]));
+    int it = 0;
+    if (weighted && finite) {
+        T mx = -INFINITY;
+        for (int j = lane; j < n; j += 32) {
+            T pred = T(0);
+            for (int a = 0; a < p; ++a) pred = fma(xs[j * px + a], pv[a], pred);
+            mx = fmax(mx, pred);
+        }
+        mx = warp_max(mx);
+        for (; it < max_rw; ++it) {
+            for (int j = lane; j < n; j += 32) {
+                T pred = T(0);
+                for (int a = 0; a < p; ++a) pred = fma(xs[j * px + a], pv[a], pred);
+                ws[j] = dev_exp<T>(T(2) * (pred - mx));
+            }
+            __syncwarp();
+            // Four entries per lane at a time, so that their sums over the measurements
+            // overlap (each in its own order).
+            for (int e0 = lane; e0 < pp; e0 += 4 * 32) {
+                int ia[4], ib[4];
+                T acc[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int e = e0 + 32 * q;
+                    ia[q] = e < pp ? ea[e] : 0;
+                    ib[q] = e < pp ? eb[e] : 0;
+                    acc[q] = T(0);
+                }
+                for (int j = 0; j < n; ++j) {
+                    const T wj = ws[j];
+                    const T* xr = xs + j * px;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[q] = fma(wj * xr[ia[q]], xr[ib[q]], acc[q]);
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (e0 + 32 * q < pp) gm[ib[q] * px + ia[q]] = acc[q];  // lower triangle
+            }
+            if (lane < p) {
+                T acc = T(0);
+                for (int j = 0; j < n; ++j) acc = fma(ws[j] * xs[j * px + lane], ys[j], acc);
+                rv[lane] = acc;
+            }
+            __syncwarp();
+            bool ok = warp_ldlt_solve<T>(gm, p, px, rv, cv, lane);
+            if (ok) {
+                for (int a = 0; a < p; ++a) ok &= bool(isfinite(rv[a]));
+            }
+            if (!ok) {
+                if (lane < p) pv[lane] = ov[lane];
+                __syncwarp();
+                ++it;
+                break;
+            }
+            T change = T(0), mxn = -INFINITY;
+            for (int j = lane; j < n; j += 32) {
+                T po = T(0), pn = T(0);
+                for (int a = 0; a < p; ++a) {
+                    po = fma(xs[j * px + a], pv[a], po);
+                    pn = fma(xs[j * px + a], rv[a], pn);
+                }
+                change = fmax(change, fabs(pn - po));
+                mxn = fmax(mxn, pn);
+            }
+            change = warp_max(change);
+            mxn = warp_max(mxn);
+            __syncwarp();
+            if (lane < p) pv[lane] = rv[lane];
+            __syncwarp();
+            mx = mxn;
+            if (!(change > tol)) {
+                ++it;
+                break;
+            }
+        }
+    }
+    // Constraint check on the scaled parameters (cpp/src/dwi/log_fit.cpp:150,256).
+    bool violated = false;
+    if (d.m > 0) {
+        bool fin = true;
+        for (int a = 0; a < p; ++a) fin &= bool(isfinite(pv[a]));
+        if (fin) {
+            bool neg = false;
+            for (int i = lane; i < d.m; i += 32) {
+                T val = T(0);
+                for (int a = 0; a < p; ++a) val = fma(d.g[size_t(i) * p + a], pv[a], val);
+                neg |= val < T(0);
+            }
+            violated = __any_sync(0xffffffffu, neg);
+        }
+    }
+    *violated_out = violated;
+    return it;
+}
+
 template <class T, class Src>
 __global__ void __launch_bounds__(kWarps * 32) fit_log_warp_kernel(
     LogDesignDevice<T> d, Src src, int64_t v, int weighted, int max_rw, T tol,
     double* __restrict__ params, uint8_t* __restrict__ broke, int32_t* __restrict__ iterations,
     ViolatorList<T> violators) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int n = d.n, p = d.p, px = p | 1, pp = p * (p + 1) / 2;
-    const WarpLayout<T> lay{n, p, px, pp};
-    T* xs = reinterpret_cast<T*>(smem_raw);
-    T* pinvt = xs + size_t(n) * px;
-    uint8_t* ea = reinterpret_cast<uint8_t*>(reinterpret_cast<T*>(smem_raw) + lay.design_elems() +
-                                             kWarps * lay.warp_elems());
-    uint8_t* eb = ea + pp;
-    for (int i = threadIdx.x; i < n * p; i += blockDim.x) {
-        const int r = i / p, c = i % p;
-        xs[r * px + c] = d.x[i];
-        pinvt[i] = d.pinvt[i];
-    }
-    for (int e = threadIdx.x; e < pp; e += blockDim.x) {
-        // Entry e of the packed upper triangle, row by row.
-        int a = 0, rem = e;
-        while (rem >= p - a) { rem -= p - a; ++a; }
-        ea[e] = uint8_t(a);
-        eb[e] = uint8_t(a + rem);
-    }
-    __syncthreads();
-
+    const int p = d.p;
+    const WarpLayout<T> lay{d.n, p, p | 1, p * (p + 1) / 2};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    T* ys = reinterpret_cast<T*>(smem_raw) + lay.design_elems() + warp * lay.warp_elems();
-    T* ws = ys + n;
-    T* gm = ws + n;
-    T* pv = gm + size_t(p) * px;  // current parameters
-    T* rv = pv + 32;              // right-hand side / next parameters
-    T* ov = rv + 32;              // ordinary fit
-    T* cv = ov + 32;              // column scratch of the solve
-
+    const WarpSmem<T> w = carve_warp<T>(smem_raw, lay, warp);
+    stage_warp_design<T>(d, lay, w);
+    __syncthreads();
     for (int64_t voxel = int64_t(blockIdx.x) * kWarps + warp; voxel < v;
          voxel += int64_t(gridDim.x) * kWarps) {
-        src.template warp_stage<T>(voxel, ys, lane);
-        __syncwarp();
-        // Ordinary fit.
-        if (lane < p) {
-            T acc = T(0);
-            for (int j = 0; j < n; ++j) acc = fma(pinvt[j * p + lane], ys[j], acc);
-            ov[lane] = acc;
-            pv[lane] = acc;
-        }
-        __syncwarp();
-        bool finite = true;
-        for (int a = 0; a < p; ++a) finite &= bool(isfinite(pv[a]));
-        int it = 0;
-        if (weighted && finite) {
-            T mx = -INFINITY;
-            for (int j = lane; j < n; j += 32) {
-                T pred = T(0);
-                for (int a = 0; a < p; ++a) pred = fma(xs[j * px + a], pv[a], pred);
-                mx = fmax(mx, pred);
-            }
-            mx = warp_max(mx);
-            for (; it < max_rw; ++it) {
-                for (int j = lane; j < n; j += 32) {
-                    T pred = T(0);
-                    for (int a = 0; a < p; ++a) pred = fma(xs[j * px + a], pv[a], pred);
-                    ws[j] = dev_exp<T>(T(2) * (pred - mx));
-                }
-                __syncwarp();
-                // Four entries per lane at a time, so that their sums over the measurements
-                // overlap (each in its own order).
-                for (int e0 = lane; e0 < pp; e0 += 4 * 32) {
-                    int ia[4], ib[4];
-                    T acc[4];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int e = e0 + 32 * q;
-                        ia[q] = e < pp ? ea[e] : 0;
-                        ib[q] = e < pp ? eb[e] : 0;
-                        acc[q] = T(0);
-                    }
-                    for (int j = 0; j < n; ++j) {
-                        const T wj = ws[j];
-                        const T* xr = xs + j * px;
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) acc[q] = fma(wj * xr[ia[q]], xr[ib[q]], acc[q]);
-                    }
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        if (e0 + 32 * q < pp) gm[ib[q] * px + ia[q]] = acc[q];  // lower triangle
-                }
-                if (lane < p) {
-                    T acc = T(0);
-                    for (int j = 0; j < n; ++j) acc = fma(ws[j] * xs[j * px + lane], ys[j], acc);
-                    rv[lane] = acc;
-                }
-                __syncwarp();
-                bool ok = warp_ldlt_solve<T>(gm, p, px, rv, cv, lane);
-                if (ok) {
-                    for (int a = 0; a < p; ++a) ok &= bool(isfinite(rv[a]));
-                }
-                if (!ok) {
-                    if (lane < p) pv[lane] = ov[lane];
-                    __syncwarp();
-                    ++it;
-                    break;
-                }
-                T change = T(0), mxn = -INFINITY;
-                for (int j = lane; j < n; j += 32) {
-                    T po = T(0), pn = T(0);
-                    for (int a = 0; a < p; ++a) {
-                        po = fma(xs[j * px + a], pv[a], po);
-                        pn = fma(xs[j * px + a], rv[a], pn);
-                    }
-                    change = fmax(change, fabs(pn - po));
-                    mxn = fmax(mxn, pn);
-                }
-                change = warp_max(change);
-                mxn = warp_max(mxn);
-                __syncwarp();
-                if (lane < p) pv[lane] = rv[lane];
-                __syncwarp();
-                mx = mxn;
-                if (!(change > tol)) {
-                    ++it;
-                    break;
-                }
-            }
-        }
-        // Constraint check on the scaled parameters (cpp/src/dwi/log_fit.cpp:150,256).
         bool violated = false;
-        if (d.m > 0) {
-            bool fin = true;
-            for (int a = 0; a < p; ++a) fin &= bool(isfinite(pv[a]));
-            if (fin) {
-                bool neg = false;
-                for (int i = lane; i < d.m; i += 32) {
-                    T val = T(0);
-                    for (int a = 0; a < p; ++a) val = fma(d.g[size_t(i) * p + a], pv[a], val);
-                    neg |= val < T(0);
-                }
-                violated = __any_sync(0xffffffffu, neg);
-            }
-        }
+        const int it = log_warp_voxel<T>(d, lay, w, src, voxel, weighted, max_rw, tol, &violated, lane);
+        const T* pv = w.pv;
         if (lane < p) params[voxel * p + lane] = double(pv[lane]) / d.scales64[lane];
         if (lane == 0) {
             broke[voxel] = violated ? 1 : 0;
@@ -231,6 +280,66 @@ __global__ void __launch_bounds__(kWarps * 32) fit_log_warp_kernel(
             }
         }
         __syncwarp();
+    }
+}
+
+// The DKI family of a batch (batch.cuh): CTAs take tickets of kDkiBatchVoxels voxels of one
+// volume from a device counter across every DKI volume (each warp fits every kWarps-th voxel of
+// the ticket) and restage the design when the ticket moves to another volume. Violators go to
+// one list for the whole family, with their volume.
+__global__ void __launch_bounds__(kWarps * 32) batch_log_warp_kernel(
+    const DkiBatchJob* __restrict__ jobs, const int64_t* __restrict__ first, int n_jobs, int weighted,
+    int max_rw, double tol, int* __restrict__ queue, BatchViolators violators) {
+    using T = double;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ long long ticket;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t total = first[n_jobs];
+    int cur = -1;
+    WarpLayout<T> lay{0, 0, 1, 0};
+    WarpSmem<T> w{};
+    for (;;) {
+        if (threadIdx.x == 0) ticket = atomicAdd(reinterpret_cast<unsigned long long*>(queue), 1ull);
+        __syncthreads();
+        const int64_t t = ticket;
+        if (t >= total) break;
+        const int j = ticket_job(first, n_jobs, t);
+        const DkiBatchJob& job = jobs[j];
+        const LogDesignDevice<T> d = job.d;
+        if (j != cur) {
+            const int p = d.p;
+            lay = WarpLayout<T>{d.n, p, p | 1, p * (p + 1) / 2};
+            w = carve_warp<T>(smem_raw, lay, warp);
+            stage_warp_design<T>(d, lay, w);
+            cur = j;
+        }
+        __syncthreads();
+        const CappedSource src{job.s, job.s0, job.floor, job.is_b0, d.n};
+        const int64_t v = job.v, block_first = (t - first[j]) * kDkiBatchVoxels;
+        const int p = d.p;
+        for (int k = warp; k < kDkiBatchVoxels; k += kWarps) {
+            const int64_t voxel = block_first + k;
+            if (voxel >= v) break;
+            bool violated = false;
+            log_warp_voxel<T>(d, lay, w, src, voxel, weighted, max_rw, T(tol), &violated, lane);
+            const T* pv = w.pv;
+            if (lane < p) job.params[voxel * p + lane] = pv[lane] / d.scales64[lane];
+            if (lane == 0) job.broke[voxel] = violated ? 1 : 0;
+            if (violated) {
+                int slot = 0;
+                if (lane == 0) slot = atomicAdd(violators.count, 1);
+                slot = __shfl_sync(0xffffffffu, slot, 0);
+                if (slot < violators.capacity) {
+                    if (lane == 0) {
+                        violators.job[slot] = j;
+                        violators.voxel[slot] = voxel;
+                    }
+                    if (lane < p) violators.params[size_t(slot) * p + lane] = pv[lane];
+                }
+            }
+            __syncwarp();
+        }
+        __syncthreads();
     }
 }
 
@@ -271,6 +380,30 @@ void launch_log_warp(const LogDesignDevice<T>& d, const CappedSource& src, int64
                      const ViolatorList<T>& violators, cudaStream_t stream) {
     launch_warp_impl<T, CappedSource>(d, src, v, weighted, max_rw, tol, params, broke, iterations, violators,
                                       stream);
+}
+
+size_t batch_log_warp_smem(int n_max, int p) {
+    return WarpLayout<double>{n_max, p, p | 1, p * (p + 1) / 2}.bytes(kWarps);
+}
+
+void launch_batch_log_warp(const DkiBatchJob* jobs, const int64_t* first, int n_jobs, int n_max, int p,
+                           int64_t tickets, int weighted, int max_rw, double tol, int* queue,
+                           const BatchViolators& violators, cudaStream_t stream) {
+    if (n_jobs == 0 || tickets == 0) return;
+    const size_t smem = batch_log_warp_smem(n_max, p);
+    require(smem <= 227 * 1024, "the design is too large for the shared-memory log fit");
+    auto kernel = batch_log_warp_kernel;
+    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+               "cudaFuncSetAttribute");
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kWarps * 32, smem),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    const int64_t grid = std::min<int64_t>(tickets, int64_t(sm_count()) * std::max(per_sm, 1));
+    cuda_check(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), stream), "cudaMemsetAsync");
+    LaunchScope scope("batch_log_warp_kernel", stream);
+    kernel<<<unsigned(grid), kWarps * 32, smem, stream>>>(jobs, first, n_jobs, weighted, max_rw, tol, queue,
+                                                          violators);
+    cuda_check(cudaGetLastError(), "batch_log_warp_kernel launch");
 }
 
 template void launch_log_warp<double>(const LogDesignDevice<double>&, const LogSource&, int64_t, int, int, double,

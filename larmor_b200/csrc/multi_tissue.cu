@@ -31,6 +31,7 @@
 #include <string>
 #include <vector>
 
+#include "batch.cuh"
 #include "common.cuh"
 #include "host_la.hpp"
 #include "drl.cuh"
@@ -96,28 +97,22 @@ constexpr int kCorrDepth = 16;   // measurements per shared-memory stage
 
 // corr(v, j) = sum_i K(i, j) signal(v, i), i increasing, for the listed voxels: 128 threads as
 // 8 voxel lanes x 16 column lanes, each with 4 voxels x RC columns of the tile.
+// corr(v, j) for the kCorrVoxels voxels vox[] (shared; -1: none) and the columns col0 .. col0 +
+// 16 RC - 1 of the tile: 128 threads as 8 voxel lanes x 16 column lanes, each with 4 voxels x RC
+// columns; each entry summed in increasing measurement order.
 template <int RC>
-__global__ void __launch_bounds__(128) correlate_kernel(SignalDev S, const int* __restrict__ list, int64_t count,
-                                                        const int* __restrict__ count_dev,
-                                                        const double* __restrict__ k, int c,
-                                                        double* __restrict__ corr, int ldc) {
+__device__ __forceinline__ void correlate_tile(const SignalDev& S, const int64_t* vox, const double* __restrict__ k,
+                                               int c, int col0, double* __restrict__ corr, int ldc) {
     constexpr int TC = 16 * RC;
     __shared__ double sig_t[kCorrDepth][kCorrVoxels + 1];
     __shared__ double k_t[kCorrDepth][TC];
-    __shared__ int64_t vox[kCorrVoxels];
     const int tid = threadIdx.x, tv = tid & 7, tc = tid >> 3;
-    const int64_t p0 = int64_t(blockIdx.x) * kCorrVoxels;
-    const int col0 = blockIdx.y * TC;
     const int m = S.m;
-    if (count_dev) count = min(count, int64_t(*count_dev));
-    if (p0 >= count) return;
-    if (tid < kCorrVoxels) vox[tid] = p0 + tid < count ? listed(list, p0 + tid) : -1;
     double acc[4][RC];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < RC; ++b) acc[a][b] = 0.0;
-    __syncthreads();
     for (int i0 = 0; i0 < m; i0 += kCorrDepth) {
         const int depth = min(kCorrDepth, m - i0);
         for (int e = tid; e < kCorrVoxels * kCorrDepth; e += 128) {
@@ -154,6 +149,23 @@ __global__ void __launch_bounds__(128) correlate_kernel(SignalDev S, const int* 
             if (col < c) corr[voxel * ldc + col] = acc[a][b];
         }
     }
+}
+
+// corr(v, j) = sum_i K(i, j) signal(v, i) for the listed voxels: a CTA per tile of kCorrVoxels
+// voxels x 16 RC columns.
+template <int RC>
+__global__ void __launch_bounds__(128) correlate_kernel(SignalDev S, const int* __restrict__ list, int64_t count,
+                                                        const int* __restrict__ count_dev,
+                                                        const double* __restrict__ k, int c,
+                                                        double* __restrict__ corr, int ldc) {
+    __shared__ int64_t vox[kCorrVoxels];
+    const int tid = threadIdx.x;
+    const int64_t p0 = int64_t(blockIdx.x) * kCorrVoxels;
+    if (count_dev) count = min(count, int64_t(*count_dev));
+    if (p0 >= count) return;
+    if (tid < kCorrVoxels) vox[tid] = p0 + tid < count ? listed(list, p0 + tid) : -1;
+    __syncthreads();
+    correlate_tile<RC>(S, vox, k, c, blockIdx.y * 16 * RC, corr, ldc);
 }
 
 // ---- ridge NNLS ------------------------------------------------------------------------
@@ -1033,6 +1045,253 @@ __global__ void __launch_bounds__(kMtWarps * 32, 4) hr_fractions_kernel(
     }
 }
 
+// ---- batches (batch.cuh): every mFOD volume of a batch through one queue per stage ------------
+
+// A volume of a batch: its solvers and kernels, signals, shell weights and outputs.
+struct MfodBatchJob {
+    int64_t v, off;  // voxels; the row of its first voxel in the batch's per-voxel state
+    RidgeDev lr, hr;
+    TissueDev lrt, hrt;
+    const double* s;   // (v, m) S0-normalised signals
+    const double* w;   // (m,) shell weights
+    double* fods;      // (v, hr.c)
+    double* fractions; // (v, hrt.nb + hrt.ci)
+    int32_t* rounds;   // (v,) or null
+    uint8_t* status;   // (v,) or null
+};
+
+// The per-voxel state of a batch (volume j's voxel v at row off_j + v) and the stage's tickets.
+struct MfodBatchState {
+    const MfodBatchJob* jobs;
+    int n_jobs, ci, ldc, ldx;  // isotropic tissues; row strides of corr and of the low-resolution FODs
+    double *fiso, *prev, *corr, *xlr;
+    int32_t* rounds;
+    uint8_t* bad;
+    int64_t* vfirst;   // (n_jobs + 1) this stage's first voxel ticket per volume
+    int64_t* tfirst;   // (n_jobs + 1) its first correlation tile per volume
+    int64_t* redo;     // volume << 32 | voxel, for the one-warp NNLS
+    int* redo_count;
+};
+
+// A round's lists are per-volume segments of one array (volume j's at row off_j), null for
+// every voxel of every volume.
+struct BatchItem {
+    int job;
+    int64_t voxel;
+};
+
+__device__ __forceinline__ BatchItem batch_item(const MfodBatchState& B, const int* list, int64_t p) {
+    const int j = ticket_job(B.vfirst, B.n_jobs, p);
+    const int64_t q = p - B.vfirst[j];
+    return BatchItem{j, list ? int64_t(list[B.jobs[j].off + q]) : q};
+}
+
+__device__ __forceinline__ SignalDev batch_signal(const MfodBatchState& B, const MfodBatchJob& J, const TissueDev& T) {
+    return SignalDev{J.s, J.w, T.wiso, B.fiso + J.off * B.ci, T.m, B.ci};
+}
+
+// The tickets of a stage from each volume's count (null: every voxel).
+__global__ void batch_plan_kernel(MfodBatchState B, const int* __restrict__ counts) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int64_t a = 0, b = 0;
+    for (int j = 0; j < B.n_jobs; ++j) {
+        B.vfirst[j] = a;
+        B.tfirst[j] = b;
+        const int64_t c = counts ? int64_t(counts[j]) : B.jobs[j].v;
+        a += c;
+        b += (c + kCorrVoxels - 1) / kCorrVoxels;
+    }
+    B.vfirst[B.n_jobs] = a;
+    B.tfirst[B.n_jobs] = b;
+}
+
+// correlate_kernel over every volume: a CTA per (volume, tile of kCorrVoxels listed voxels).
+template <int RC, bool HR>
+__global__ void __launch_bounds__(128) batch_correlate_kernel(MfodBatchState B, const int* __restrict__ list) {
+    __shared__ int64_t vox[kCorrVoxels];
+    const int64_t t = blockIdx.x;
+    if (t >= B.tfirst[B.n_jobs]) return;
+    const int j = ticket_job(B.tfirst, B.n_jobs, t);
+    const MfodBatchJob& J = B.jobs[j];
+    const int64_t count = B.vfirst[j + 1] - B.vfirst[j];
+    const int64_t p0 = (t - B.tfirst[j]) * kCorrVoxels;
+    const int tid = threadIdx.x;
+    if (tid < kCorrVoxels) {
+        const int64_t q = p0 + tid;
+        vox[tid] = q < count ? (list ? int64_t(list[J.off + q]) : q) : -1;
+    }
+    __syncthreads();
+    const RidgeDev R = HR ? J.hr : J.lr;
+    const TissueDev T = HR ? J.hrt : J.lrt;
+    correlate_tile<RC>(batch_signal(B, J, T), vox, R.k, R.c, blockIdx.y * 16 * RC, B.corr + J.off * B.ldc, B.ldc);
+}
+
+// ridge_nnls_half_kernel over every volume's list.
+template <int CPL>
+__global__ void __launch_bounds__(kMtWarps * 32, 6) batch_half_kernel(MfodBatchState B, const int* __restrict__ list,
+                                                                     int c_max, int* queue,
+                                                                     double* __restrict__ workspace,
+                                                                     size_t slot_size) {
+    __shared__ HalfState<CPL> states[2 * kMtWarps];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const HalfWarp hw(threadIdx.x & 31);
+    const int gid = int(threadIdx.x >> 4);
+    HalfState<CPL>& st = states[gid];
+    const HalfSlot sl = carve_half(workspace + (size_t(blockIdx.x) * 2 * kMtWarps + gid) * slot_size,
+                                   smem_raw + gid * half_smem_bytes(c_max), c_max);
+    const int64_t total = B.vfirst[B.n_jobs];
+    for (;;) {
+        long long p = 0;
+        if (hw.lane == 0) p = atomicAdd(queue, 1);
+        p = hw.from(p, 0);
+        if (p >= total) break;
+        const BatchItem it = batch_item(B, list, p);
+        const MfodBatchJob& J = B.jobs[it.job];
+        const RidgeDev R = J.lr;
+        const int64_t row = J.off + it.voxel;
+        if (ridge_nnls_half<CPL>(R, B.corr + row * B.ldc, sl, st, hw)) {
+            for (int j = hw.lane; j < R.c; j += kHalf) B.xlr[row * B.ldx + j] = sl.x[j];
+        } else if (hw.lane == 0) {
+            B.redo[atomicAdd(B.redo_count, 1)] = (int64_t(it.job) << 32) | it.voxel;
+        }
+        hw.sync();
+    }
+}
+
+// ridge_nnls_kernel over the voxels the first passes handed back, from every volume.
+template <int VPL, int CPL, bool HR>
+__global__ void __launch_bounds__(kMtWarps * 32, (CPL <= 2 ? 6 : 4)) batch_redo_kernel(
+    MfodBatchState B, int c_max, int* queue, double* __restrict__ workspace, size_t slot_size) {
+    using State = NnlsState<VPL * 32, CPL * 32>;
+    __shared__ State states[kMtWarps];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    State& st = states[warp];
+    double* slot = workspace + (size_t(blockIdx.x) * kMtWarps + warp) * slot_size;
+    unsigned char* wsm = smem_raw + warp * nnls_smem_bytes(c_max, VPL * 32);
+    const int total = *B.redo_count;
+    for (;;) {
+        int p = 0;
+        if (lane == 0) p = atomicAdd(queue, 1);
+        p = __shfl_sync(0xffffffffu, p, 0);
+        if (p >= total) break;
+        const int64_t e = B.redo[p];
+        const MfodBatchJob& J = B.jobs[int(e >> 32)];
+        const int64_t voxel = e & 0xffffffffll;
+        const RidgeDev R = HR ? J.hr : J.lr;
+        const TissueDev T = HR ? J.hrt : J.lrt;
+        NnlsSlot sl = carve_nnls(slot, wsm, R.m, R.c, VPL * 32);
+        const int64_t row = J.off + voxel;
+        const bool ok = ridge_nnls<VPL, CPL>(R, batch_signal(B, J, T), voxel, B.corr + row * B.ldc, sl, st, lane);
+        double* x = HR ? J.fods + voxel * R.c : B.xlr + row * B.ldx;
+        for (int j = lane; j < R.c; j += 32) x[j] = sl.x[j];
+        if (lane == 0 && !ok) B.bad[row] = 1;
+        __syncwarp();
+    }
+}
+
+// ridge_nnls_first_kernel<1, 10> over every voxel of every volume.
+__global__ void __launch_bounds__(kMtWarps * 32, 5) batch_first_kernel(MfodBatchState B, int c_max, int* queue,
+                                                                      double* __restrict__ workspace,
+                                                                      size_t slot_size) {
+    using State = NnlsState<32, 10 * 32>;
+    __shared__ State states[kMtWarps];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    State& st = states[warp];
+    double* slot = workspace + (size_t(blockIdx.x) * kMtWarps + warp) * slot_size;
+    unsigned char* wsm = smem_raw + warp * nnls_smem_bytes(c_max, 32);
+    const int64_t total = B.vfirst[B.n_jobs];
+    for (;;) {
+        long long p = 0;
+        if (lane == 0) p = atomicAdd(queue, 1);
+        p = __shfl_sync(0xffffffffu, p, 0);
+        if (p >= total) break;
+        const BatchItem it = batch_item(B, nullptr, p);
+        const MfodBatchJob& J = B.jobs[it.job];
+        const RidgeDev R = J.hr;
+        NnlsSlot sl = carve_nnls(slot, wsm, R.m, R.c, 32);
+        const int64_t row = J.off + it.voxel;
+        bool again = false;
+        ridge_nnls<1, 10, true>(R, batch_signal(B, J, J.hrt), it.voxel, B.corr + row * B.ldc, sl, st, lane, &again);
+        if (again) {
+            if (lane == 0) B.redo[atomicAdd(B.redo_count, 1)] = (int64_t(it.job) << 32) | it.voxel;
+        } else {
+            for (int j = lane; j < R.c; j += 32) J.fods[it.voxel * R.c + j] = sl.x[j];
+        }
+        __syncwarp();
+    }
+}
+
+// lr_fractions_kernel over every volume's list; the next round's list goes to each volume's
+// segment.
+__global__ void __launch_bounds__(kMtWarps * 32, 4) batch_lr_fractions_kernel(
+    MfodBatchState B, const int* __restrict__ list, int round, int max_rounds, double fraction_tol,
+    int* __restrict__ next, int* next_counts, int* queue, double* __restrict__ workspace, size_t slot_size) {
+    __shared__ FracState states[kMtWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    FracState& st = states[warp];
+    double* slot = workspace + (size_t(blockIdx.x) * kMtWarps + warp) * slot_size;
+    const int ci = B.ci;
+    const int64_t total = B.vfirst[B.n_jobs];
+    for (;;) {
+        long long p = 0;
+        if (lane == 0) p = atomicAdd(queue, 1);
+        p = __shfl_sync(0xffffffffu, p, 0);
+        if (p >= total) break;
+        const BatchItem it = batch_item(B, list, p);
+        const MfodBatchJob& J = B.jobs[it.job];
+        const TissueDev T = J.lrt;
+        const FracSlot sl = carve_frac(slot, T.m, T.ca, 1 + T.ci);
+        const int64_t row = J.off + it.voxel;
+        fractions(T, B.xlr + row * B.ldx, J.s + it.voxel * T.m, false, -1.0, sl, st, lane);
+        bool converged = round > 0;
+        for (int j = 0; j <= ci; ++j) converged &= fabs(st.fr[j] - B.prev[row * (ci + 1) + j]) < fraction_tol;
+        __syncwarp();
+        if (lane < ci) B.fiso[row * ci + lane] = st.fr[1 + lane];
+        if (converged || round + 1 >= max_rounds) {
+            if (lane == 0) B.rounds[row] = round + 1;
+        } else {
+            if (lane <= ci) B.prev[row * (ci + 1) + lane] = st.fr[lane];
+            if (lane == 0) next[J.off + atomicAdd(next_counts + it.job, 1)] = int(it.voxel);
+        }
+        __syncwarp();
+    }
+}
+
+// hr_fractions_kernel over every voxel of every volume.
+__global__ void __launch_bounds__(kMtWarps * 32, 4) batch_hr_fractions_kernel(MfodBatchState B, double final_tol,
+                                                                             int* queue,
+                                                                             double* __restrict__ workspace,
+                                                                             size_t slot_size) {
+    __shared__ FracState states[kMtWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    FracState& st = states[warp];
+    double* slot = workspace + (size_t(blockIdx.x) * kMtWarps + warp) * slot_size;
+    const int64_t total = B.vfirst[B.n_jobs];
+    for (;;) {
+        long long p = 0;
+        if (lane == 0) p = atomicAdd(queue, 1);
+        p = __shfl_sync(0xffffffffu, p, 0);
+        if (p >= total) break;
+        const BatchItem it = batch_item(B, nullptr, p);
+        const MfodBatchJob& J = B.jobs[it.job];
+        const TissueDev T = J.hrt;
+        const int nf = T.nb + T.ci;
+        const FracSlot sl = carve_frac(slot, T.m, T.ca, nf);
+        const int64_t row = J.off + it.voxel;
+        fractions(T, J.fods + it.voxel * T.ca, J.s + it.voxel * T.m, true, final_tol, sl, st, lane);
+        double sum = kFractionSumOffset;
+        for (int g = 0; g < nf; ++g) sum += st.fr[g];
+        for (int g = lane; g < nf; g += 32) J.fractions[it.voxel * nf + g] = st.fr[g] / sum;
+        if (lane == 0) {
+            if (J.rounds) J.rounds[it.voxel] = B.rounds[row];
+            if (J.status) J.status[it.voxel] = B.bad[row];
+        }
+        __syncwarp();
+    }
+}
+
 // ---- host side -------------------------------------------------------------------------
 
 // The warps of a persistent grid: as many as the SMs hold at once (or one per item), in whole
@@ -1408,6 +1667,245 @@ static int fit_multi_tissue(const double* signals, int64_t v, const double* weig
         }
     });
 }
+
+// ---- batches (batch.cuh): the mFOD family --------------------------------------------------
+
+namespace lar {
+
+struct MfodBatch {
+    std::vector<MfodBatchJob> jobs;
+    std::vector<std::vector<double>> weights;
+    std::vector<std::unique_ptr<DeviceArray<double>>> weights_dev;
+    int max_rounds = -1;
+    double fraction_tol = 0.0, final_tol = 0.0;
+    int ci = -1, m_max = 0, c_lr_max = 0, c_hr_max = 0, nf_max = 0;
+    int64_t voxels = 0, tiles = 0;
+    // Finalized: the device job table, the per-voxel state and the launch shapes.
+    DeviceArray<MfodBatchJob> d_jobs;
+    void* scratch = nullptr;
+    MfodBatchState B{};
+    int *list[2] = {nullptr, nullptr}, *counts[2] = {nullptr, nullptr}, *queue = nullptr;
+    double* slots = nullptr;
+    int64_t half_warps = 0, lr_slots = 0, first_slots = 0, hr_slots = 0, lf_slots = 0, hf_slots = 0;
+    size_t half_smem = 0, lr_smem = 0, first_smem = 0, hr_smem = 0;
+    size_t lr_slot = 0, first_slot = 0, hr_slot = 0, lf_slot = 0, hf_slot = 0;
+    ~MfodBatch() {
+        if (scratch) cudaFree(scratch);
+    }
+};
+
+MfodBatch* mfod_batch_create() { return new MfodBatch(); }
+
+void mfod_batch_destroy(MfodBatch* b) { delete b; }
+
+void mfod_batch_add(MfodBatch* b, const double* signals, int64_t v, const double* weights, lar_deconv_kernel lr,
+                    lar_fod_solver lr_solver, lar_deconv_kernel hr, lar_fod_solver hr_solver, int64_t max_outer,
+                    double fraction_tol, double final_tol_x, double* fods, double* fractions, int32_t* rounds,
+                    uint8_t* status) {
+    require(lr && hr && lr_solver && hr_solver, "kernels and solvers must not be NULL");
+    require(weights != nullptr, "weights must not be NULL");
+    const int64_t m = hr->m;
+    require(lr->m == m, "signals, weights and the kernels' measurements do not match");
+    require(lr->ci == hr->ci, "the two kernels have different numbers of isotropic tissues");
+    require(lr_solver->host.c == lr->ca && lr_solver->host.m == m && hr_solver->host.c == hr->ca &&
+                hr_solver->host.m == m,
+            "a solver does not match its kernel");
+    require(lr_solver->kind == 0 && hr_solver->kind == 0 && lr_solver->host.normal_equations &&
+                hr_solver->host.normal_equations,
+            "a batch takes ridge NNLS (L2NNLS) solvers with normal equations");
+    require(lr->ca <= 48 && hr->ca > 64 && hr->ca <= 320,
+            "a batch takes low-resolution kernels of at most 48 directions and high-resolution ones of 65 to 320");
+    require(max_outer >= 0 && v >= 0, "max_outer and v must be at least 0");
+    require(v == 0 || (signals && fods && fractions), "signals, fods and fractions must not be NULL");
+    const int rounds_cap = int(std::min<int64_t>(max_outer, 1 << 20));
+    if (b->max_rounds < 0) {
+        b->max_rounds = rounds_cap;
+        b->fraction_tol = fraction_tol;
+        b->final_tol = final_tol_x;
+        b->ci = int(lr->ci);
+    }
+    require(rounds_cap == b->max_rounds && fraction_tol == b->fraction_tol && final_tol_x == b->final_tol,
+            "every mFOD job of a batch takes the same max_outer, fraction_tol and final_tol_x");
+    require(int(lr->ci) == b->ci, "every mFOD job of a batch has the same isotropic tissues");
+    MfodBatchJob j{};
+    j.v = v;
+    j.off = b->voxels;
+    j.lr = lr_solver->view();
+    j.hr = hr_solver->view();
+    j.lrt = lr->view();
+    j.hrt = hr->view();
+    j.s = signals;
+    j.fods = fods;
+    j.fractions = fractions;
+    j.rounds = rounds;
+    j.status = status;
+    b->jobs.push_back(j);
+    b->weights.emplace_back(weights, weights + m);
+    b->voxels += v;
+    b->tiles += (v + kCorrVoxels - 1) / kCorrVoxels;
+    b->m_max = std::max(b->m_max, int(m));
+    b->c_lr_max = std::max(b->c_lr_max, int(lr->ca));
+    b->c_hr_max = std::max(b->c_hr_max, int(hr->ca));
+    b->nf_max = std::max(b->nf_max, int(hr->nb + hr->ci));
+}
+
+void mfod_batch_finalize(MfodBatch* b) {
+    if (b->jobs.empty()) return;
+    require(b->voxels < (int64_t(1) << 31), "at most 2^31 - 1 mFOD voxels per batch");
+    for (size_t k = 0; k < b->jobs.size(); ++k) {
+        b->weights_dev.push_back(std::make_unique<DeviceArray<double>>());
+        b->weights_dev.back()->upload(b->weights[k].data(), b->weights[k].size());
+        b->jobs[k].w = b->weights_dev.back()->ptr;
+    }
+    b->d_jobs.upload(b->jobs.data(), b->jobs.size());
+    const int64_t V = b->voxels, nj = int64_t(b->jobs.size());
+    const int ci = b->ci, mi = b->m_max, ldc = std::max(b->c_lr_max, b->c_hr_max), ldx = b->c_lr_max;
+    // Launch shapes: the single-volume fit's persistent grids, sized for the whole batch.
+    b->half_smem = half_smem_bytes(b->c_lr_max) * 2 * kMtWarps;
+    b->half_warps = resident_slots(batch_half_kernel<3>, b->half_smem, V, "sd.nnls.ctas_per_sm");
+    b->lr_smem = nnls_smem_bytes(b->c_lr_max, 32) * kMtWarps;
+    b->lr_slots = resident_slots(batch_redo_kernel<1, 2, false>, b->lr_smem, V, "sd.nnls.ctas_per_sm");
+    b->first_smem = nnls_smem_bytes(b->c_hr_max, 32) * kMtWarps;
+    b->first_slots = resident_slots(batch_first_kernel, b->first_smem, V, "sd.nnls.ctas_per_sm");
+    b->hr_smem = nnls_smem_bytes(b->c_hr_max, kCholCap) * kMtWarps;
+    b->hr_slots = resident_slots(batch_redo_kernel<kCholCap / 32, 10, true>, b->hr_smem, V, "sd.nnls.ctas_per_sm");
+    b->lf_slots = resident_slots(batch_lr_fractions_kernel, 0, V, "sd.fractions.ctas_per_sm");
+    b->hf_slots = resident_slots(batch_hr_fractions_kernel, 0, V, "sd.fractions.ctas_per_sm");
+    b->lr_slot = nnls_slot_doubles(mi, 32);
+    b->first_slot = nnls_slot_doubles(mi, 32);
+    b->hr_slot = nnls_slot_doubles(mi, kCholCap);
+    b->lf_slot = frac_slot_doubles(mi, b->c_lr_max, 1 + ci);
+    b->hf_slot = frac_slot_doubles(mi, b->c_hr_max, b->nf_max);
+    const size_t slot_doubles = std::max(
+        {size_t(2 * b->half_warps) * half_slot_doubles(), size_t(b->lr_slots) * b->lr_slot,
+         size_t(b->first_slots) * b->first_slot, size_t(b->hr_slots) * b->hr_slot, size_t(b->lf_slots) * b->lf_slot,
+         size_t(b->hf_slots) * b->hf_slot});
+    auto carve_all = [&](Carver& cv) {
+        MfodBatchState s{};
+        s.jobs = b->d_jobs.ptr;
+        s.n_jobs = int(nj);
+        s.ci = ci;
+        s.ldc = ldc;
+        s.ldx = ldx;
+        s.fiso = cv.take<double>(size_t(V) * std::max(ci, 1));
+        s.prev = cv.take<double>(size_t(V) * (ci + 1));
+        s.corr = cv.take<double>(size_t(V) * ldc);
+        s.xlr = cv.take<double>(size_t(V) * ldx);
+        s.rounds = cv.take<int32_t>(size_t(V));
+        s.bad = cv.take<uint8_t>(size_t(V));
+        s.vfirst = cv.take<int64_t>(size_t(nj) + 1);
+        s.tfirst = cv.take<int64_t>(size_t(nj) + 1);
+        s.redo = cv.take<int64_t>(size_t(V));
+        s.redo_count = cv.take<int>(1);
+        b->list[0] = cv.take<int>(size_t(V));
+        b->list[1] = cv.take<int>(size_t(V));
+        b->counts[0] = cv.take<int>(size_t(nj));
+        b->counts[1] = cv.take<int>(size_t(nj));
+        b->queue = cv.take<int>(1);
+        b->slots = cv.take<double>(slot_doubles);
+        return s;
+    };
+    Carver sizing{nullptr};
+    carve_all(sizing);
+    cuda_check(cudaMalloc(&b->scratch, sizing.used), "cudaMalloc (mFOD batch state)");
+    Carver cv{static_cast<char*>(b->scratch)};
+    b->B = carve_all(cv);
+}
+
+void mfod_batch_run(MfodBatch* b, cudaStream_t st) {
+    if (b->jobs.empty() || b->voxels == 0) return;
+    const MfodBatchState& B = b->B;
+    const int64_t V = b->voxels, nj = int64_t(b->jobs.size());
+    const int ci = b->ci;
+    auto blocks = [](int64_t slots, int64_t count) {
+        return unsigned(std::max<int64_t>(1, std::min<int64_t>(slots / kMtWarps, (count + kMtWarps - 1) / kMtWarps)));
+    };
+    auto zero = [&](void* p, size_t bytes) { cuda_check(cudaMemsetAsync(p, 0, bytes, st), "cudaMemsetAsync"); };
+    auto launched = [](const char* what) { cuda_check(cudaGetLastError(), what); };
+    if (ci > 0) zero(B.fiso, size_t(V) * ci * sizeof(double));
+    zero(B.rounds, size_t(V) * sizeof(int32_t));
+    zero(B.bad, size_t(V));
+    const unsigned lr_redo_blocks = std::min<unsigned>(blocks(b->lr_slots, V), unsigned(sm_count()));
+    const unsigned hr_redo_blocks = std::min<unsigned>(blocks(b->hr_slots, V), unsigned(sm_count()));
+    // Every round is enqueued: each stage reads its tickets on the device, so a round whose
+    // lists are all empty costs only its launches.
+    const int* cur = nullptr;
+    const int* cur_counts = nullptr;
+    int side = 0;
+    for (int round = 0; round < b->max_rounds; ++round) {
+        int* nxt = b->list[side];
+        int* nxt_counts = b->counts[side];
+        {
+            LaunchScope scope("batch_plan_kernel", st);
+            batch_plan_kernel<<<1, 32, 0, st>>>(B, cur_counts);
+            launched("batch_plan_kernel launch");
+        }
+        {
+            LaunchScope scope("batch_correlate_kernel", st);
+            batch_correlate_kernel<3, false><<<unsigned(b->tiles), 128, 0, st>>>(B, cur);
+            launched("batch_correlate_kernel launch");
+        }
+        zero(b->queue, sizeof(int));
+        zero(nxt_counts, size_t(nj) * sizeof(int));
+        zero(B.redo_count, sizeof(int));
+        {
+            LaunchScope scope("batch_half_kernel<3>", st);
+            batch_half_kernel<3><<<blocks(b->half_warps, (V + 1) / 2), kMtWarps * 32, b->half_smem, st>>>(
+                B, cur, b->c_lr_max, b->queue, b->slots, half_slot_doubles());
+            launched("batch_half_kernel launch");
+        }
+        zero(b->queue, sizeof(int));
+        {
+            LaunchScope scope("batch_redo_kernel<1,2>", st);
+            batch_redo_kernel<1, 2, false><<<lr_redo_blocks, kMtWarps * 32, b->lr_smem, st>>>(
+                B, b->c_lr_max, b->queue, b->slots, b->lr_slot);
+            launched("batch_redo_kernel launch");
+        }
+        zero(b->queue, sizeof(int));
+        {
+            LaunchScope scope("batch_lr_fractions_kernel", st);
+            batch_lr_fractions_kernel<<<blocks(b->lf_slots, V), kMtWarps * 32, 0, st>>>(
+                B, cur, round, b->max_rounds, b->fraction_tol, nxt, nxt_counts, b->queue, b->slots, b->lf_slot);
+            launched("batch_lr_fractions_kernel launch");
+        }
+        cur = nxt;
+        cur_counts = nxt_counts;
+        side ^= 1;
+    }
+    {
+        LaunchScope scope("batch_plan_kernel", st);
+        batch_plan_kernel<<<1, 32, 0, st>>>(B, nullptr);
+        launched("batch_plan_kernel launch");
+    }
+    {
+        LaunchScope scope("batch_correlate_kernel", st);
+        batch_correlate_kernel<4, true><<<dim3(unsigned(b->tiles), unsigned((b->c_hr_max + 63) / 64)), 128, 0, st>>>(
+            B, nullptr);
+        launched("batch_correlate_kernel launch");
+    }
+    zero(b->queue, sizeof(int));
+    zero(B.redo_count, sizeof(int));
+    {
+        LaunchScope scope("batch_first_kernel<1,10>", st);
+        batch_first_kernel<<<blocks(b->first_slots, V), kMtWarps * 32, b->first_smem, st>>>(
+            B, b->c_hr_max, b->queue, b->slots, b->first_slot);
+        launched("batch_first_kernel launch");
+    }
+    zero(b->queue, sizeof(int));
+    {
+        LaunchScope scope("batch_redo_kernel<8,10>", st);
+        batch_redo_kernel<kCholCap / 32, 10, true><<<hr_redo_blocks, kMtWarps * 32, b->hr_smem, st>>>(
+            B, b->c_hr_max, b->queue, b->slots, b->hr_slot);
+        launched("batch_redo_kernel launch");
+    }
+    zero(b->queue, sizeof(int));
+    LaunchScope scope("batch_hr_fractions_kernel", st);
+    batch_hr_fractions_kernel<<<blocks(b->hf_slots, V), kMtWarps * 32, 0, st>>>(B, b->final_tol, b->queue, b->slots,
+                                                                              b->hf_slot);
+    launched("batch_hr_fractions_kernel launch");
+}
+
+}  // namespace lar
 
 extern "C" {
 

@@ -51,6 +51,24 @@ def test_design_create_refuses_bad_shapes_without_a_gpu():
     assert b"n >= p" in _lib.lib().lar_last_error()
 
 
+def test_batch_refuses_misuse_without_a_gpu():
+    import ctypes
+
+    from larmor_b200 import _lib
+
+    lib = _lib.lib()
+    batch = ctypes.c_void_p()
+    assert lib.lar_batch_create(ctypes.byref(batch)) == _lib.LAR_OK
+    try:
+        assert lib.lar_batch_run(batch, _lib.LAR_BATCH_DTI, None) == _lib.LAR_ERR_INVALID
+        assert b"finalize" in lib.lar_last_error()
+        status = lib.lar_batch_add_dti(batch, None, None, None, 10, 1, 20, 1e-6, None, None)
+        assert status == _lib.LAR_ERR_INVALID
+        assert b"must not be NULL" in lib.lar_last_error()
+    finally:
+        lib.lar_batch_destroy(batch)
+
+
 DESIGN = np.column_stack([np.ones(43), np.random.default_rng(3).normal(size=(43, 6))])
 
 

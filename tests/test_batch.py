@@ -1,6 +1,7 @@
 """The batched uneven fit (many volumes, one CUDA graph): the job generator and branch plan on
-the CPU, and on the GPU every job's graph result against the same job fitted eagerly and, for
-mFOD, against the public fit_multi_tissue."""
+the CPU, and on the GPU every job's result from the per-family work queues (captured in a graph)
+and from the per-job kernel chains against the same job fitted alone and, for mFOD, against the
+public fit_multi_tissue, bit for bit."""
 
 from __future__ import annotations
 
@@ -36,7 +37,8 @@ def test_branches_balance_longest_first():
 
 
 @pytest.mark.gpu
-def test_graph_batch_equals_eager_fits(cuda):
+@pytest.mark.parametrize("queue", [True, False], ids=["family_queues", "job_chains"])
+def test_graph_batch_equals_eager_fits(cuda, queue):
     import torch
 
     from larmor_b200 import _core
@@ -45,7 +47,7 @@ def test_graph_batch_equals_eager_fits(cuda):
 
     jobs = generate_jobs(seed=5, n_volumes=9, min_voxels=300, max_voxels=3000, mix=(1, 1, 1))
     assert {j.kind for j in jobs} == {"dti", "dki", "mfod"}
-    graph = Batch(jobs, branches=3)
+    graph = Batch(jobs, branches=3, queue=queue)
     graph.capture()
     for o in (j.out for j in jobs):
         for t in o.values():
@@ -53,7 +55,7 @@ def test_graph_batch_equals_eager_fits(cuda):
     graph.run()
     torch.cuda.synchronize()
     got = [{k: t.cpu().numpy().copy() for k, t in j.out.items()} for j in jobs]
-    eager = Batch(jobs, branches=1)
+    eager = Batch(jobs, branches=1, queue=False)
     eager.run_eager()
     torch.cuda.synchronize()
     for j, g in zip(jobs, got):
