@@ -182,7 +182,8 @@ int lar_batch_finalize(lar_batch batch) {
             upload_vector(b.dki_fit_first, fit_first);
             upload_vector(b.dki_maps_first, maps_first);
             b.violators.capacity = int(dki_voxels);
-            viol_bytes = size_t(dki_voxels) * (sizeof(int) + sizeof(int64_t) + 22 * sizeof(double)) + 256;
+            // Rounded up to 256 bytes: the re-fit's slots (doubles) follow.
+            viol_bytes = (size_t(dki_voxels) * (sizeof(int) + sizeof(int64_t) + 22 * sizeof(double)) + 255) / 256 * 256;
             if (b.dki_mmax > 0) {
                 b.refit_slot_doubles = batch_refit_slot_doubles(b.dki_nmax, 22, b.dki_mmax);
                 b.refit_nslots = int(std::max<int64_t>(4, std::min<int64_t>((dki_voxels + 3) / 4 * 4,
