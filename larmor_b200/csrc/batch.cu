@@ -74,7 +74,7 @@ struct lar_batch_s {
     DeviceArray<DkiBatchJob> d_dki;
     DeviceArray<int64_t> dki_fit_first, dki_maps_first;
     int64_t dki_fit_tickets = 0, dki_maps_tickets = 0;
-    int dki_nmax = 0, dki_mmax = 0;
+    int dki_nmax = 0, dki_mmax = 0, dki_warps = 0;
     BatchViolators violators;
     double* refit_slots = nullptr;
     int refit_nslots = 0;
@@ -159,7 +159,7 @@ int lar_batch_finalize(lar_batch batch) {
             upload_vector(b.d_dti, b.dti);
             upload_vector(b.dti_first, first);
         }
-        // DKI: tickets of kDkiBatchVoxels for the fit, kMapsBatchVoxels for the maps; one violator
+        // DKI: tickets of kDkiVoxelsPerWarp voxels per warp of the fit's CTA, kMapsBatchVoxels for the maps; one violator
         // list for the family (every voxel may break a constraint) and the re-fit's warp slots.
         voxels.clear();
         int64_t dki_voxels = 0;
@@ -171,10 +171,10 @@ int lar_batch_finalize(lar_batch batch) {
         }
         size_t viol_bytes = 0, slot_bytes = 0;
         if (!b.dki.empty()) {
-            require(batch_log_warp_smem(b.dki_nmax, 22) <= 227 * 1024,
-                    "a DKI table of the batch is too large for the shared-memory log fit");
+            b.dki_warps = batch_log_warp_warps(b.dki_nmax, 22);
+            require(b.dki_warps > 0, "a DKI table of the batch is too large for the shared-memory log fit");
             require(dki_voxels < (int64_t(1) << 31), "at most 2^31 - 1 DKI voxels per batch");
-            const auto fit_first = ticket_starts(voxels, kDkiBatchVoxels);
+            const auto fit_first = ticket_starts(voxels, int64_t(kDkiVoxelsPerWarp) * b.dki_warps);
             const auto maps_first = ticket_starts(voxels, kMapsBatchVoxels);
             b.dki_fit_tickets = fit_first.back();
             b.dki_maps_tickets = maps_first.back();
@@ -225,7 +225,7 @@ int lar_batch_run(lar_batch batch, int families, void* stream) {
                              b.dti_fit.weighted, b.dti_fit.max_rw, b.dti_fit.tol, b.counters, st);
         if ((families & LAR_BATCH_DKI) && !b.dki.empty()) {
             cuda_check(cudaMemsetAsync(b.violators.count, 0, sizeof(int), st), "cudaMemsetAsync");
-            launch_batch_log_warp(b.d_dki.ptr, b.dki_fit_first.ptr, int(b.dki.size()), b.dki_nmax, 22,
+            launch_batch_log_warp(b.d_dki.ptr, b.dki_fit_first.ptr, int(b.dki.size()), b.dki_nmax, 22, b.dki_warps,
                                   b.dki_fit_tickets, b.dki_fit.weighted, b.dki_fit.max_rw, b.dki_fit.tol,
                                   b.counters + 2, b.violators, st);
             if (b.dki_mmax > 0)

@@ -70,15 +70,18 @@ struct BatchViolators {
 
 // Voxels per ticket of the family stages.
 constexpr int kDtiBatchBlock = 32;   // one CTA of the DTI fit (thread per voxel)
-constexpr int kDkiBatchVoxels = 16;  // one CTA of the DKI log fit (4 warps x 4 voxels)
+constexpr int kDkiVoxelsPerWarp = 4;  // a ticket of the DKI log fit: 4 voxels per warp of its CTA
 constexpr int kMapsBatchVoxels = 128;
 
 // Launch shapes and shared memory of the family stages (sized for the largest table).
 size_t batch_dti_smem(int n_max);
-size_t batch_log_warp_smem(int n_max, int p);
+// Warps per CTA of the DKI log fit (12, 8 or 4; 0: the largest table does not fit) and its
+// shared memory.
+int batch_log_warp_warps(int n_max, int p);
+size_t batch_log_warp_smem(int n_max, int p, int warps);
 void launch_batch_dti(const DtiBatchJob* jobs, const int64_t* first, int n_jobs, int n_max, int64_t tickets,
                       int weighted, int max_rw, double tol, int* queue, cudaStream_t stream);
-void launch_batch_log_warp(const DkiBatchJob* jobs, const int64_t* first, int n_jobs, int n_max, int p,
+void launch_batch_log_warp(const DkiBatchJob* jobs, const int64_t* first, int n_jobs, int n_max, int p, int warps,
                            int64_t tickets, int weighted, int max_rw, double tol, int* queue,
                            const BatchViolators& violators, cudaStream_t stream);
 size_t batch_refit_slot_doubles(int n_max, int p, int m_max);

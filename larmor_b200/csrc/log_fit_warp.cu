@@ -86,12 +86,13 @@ struct WarpSmem {
 };
 
 template <class T>
-__device__ __forceinline__ WarpSmem<T> carve_warp(unsigned char* smem_raw, const WarpLayout<T>& lay, int warp) {
+__device__ __forceinline__ WarpSmem<T> carve_warp(unsigned char* smem_raw, const WarpLayout<T>& lay, int warps,
+                                                  int warp) {
     WarpSmem<T> w;
     T* base = reinterpret_cast<T*>(smem_raw);
     w.xs = base;
     w.pinvt = base + size_t(lay.n) * lay.px;
-    w.ea = reinterpret_cast<uint8_t*>(base + lay.design_elems() + kWarps * lay.warp_elems());
+    w.ea = reinterpret_cast<uint8_t*>(base + lay.design_elems() + warps * lay.warp_elems());
     w.eb = w.ea + lay.pp;
     w.ys = base + lay.design_elems() + warp * lay.warp_elems();
     w.ws = w.ys + lay.n;
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(kWarps * 32) fit_log_warp_kernel(
     const int p = d.p;
     const WarpLayout<T> lay{d.n, p, p | 1, p * (p + 1) / 2};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const WarpSmem<T> w = carve_warp<T>(smem_raw, lay, warp);
+    const WarpSmem<T> w = carve_warp<T>(smem_raw, lay, kWarps, warp);
     stage_warp_design<T>(d, lay, w);
     __syncthreads();
     for (int64_t voxel = int64_t(blockIdx.x) * kWarps + warp; voxel < v;
@@ -283,11 +284,14 @@ __global__ void __launch_bounds__(kWarps * 32) fit_log_warp_kernel(
     }
 }
 
-// The DKI family of a batch (batch.cuh): CTAs take tickets of kDkiBatchVoxels voxels of one
-// volume from a device counter across every DKI volume (each warp fits every kWarps-th voxel of
-// the ticket) and restage the design when the ticket moves to another volume. Violators go to
-// one list for the whole family, with their volume.
-__global__ void __launch_bounds__(kWarps * 32) batch_log_warp_kernel(
+// The DKI family of a batch (batch.cuh): CTAs of WARPS warps take tickets of
+// kDkiVoxelsPerWarp * WARPS voxels of one volume from a device counter across every DKI volume
+// (each warp fits every WARPS-th voxel of the ticket) and restage the design when the ticket
+// moves to another volume. The shared memory is sized for the family's largest table, so the
+// CTAs are wider than the single-volume fit's: more warps share one staged design. Violators go
+// to one list for the whole family, with their volume.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) batch_log_warp_kernel(
     const DkiBatchJob* __restrict__ jobs, const int64_t* __restrict__ first, int n_jobs, int weighted,
     int max_rw, double tol, int* __restrict__ queue, BatchViolators violators) {
     using T = double;
@@ -309,15 +313,15 @@ __global__ void __launch_bounds__(kWarps * 32) batch_log_warp_kernel(
         if (j != cur) {
             const int p = d.p;
             lay = WarpLayout<T>{d.n, p, p | 1, p * (p + 1) / 2};
-            w = carve_warp<T>(smem_raw, lay, warp);
+            w = carve_warp<T>(smem_raw, lay, WARPS, warp);
             stage_warp_design<T>(d, lay, w);
             cur = j;
         }
         __syncthreads();
         const CappedSource src{job.s, job.s0, job.floor, job.is_b0, d.n};
-        const int64_t v = job.v, block_first = (t - first[j]) * kDkiBatchVoxels;
+        const int64_t v = job.v, block_first = (t - first[j]) * (kDkiVoxelsPerWarp * WARPS);
         const int p = d.p;
-        for (int k = warp; k < kDkiBatchVoxels; k += kWarps) {
+        for (int k = warp; k < kDkiVoxelsPerWarp * WARPS; k += WARPS) {
             const int64_t voxel = block_first + k;
             if (voxel >= v) break;
             bool violated = false;
@@ -382,28 +386,49 @@ void launch_log_warp(const LogDesignDevice<T>& d, const CappedSource& src, int64
                                       stream);
 }
 
-size_t batch_log_warp_smem(int n_max, int p) {
-    return WarpLayout<double>{n_max, p, p | 1, p * (p + 1) / 2}.bytes(kWarps);
+size_t batch_log_warp_smem(int n_max, int p, int warps) {
+    return WarpLayout<double>{n_max, p, p | 1, p * (p + 1) / 2}.bytes(warps);
 }
 
-void launch_batch_log_warp(const DkiBatchJob* jobs, const int64_t* first, int n_jobs, int n_max, int p,
-                           int64_t tickets, int weighted, int max_rw, double tol, int* queue,
-                           const BatchViolators& violators, cudaStream_t stream) {
-    if (n_jobs == 0 || tickets == 0) return;
-    const size_t smem = batch_log_warp_smem(n_max, p);
-    require(smem <= 227 * 1024, "the design is too large for the shared-memory log fit");
-    auto kernel = batch_log_warp_kernel;
+int batch_log_warp_warps(int n_max, int p) {
+    for (int warps : {12, 8, 4})
+        if (batch_log_warp_smem(n_max, p, warps) <= 227 * 1024) return warps;
+    return 0;
+}
+
+template <int WARPS>
+void launch_batch_log_warp_impl(const DkiBatchJob* jobs, const int64_t* first, int n_jobs, size_t smem,
+                                int64_t tickets, int weighted, int max_rw, double tol, int* queue,
+                                const BatchViolators& violators, cudaStream_t stream) {
+    auto kernel = batch_log_warp_kernel<WARPS>;
     cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                "cudaFuncSetAttribute");
     int per_sm = 0;
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kWarps * 32, smem),
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, WARPS * 32, smem),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     const int64_t grid = std::min<int64_t>(tickets, int64_t(sm_count()) * std::max(per_sm, 1));
     cuda_check(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), stream), "cudaMemsetAsync");
     LaunchScope scope("batch_log_warp_kernel", stream);
-    kernel<<<unsigned(grid), kWarps * 32, smem, stream>>>(jobs, first, n_jobs, weighted, max_rw, tol, queue,
-                                                          violators);
+    kernel<<<unsigned(grid), WARPS * 32, smem, stream>>>(jobs, first, n_jobs, weighted, max_rw, tol, queue,
+                                                         violators);
     cuda_check(cudaGetLastError(), "batch_log_warp_kernel launch");
+}
+
+void launch_batch_log_warp(const DkiBatchJob* jobs, const int64_t* first, int n_jobs, int n_max, int p, int warps,
+                           int64_t tickets, int weighted, int max_rw, double tol, int* queue,
+                           const BatchViolators& violators, cudaStream_t stream) {
+    if (n_jobs == 0 || tickets == 0) return;
+    const size_t smem = batch_log_warp_smem(n_max, p, warps);
+    require(smem <= 227 * 1024, "the design is too large for the shared-memory log fit");
+    if (warps == 12)
+        launch_batch_log_warp_impl<12>(jobs, first, n_jobs, smem, tickets, weighted, max_rw, tol, queue, violators,
+                                       stream);
+    else if (warps == 8)
+        launch_batch_log_warp_impl<8>(jobs, first, n_jobs, smem, tickets, weighted, max_rw, tol, queue, violators,
+                                      stream);
+    else
+        launch_batch_log_warp_impl<4>(jobs, first, n_jobs, smem, tickets, weighted, max_rw, tol, queue, violators,
+                                      stream);
 }
 
 template void launch_log_warp<double>(const LogDesignDevice<double>&, const LogSource&, int64_t, int, int, double,
