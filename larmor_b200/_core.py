@@ -100,8 +100,13 @@ class _Transfers:
     def upload(self, torch, a: np.ndarray, dev):
         """A new C-contiguous device tensor with the contents of the host array a."""
         out = torch.empty(a.shape, dtype=getattr(torch, a.dtype.name), device=dev)
+        return self.upload_into(torch, a, out)
+
+    def upload_into(self, torch, a: np.ndarray, out):
+        """Copies the host array a into the contiguous device tensor out of the same size, on the
+        current stream; returns out."""
         if a.nbytes < (1 << 20):
-            out.copy_(torch.from_numpy(a))
+            out.copy_(torch.from_numpy(np.ascontiguousarray(a)))
             return out
         with self.lock:
             return self._upload(torch, a, out)
@@ -125,8 +130,12 @@ class _Transfers:
         """A new numpy array with the contents of the device tensor t (waits for t's stream)."""
         t = t.contiguous()
         out = np.empty(tuple(t.shape), dtype=np.dtype(str(t.dtype).replace("torch.", "")))
-        nbytes = out.nbytes
-        if nbytes < (1 << 20):
+        return self.download_into(torch, t, out)
+
+    def download_into(self, torch, t, out: np.ndarray) -> np.ndarray:
+        """Copies the contiguous device tensor t into the C-contiguous host array out of the same
+        size, through the current stream (waits for the copies); returns out."""
+        if out.nbytes < (1 << 20):
             out[...] = t.cpu().numpy()
             return out
         with self.lock:
@@ -548,9 +557,61 @@ def fit_multi_tissue(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, 
     _require_threads(n_threads)
     if max_outer < 0:
         raise ValueError("max_outer must be at least 0")
+    if signals.shape[0] >= _PIECES * _PIECE_MIN:
+        return _fit_multi_tissue_pipelined(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol,
+                                           final_tol_x)
     fods, fractions = _fit_multi_tissue_on_device(signals, weights, lr, lr_solver, hr, hr_solver, max_outer,
                                                   fraction_tol, final_tol_x)
     return _to_host(fods), _to_host(fractions)
+
+
+# The drop-in multi-tissue call cuts a large volume into this many pieces of voxels (each of at
+# least _PIECE_MIN), so that one piece's upload and another's download overlap a third's fit.
+_PIECES = 8
+_PIECE_MIN = 32768
+_copy_streams: dict = {}
+
+
+def _fit_multi_tissue_pipelined(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol,
+                                final_tol_x):
+    """fit_multi_tissue of checked host arrays, piece by piece: a piece's signals go up on one
+    copy stream while the previous piece is fitted on the caller's stream (every round enqueued
+    with its count read on the device, so the host never waits on a fit), and the results come
+    down on a second copy stream once their piece is fitted. Each voxel's fit depends on its own
+    signals only, so the results equal one call over the whole array."""
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    v, m = signals.shape
+    nf = hr.nb + hr.ci
+    fods = np.empty((v, hr.ca), dtype=np.float64)
+    fractions = np.empty((v, nf), dtype=np.float64)
+    d_sig = torch.empty((v, m), dtype=torch.float64, device=dev)
+    d_fods = torch.empty((v, hr.ca), dtype=torch.float64, device=dev)
+    d_fr = torch.empty((v, nf), dtype=torch.float64, device=dev)
+    if dev.index not in _copy_streams:
+        _copy_streams[dev.index] = (torch.cuda.Stream(dev), torch.cuda.Stream(dev))
+    up, down = _copy_streams[dev.index]
+    compute = torch.cuda.current_stream(dev)
+    step = -(-v // _PIECES)
+    pieces = [(a, min(a + step, v)) for a in range(0, v, step)]
+    fitted = []
+    up.wait_stream(compute)  # the device arrays were allocated on the caller's stream
+    for a, b in pieces:
+        with torch.cuda.stream(up):
+            _transfers.upload_into(torch, signals[a:b], d_sig[a:b])
+        compute.wait_stream(up)
+        fit_multi_tissue_device(d_sig[a:b], weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol,
+                                final_tol_x, d_fods[a:b], d_fr[a:b], asynchronous=True)
+        done = torch.cuda.Event()
+        done.record(compute)
+        fitted.append(done)
+    for (a, b), done in zip(pieces, fitted):
+        down.wait_event(done)
+        with torch.cuda.stream(down):
+            _transfers.download_into(torch, d_fods[a:b], fods[a:b])
+            _transfers.download_into(torch, d_fr[a:b], fractions[a:b])
+    compute.wait_stream(down)
+    return fods, fractions
 
 
 def _fit_multi_tissue_on_device(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, fraction_tol,

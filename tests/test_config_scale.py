@@ -153,6 +153,11 @@ def test_mfod_config3_matches_the_oracle_on_a_strided_sample(cuda, oracle):
     np.testing.assert_array_equal(got != 0, ref != 0)
     assert rel.max() <= 1e-9
     assert np.abs(got_fr - ref_fr).max() <= 1e-10
+    # The drop-in call with host arrays (fitted in pieces that overlap their copies) gives the
+    # device call's results bit for bit.
+    host_fods, host_fr = _core.fit_multi_tissue(norm, lr.weights, k_lr, lr_solver, k_hr, hr_solver, 50, 1e-7, 1e-2, 1)
+    np.testing.assert_array_equal(host_fods, fods.cpu().numpy())
+    np.testing.assert_array_equal(host_fr, fr.cpu().numpy())
 
 
 def test_msmt_config3_matches_the_oracle_on_a_strided_sample(cuda, oracle):
