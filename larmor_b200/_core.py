@@ -567,7 +567,7 @@ def fit_multi_tissue(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, 
 
 # The drop-in multi-tissue call cuts a large volume into this many pieces of voxels (each of at
 # least _PIECE_MIN), so that one piece's upload and another's download overlap a third's fit.
-_PIECES = 8
+_PIECES = 4
 _PIECE_MIN = 32768
 _copy_streams: dict = {}
 
