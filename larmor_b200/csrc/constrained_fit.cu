@@ -45,9 +45,12 @@ constexpr double kFeasibilityMargin = 1e-12;
 constexpr int kInnerStepsPerConstraint = 50;
 constexpr double kConstraintTolerance = 1e-9;
 
+// Whether the column sums' substitutions (31 x 32 doubles) fit in the QR's rows below R.
+__host__ __device__ inline bool refit_ysub_aliased(int n, int p) { return size_t(n - p) * p >= 31 * 32; }
+
 // A warp's shared-memory doubles (see refit_violator).
 __host__ __device__ inline size_t refit_smem_doubles(int n, int p) {
-    return size_t(n) * p + 2 * size_t(n) + size_t(p + 1) * kSmemActive;
+    return size_t(n) * p + 2 * size_t(n) + size_t(p + 1) * kSmemActive + (refit_ysub_aliased(n, p) ? 0 : 31 * 32);
 }
 
 __device__ __forceinline__ double wsum(double v) { return warp_sum(v); }
@@ -150,26 +153,13 @@ __device__ int implicit_nnls(const ImplicitSystem& sys, const double* d, double 
         // increasing order: the first on a tie).
         double bv = 0.0;
         int bi = -1;
-        // Two columns per pass, so that both columns' loads are in flight together.
-        for (int c0 = lane; c0 < m; c0 += 64) {
-            const int c1 = c0 + 32;
-            const bool has1 = c1 < m;
-            double w0 = 0.0, w1 = 0.0;
-#pragma unroll 4
-            for (int a = 0; a < p; ++a) {
-                const double ta = t[a];
-                const double g0 = sys.gt[size_t(a) * m + c0];
-                const double g1 = has1 ? sys.gt[size_t(a) * m + c1] : 0.0;
-                w0 += g0 * ta;
-                w1 += g1 * ta;
-            }
-            if (!s.flag[c0] && (bi < 0 || w0 > bv)) {
-                bv = w0;
-                bi = c0;
-            }
-            if (has1 && !s.flag[c1] && (bi < 0 || w1 > bv)) {
-                bv = w1;
-                bi = c1;
+        for (int c = lane; c < m; c += 32) {
+            if (s.flag[c]) continue;
+            double w = 0.0;
+            for (int a = 0; a < p; ++a) w += sys.gt[size_t(a) * m + c] * t[a];
+            if (bi < 0 || w > bv) {
+                bv = w;
+                bi = c;
             }
         }
         const int e = warp_argmax_first(bv, bi);
@@ -247,11 +237,13 @@ __device__ __forceinline__ void refit_violator(const LogDesignDevice<double>& d,
                                                double* wsm, double* out, int lane) {
     const int n = d.n, p = d.p, m = d.m, rows = p + 1;
     // Shared memory (refit_smem_doubles): the weighted design and its QR, the signals, the root
-    // weights and the NNLS fits' QR of up to kSmemActive columns.
+    // weights, the NNLS fits' QR of up to kSmemActive columns, and the column sums' forward
+    // substitutions (in the rows of the QR below R, which are dead by then, when they fit).
     double* qr = wsm;                           // (n, p) row-major
     double* ys = qr + size_t(n) * p;            // (n,) log signals, then weighted
     double* rw = ys + n;                        // (n,) root weights
     double* ssub = rw + n;                      // (kSmemActive, rows)
+    double* ysub = refit_ysub_aliased(n, p) ? qr + size_t(p) * p : ssub + size_t(rows) * kSmemActive;
     // The warp's global slot (constrained_slot_doubles): the NNLS system's formed columns, the
     // QR of more than kSmemActive active columns, the NNLS vectors and flags.
     double* cache = slot;                       // (m, rows): column c of C at cache[c * rows]
@@ -369,32 +361,24 @@ __device__ __forceinline__ void refit_violator(const LogDesignDevice<double>& d,
     }
     __syncwarp();
     // The NNLS tolerance 10 eps norm1(C) max(p + 1, m) needs every column's absolute sum:
-    // sum_i |(R^-T g_c)_i| + |g_c p_free|. Lanes over constraints; the columns themselves are
-    // not kept.
+    // sum_i |(R^-T g_c)_i| + |g_c p_free|. Lanes over constraints, each substitution's
+    // entries in the warp's shared column of ysub; the columns themselves are not kept.
     double colsum_max = 0.0;
     for (int c = lane; c < m; c += 32) {
-        // The constraint's row in registers first (its loads in flight together), then the
-        // substitution in registers, fully unrolled (p <= 31); R is a shared-memory broadcast.
         const double* gc = d.g + size_t(c) * p;
-        double g[31], y[31];
-#pragma unroll
-        for (int i = 0; i < 31; ++i) g[i] = i < p ? gc[i] : 0.0;
         double acc_abs = 0.0, gf = 0.0;
-#pragma unroll
-        for (int i = 0; i < 31; ++i) {
-            if (i < p) {
-                // Even k into s0, odd k into s1, each in increasing k.
-                double s0 = g[i], s1 = 0.0;
-#pragma unroll
-                for (int k = 0; k < i; ++k) {
-                    if (k & 1) s1 -= qr[size_t(k) * p + i] * y[k];
-                    else s0 -= qr[size_t(k) * p + i] * y[k];
-                }
-                const double si = (s0 + s1) / qr[size_t(i) * p + i];
-                y[i] = si;
-                acc_abs += fabs(si);
-                gf += g[i] * pfree[i];
+        for (int i = 0; i < p; ++i) {
+            double s0 = gc[i], s1 = 0.0;
+            int k = 0;
+            for (; k + 1 < i; k += 2) {
+                s0 -= qr[size_t(k) * p + i] * ysub[k * 32 + lane];
+                s1 -= qr[size_t(k + 1) * p + i] * ysub[(k + 1) * 32 + lane];
             }
+            if (k < i) s0 -= qr[size_t(k) * p + i] * ysub[k * 32 + lane];
+            const double si = (s0 + s1) / qr[size_t(i) * p + i];
+            ysub[i * 32 + lane] = si;
+            acc_abs += fabs(si);
+            gf += gc[i] * pfree[i];
         }
         acc_abs += fabs(gf);
         colsum_max = fmax(colsum_max, acc_abs);
@@ -459,10 +443,9 @@ __device__ __forceinline__ void refit_violator(const LogDesignDevice<double>& d,
     __syncwarp();
 }
 
-// One warp per CTA: the warp's state takes a large share of an SM's shared memory (and up to 255
-// registers, which the fully unrolled column sums use).
+// One warp per CTA: the warp's state takes most of an SM's shared memory share.
 template <class Src>
-__global__ void __maxnreg__(255) constrained_fit_kernel(LogDesignDevice<double> d, Src src, int weighted,
+__global__ void __launch_bounds__(32) constrained_fit_kernel(LogDesignDevice<double> d, Src src, int weighted,
                                                              ViolatorList<double> list, int* queue,
                                                              double* __restrict__ workspace, size_t slot_doubles,
                                                              double* __restrict__ params) {
@@ -486,7 +469,7 @@ __global__ void __maxnreg__(255) constrained_fit_kernel(LogDesignDevice<double> 
 // The DKI family of a batch (batch.cuh): warps take the violators of every DKI volume from one
 // list, each with its volume's design, signals and outputs (shared memory sized for the
 // family's largest table).
-__global__ void __maxnreg__(255) batch_refit_kernel(const DkiBatchJob* __restrict__ jobs, BatchViolators list,
+__global__ void __launch_bounds__(32) batch_refit_kernel(const DkiBatchJob* __restrict__ jobs, BatchViolators list,
                                                          int weighted, int* queue, double* __restrict__ workspace,
                                                          size_t slot_doubles) {
     __shared__ WarpShared sh;
