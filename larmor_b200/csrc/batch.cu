@@ -78,7 +78,7 @@ struct lar_batch_s {
     BatchViolators violators;
     double* refit_slots = nullptr;
     int refit_nslots = 0;
-    size_t refit_slot_doubles = 0, refit_smem = 0;
+    size_t refit_slot_doubles = 0;
     // mFOD
     std::unique_ptr<MfodBatch, void (*)(MfodBatch*)> mfod{nullptr, mfod_batch_destroy};
     // Device scratch: counters, then the violator list and the re-fit slots.
@@ -186,9 +186,8 @@ int lar_batch_finalize(lar_batch batch) {
             viol_bytes = (size_t(dki_voxels) * (sizeof(int) + sizeof(int64_t) + 22 * sizeof(double)) + 255) / 256 * 256;
             if (b.dki_mmax > 0) {
                 b.refit_slot_doubles = batch_refit_slot_doubles(b.dki_nmax, 22, b.dki_mmax);
-                // Shared memory for every table of the family (its layout depends on n).
-                for (const auto& j : b.dki) b.refit_smem = std::max(b.refit_smem, batch_refit_smem_bytes(j.d.n, 22));
-                b.refit_nslots = int(std::max<int64_t>(1, std::min<int64_t>(dki_voxels, batch_refit_slots(b.refit_smem))));
+                b.refit_nslots = int(std::max<int64_t>(4, std::min<int64_t>((dki_voxels + 3) / 4 * 4,
+                                                                            batch_refit_slots())));
                 slot_bytes = size_t(b.refit_nslots) * b.refit_slot_doubles * sizeof(double);
             }
         }
@@ -231,7 +230,7 @@ int lar_batch_run(lar_batch batch, int families, void* stream) {
                                   b.counters + 2, b.violators, st);
             if (b.dki_mmax > 0)
                 launch_batch_refit(b.d_dki.ptr, b.violators, b.dki_fit.weighted, b.counters + 5, b.refit_slots,
-                                   b.refit_nslots, b.refit_slot_doubles, b.refit_smem, st);
+                                   b.refit_nslots, b.refit_slot_doubles, st);
             launch_batch_dki_maps(b.d_dki.ptr, b.dki_maps_first.ptr, int(b.dki.size()), b.dki_maps_tickets, st);
         }
         if ((families & LAR_BATCH_MFOD) && b.mfod) mfod_batch_run(b.mfod.get(), st);

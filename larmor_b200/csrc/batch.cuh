@@ -85,10 +85,9 @@ void launch_batch_log_warp(const DkiBatchJob* jobs, const int64_t* first, int n_
                            int64_t tickets, int weighted, int max_rw, double tol, int* queue,
                            const BatchViolators& violators, cudaStream_t stream);
 size_t batch_refit_slot_doubles(int n_max, int p, int m_max);
-size_t batch_refit_smem_bytes(int n, int p);
-int batch_refit_slots(size_t smem_bytes);
+int batch_refit_slots();
 void launch_batch_refit(const DkiBatchJob* jobs, const BatchViolators& violators, int weighted, int* queue,
-                        double* workspace, int slots, size_t slot_doubles, size_t smem_bytes, cudaStream_t stream);
+                        double* workspace, int slots, size_t slot_doubles, cudaStream_t stream);
 void launch_batch_dki_maps(const DkiBatchJob* jobs, const int64_t* first, int n_jobs, int64_t tickets,
                            cudaStream_t stream);
 

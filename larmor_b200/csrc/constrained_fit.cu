@@ -39,19 +39,11 @@ namespace lar {
 
 namespace {
 
-constexpr int kSmemActive = 32;  // active columns whose QR fits of the NNLS run in shared memory
+constexpr int kCWarps = 4;
 constexpr double kEps = kEps64;
 constexpr double kFeasibilityMargin = 1e-12;
 constexpr int kInnerStepsPerConstraint = 50;
 constexpr double kConstraintTolerance = 1e-9;
-
-// Whether the column sums' substitutions (31 x 32 doubles) fit in the QR's rows below R.
-__host__ __device__ inline bool refit_ysub_aliased(int n, int p) { return size_t(n - p) * p >= 31 * 32; }
-
-// A warp's shared-memory doubles (see refit_violator).
-__host__ __device__ inline size_t refit_smem_doubles(int n, int p) {
-    return size_t(n) * p + 2 * size_t(n) + size_t(p + 1) * kSmemActive + (refit_ysub_aliased(n, p) ? 0 : 31 * 32);
-}
 
 __device__ __forceinline__ double wsum(double v) { return warp_sum(v); }
 __device__ __forceinline__ double wmax(double v) { return warp_max(v); }
@@ -62,6 +54,7 @@ struct WarpShared {
     double tau[32];     // reflectors of the weighted design
     double qtau[kMaxActive], qnu[kMaxActive], qnd[kMaxActive], rv[32], res[32];
     double t[32];       // R^-1 r[:p] - r[p] p_free of the gradient
+    double ysub[31 * 32];  // one forward substitution per lane, entry i at [i * 32 + lane]
     int qperm[kMaxActive];
     int act[kMaxActive];
     int n_act;
@@ -112,15 +105,9 @@ struct CachedColumns {
 // C's gradient C^T (d - C u) = G t and the active columns from the cache. Returns 1 when the
 // method ended by its rule, 0 when the inner-step limit ran out, -1 past acap active columns.
 __device__ int implicit_nnls(const ImplicitSystem& sys, const double* d, double tol, int max_inner, NnlsScratch s,
-                             double* t, double* ssub, int lane) {
+                             double* t, int lane) {
     const int m = sys.m, p = sys.p, rows = p + 1;
     const CachedColumns cols{sys.cache, rows};
-    // The active columns' QR in shared memory (ssub) while at most kSmemActive are active.
-    auto fit = [&]() {
-        QrScratch q = s.qr;
-        if (*s.n_act <= kSmemActive) q.sub = ssub;
-        warp_qr_least_squares_cols(cols, rows, s.act, *s.n_act, d, q, s.z, lane);
-    };
     for (int j = lane; j < m; j += 32) {
         s.u[j] = 0.0;
         s.z[j] = 0.0;
@@ -178,7 +165,7 @@ __device__ int implicit_nnls(const ImplicitSystem& sys, const double* d, double 
             s.flag[e] = 1;
         }
         __syncwarp();
-        fit();
+        warp_qr_least_squares_cols(cols, rows, s.act, *s.n_act, d, s.qr, s.z, lane);
         for (;;) {
             const int n2 = *s.n_act;
             bool any = false;
@@ -222,7 +209,7 @@ __device__ int implicit_nnls(const ImplicitSystem& sys, const double* d, double 
                 *s.n_act = w;
             }
             __syncwarp();
-            fit();
+            warp_qr_least_squares_cols(cols, rows, s.act, *s.n_act, d, s.qr, s.z, lane);
         }
         for (int j = lane; j < m; j += 32) s.u[j] = s.flag[j] ? s.z[j] : 0.0;
         __syncwarp();
@@ -234,24 +221,17 @@ __device__ int implicit_nnls(const ImplicitSystem& sys, const double* d, double 
 template <class Src>
 __device__ __forceinline__ void refit_violator(const LogDesignDevice<double>& d, const Src& src, int weighted,
                                                int64_t voxel, const double* pin, double* slot, WarpShared& sh,
-                                               double* wsm, double* out, int lane) {
+                                               double* out, int lane) {
     const int n = d.n, p = d.p, m = d.m, rows = p + 1;
-    // Shared memory (refit_smem_doubles): the weighted design and its QR, the signals, the root
-    // weights, the NNLS fits' QR of up to kSmemActive columns, and the column sums' forward
-    // substitutions (in the rows of the QR below R, which are dead by then, when they fit).
-    double* qr = wsm;                           // (n, p) row-major
-    double* ys = qr + size_t(n) * p;            // (n,) log signals, then weighted
-    double* rw = ys + n;                        // (n,) root weights
-    double* ssub = rw + n;                      // (kSmemActive, rows)
-    double* ysub = refit_ysub_aliased(n, p) ? qr + size_t(p) * p : ssub + size_t(rows) * kSmemActive;
-    // The warp's global slot (constrained_slot_doubles): the NNLS system's formed columns, the
-    // QR of more than kSmemActive active columns, the NNLS vectors and flags.
-    double* cache = slot;                       // (m, rows): column c of C at cache[c * rows]
+    double* qr = slot;                          // (n, p) row-major
+    double* cache = qr + size_t(n) * p;         // (m, rows): column c of C at cache[c * rows]
     double* sub = cache + size_t(rows) * m;     // (kMaxActive, rows) QR of the active columns
     double* u = sub + size_t(rows) * kMaxActive;  // (m,)
     double* z = u + m;                          // (m,)
-    uint8_t* flag = reinterpret_cast<uint8_t*>(z + m);  // (m,) active flags
-    uint8_t* ready = flag + m;                          // (m,) whether cache holds column c
+    double* ys = z + m;                         // (n,) log signals, then weighted
+    double* rw = ys + n;                        // (n,) root weights
+    uint8_t* flag = reinterpret_cast<uint8_t*>(rw + n);  // (m,) active flags
+    uint8_t* ready = flag + m;                           // (m,) whether cache holds column c
     double* pu = sh.vec[0];
     if (lane < p) pu[lane] = pin[lane];
     src.template warp_stage<double>(voxel, ys, lane);
@@ -364,6 +344,7 @@ __device__ __forceinline__ void refit_violator(const LogDesignDevice<double>& d,
     // sum_i |(R^-T g_c)_i| + |g_c p_free|. Lanes over constraints, each substitution's
     // entries in the warp's shared column of ysub; the columns themselves are not kept.
     double colsum_max = 0.0;
+    double* ysub = sh.ysub;
     for (int c = lane; c < m; c += 32) {
         const double* gc = d.g + size_t(c) * p;
         double acc_abs = 0.0, gf = 0.0;
@@ -394,7 +375,7 @@ __device__ __forceinline__ void refit_violator(const LogDesignDevice<double>& d,
     const ImplicitSystem sys{d.g, d.gt, qr, pfree, cache, ready, p, m};
     NnlsScratch ns{u, z, flag, sh.act, &sh.n_act, sh.res,
                    QrScratch{sub, sh.qtau, sh.qnu, sh.qnd, sh.qperm, sh.rv}, kMaxActive};
-    const int outcome = implicit_nnls(sys, unit, tol, kInnerStepsPerConstraint * m, ns, sh.t, ssub, lane);
+    const int outcome = implicit_nnls(sys, unit, tol, kInnerStepsPerConstraint * m, ns, sh.t, lane);
     if (outcome != 1) return;
     double* res = sh.vec[2];
     // Residual C u - e_p over the active columns (u is zero elsewhere).
@@ -443,17 +424,16 @@ __device__ __forceinline__ void refit_violator(const LogDesignDevice<double>& d,
     __syncwarp();
 }
 
-// One warp per CTA: the warp's state takes most of an SM's shared memory share.
 template <class Src>
-__global__ void __launch_bounds__(32) constrained_fit_kernel(LogDesignDevice<double> d, Src src, int weighted,
-                                                             ViolatorList<double> list, int* queue,
-                                                             double* __restrict__ workspace, size_t slot_doubles,
-                                                             double* __restrict__ params) {
-    __shared__ WarpShared sh;
-    extern __shared__ __align__(16) double wsm[];
-    const int lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(kCWarps * 32, 4) constrained_fit_kernel(
+    LogDesignDevice<double> d, Src src, int weighted, ViolatorList<double> list, int* queue,
+    double* __restrict__ workspace, size_t slot_doubles, double* __restrict__ params) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WarpShared* shared = reinterpret_cast<WarpShared*>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpShared& sh = shared[warp];
     const int p = d.p;
-    double* slot = workspace + size_t(blockIdx.x) * slot_doubles;
+    double* slot = workspace + (size_t(blockIdx.x) * kCWarps + warp) * slot_doubles;
     const int total = min(*list.count, list.capacity);
     for (;;) {
         int idx = 0;
@@ -461,21 +441,21 @@ __global__ void __launch_bounds__(32) constrained_fit_kernel(LogDesignDevice<dou
         idx = __shfl_sync(0xffffffffu, idx, 0);
         if (idx >= total) break;
         const int64_t voxel = list.voxel[idx];
-        refit_violator<Src>(d, src, weighted, voxel, list.params + size_t(idx) * p, slot, sh, wsm,
-                            params + voxel * p, lane);
+        refit_violator<Src>(d, src, weighted, voxel, list.params + size_t(idx) * p, slot, sh, params + voxel * p,
+                            lane);
     }
 }
 
 // The DKI family of a batch (batch.cuh): warps take the violators of every DKI volume from one
-// list, each with its volume's design, signals and outputs (shared memory sized for the
-// family's largest table).
-__global__ void __launch_bounds__(32) batch_refit_kernel(const DkiBatchJob* __restrict__ jobs, BatchViolators list,
-                                                         int weighted, int* queue, double* __restrict__ workspace,
-                                                         size_t slot_doubles) {
-    __shared__ WarpShared sh;
-    extern __shared__ __align__(16) double wsm[];
-    const int lane = threadIdx.x & 31;
-    double* slot = workspace + size_t(blockIdx.x) * slot_doubles;
+// list, each with its volume's design, signals and outputs.
+__global__ void __launch_bounds__(kCWarps * 32, 4) batch_refit_kernel(
+    const DkiBatchJob* __restrict__ jobs, BatchViolators list, int weighted, int* queue,
+    double* __restrict__ workspace, size_t slot_doubles) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WarpShared* shared = reinterpret_cast<WarpShared*>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpShared& sh = shared[warp];
+    double* slot = workspace + (size_t(blockIdx.x) * kCWarps + warp) * slot_doubles;
     const int total = min(*list.count, list.capacity);
     for (;;) {
         int idx = 0;
@@ -486,53 +466,45 @@ __global__ void __launch_bounds__(32) batch_refit_kernel(const DkiBatchJob* __re
         const LogDesignDevice<double> d = job.d;
         const CappedSource src{job.s, job.s0, job.floor, job.is_b0, d.n};
         const int64_t voxel = list.voxel[idx];
-        refit_violator<CappedSource>(d, src, weighted, voxel, list.params + size_t(idx) * d.p, slot, sh, wsm,
+        refit_violator<CappedSource>(d, src, weighted, voxel, list.params + size_t(idx) * d.p, slot, sh,
                                      job.params + voxel * d.p, lane);
     }
 }
 
 }  // namespace
 
-// The re-fit's dynamic shared memory for designs of n measurements and p parameters.
-size_t constrained_smem_bytes(int n, int p) { return refit_smem_doubles(n, p) * sizeof(double); }
+constexpr size_t kCSmem = kCWarps * sizeof(WarpShared);
 
-template <class Kernel>
-void allow_refit_smem(Kernel kernel, size_t bytes) {
-    require(bytes + sizeof(WarpShared) <= 227 * 1024,
-            "the constrained re-fit keeps the weighted design in shared memory: at most about 1000 "
-            "measurements x 22 parameters");
-    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)),
+template <class Src>
+void allow_smem() {
+    static_assert(kCSmem <= 200 * 1024, "the re-fit's shared state outgrows an SM");
+    cuda_check(cudaFuncSetAttribute(constrained_fit_kernel<Src>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(kCSmem)),
                "cudaFuncSetAttribute");
 }
 
-int constrained_resident_warps(int n, int p) {
-    const size_t bytes = constrained_smem_bytes(n, p);
-    allow_refit_smem(constrained_fit_kernel<CappedSource>, bytes);
+int constrained_resident_warps() {
     int per_sm = 0;
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, constrained_fit_kernel<CappedSource>, 32, bytes),
+    allow_smem<CappedSource>();
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, constrained_fit_kernel<CappedSource>,
+                                                             kCWarps * 32, kCSmem),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    return sm_count() * ctas_per_sm(per_sm, "dki.refit.ctas_per_sm");
+    return sm_count() * ctas_per_sm(per_sm, "dki.refit.ctas_per_sm") * kCWarps;
 }
 
-size_t batch_refit_slot_doubles(int /*n_max*/, int p, int m_max) { return constrained_slot_doubles(0, p, m_max); }
+size_t batch_refit_slot_doubles(int n_max, int p, int m_max) { return constrained_slot_doubles(n_max, p, m_max); }
 
-size_t batch_refit_smem_bytes(int n, int p) { return constrained_smem_bytes(n, p); }
-
-int batch_refit_slots(size_t smem_bytes) {
-    allow_refit_smem(batch_refit_kernel, smem_bytes);
-    int per_sm = 0;
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_refit_kernel, 32, smem_bytes),
-               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    return sm_count() * ctas_per_sm(per_sm, "dki.refit.ctas_per_sm");
-}
+int batch_refit_slots() { return constrained_resident_warps(); }
 
 void launch_batch_refit(const DkiBatchJob* jobs, const BatchViolators& violators, int weighted, int* queue,
-                        double* workspace, int slots, size_t slot_doubles, size_t smem_bytes, cudaStream_t stream) {
-    allow_refit_smem(batch_refit_kernel, smem_bytes);
+                        double* workspace, int slots, size_t slot_doubles, cudaStream_t stream) {
+    const int blocks = std::max(1, slots / kCWarps);
+    cuda_check(cudaFuncSetAttribute(batch_refit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kCSmem)),
+               "cudaFuncSetAttribute");
     cuda_check(cudaMemsetAsync(queue, 0, sizeof(int), stream), "cudaMemsetAsync");
     LaunchScope scope("batch_refit_kernel", stream);
-    batch_refit_kernel<<<std::max(1, slots), 32, smem_bytes, stream>>>(jobs, violators, weighted, queue, workspace,
-                                                                       slot_doubles);
+    batch_refit_kernel<<<blocks, kCWarps * 32, kCSmem, stream>>>(jobs, violators, weighted, queue, workspace,
+                                                                 slot_doubles);
     cuda_check(cudaGetLastError(), "batch_refit_kernel launch");
 }
 
@@ -541,10 +513,10 @@ void launch_constrained(const LogDesignDevice<double>& d, const Src& src, int we
                         const ViolatorList<double>& list, int /*list_count_host_bound*/, int* queue,
                         double* workspace, int slots, double* params, cudaStream_t stream) {
     require(d.p + 1 <= 32, "the constrained fit takes at most 31 parameters");
-    const size_t bytes = constrained_smem_bytes(d.n, d.p);
-    allow_refit_smem(constrained_fit_kernel<Src>, bytes);
+    const int blocks = std::max(1, slots / kCWarps);
+    allow_smem<Src>();
     LaunchScope scope("constrained_fit_kernel", stream);
-    constrained_fit_kernel<Src><<<std::max(1, slots), 32, bytes, stream>>>(
+    constrained_fit_kernel<Src><<<blocks, kCWarps * 32, kCSmem, stream>>>(
         d, src, weighted, list, queue, workspace, constrained_slot_doubles(d.n, d.p, d.m), params);
     cuda_check(cudaGetLastError(), "constrained_fit_kernel launch");
 }

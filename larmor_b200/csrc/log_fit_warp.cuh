@@ -31,20 +31,18 @@ void launch_log_warp(const LogDesignDevice<T>& d, const CappedSource& src, int64
 // Largest number of active NNLS columns the constrained re-fit keeps in its QR workspace.
 constexpr int kMaxActive = 64;
 
-// Doubles of global workspace one warp of the constrained re-fit uses (the NNLS system's formed
-// columns, the QR of many active columns, the NNLS vectors and flags; the weighted design lives
-// in shared memory).
-inline size_t constrained_slot_doubles(int /*n*/, int p, int m) {
-    return size_t(p + 1) * m + size_t(p + 1) * kMaxActive + 2 * size_t(m) + (2 * size_t(m) + 7) / 8 + 64;
+// Doubles of global workspace one warp of the constrained re-fit uses.
+inline size_t constrained_slot_doubles(int n, int p, int m) {
+    return size_t(n) * p + size_t(p + 1) * m + size_t(p + 1) * kMaxActive + 2 * size_t(m) + 2 * size_t(n) +
+           (2 * size_t(m) + 7) / 8 + 64;
 }
 
 // Re-fits the violators of `list` subject to g p >= 0 (cpp/src/dwi/log_fit.cpp:170-216), in
 // FP64, writing the constrained parameters (divided by the column scales) over `params` where
 // the re-fit succeeds. `workspace` holds `slots` warp slots of constrained_slot_doubles()
 // doubles; `queue` is a device int the kernel uses as its work counter (zeroed by the caller).
-// The warps (one per CTA) of the constrained re-fit of designs of n measurements and p parameters
-// that fit on the GPU at once (its grid's size).
-int constrained_resident_warps(int n, int p);
+// The warps of the constrained re-fit that fit on the GPU at once (its grid's size).
+int constrained_resident_warps();
 
 template <class Src>
 void launch_constrained(const LogDesignDevice<double>& d, const Src& src, int weighted,
