@@ -565,9 +565,12 @@ def fit_multi_tissue(signals, weights, lr, lr_solver, hr, hr_solver, max_outer, 
     return _to_host(fods), _to_host(fractions)
 
 
-# The drop-in multi-tissue call cuts a large volume into this many pieces of voxels (each of at
-# least _PIECE_MIN), so that one piece's upload and another's download overlap a third's fit.
-_PIECES = 4
+# The drop-in multi-tissue call cuts a large volume into pieces of voxels (at least _PIECE_MIN
+# voxels in all per piece count), so that one piece's upload and another's download overlap a
+# third's fit: a small first piece (its upload is the wait before the first fit) and a smaller
+# last one (its download is the wait after the last fit).
+_PIECE_SHARES = (0.10, 0.30, 0.35, 0.25)
+_PIECES = len(_PIECE_SHARES)
 _PIECE_MIN = 32768
 _copy_streams: dict = {}
 
@@ -592,8 +595,10 @@ def _fit_multi_tissue_pipelined(signals, weights, lr, lr_solver, hr, hr_solver, 
         _copy_streams[dev.index] = (torch.cuda.Stream(dev), torch.cuda.Stream(dev))
     up, down = _copy_streams[dev.index]
     compute = torch.cuda.current_stream(dev)
-    step = -(-v // _PIECES)
-    pieces = [(a, min(a + step, v)) for a in range(0, v, step)]
+    ends = np.rint(np.cumsum(_PIECE_SHARES) * v).astype(np.int64)
+    ends[-1] = v
+    starts = np.concatenate([[0], ends[:-1]])
+    pieces = [(int(a), int(b)) for a, b in zip(starts, ends) if b > a]
     fitted = []
     up.wait_stream(compute)  # the device arrays were allocated on the caller's stream
     for a, b in pieces:
