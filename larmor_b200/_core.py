@@ -92,6 +92,19 @@ class _Transfers:
         for f in [self.pool.submit(np.copyto, dst[a:b], src[a:b]) for a, b in parts]:
             f.result()
 
+    def prefault(self, torch, arrays) -> None:
+        """Writes zeros over newly allocated host arrays on the copy threads, so that their pages
+        are mapped before the copies from the device need them (a first touch costs more than the
+        copy itself)."""
+        self._setup(torch)
+        jobs = []
+        for arr in arrays:
+            flat = arr.reshape(-1).view(np.uint8)
+            step = max(1 << 22, -(-len(flat) // self.THREADS))
+            jobs += [self.pool.submit(flat[a:a + step].fill, 0) for a in range(0, len(flat), step)]
+        for f in jobs:
+            f.result()
+
     def _wait(self, k: int) -> None:
         if self.events[k] is not None:
             self.events[k].synchronize()
@@ -610,6 +623,8 @@ def _fit_multi_tissue_pipelined(signals, weights, lr, lr_solver, hr, hr_solver, 
         done = torch.cuda.Event()
         done.record(compute)
         fitted.append(done)
+    # While the GPU fits, the output pages are mapped (fresh host memory faults on first touch).
+    _transfers.prefault(torch, (fods, fractions))
     for (a, b), done in zip(pieces, fitted):
         down.wait_event(done)
         with torch.cuda.stream(down):

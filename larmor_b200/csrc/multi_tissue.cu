@@ -93,6 +93,7 @@ __device__ __forceinline__ int64_t listed(const int* list, int64_t p) { return l
 // ---- correlations ----------------------------------------------------------------------
 
 constexpr int kCorrVoxels = 32;  // voxels per CTA tile
+constexpr int kCorrResidentCtas = 8;  // CTAs per SM of a correlation grid whose count is on the device
 constexpr int kCorrDepth = 16;   // measurements per shared-memory stage
 
 // corr(v, j) = sum_i K(i, j) signal(v, i), i increasing, for the listed voxels: 128 threads as
@@ -151,8 +152,9 @@ __device__ __forceinline__ void correlate_tile(const SignalDev& S, const int64_t
     }
 }
 
-// corr(v, j) = sum_i K(i, j) signal(v, i) for the listed voxels: a CTA per tile of kCorrVoxels
-// voxels x 16 RC columns.
+// corr(v, j) = sum_i K(i, j) signal(v, i) for the listed voxels: tiles of kCorrVoxels voxels x
+// 16 RC columns, a CTA's tiles strided by the grid (a round whose count lives on the device is
+// launched with a resident-sized grid, so an empty round costs little).
 template <int RC>
 __global__ void __launch_bounds__(128) correlate_kernel(SignalDev S, const int* __restrict__ list, int64_t count,
                                                         const int* __restrict__ count_dev,
@@ -160,12 +162,13 @@ __global__ void __launch_bounds__(128) correlate_kernel(SignalDev S, const int* 
                                                         double* __restrict__ corr, int ldc) {
     __shared__ int64_t vox[kCorrVoxels];
     const int tid = threadIdx.x;
-    const int64_t p0 = int64_t(blockIdx.x) * kCorrVoxels;
     if (count_dev) count = min(count, int64_t(*count_dev));
-    if (p0 >= count) return;
-    if (tid < kCorrVoxels) vox[tid] = p0 + tid < count ? listed(list, p0 + tid) : -1;
-    __syncthreads();
-    correlate_tile<RC>(S, vox, k, c, blockIdx.y * 16 * RC, corr, ldc);
+    for (int64_t p0 = int64_t(blockIdx.x) * kCorrVoxels; p0 < count; p0 += int64_t(gridDim.x) * kCorrVoxels) {
+        __syncthreads();  // the previous tile's voxels are read
+        if (tid < kCorrVoxels) vox[tid] = p0 + tid < count ? listed(list, p0 + tid) : -1;
+        __syncthreads();
+        correlate_tile<RC>(S, vox, k, c, blockIdx.y * 16 * RC, corr, ldc);
+    }
 }
 
 // ---- ridge NNLS ------------------------------------------------------------------------
@@ -1109,21 +1112,24 @@ __global__ void batch_plan_kernel(MfodBatchState B, const int* __restrict__ coun
 template <int RC, bool HR>
 __global__ void __launch_bounds__(128) batch_correlate_kernel(MfodBatchState B, const int* __restrict__ list) {
     __shared__ int64_t vox[kCorrVoxels];
-    const int64_t t = blockIdx.x;
-    if (t >= B.tfirst[B.n_jobs]) return;
-    const int j = ticket_job(B.tfirst, B.n_jobs, t);
-    const MfodBatchJob& J = B.jobs[j];
-    const int64_t count = B.vfirst[j + 1] - B.vfirst[j];
-    const int64_t p0 = (t - B.tfirst[j]) * kCorrVoxels;
     const int tid = threadIdx.x;
-    if (tid < kCorrVoxels) {
-        const int64_t q = p0 + tid;
-        vox[tid] = q < count ? (list ? int64_t(list[J.off + q]) : q) : -1;
+    const int64_t total = B.tfirst[B.n_jobs];
+    for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+        const int j = ticket_job(B.tfirst, B.n_jobs, t);
+        const MfodBatchJob& J = B.jobs[j];
+        const int64_t count = B.vfirst[j + 1] - B.vfirst[j];
+        const int64_t p0 = (t - B.tfirst[j]) * kCorrVoxels;
+        __syncthreads();  // the previous tile's voxels are read
+        if (tid < kCorrVoxels) {
+            const int64_t q = p0 + tid;
+            vox[tid] = q < count ? (list ? int64_t(list[J.off + q]) : q) : -1;
+        }
+        __syncthreads();
+        const RidgeDev R = HR ? J.hr : J.lr;
+        const TissueDev T = HR ? J.hrt : J.lrt;
+        correlate_tile<RC>(batch_signal(B, J, T), vox, R.k, R.c, blockIdx.y * 16 * RC, B.corr + J.off * B.ldc,
+                           B.ldc);
     }
-    __syncthreads();
-    const RidgeDev R = HR ? J.hr : J.lr;
-    const TissueDev T = HR ? J.hrt : J.lrt;
-    correlate_tile<RC>(batch_signal(B, J, T), vox, R.k, R.c, blockIdx.y * 16 * RC, B.corr + J.off * B.ldc, B.ldc);
 }
 
 // ridge_nnls_half_kernel over every volume's list.
@@ -1340,7 +1346,11 @@ inline NnlsLaunch nnls_variant(int c) {
 inline void launch_correlate(const SignalDev& S, const int* list, int64_t count, const int* count_dev,
                              const RidgeDev& R, double* corr, int ldc, cudaStream_t st) {
     if (count == 0) return;
-    const unsigned gx = unsigned((count + kCorrVoxels - 1) / kCorrVoxels);
+    // count is exact unless the round's count lives on the device (count_dev): then it is an
+    // upper bound and the grid stays resident-sized, the CTAs striding over the live tiles.
+    int64_t tiles = (count + kCorrVoxels - 1) / kCorrVoxels;
+    if (count_dev) tiles = std::min<int64_t>(tiles, int64_t(sm_count()) * kCorrResidentCtas);
+    const unsigned gx = unsigned(tiles);
     LaunchScope scope("correlate_kernel", st);
     if (R.c <= 48) {
         correlate_kernel<3><<<dim3(gx, 1), 128, 0, st>>>(S, list, count, count_dev, R.k, R.c, corr, ldc);
@@ -1825,6 +1835,8 @@ void mfod_batch_run(MfodBatch* b, cudaStream_t st) {
     if (ci > 0) zero(B.fiso, size_t(V) * ci * sizeof(double));
     zero(B.rounds, size_t(V) * sizeof(int32_t));
     zero(B.bad, size_t(V));
+    // The correlation grids stay resident-sized: a round's tiles are only known on the device.
+    const unsigned corr_grid = unsigned(std::min<int64_t>(b->tiles, int64_t(sm_count()) * kCorrResidentCtas));
     const unsigned lr_redo_blocks = std::min<unsigned>(blocks(b->lr_slots, V), unsigned(sm_count()));
     const unsigned hr_redo_blocks = std::min<unsigned>(blocks(b->hr_slots, V), unsigned(sm_count()));
     // Every round is enqueued: each stage reads its tickets on the device, so a round whose
@@ -1842,7 +1854,7 @@ void mfod_batch_run(MfodBatch* b, cudaStream_t st) {
         }
         {
             LaunchScope scope("batch_correlate_kernel", st);
-            batch_correlate_kernel<3, false><<<unsigned(b->tiles), 128, 0, st>>>(B, cur);
+            batch_correlate_kernel<3, false><<<corr_grid, 128, 0, st>>>(B, cur);
             launched("batch_correlate_kernel launch");
         }
         zero(b->queue, sizeof(int));
@@ -1879,7 +1891,7 @@ void mfod_batch_run(MfodBatch* b, cudaStream_t st) {
     }
     {
         LaunchScope scope("batch_correlate_kernel", st);
-        batch_correlate_kernel<4, true><<<dim3(unsigned(b->tiles), unsigned((b->c_hr_max + 63) / 64)), 128, 0, st>>>(
+        batch_correlate_kernel<4, true><<<dim3(corr_grid, unsigned((b->c_hr_max + 63) / 64)), 128, 0, st>>>(
             B, nullptr);
         launched("batch_correlate_kernel launch");
     }
