@@ -138,6 +138,15 @@ def committed_issue(kernel: str, workload: str, algorithmic_bytes: float) -> dic
             "warp_instructions_per_voxel_round": entry.get("warp_instructions_per_voxel_round")}
 
 
+def committed_fp64(kernel: str, workload: str) -> dict | None:
+    """FP64 CUDA-core FLOP per voxel of a kernel from its committed ncu capture
+    (profiles/fp64.json), or None."""
+    path = ROOT / "profiles" / "fp64.json"
+    if not path.exists():
+        return None
+    return json.loads(path.read_text()).get("kernels", {}).get(f"{workload}:{kernel}")
+
+
 # ---- clocks ------------------------------------------------------------------------------
 
 class ClockSampler:
@@ -1518,6 +1527,21 @@ def measure(wl, args, world: int, rank: int, dist, dev) -> dict:
             "warp_instructions_per_voxel_round": issue["warp_instructions_per_voxel_round"],
             "threads_per_instruction": issue["threads_per_instruction"],
             "source": "profiles/issue.json (ncu smsp__inst_executed.sum per algorithmic byte, scaled to this launch)"}
+    fp64 = committed_fp64(top, wl.name)
+    if fp64 is not None and avg_launch_s > 0:
+        # The FP64 roofline of a CUDA-core FP64 kernel: its FLOP (counted per voxel by ncu)
+        # against the FP64 pipe's rate, 32 FP64 FMA per SM per cycle (the pipe's active
+        # fraction in the capture matches this rate: 38.6% busy at 7.5 TFLOP/s).
+        sm_mhz = line["clocks"].get("sm_mhz") or line["clocks"].get("sm_max_mhz") or 1965.0
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        peak = sms * 32 * 2 * sm_mhz * 1e6 / 1e12
+        achieved = fp64["fp64_flop_per_voxel"] * (voxels_all / world) * args.steps / max(top_launches, 1) \
+            / avg_launch_s / 1e12
+        line["fp64_roofline"] = {
+            "kernel": top, "unit": "TFLOP/s", "achieved": achieved, "peak": peak, "frac": achieved / peak,
+            "peak_basis": f"{sms} SMs x 32 FP64 FMA x 2 per cycle at the median SM clock {sm_mhz} MHz",
+            "fp64_flop_per_voxel": fp64["fp64_flop_per_voxel"],
+            "source": "profiles/fp64.json (ncu FP64 instruction counts of the same kernel and volume)"}
     if hasattr(wl, "extra"):
         def timed_host(step):
             for _ in range(args.warmup):
