@@ -672,7 +672,10 @@ class MsmtWorkload(_SdWorkloadBase):
 
     name = "msmt_csd_lsi_110x110x70"
     kernels = ("lsi_kernel",)
-    has_fp32 = False
+    has_fp32 = True
+    fp32_steps = 1
+    fp32_what = ("lar_fit_lsi_plain_fp32: one warp per voxel runs the LSI steps in FP32, the Cholesky factor of the "
+                 "active constraints formed anew for every fit, no QR fallback")
     bytes_per_voxel = 8 * 280 + 8 * 47 + 1
 
     def __init__(self, seed: int) -> None:
@@ -695,10 +698,16 @@ class MsmtWorkload(_SdWorkloadBase):
         self.h_conv = torch.empty((self.v,), dtype=torch.uint8).pin_memory()
         self.h2d_bytes = self.signals.nbytes
         self.d2h_bytes = self.v * (47 * 8 + 1)
+        self.d_signals32 = self.d_signals.float()
+        self.d_x32 = torch.empty((self.v, 47), dtype=torch.float32, device=dev)
+        self.d_status32 = torch.empty((self.v,), dtype=torch.uint8, device=dev)
 
     def step_device(self, precision=0):
         from larmor_b200 import _core
 
+        if precision == 1:
+            _core.fit_lsi_plain_fp32_device(self.design, self.d_signals32, self.d_x32, self.d_status32)
+            return
         _core.fit_lsi_device(self.design, self.d_signals, self.d_x, self.d_conv)
 
     def kernel_bytes(self) -> dict:
@@ -723,9 +732,36 @@ class MsmtWorkload(_SdWorkloadBase):
         n = min(self.v, 8192)
         done, t0 = 0, time.perf_counter()
         while time.perf_counter() - t0 < budget_s:
-            o.fit_lsi(f, g, ridge, self.signals[:n], n_threads=threads)
+            out = o.fit_lsi(f, g, ridge, self.signals[:n], n_threads=threads)
             done += n
+        self.reference_out = out
         return done, time.perf_counter() - t0, f"first {n} voxels of the volume, repeated for ~{budget_s:.0f} s"
+
+    def _against_oracle(self, x) -> dict:
+        ref, ref_conv = self.reference_out
+        got = x[:len(ref)].double().cpu().numpy()
+        scale = np.maximum(np.abs(ref).max(axis=1), 1e-300)
+        rel = np.abs(got - ref).max(axis=1) / scale
+        return {"voxels": int(len(ref)), "x_rel_max": float(rel.max()), "x_rel_median": float(np.median(rel)),
+                "x_rel_p99": float(np.percentile(rel, 99))}
+
+    def parity(self) -> dict:
+        """The device fit against the FP64 oracle on the cpu_baseline sample: each voxel's largest
+        coefficient error relative to its largest coefficient."""
+        out = self._against_oracle(self.d_x)
+        out.update({"against": "FP64 oracle (C++ restatement of cpp/src/sd/lsi.cpp)", "sample": "first voxels",
+                    "converged_identical": float((self.d_conv[:out["voxels"]].cpu().numpy().astype(bool)
+                                                  == self.reference_out[1]).mean()),
+                    "tolerance": {"x_rel": 1e-4}})
+        out["within_tolerance"] = bool(out["x_rel_max"] <= 1e-4)
+        return out
+
+    def fp32_parity(self) -> dict:
+        """The plain FP32 fit against the same FP64 oracle fit."""
+        self.step_device(precision=1)
+        out = self._against_oracle(self.d_x32)
+        out["status_nonzero"] = float((self.d_status32[:out["voxels"]].cpu().numpy() != 0).mean())
+        return out
 
 
 def _job_kernel_bytes(job) -> dict:

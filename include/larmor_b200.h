@@ -172,6 +172,15 @@ int lar_lsi_design_matrices(lar_lsi_design design, double* q_t, double* back, do
 int lar_fit_lsi(lar_lsi_design design, const double* signals, int64_t v, int only_qr, double* x,
                 uint8_t* converged, uint8_t* status, int32_t* outer, uint8_t* active, void* stream);
 
+/* The plain single-precision LSI fit, the comparison baseline of lar_fit_lsi (no counterpart in
+ * the reference): float32 signals (v, m) (device) in, float32 solutions x (v, n) (device) out;
+ * one warp per voxel runs the reference's steps in FP32 with the Cholesky factor of the active
+ * constraints formed anew for every fit and no QR fallback. status (v,) (device uint8, may be
+ * NULL): 0 converged, 1 the factor failed or more than 64 constraints became active, 2 f = 0
+ * (the unconstrained solution), 3 a step limit. */
+int lar_fit_lsi_plain_fp32(lar_lsi_design design, const float* signals, int64_t v, float* x, uint8_t* status,
+                           void* stream);
+
 /* ---- Multi-tissue spherical deconvolution (SDModel, method mFOD) ---------------------- */
 
 typedef struct lar_fod_solver_s* lar_fod_solver;

@@ -413,6 +413,15 @@ def fit_lsi_device(design: LsiDesign, signals, x, converged, status=None, outer=
         _lib.ptr(status), _lib.ptr(outer), _lib.ptr(active), _stream(torch)))
 
 
+def fit_lsi_plain_fp32_device(design: LsiDesign, signals, x, status=None) -> None:
+    """The plain single-precision LSI fit, the comparison baseline of fit_lsi_device: float32
+    signals (v, m) in, float32 solutions (v, n) out (torch CUDA tensors); status (v,) uint8: 0
+    converged, 1 factor failed, 2 f = 0, 3 step limit (lar_fit_lsi_plain_fp32)."""
+    torch = _torch()
+    _lib.check(_lib.lib().lar_fit_lsi_plain_fp32(
+        design.handle, _lib.ptr(signals), signals.shape[0], _lib.ptr(x), _lib.ptr(status), _stream(torch)))
+
+
 class _Handle:
     """Owns a C-ABI handle and destroys it with the given function."""
 

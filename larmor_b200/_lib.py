@@ -36,6 +36,7 @@ SIGNATURES: dict[str, tuple] = {
     "lar_lsi_design_destroy": (None, [_p]),
     "lar_lsi_design_matrices": (_i32, [_p, _p, _p, _p, _p, _p]),
     "lar_fit_lsi": (_i32, [_p, _p, _i64, _i32, _p, _p, _p, _p, _p, _p]),
+    "lar_fit_lsi_plain_fp32": (_i32, [_p, _p, _i64, _p, _p, _p]),
     "lar_l2nnls_create": (_i32, [_p, _i64, _i64, _f64, _f64, _p]),
     "lar_fod_solver_destroy": (None, [_p]),
     "lar_deconv_kernel_create": (_i32, [_p, _i64, _i64, _p, _p, _i64, _p, _i64, _p]),

@@ -27,6 +27,7 @@
 
 #include "common.cuh"
 #include "host_la.hpp"
+#include "plain_fp32.cuh"
 #include "warp_chol.cuh"
 #include "warp_nnls.cuh"
 
@@ -373,6 +374,8 @@ __global__ void __launch_bounds__(kLsiWarps * 32, 4) lsi_kernel(LsiDevice D, con
 struct lar_lsi_design_s {
     lar::host::LsiDesignHost host;
     lar::DeviceArray<double> qt, back, et, e, gram, abs_sums;
+    // FP32 copies for the plain single-precision fit (the comparison baseline).
+    lar::DeviceArray<float> qt32, back32, et32, e32, gram32, abs_sums32;
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
     ~lar_lsi_design_s() {
@@ -407,6 +410,16 @@ int lar_lsi_design_create(const double* a, int64_t m, int64_t n, const double* g
         h->e.upload(d.e.data(), d.e.size());
         h->gram.upload(d.gram.data(), d.gram.size());
         h->abs_sums.upload(d.abs_sums.data(), d.abs_sums.size());
+        auto upload32 = [](DeviceArray<float>& dst, const std::vector<double>& src) {
+            const std::vector<float> f(src.begin(), src.end());
+            dst.upload(f.data(), f.size());
+        };
+        upload32(h->qt32, qt);
+        upload32(h->back32, d.back);
+        upload32(h->et32, et);
+        upload32(h->e32, d.e);
+        upload32(h->gram32, d.gram);
+        upload32(h->abs_sums32, d.abs_sums);
         *out = h.release();
     });
 }
@@ -468,6 +481,20 @@ int lar_fit_lsi(lar_lsi_design design, const double* signals, int64_t v, int onl
             D, signals, v, only_qr, reinterpret_cast<int*>(base), cap, reinterpret_cast<double*>(base + 256), slot,
             x, converged, status, outer, active);
         cuda_check(cudaGetLastError(), "lsi_kernel launch");
+    });
+}
+
+int lar_fit_lsi_plain_fp32(lar_lsi_design design, const float* signals, int64_t v, float* x, uint8_t* status,
+                           void* stream) {
+    return guarded([&] {
+        require(design != nullptr, "design must not be NULL");
+        require(v >= 0, "v must be at least 0");
+        if (v == 0) return;
+        require(signals && x, "signals and x must not be NULL");
+        const auto& h = design->host;
+        const PlainLsi D{int(h.m), int(h.n), int(h.k), design->qt32.ptr, design->back32.ptr, design->et32.ptr,
+                         design->e32.ptr, design->gram32.ptr, design->abs_sums32.ptr};
+        launch_plain_lsi(D, signals, v, x, status, static_cast<cudaStream_t>(stream));
     });
 }
 

@@ -104,9 +104,17 @@ __device__ int steepest(const float* g, const unsigned char* act, int c, int lan
     return bi;
 }
 
+// A Gram matrix stored whole, (c, c) row-major.
+struct DenseGram {
+    const float* g;
+    int c;
+    __device__ __forceinline__ float operator()(int i, int j) const { return g[size_t(i) * c + j]; }
+};
+
 // z = the solution of G_AA z_A = corr_A on the active columns (0 elsewhere), by a Cholesky
 // factor of G_AA formed anew; false when the active set exceeds NA or a pivot fails.
-__device__ bool solve_active(const float* __restrict__ G, int c, const Scratch& s, int lane) {
+template <class Gram>
+__device__ bool solve_active(const Gram& G, int c, const Scratch& s, int lane) {
     int na = 0;
     for (int base = 0; base < c; base += 32) {
         const int j = base + lane;
@@ -123,7 +131,7 @@ __device__ bool solve_active(const float* __restrict__ G, int c, const Scratch& 
     __syncwarp();
     for (int e = lane; e < na * na; e += 32) {
         const int r = e / na, q = e - r * na;
-        if (q <= r) s.L[r * NA + q] = G[size_t(s.idx[r]) * c + s.idx[q]];
+        if (q <= r) s.L[r * NA + q] = G(s.idx[r], s.idx[q]);
     }
     __syncwarp();
     // Left-looking Cholesky, one column at a time.
@@ -165,7 +173,8 @@ __device__ bool solve_active(const float* __restrict__ G, int c, const Scratch& 
 }
 
 // Lawson-Hanson on (G, corr): x >= 0. 0: converged; 1: the factor failed; 2: a step limit.
-__device__ int plain_nnls(const float* __restrict__ G, int c, float tol, const Scratch& s, int lane) {
+template <class Gram>
+__device__ int plain_nnls(const Gram& G, int c, float tol, const Scratch& s, int lane) {
     for (int j = lane; j < c; j += 32) {
         s.x[j] = 0.f;
         s.act[j] = 0;
@@ -231,7 +240,7 @@ __device__ int plain_nnls(const float* __restrict__ G, int c, float tol, const S
             float acc = s.corr[j];
             for (int k = 0; k < na; ++k) {
                 const int i = s.idx[k];
-                acc -= G[size_t(i) * c + j] * s.x[i];
+                acc -= G(i, j) * s.x[i];
             }
             s.g[j] = acc;
         }
@@ -442,7 +451,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) plain_fp32_mfod_kernel(
         for (int round = 0; round < max_rounds; ++round) {
             ++rounds;
             stage_correlations(lr, f_iso, s, lane);
-            status = max(status, plain_nnls(lr.gram, lr.c, lr.tol, s, lane));
+            status = max(status, plain_nnls(DenseGram{lr.gram, lr.c}, lr.c, lr.tol, s, lane));
             plain_fractions(lr, s.x, s, false, -1.f, lane);
             bool converged = true;
             for (int j = 0; j < 1 + ci; ++j) converged &= fabsf(fr[j] - prev[j]) < fraction_tol;
@@ -454,7 +463,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) plain_fp32_mfod_kernel(
             __syncwarp();
         }
         stage_correlations(hr, f_iso, s, lane);
-        status = max(status, plain_nnls(hr.gram, hr.c, hr.tol, s, lane));
+        status = max(status, plain_nnls(DenseGram{hr.gram, hr.c}, hr.c, hr.tol, s, lane));
         for (int j = lane; j < hr.c; j += 32) fods[voxel * hr.c + j] = s.x[j];
         const int nf = plain_fractions(hr, s.x, s, true, final_tol, lane);
         float total = kPlainFractionOffset;
@@ -468,7 +477,131 @@ __global__ void __launch_bounds__(kPlainWarps * 32) plain_fp32_mfod_kernel(
     }
 }
 
+// ---- MSMT-CSD (LSI) -------------------------------------------------------------------------
+
+// The plain single-precision LSI fit, the comparison baseline of lsi_kernel: one warp per voxel in
+// FP32 with the textbook forms of the reference's steps (cpp/src/sd/lsi.cpp:253-338):
+// rotated = q_t s; f = -E rotated scaled to max |f| = 1 (the unconstrained solution back rotated
+// when f = 0); the LDP multipliers u >= 0 by Lawson-Hanson on H = E E^T + f f^T with right-hand
+// side f (plain_nnls: the gradient f - H u is the LDP's f (1 - f.u) - E E^T u, the Cholesky factor
+// of H_AA formed anew for every fit); x = back (scale E^T u / (1 - f.u) + rotated). No QR
+// fallback: a voxel whose factor fails (or outgrows kPlainMaxActive) gets status 1, a step
+// limit status 3, f = 0 status 2.
+struct LdpGram {
+    const float* gram;  // (k, k) E E^T
+    const float* f;     // (k,) the voxel's scaled bounds
+    int k;
+    __device__ __forceinline__ float operator()(int i, int j) const { return gram[size_t(i) * k + j] + f[i] * f[j]; }
+};
+
+__host__ __device__ inline size_t plain_lsi_warp_bytes(int k) {
+    const size_t floats = 2 * 64 + size_t(4) * k + size_t(NA) * NA + NA + 64;
+    return (floats * 4 + (NA + 4) * 4 + size_t(k) + 15) / 16 * 16;
+}
+
+__device__ Scratch carve_lsi(unsigned char* base, int k, float*& rot, float*& tv) {
+    Scratch s{};
+    float* f = reinterpret_cast<float*>(base);
+    rot = f;
+    tv = rot + 64;
+    s.corr = tv + 64;  // the bounds f: the NNLS right-hand side
+    s.x = s.corr + k;  // the multipliers u
+    s.z = s.x + k;
+    s.g = s.z + k;
+    s.L = s.g + k;
+    s.y = s.L + NA * NA;
+    s.small = s.y + NA;
+    s.idx = reinterpret_cast<int*>(s.small + 64);
+    s.meta = s.idx + NA;
+    s.act = reinterpret_cast<unsigned char*>(s.meta + 4);
+    return s;
+}
+
+__global__ void __launch_bounds__(kPlainWarps * 32) plain_lsi_kernel(PlainLsi D, const float* __restrict__ signals,
+                                                                     int64_t v, float* __restrict__ x_out,
+                                                                     uint8_t* __restrict__ status_out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m = D.m, n = D.n, k = D.k;
+    float *rot, *tv;
+    const Scratch s = carve_lsi(smem_raw + warp * plain_lsi_warp_bytes(k), k, rot, tv);
+    float* f = s.corr;
+    for (int64_t voxel = int64_t(blockIdx.x) * kPlainWarps + warp; voxel < v;
+         voxel += int64_t(gridDim.x) * kPlainWarps) {
+        const float* sv = signals + voxel * m;
+        for (int i = lane; i < n; i += 32) {
+            float acc = 0.f;
+            for (int j = 0; j < m; ++j) acc += D.qt[size_t(j) * n + i] * sv[j];
+            rot[i] = acc;
+        }
+        __syncwarp();
+        float scale = 0.f;
+        for (int j = lane; j < k; j += 32) {
+            float acc = 0.f;
+            for (int i = 0; i < n; ++i) acc += D.et[size_t(i) * k + j] * rot[i];
+            f[j] = -acc;
+            scale = fmaxf(scale, fabsf(acc));
+        }
+        scale = wmax(scale);
+        __syncwarp();
+        uint8_t st = 0;
+        if (!(scale > 0.f)) {
+            for (int i = lane; i < n; i += 32) {
+                float acc = 0.f;
+                for (int j = 0; j < n; ++j) acc += D.back[size_t(i) * n + j] * rot[j];
+                x_out[voxel * n + i] = acc;
+            }
+            st = 2;
+        } else {
+            float norm1 = 0.f;
+            for (int j = lane; j < k; j += 32) {
+                f[j] /= scale;
+                norm1 = fmaxf(norm1, D.abs_sums[j] + fabsf(f[j]));
+            }
+            norm1 = wmax(norm1);
+            __syncwarp();
+            const float tol = 10.f * kEps32 * norm1 * float(max(n + 1, k));
+            const int r = plain_nnls(LdpGram{D.gram, f, k}, k, tol, s, lane);
+            st = r == 0 ? 0 : (r == 1 ? 1 : 3);
+            float fu = 0.f;
+            for (int j = lane; j < k; j += 32) fu += f[j] * s.x[j];
+            fu = wsum(fu);
+            for (int i = lane; i < n; i += 32) {
+                float acc = 0.f;
+                for (int j = 0; j < k; ++j) acc += D.e[size_t(j) * n + i] * s.x[j];
+                tv[i] = scale * acc / (1.f - fu) + rot[i];
+            }
+            __syncwarp();
+            for (int i = lane; i < n; i += 32) {
+                float acc = 0.f;
+                for (int j = 0; j < n; ++j) acc += D.back[size_t(i) * n + j] * tv[j];
+                x_out[voxel * n + i] = acc;
+            }
+        }
+        if (lane == 0 && status_out) status_out[voxel] = st;
+        __syncwarp();
+    }
+}
+
 }  // namespace
+
+void launch_plain_lsi(const PlainLsi& D, const float* signals, int64_t v, float* x, uint8_t* status,
+                      cudaStream_t stream) {
+    if (v == 0) return;
+    require(D.n <= kPlainLsiMaxParameters && D.k <= kPlainLsiMaxConstraints,
+            "the plain FP32 LSI fit takes at most 63 parameters and 512 constraints");
+    const size_t smem = plain_lsi_warp_bytes(D.k) * kPlainWarps;
+    cuda_check(cudaFuncSetAttribute(plain_lsi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+               "cudaFuncSetAttribute");
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plain_lsi_kernel, kPlainWarps * 32, smem),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    const int64_t blocks = std::max<int64_t>(
+        1, std::min<int64_t>((v + kPlainWarps - 1) / kPlainWarps, int64_t(sm_count()) * std::max(per_sm, 1)));
+    LaunchScope scope("plain_lsi_kernel", stream);
+    plain_lsi_kernel<<<unsigned(blocks), kPlainWarps * 32, smem, stream>>>(D, signals, v, x, status);
+    cuda_check(cudaGetLastError(), "plain_lsi_kernel launch");
+}
 
 void launch_plain_fp32(const PlainStage& lr, const PlainStage& hr, const float* signals, int64_t v,
                        const float* weights, int max_rounds, float fraction_tol, float final_tol, float* fods,

@@ -27,6 +27,23 @@ constexpr int kPlainMaxColumns = 320;
 constexpr int kPlainMaxActive = 64;
 constexpr int kPlainMaxGroups = 4;
 
+// The LSI design of MSMT-CSD in FP32 (lsi.cu's matrices, the same layouts).
+struct PlainLsi {
+    int m, n, k;
+    const float* qt;        // (m, n): q_t transposed
+    const float* back;      // (n, n)
+    const float* et;        // (n, k): E transposed
+    const float* e;         // (k, n)
+    const float* gram;      // (k, k): E E^T
+    const float* abs_sums;  // (k,)
+};
+
+constexpr int kPlainLsiMaxConstraints = 512;
+constexpr int kPlainLsiMaxParameters = 63;
+
+void launch_plain_lsi(const PlainLsi& D, const float* signals, int64_t v, float* x, uint8_t* status,
+                      cudaStream_t stream);
+
 void launch_plain_fp32(const PlainStage& lr, const PlainStage& hr, const float* signals, int64_t v,
                        const float* weights, int max_rounds, float fraction_tol, float final_tol, float* fods,
                        float* fractions, int32_t* rounds, uint8_t* status, cudaStream_t stream);

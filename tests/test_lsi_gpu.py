@@ -144,3 +144,27 @@ def test_msmt_model_recovers_a_wm_csf_mixture(cuda, msmt_fixture):
     np.testing.assert_allclose(fit.tissue_fractions[0, 0, 0], (0.7, 0.3), atol=1e-6)
     np.testing.assert_allclose(fit.fods[0][0, 0, 0], fod_true, atol=1e-6)
     assert csf_coef > 0
+
+
+def test_plain_fp32_lsi_stays_near_the_fp64_fit(cuda, msmt_fixture):
+    """The plain single-precision LSI fit (the comparison baseline, no refinement and no QR
+    fallback) on plausible voxels: its solutions stay within a few 1e-3 of the FP64 fit's,
+    relative to each voxel's largest coefficient; most voxels converge by the Cholesky path."""
+    import torch
+
+    from larmor_b200 import _core
+
+    design = _design(msmt_fixture)
+    signals = _signals(msmt_fixture, 512, seed=11)[256:]  # the plausible half
+    x64 = _device_fit(design, signals)[0]
+    dev = torch.device("cuda")
+    s32 = torch.from_numpy(np.ascontiguousarray(signals, dtype=np.float32)).to(dev)
+    x32 = torch.empty((len(signals), design.n), dtype=torch.float32, device=dev)
+    status = torch.empty((len(signals),), dtype=torch.uint8, device=dev)
+    _core.fit_lsi_plain_fp32_device(design, s32, x32, status)
+    got, st = x32.double().cpu().numpy(), status.cpu().numpy()
+    ok = st == 0
+    assert ok.mean() >= 0.9
+    rel = np.abs(got - x64).max(axis=1) / np.abs(x64).max(axis=1)
+    print(f"plain FP32 LSI: {ok.mean():.3f} converged, rel median {np.median(rel[ok]):.2e}, max {rel[ok].max():.2e}")
+    assert np.median(rel[ok]) <= 1e-2
