@@ -146,25 +146,59 @@ def test_msmt_model_recovers_a_wm_csf_mixture(cuda, msmt_fixture):
     assert csf_coef > 0
 
 
-def test_plain_fp32_lsi_stays_near_the_fp64_fit(cuda, msmt_fixture):
-    """The plain single-precision LSI fit (the comparison baseline, no refinement and no QR
-    fallback) on plausible voxels: its solutions stay within a few 1e-3 of the FP64 fit's,
-    relative to each voxel's largest coefficient; most voxels converge by the Cholesky path."""
+def _plain_fp32(design, signals):
     import torch
 
     from larmor_b200 import _core
 
-    design = _design(msmt_fixture)
-    signals = _signals(msmt_fixture, 512, seed=11)[256:]  # the plausible half
-    x64 = _device_fit(design, signals)[0]
     dev = torch.device("cuda")
     s32 = torch.from_numpy(np.ascontiguousarray(signals, dtype=np.float32)).to(dev)
     x32 = torch.empty((len(signals), design.n), dtype=torch.float32, device=dev)
     status = torch.empty((len(signals),), dtype=torch.uint8, device=dev)
     _core.fit_lsi_plain_fp32_device(design, s32, x32, status)
-    got, st = x32.double().cpu().numpy(), status.cpu().numpy()
+    return x32.double().cpu().numpy(), status.cpu().numpy()
+
+
+def test_plain_fp32_lsi_known_answers_and_a_well_conditioned_problem(cuda):
+    """The plain single-precision LSI fit (the comparison baseline: FP32, the active Cholesky
+    factor formed anew for every fit, no QR fallback) gives the known answers and, on a
+    well-conditioned random problem, the FP64 fit's solutions to single precision."""
+    from larmor_b200 import _core
+
+    d = _core.LsiDesign(np.eye(3), np.eye(3), 0.0)
+    x, st = _plain_fp32(d, np.array([[2.0, -1.0, 3.0]]))
+    np.testing.assert_allclose(x[0], [2.0, 0.0, 3.0], atol=1e-5)
+    assert st[0] == 0
+    d = _core.LsiDesign(np.eye(2), np.array([[-1.0, -1.0]]), 0.0)
+    x, _ = _plain_fp32(d, np.array([[0.5, 0.5]]))
+    np.testing.assert_allclose(x[0], [0.0, 0.0], atol=1e-5)
+    # x >= 0 and 20 non-negative combinations of x: the feasible cone is the orthant.
+    rng = np.random.default_rng(5)
+    a = rng.standard_normal((60, 10))
+    g = np.vstack([np.eye(10), rng.uniform(0.0, 1.0, (20, 10))])
+    d = _core.LsiDesign(a, g, 0.0)
+    signals = rng.standard_normal((256, 60))
+    x64 = _device_fit(d, signals)[0]
+    x32, st = _plain_fp32(d, signals)
+    ok = st == 0
+    assert ok.mean() >= 0.95
+    rel = np.abs(x32 - x64).max(axis=1) / np.abs(x64).max(axis=1)
+    print(f"plain FP32 LSI, random orthant problem: rel median {np.median(rel[ok]):.2e}, max {rel[ok].max():.2e}")
+    assert np.median(rel[ok]) <= 1e-4
+
+
+def test_plain_fp32_lsi_on_the_msmt_problem(cuda, msmt_fixture):
+    """On MSMT-CSD's problem (47 unknowns, 302 constraints, ~40 active) the least-distance
+    system E_A E_A^T + f_A f_A^T is near-singular, so the plain FP32 fit converges but lands far
+    from the FP64 solution: this is the baseline the FP64 path is compared with. Its results are
+    finite and most voxels converge."""
+    design = _design(msmt_fixture)
+    signals = _signals(msmt_fixture, 512, seed=11)[256:]  # the plausible half
+    x64 = _device_fit(design, signals)[0]
+    got, st = _plain_fp32(design, signals)
     ok = st == 0
     assert ok.mean() >= 0.9
+    assert np.isfinite(got[ok]).all()
     rel = np.abs(got - x64).max(axis=1) / np.abs(x64).max(axis=1)
-    print(f"plain FP32 LSI: {ok.mean():.3f} converged, rel median {np.median(rel[ok]):.2e}, max {rel[ok].max():.2e}")
-    assert np.median(rel[ok]) <= 1e-2
+    print(f"plain FP32 LSI on MSMT: {ok.mean():.3f} converged, rel median {np.median(rel[ok]):.2e}, "
+          f"max {rel[ok].max():.2e}")
