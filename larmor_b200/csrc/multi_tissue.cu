@@ -632,7 +632,7 @@ __device__ __forceinline__ bool ridge_nnls_half(const RidgeDev R, const double* 
 // Two listed voxels per warp, one per half, pulled from a device counter: x(v) <- the ridge
 // NNLS of corr(v), or v appended to `redo` when it needs the QR fallback.
 template <int CPL>
-__global__ void __launch_bounds__(kMtWarps * 32, 6) ridge_nnls_half_kernel(
+__global__ void __launch_bounds__(kMtWarps * 32, 8) ridge_nnls_half_kernel(
     RidgeDev R, const int* __restrict__ list, int64_t count, const int* __restrict__ count_dev,
     const double* __restrict__ corr, int ldc, double* __restrict__ x_out, int ldx, int* __restrict__ redo,
     int* redo_count, int* queue, double* __restrict__ workspace, size_t slot_size) {
@@ -985,7 +985,7 @@ __device__ __forceinline__ void fractions(const TissueDev T, const double* fod, 
 // takes the isotropic fractions; a voxel whose fractions all moved by less than fraction_tol, or
 // that used its last round, records its round count, the others join the next round's list
 // with their fractions kept for the next comparison.
-__global__ void __launch_bounds__(kMtWarps * 32, 4) lr_fractions_kernel(
+__global__ void __launch_bounds__(kMtWarps * 32, 5) lr_fractions_kernel(
     TissueDev T, const double* __restrict__ signals, const double* __restrict__ fods, int ldf,
     const int* __restrict__ list, int64_t count, const int* __restrict__ count_dev, int round, int max_rounds,
     double fraction_tol, double* __restrict__ fiso, double* __restrict__ prev, int32_t* __restrict__ rounds,
@@ -1134,7 +1134,7 @@ __global__ void __launch_bounds__(128) batch_correlate_kernel(MfodBatchState B, 
 
 // ridge_nnls_half_kernel over every volume's list.
 template <int CPL>
-__global__ void __launch_bounds__(kMtWarps * 32, 6) batch_half_kernel(MfodBatchState B, const int* __restrict__ list,
+__global__ void __launch_bounds__(kMtWarps * 32, 8) batch_half_kernel(MfodBatchState B, const int* __restrict__ list,
                                                                      int c_max, int* queue,
                                                                      double* __restrict__ workspace,
                                                                      size_t slot_size) {
@@ -1231,7 +1231,7 @@ __global__ void __launch_bounds__(kMtWarps * 32, 5) batch_first_kernel(MfodBatch
 
 // lr_fractions_kernel over every volume's list; the next round's list goes to each volume's
 // segment.
-__global__ void __launch_bounds__(kMtWarps * 32, 4) batch_lr_fractions_kernel(
+__global__ void __launch_bounds__(kMtWarps * 32, 5) batch_lr_fractions_kernel(
     MfodBatchState B, const int* __restrict__ list, int round, int max_rounds, double fraction_tol,
     int* __restrict__ next, int* next_counts, int* queue, double* __restrict__ workspace, size_t slot_size) {
     __shared__ FracState states[kMtWarps];
