@@ -1231,7 +1231,7 @@ __global__ void __launch_bounds__(kMtWarps * 32, 5) batch_first_kernel(MfodBatch
 
 // lr_fractions_kernel over every volume's list; the next round's list goes to each volume's
 // segment.
-__global__ void __launch_bounds__(kMtWarps * 32, 5) batch_lr_fractions_kernel(
+__global__ void __launch_bounds__(kMtWarps * 32, 4) batch_lr_fractions_kernel(
     MfodBatchState B, const int* __restrict__ list, int round, int max_rounds, double fraction_tol,
     int* __restrict__ next, int* next_counts, int* queue, double* __restrict__ workspace, size_t slot_size) {
     __shared__ FracState states[kMtWarps];
