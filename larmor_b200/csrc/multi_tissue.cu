@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(kMtWarps * 32, (CPL <= 2 ? 6 : 4)) ridge_nnls_
 // start. Below the capacity the two take the same steps with the same factor code, so every
 // voxel gets the result the full-factor kernel gives.
 template <int VPL, int CPL>
-__global__ void __launch_bounds__(kMtWarps * 32, 5) ridge_nnls_first_kernel(
+__global__ void __launch_bounds__(kMtWarps * 32, 4) ridge_nnls_first_kernel(
     RidgeDev R, SignalDev S, int64_t count, const double* __restrict__ corr, int ldc, double* __restrict__ x_out,
     int ldx, int* __restrict__ redo, int* redo_count, int* queue, double* __restrict__ workspace, size_t slot_size) {
     using State = NnlsState<VPL * 32, CPL * 32>;
@@ -1020,7 +1020,7 @@ __global__ void __launch_bounds__(kMtWarps * 32, 5) lr_fractions_kernel(
 
 // The final per-block fractions of every voxel, normalised to sum to 1 (+1e-16), with the round
 // counts and statuses (cpp/src/sd/multi_tissue.cpp:127-148).
-__global__ void __launch_bounds__(kMtWarps * 32, 4) hr_fractions_kernel(
+__global__ void __launch_bounds__(kMtWarps * 32, 5) hr_fractions_kernel(
     TissueDev T, const double* __restrict__ signals, const double* __restrict__ fods, int64_t count,
     double final_tol, const int32_t* __restrict__ rounds_in, const uint8_t* __restrict__ bad,
     double* __restrict__ fractions_out, int32_t* __restrict__ rounds_out, uint8_t* __restrict__ status, int* queue,
