@@ -49,16 +49,57 @@ __device__ __forceinline__ double wsum(double v) { return warp_sum(v); }
 __device__ __forceinline__ double wmax(double v) { return warp_max(v); }
 
 // Per-warp shared state (p + 1 <= 32).
-struct WarpShared {
+struct WarpState {
     double vec[4][32];  // p- or (p+1)-sized vectors: unconstrained and free solutions, scratch
     double tau[32];     // reflectors of the weighted design
     double qtau[kMaxActive], qnu[kMaxActive], qnd[kMaxActive], rv[32], res[32];
     double t[32];       // R^-1 r[:p] - r[p] p_free of the gradient
-    double ysub[31 * 32];  // one forward substitution per lane, entry i at [i * 32 + lane]
     int qperm[kMaxActive];
     int act[kMaxActive];
     int n_act;
 };
+
+// With the column sums' forward substitutions (one per lane, entry i at [i * 32 + lane]).
+struct WarpShared : WarpState {
+    double ysub[31 * 32];
+};
+
+constexpr int kSmemActive = 32;  // active NNLS columns whose QR fits can run in shared memory
+
+// Where a violator's re-fit keeps its arrays: the weighted design's QR (n, p), the log signals and
+// root weights (n each), the column sums' substitutions (31 x 32), the NNLS system's formed
+// columns (m, p + 1), the QR of the active columns (kMaxActive, p + 1; ssub, when set, holds
+// that of up to kSmemActive columns in shared memory), the NNLS vectors and flags (m each).
+struct RefitMem {
+    double *qr, *ys, *rw, *ysub, *ssub, *cache, *sub, *u, *z;
+    uint8_t *flag, *ready;
+};
+
+// The slot layout of a warp (constrained_slot_doubles), with qr, ys and rw in it.
+__device__ __forceinline__ RefitMem slot_refit_mem(double* slot, int n, int p, int m) {
+    RefitMem r;
+    const int rows = p + 1;
+    r.qr = slot;
+    r.cache = r.qr + size_t(n) * p;
+    r.sub = r.cache + size_t(rows) * m;
+    r.u = r.sub + size_t(rows) * kMaxActive;
+    r.z = r.u + m;
+    r.ys = r.z + m;
+    r.rw = r.ys + n;
+    r.flag = reinterpret_cast<uint8_t*>(r.rw + n);
+    r.ready = r.flag + m;
+    r.ysub = nullptr;
+    r.ssub = nullptr;
+    return r;
+}
+
+// Whether the column sums' substitutions fit in the QR's rows below R (dead by then).
+__host__ __device__ inline bool refit_ysub_aliased(int n, int p) { return size_t(n - p) * p >= 31 * 32; }
+
+// A warp's shared-memory doubles when its QR, signals, weights and small NNLS fits live there.
+__host__ __device__ inline size_t refit_smem_doubles(int n, int p) {
+    return size_t(n) * p + 2 * size_t(n) + size_t(p + 1) * kSmemActive + (refit_ysub_aliased(n, p) ? 0 : 31 * 32);
+}
 
 // The NNLS system C = [R^-T G^T; -(G p_free)^T] of one voxel, formed column by column on demand.
 struct ImplicitSystem {
@@ -105,9 +146,15 @@ struct CachedColumns {
 // C's gradient C^T (d - C u) = G t and the active columns from the cache. Returns 1 when the
 // method ended by its rule, 0 when the inner-step limit ran out, -1 past acap active columns.
 __device__ int implicit_nnls(const ImplicitSystem& sys, const double* d, double tol, int max_inner, NnlsScratch s,
-                             double* t, int lane) {
+                             double* t, double* ssub, int lane) {
     const int m = sys.m, p = sys.p, rows = p + 1;
     const CachedColumns cols{sys.cache, rows};
+    // The fit on the active columns, its QR in shared memory (ssub) when given and large enough.
+    auto fit = [&]() {
+        QrScratch q = s.qr;
+        if (ssub != nullptr && *s.n_act <= kSmemActive) q.sub = ssub;
+        warp_qr_least_squares_cols(cols, rows, s.act, *s.n_act, d, q, s.z, lane);
+    };
     for (int j = lane; j < m; j += 32) {
         s.u[j] = 0.0;
         s.z[j] = 0.0;
@@ -165,7 +212,7 @@ __device__ int implicit_nnls(const ImplicitSystem& sys, const double* d, double 
             s.flag[e] = 1;
         }
         __syncwarp();
-        warp_qr_least_squares_cols(cols, rows, s.act, *s.n_act, d, s.qr, s.z, lane);
+        fit();
         for (;;) {
             const int n2 = *s.n_act;
             bool any = false;
@@ -209,7 +256,7 @@ __device__ int implicit_nnls(const ImplicitSystem& sys, const double* d, double 
                 *s.n_act = w;
             }
             __syncwarp();
-            warp_qr_least_squares_cols(cols, rows, s.act, *s.n_act, d, s.qr, s.z, lane);
+            fit();
         }
         for (int j = lane; j < m; j += 32) s.u[j] = s.flag[j] ? s.z[j] : 0.0;
         __syncwarp();
@@ -220,18 +267,18 @@ __device__ int implicit_nnls(const ImplicitSystem& sys, const double* d, double 
 // pin): where every step succeeds, out (p) gets the constrained parameters.
 template <class Src>
 __device__ __forceinline__ void refit_violator(const LogDesignDevice<double>& d, const Src& src, int weighted,
-                                               int64_t voxel, const double* pin, double* slot, WarpShared& sh,
+                                               int64_t voxel, const double* pin, const RefitMem& mem, WarpState& sh,
                                                double* out, int lane) {
     const int n = d.n, p = d.p, m = d.m, rows = p + 1;
-    double* qr = slot;                          // (n, p) row-major
-    double* cache = qr + size_t(n) * p;         // (m, rows): column c of C at cache[c * rows]
-    double* sub = cache + size_t(rows) * m;     // (kMaxActive, rows) QR of the active columns
-    double* u = sub + size_t(rows) * kMaxActive;  // (m,)
-    double* z = u + m;                          // (m,)
-    double* ys = z + m;                         // (n,) log signals, then weighted
-    double* rw = ys + n;                        // (n,) root weights
-    uint8_t* flag = reinterpret_cast<uint8_t*>(rw + n);  // (m,) active flags
-    uint8_t* ready = flag + m;                           // (m,) whether cache holds column c
+    double* const qr = mem.qr;
+    double* const cache = mem.cache;
+    double* const sub = mem.sub;
+    double* const u = mem.u;
+    double* const z = mem.z;
+    double* const ys = mem.ys;
+    double* const rw = mem.rw;
+    uint8_t* const flag = mem.flag;
+    uint8_t* const ready = mem.ready;
     double* pu = sh.vec[0];
     if (lane < p) pu[lane] = pin[lane];
     src.template warp_stage<double>(voxel, ys, lane);
@@ -344,7 +391,7 @@ __device__ __forceinline__ void refit_violator(const LogDesignDevice<double>& d,
     // sum_i |(R^-T g_c)_i| + |g_c p_free|. Lanes over constraints, each substitution's
     // entries in the warp's shared column of ysub; the columns themselves are not kept.
     double colsum_max = 0.0;
-    double* ysub = sh.ysub;
+    double* ysub = mem.ysub;
     for (int c = lane; c < m; c += 32) {
         const double* gc = d.g + size_t(c) * p;
         double acc_abs = 0.0, gf = 0.0;
@@ -375,7 +422,7 @@ __device__ __forceinline__ void refit_violator(const LogDesignDevice<double>& d,
     const ImplicitSystem sys{d.g, d.gt, qr, pfree, cache, ready, p, m};
     NnlsScratch ns{u, z, flag, sh.act, &sh.n_act, sh.res,
                    QrScratch{sub, sh.qtau, sh.qnu, sh.qnd, sh.qperm, sh.rv}, kMaxActive};
-    const int outcome = implicit_nnls(sys, unit, tol, kInnerStepsPerConstraint * m, ns, sh.t, lane);
+    const int outcome = implicit_nnls(sys, unit, tol, kInnerStepsPerConstraint * m, ns, sh.t, mem.ssub, lane);
     if (outcome != 1) return;
     double* res = sh.vec[2];
     // Residual C u - e_p over the active columns (u is zero elsewhere).
@@ -441,7 +488,40 @@ __global__ void __launch_bounds__(kCWarps * 32, 4) constrained_fit_kernel(
         idx = __shfl_sync(0xffffffffu, idx, 0);
         if (idx >= total) break;
         const int64_t voxel = list.voxel[idx];
-        refit_violator<Src>(d, src, weighted, voxel, list.params + size_t(idx) * p, slot, sh, params + voxel * p,
+        RefitMem mem = slot_refit_mem(slot, d.n, p, d.m);
+        mem.ysub = sh.ysub;
+        refit_violator<Src>(d, src, weighted, voxel, list.params + size_t(idx) * p, mem, sh, params + voxel * p,
+                            lane);
+    }
+}
+
+// The same re-fit with one warp per CTA and the weighted design's QR, signals, weights and the
+// QR of up to kSmemActive active NNLS columns in shared memory (refit_smem_doubles): a violator
+// takes ~3x fewer warp cycles than with them in the global slot, at fewer warps per SM, which
+// pays while a warp's state stays small (a modest table; see launch_constrained).
+template <class Src>
+__global__ void __launch_bounds__(32) constrained_fit_smem_kernel(
+    LogDesignDevice<double> d, Src src, int weighted, ViolatorList<double> list, int* queue,
+    double* __restrict__ workspace, size_t slot_doubles, double* __restrict__ params) {
+    __shared__ WarpState sh;
+    extern __shared__ __align__(16) double wsm[];
+    const int lane = threadIdx.x & 31;
+    const int n = d.n, p = d.p, rows = p + 1;
+    double* slot = workspace + size_t(blockIdx.x) * slot_doubles;
+    RefitMem mem = slot_refit_mem(slot, n, p, d.m);
+    mem.qr = wsm;
+    mem.ys = mem.qr + size_t(n) * p;
+    mem.rw = mem.ys + n;
+    mem.ssub = mem.rw + n;
+    mem.ysub = refit_ysub_aliased(n, p) ? mem.qr + size_t(p) * p : mem.ssub + size_t(rows) * kSmemActive;
+    const int total = min(*list.count, list.capacity);
+    for (;;) {
+        int idx = 0;
+        if (lane == 0) idx = atomicAdd(queue, 1);
+        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (idx >= total) break;
+        const int64_t voxel = list.voxel[idx];
+        refit_violator<Src>(d, src, weighted, voxel, list.params + size_t(idx) * p, mem, sh, params + voxel * p,
                             lane);
     }
 }
@@ -466,7 +546,9 @@ __global__ void __launch_bounds__(kCWarps * 32, 4) batch_refit_kernel(
         const LogDesignDevice<double> d = job.d;
         const CappedSource src{job.s, job.s0, job.floor, job.is_b0, d.n};
         const int64_t voxel = list.voxel[idx];
-        refit_violator<CappedSource>(d, src, weighted, voxel, list.params + size_t(idx) * d.p, slot, sh,
+        RefitMem mem = slot_refit_mem(slot, d.n, d.p, d.m);
+        mem.ysub = sh.ysub;
+        refit_violator<CappedSource>(d, src, weighted, voxel, list.params + size_t(idx) * d.p, mem, sh,
                                      job.params + voxel * d.p, lane);
     }
 }
@@ -483,7 +565,17 @@ void allow_smem() {
                "cudaFuncSetAttribute");
 }
 
-int constrained_resident_warps() {
+// The shared-memory re-fit is used while a warp's state stays within this many bytes (at least
+// five warps per SM): on the 134-measurement DKI table (35 KB, six warps per SM) it took 187 ms
+// against 213 ms with the state in the global slot at sixteen warps per SM, on the 288-measurement
+// tables (65 KB, three warps per SM) it lost.
+constexpr size_t kSmemRefitMaxBytes = 40 * 1024;
+
+bool use_smem_refit(int n, int p) {
+    return refit_smem_doubles(n, p) * sizeof(double) + sizeof(WarpState) <= kSmemRefitMaxBytes;
+}
+
+int global_resident_warps() {
     int per_sm = 0;
     allow_smem<CappedSource>();
     cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, constrained_fit_kernel<CappedSource>,
@@ -492,9 +584,27 @@ int constrained_resident_warps() {
     return sm_count() * ctas_per_sm(per_sm, "dki.refit.ctas_per_sm") * kCWarps;
 }
 
+template <class Kernel>
+void allow_refit_smem(Kernel kernel, size_t bytes) {
+    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)),
+               "cudaFuncSetAttribute");
+}
+
+int constrained_resident_warps(int n, int p) {
+    if (!use_smem_refit(n, p)) return global_resident_warps();
+    const size_t bytes = refit_smem_doubles(n, p) * sizeof(double);
+    allow_refit_smem(constrained_fit_smem_kernel<CappedSource>, bytes);
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, constrained_fit_smem_kernel<CappedSource>, 32,
+                                                             bytes),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    return sm_count() * ctas_per_sm(per_sm, "dki.refit.ctas_per_sm") / 4 * 4;
+}
+
 size_t batch_refit_slot_doubles(int n_max, int p, int m_max) { return constrained_slot_doubles(n_max, p, m_max); }
 
-int batch_refit_slots() { return constrained_resident_warps(); }
+// Batches keep the global slot: their shared memory would be sized for the largest table.
+int batch_refit_slots() { return global_resident_warps(); }
 
 void launch_batch_refit(const DkiBatchJob* jobs, const BatchViolators& violators, int weighted, int* queue,
                         double* workspace, int slots, size_t slot_doubles, cudaStream_t stream) {
@@ -513,6 +623,15 @@ void launch_constrained(const LogDesignDevice<double>& d, const Src& src, int we
                         const ViolatorList<double>& list, int /*list_count_host_bound*/, int* queue,
                         double* workspace, int slots, double* params, cudaStream_t stream) {
     require(d.p + 1 <= 32, "the constrained fit takes at most 31 parameters");
+    if (use_smem_refit(d.n, d.p)) {
+        const size_t bytes = refit_smem_doubles(d.n, d.p) * sizeof(double);
+        allow_refit_smem(constrained_fit_smem_kernel<Src>, bytes);
+        LaunchScope scope("constrained_fit_kernel", stream);
+        constrained_fit_smem_kernel<Src><<<std::max(1, slots), 32, bytes, stream>>>(
+            d, src, weighted, list, queue, workspace, constrained_slot_doubles(d.n, d.p, d.m), params);
+        cuda_check(cudaGetLastError(), "constrained_fit_smem_kernel launch");
+        return;
+    }
     const int blocks = std::max(1, slots / kCWarps);
     allow_smem<Src>();
     LaunchScope scope("constrained_fit_kernel", stream);

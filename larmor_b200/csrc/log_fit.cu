@@ -365,7 +365,7 @@ inline ScratchPlan plan_scratch(const lar::host::LogDesignHost& h, int64_t v) {
     s.params_off = up(s.ids_off + size_t(v) * sizeof(int64_t));
     s.slots_off = up(s.params_off + size_t(v) * h.p * sizeof(double));
     // As many warp slots as warps of the re-fit fit on the GPU at once.
-    const int64_t cap = constrained_resident_warps();
+    const int64_t cap = constrained_resident_warps(int(h.n), int(h.p));
     s.slots = int(std::max<int64_t>(4, std::min<int64_t>((v + 3) / 4 * 4, cap)));
     s.total = s.slots_off + size_t(s.slots) * constrained_slot_doubles(int(h.n), int(h.p), int(h.m)) * sizeof(double);
     return s;

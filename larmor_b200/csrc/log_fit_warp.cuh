@@ -41,8 +41,9 @@ inline size_t constrained_slot_doubles(int n, int p, int m) {
 // FP64, writing the constrained parameters (divided by the column scales) over `params` where
 // the re-fit succeeds. `workspace` holds `slots` warp slots of constrained_slot_doubles()
 // doubles; `queue` is a device int the kernel uses as its work counter (zeroed by the caller).
-// The warps of the constrained re-fit that fit on the GPU at once (its grid's size).
-int constrained_resident_warps();
+// The warps of the constrained re-fit of designs of n measurements and p parameters that fit
+// on the GPU at once (its grid's size), a multiple of 4.
+int constrained_resident_warps(int n, int p);
 
 template <class Src>
 void launch_constrained(const LogDesignDevice<double>& d, const Src& src, int weighted,

@@ -112,7 +112,7 @@ extern "C" int lar_fit_log_signal_noalloc(const double* x, int64_t n, int64_t p,
 
         require(log_s && params && broke, "log_s, params and broke must not be NULL");
         // As many warp slots as the re-fit keeps resident, as far as the array has room.
-        if (m > 0) slots = std::max(4, std::min(slots, constrained_resident_warps()) / 4 * 4);
+        if (m > 0) slots = std::max(4, std::min(slots, constrained_resident_warps(int(n), int(p))) / 4 * 4);
         unsigned char* base = noalloc_scratch_address();
         auto st = static_cast<cudaStream_t>(stream);
 
