@@ -249,8 +249,10 @@ __device__ __forceinline__ int log_warp_voxel(const LogDesignDevice<T>& d, const
     return it;
 }
 
-template <class T, class Src>
-__global__ void __launch_bounds__(kWarps * 32) fit_log_warp_kernel(
+// WARPS warps per CTA share one staged design; the launcher picks the count that keeps the most
+// warps resident (the design dominates a CTA's shared memory at DKI's table sizes).
+template <class T, class Src, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) fit_log_warp_kernel(
     LogDesignDevice<T> d, Src src, int64_t v, int weighted, int max_rw, T tol,
     double* __restrict__ params, uint8_t* __restrict__ broke, int32_t* __restrict__ iterations,
     ViolatorList<T> violators) {
@@ -258,11 +260,11 @@ __global__ void __launch_bounds__(kWarps * 32) fit_log_warp_kernel(
     const int p = d.p;
     const WarpLayout<T> lay{d.n, p, p | 1, p * (p + 1) / 2};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const WarpSmem<T> w = carve_warp<T>(smem_raw, lay, kWarps, warp);
+    const WarpSmem<T> w = carve_warp<T>(smem_raw, lay, WARPS, warp);
     stage_warp_design<T>(d, lay, w);
     __syncthreads();
-    for (int64_t voxel = int64_t(blockIdx.x) * kWarps + warp; voxel < v;
-         voxel += int64_t(gridDim.x) * kWarps) {
+    for (int64_t voxel = int64_t(blockIdx.x) * WARPS + warp; voxel < v;
+         voxel += int64_t(gridDim.x) * WARPS) {
         bool violated = false;
         const int it = log_warp_voxel<T>(d, lay, w, src, voxel, weighted, max_rw, tol, &violated, lane);
         const T* pv = w.pv;
@@ -347,26 +349,52 @@ __global__ void __launch_bounds__(WARPS * 32) batch_log_warp_kernel(
     }
 }
 
+// The resident warps of fit_log_warp_kernel with WARPS warps per CTA (0 when its shared memory
+// does not fit a CTA), setting the kernel's shared-memory limit.
+template <class T, class Src, int WARPS>
+int64_t warp_fit_residency(const WarpLayout<T>& lay) {
+    const size_t smem = lay.bytes(WARPS);
+    if (smem > 227 * 1024) return 0;
+    auto kernel = fit_log_warp_kernel<T, Src, WARPS>;
+    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+               "cudaFuncSetAttribute");
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, WARPS * 32, smem),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    return int64_t(per_sm) * WARPS;
+}
+
+template <class T, class Src, int WARPS>
+void launch_warp_w(const LogDesignDevice<T>& d, const Src& src, int64_t v, int weighted, int max_rw, double tol,
+                   double* params, uint8_t* broke, int32_t* iterations, const ViolatorList<T>& violators,
+                   cudaStream_t stream) {
+    const WarpLayout<T> lay{d.n, d.p, d.p | 1, d.p * (d.p + 1) / 2};
+    const size_t smem = lay.bytes(WARPS);
+    const int64_t per_sm = warp_fit_residency<T, Src, WARPS>(lay) / WARPS;
+    const int64_t need = (v + WARPS - 1) / WARPS;
+    const int64_t waves = launch_setting("log.warp.waves") > 0 ? launch_setting("log.warp.waves") : 4;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sm_count()) * std::max<int64_t>(per_sm, 1) * waves));
+    LaunchScope scope("fit_log_warp_kernel", stream);
+    fit_log_warp_kernel<T, Src, WARPS><<<unsigned(grid), WARPS * 32, smem, stream>>>(
+        d, src, v, weighted, max_rw, T(tol), params, broke, iterations, violators);
+    cuda_check(cudaGetLastError(), "fit_log_warp_kernel launch");
+}
+
 template <class T, class Src>
 void launch_warp_impl(const LogDesignDevice<T>& d, const Src& src, int64_t v, int weighted, int max_rw,
                       double tol, double* params, uint8_t* broke, int32_t* iterations,
                       const ViolatorList<T>& violators, cudaStream_t stream) {
     const WarpLayout<T> lay{d.n, d.p, d.p | 1, d.p * (d.p + 1) / 2};
-    const size_t smem = lay.bytes(kWarps);
-    require(smem <= 227 * 1024, "the design is too large for the shared-memory log fit");
-    auto kernel = fit_log_warp_kernel<T, Src>;
-    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-               "cudaFuncSetAttribute");
-    int per_sm = 0;
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kWarps * 32, smem),
-               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    const int64_t need = (v + kWarps - 1) / kWarps;
-    const int64_t waves = launch_setting("log.warp.waves") > 0 ? launch_setting("log.warp.waves") : 4;
-    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sm_count()) * std::max(per_sm, 1) * waves));
-    LaunchScope scope("fit_log_warp_kernel", stream);
-    kernel<<<unsigned(grid), kWarps * 32, smem, stream>>>(d, src, v, weighted, max_rw, T(tol), params, broke,
-                                                          iterations, violators);
-    cuda_check(cudaGetLastError(), "fit_log_warp_kernel launch");
+    require(lay.bytes(kWarps) <= 227 * 1024, "the design is too large for the shared-memory log fit");
+    // The warps per CTA that keep the most warps resident (the fewest on a tie).
+    const int64_t r4 = warp_fit_residency<T, Src, 4>(lay), r8 = warp_fit_residency<T, Src, 8>(lay),
+                  r16 = warp_fit_residency<T, Src, 16>(lay);
+    if (r16 > std::max(r4, r8))
+        launch_warp_w<T, Src, 16>(d, src, v, weighted, max_rw, tol, params, broke, iterations, violators, stream);
+    else if (r8 > r4)
+        launch_warp_w<T, Src, 8>(d, src, v, weighted, max_rw, tol, params, broke, iterations, violators, stream);
+    else
+        launch_warp_w<T, Src, 4>(d, src, v, weighted, max_rw, tol, params, broke, iterations, violators, stream);
 }
 
 }  // namespace
